@@ -1,0 +1,491 @@
+#!/usr/bin/env python3
+"""Benchmark of the compressed-graph sampling hot path on B200.
+
+Workload (N=1 line): R-MAT scale 22, edge factor 32, a/b/c/d = .57/.19/.19/.05,
+seed 42, relabelled/deduped/symmetrized with graph_sort semantics and written in
+the reference's LE and GT formats (byte-identical to the reference compressor);
+then
+  (a) 1,048,576 uniform random walks of length 80 (Philox seed 7) -- the headline,
+  (b) k-hop with fanouts (25, 10) for 65,536 uniform seeds,
+  (c) a decode-only sweep of every neighbor list,
+each in LE and GT modes and on an uncompressed CSR with the same RNG stream.
+
+A "step" is one launch of the sampler over the whole batch (all walkers, all
+80 steps).  `value` = sampled edges/s with inputs resident in HBM (CUDA events
+on the launching stream, L2 flushed by a 256 MiB write between timed steps).
+`e2e` = the same metric through the public host API (grass_rw_host) from pinned
+host memory, copies of starts in and paths out inside the timed region.
+
+`--impl reference` times the reference's CPU decode+sample path -- here the
+CPU oracle's restatement of the reference decoders and app logic (the
+reference has no CPU sampler) -- on all host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "sampled edges/s (random walk, compressed graph)"
+UNIT = "edges/s"
+CACHE = os.path.join(tempfile.gettempdir(), "grass_bench_cache")
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="grass", choices=["grass", "reference"])
+    ap.add_argument("--scale", type=int, default=22)
+    ap.add_argument("--edge-factor", type=int, default=32)
+    ap.add_argument("--walkers", type=int, default=1 << 20)
+    ap.add_argument("--length", type=int, default=80)
+    ap.add_argument("--khop-seeds", type=int, default=65536)
+    ap.add_argument("--mode", default="LE", choices=["LE", "GT"])
+    ap.add_argument("--only", default="", help="comma list: rw,khop,decode,csr,e2e,cpu")
+    ap.add_argument("--no-clocks", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (one process per GPU; replicas only, no data exchange)
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def dist_init(ws, backend):
+    if ws <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def barrier(dist, dev=None):
+    if dist is not None:
+        if dev is not None:
+            dist.barrier(device_ids=[dev])
+        else:
+            dist.barrier()
+
+
+def max_over_ranks(dist, x: float, torch=None) -> float:
+    if dist is None:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, x: float, torch=None) -> float:
+    if dist is None:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------
+# synthetic graph (cached per box)
+
+def build_graph(scale, ef):
+    import grass_b200 as G
+    key = f"rmat_s{scale}_e{ef}_seed42"
+    d = os.path.join(CACHE, key)
+    done = os.path.join(d, "done.json")
+    if os.path.exists(done):
+        return d, json.load(open(done))
+    os.makedirs(d, exist_ok=True)
+    t0 = time.time()
+    rp, cols = G.rmat_graph(scale, ef, seed=42)
+    t1 = time.time()
+    meta = {"n": int(len(rp) - 1), "num_edges": int(len(cols)), "gen_s": t1 - t0}
+    for mode in ("LE", "GT"):
+        t2 = time.time()
+        G.compress_to_files(rp, cols, mode, os.path.join(d, mode))
+        meta[f"compress_{mode}_s"] = time.time() - t2
+    np.save(os.path.join(d, "rowptr.npy"), rp)
+    np.save(os.path.join(d, "cols.npy"), cols)
+    json.dump(meta, open(done, "w"))
+    return d, meta
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+
+class Clocks:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int, enabled: bool = True):
+        self.p = None
+        self.path = None
+        if not enabled:
+            return
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(gpu_index)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self) -> dict | None:
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.close()
+        sm, mx, pw = [], [], []
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+                pw.append(float(parts[3]))
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
+                "power_w_max": max(pw), "reasons": sorted(reasons)}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(workload_key: str):
+    """Per-launch DRAM bytes of the RW kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d.get(workload_key)
+
+
+# ---------------------------------------------------------------------------
+# timing
+
+def timed(torch, fn, K, W, flush, dist=None, dev=None):
+    """W untimed warm-up calls, then K calls each bracketed by CUDA events on
+    the current stream, with an L2 flush outside the events between calls.
+    Returns (per-call ms list, max over ranks of the summed device time)."""
+    for _ in range(W):
+        fn()
+    torch.cuda.synchronize()
+    barrier(dist, dev)
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(K)]
+    for a, b in evs:
+        flush()
+        a.record(st)
+        fn()
+        b.record(st)
+    torch.cuda.synchronize()
+    barrier(dist, dev)
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in evs]
+    return ms, max_over_ranks(dist, sum(ms), torch)
+
+
+def cpu_baseline(gdir, mode, n, length, seed, budget_s=12.0):
+    import oracle
+    oracle.lib()
+    og = oracle.OracleGraph(os.path.join(gdir, mode))
+    threads = oracle.max_threads()
+    W = 8192
+    best = None
+    spent = 0.0
+    while True:
+        starts = oracle.uniform_starts(n, W, 7)
+        t0 = time.perf_counter()
+        _, edges = og.rw(mode, starts, length, seed, threads)
+        dt = time.perf_counter() - t0
+        spent += dt
+        best = (W, edges, dt)
+        if dt > 2.0 or spent + 3 * dt > budget_s:
+            break
+        W *= 4
+    W, edges, dt = best
+    return {"value": edges / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{W} uniform walkers x {length} steps ({mode} decode per draw) on the "
+                      f"same graph; oracle restatement of the reference decoders + app next(), "
+                      f"OpenMP over walkers"}
+
+
+# ---------------------------------------------------------------------------
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    import oracle
+    gdir, meta = build_graph(args.scale, args.edge_factor)
+    n = meta["n"]
+    og = oracle.OracleGraph(os.path.join(gdir, args.mode))
+    threads = oracle.max_threads()
+    # bounded sample per step: sized so one step is ~1-3 s of CPU work
+    Wc = 8192
+    starts = oracle.uniform_starts(n, Wc, 7)
+    t0 = time.perf_counter()
+    og.rw(args.mode, starts, args.length, 7, threads)
+    dt = time.perf_counter() - t0
+    Wc = int(min(args.walkers, max(8192, Wc * 1.5 / max(dt, 1e-3))))
+    starts = oracle.uniform_starts(n, Wc, 7)
+    for _ in range(args.warmup):
+        og.rw(args.mode, starts, args.length, 7, threads)
+    tot_e, tot_t = 0, 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, e = og.rw(args.mode, starts, args.length, 7, threads)
+        tot_t += time.perf_counter() - t0
+        tot_e += e
+    val = tot_e / tot_t
+    sample = (f"{Wc} of the {args.walkers} uniform walkers x {args.length} steps per step, "
+              f"{args.mode} decode per draw")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * tot_t / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+        "config": workload_config(args, meta),
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference has no CPU sampler; this is the CPU oracle's restatement of its "
+                "bcg.cuh decoders and app next() with the shared Philox stream",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(args, meta):
+    return {
+        "workload": f"random walk, {args.walkers} uniform walkers x L={args.length}, "
+                    f"{args.mode} compressed R-MAT s{args.scale} ef{args.edge_factor}",
+        "graph": f"R-MAT scale {args.scale} edge factor {args.edge_factor} "
+                 f".57/.19/.19/.05 seed 42, graph_sort (undirected)",
+        "vertices": meta["n"], "directed_edges": meta["num_edges"],
+        "walkers": args.walkers, "length": args.length, "philox_seed": 7,
+        "decode_mode": args.mode, "l2": "flushed (256 MiB write) between timed steps",
+    }
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    ws, rank, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    dist = dist_init(ws, "nccl")
+    import grass_b200 as G
+
+    only = set(args.only.split(",")) if args.only else {"rw", "khop", "decode", "csr", "e2e",
+                                                         "cpu"}
+    gdir, meta = build_graph(args.scale, args.edge_factor)
+    n, E = meta["n"], meta["num_edges"]
+    W, L = args.walkers, args.length
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    flush_buf = torch.empty(64 << 20, dtype=torch.int32, device=dev)
+
+    def flush():
+        flush_buf.fill_(1)
+
+    graphs = {m: G.Graph(os.path.join(gdir, m), m, device=local) for m in ("LE", "GT")}
+    infos = {m: graphs[m].info() for m in graphs}
+    csr = graphs["LE"].csr() if ("csr" in only) else None
+
+    # per-rank walker ids offset so replicas sample different walks
+    starts = torch.empty(W, dtype=torch.int32, device=dev)
+    G.uniform_starts_device(n, W, 7 + rank, starts, stream=stream)
+    paths = torch.empty(W * (L + 1), dtype=torch.int32, device=dev)
+    ecount = torch.zeros(1, dtype=torch.int64, device=dev)
+    clocks = Clocks(local, enabled=not args.no_clocks)
+    out = {}
+
+    def rw_fn(obj):
+        return lambda: obj.rw_device(starts, W, L, 7 + rank, paths, ecount, stream=stream)
+
+    # ---- (a) random walk: headline mode first
+    order = [args.mode] + [m for m in ("LE", "GT") if m != args.mode]
+    launches0 = G.launch_count()
+    for m in order:
+        ecount.zero_()
+        graphs[m].rw_device(starts, W, L, 7 + rank, paths, ecount, stream=stream)
+        torch.cuda.synchronize()
+        edges_per_step = int(ecount.item())
+        lc0 = G.launch_count()
+        ms, tot = timed(torch, rw_fn(graphs[m]), args.steps, args.warmup, flush, dist, local)
+        lc = G.launch_count() - lc0 - args.warmup
+        all_edges = sum_over_ranks(dist, edges_per_step * args.steps, torch)
+        out[f"rw_{m}"] = {"value": all_edges / (tot / 1000.0), "ms_per_step": tot / args.steps,
+                          "edges_per_step": edges_per_step, "launches": lc,
+                          "ms_min": min(ms), "ms_max": max(ms)}
+    if "csr" in only and csr is not None:
+        ecount.zero_()
+        csr.rw_device(starts, W, L, 7 + rank, paths, ecount, stream=stream)
+        torch.cuda.synchronize()
+        e1 = int(ecount.item())
+        ms, tot = timed(torch, rw_fn(csr), args.steps, args.warmup, flush, dist, local)
+        all_edges = sum_over_ranks(dist, e1 * args.steps, torch)
+        out["rw_CSR"] = {"value": all_edges / (tot / 1000.0), "ms_per_step": tot / args.steps}
+
+    # ---- (b) k-hop (25, 10)
+    if "khop" in only:
+        S, fan = args.khop_seeds, (25, 10)
+        seeds = torch.empty(S, dtype=torch.int32, device=dev)
+        G.uniform_starts_device(n, S, 11 + rank, seeds, stream=stream)
+        hops = [torch.empty(S * w, dtype=torch.int32, device=dev) for w in G.hop_widths(fan)]
+        for name, obj in [("LE", graphs["LE"]), ("GT", graphs["GT"])] + (
+                [("CSR", csr)] if csr is not None else []):
+            ecount.zero_()
+            obj.khop_device(seeds, S, fan, 13, hops, ecount, stream=stream)
+            torch.cuda.synchronize()
+            e1 = int(ecount.item())
+            ms, tot = timed(torch, lambda o=obj: o.khop_device(seeds, S, fan, 13, hops, ecount,
+                                                               stream=stream),
+                            args.steps, args.warmup, flush, dist, local)
+            out[f"khop_{name}"] = {"value": sum_over_ranks(dist, e1 * args.steps, torch) /
+                                   (tot / 1000.0), "ms_per_step": tot / args.steps}
+        del hops
+
+    # ---- (c) decode-only sweep
+    if "decode" in only:
+        rp_d = torch.empty(n + 1, dtype=torch.int64, device=dev)
+        cl_d = torch.empty(E, dtype=torch.int32, device=dev)
+        for m in ("LE", "GT"):
+            ms, tot = timed(torch, lambda g=graphs[m]: g.decode_all_device(rp_d, cl_d,
+                                                                           stream=stream),
+                            args.steps, args.warmup, flush, dist, local)
+            stream_bytes = infos[m]["graph_file_bytes"] + (n + 1) * 8
+            out[f"decode_{m}"] = {
+                "value": sum_over_ranks(dist, E * args.steps, torch) / (tot / 1000.0),
+                "unit": "decoded edges/s", "ms_per_step": tot / args.steps,
+                "algorithmic_GBps": (stream_bytes + 4 * E + 8 * (n + 1)) / (tot / args.steps)
+                / 1e6}
+        del rp_d, cl_d
+
+    clk = clocks.stop()
+
+    # ---- accounting for the roofline of the headline kernel
+    acct = torch.zeros(3, dtype=torch.int64, device=dev)
+    graphs[args.mode].rw_account(starts, W, L, 7 + rank, acct, stream=stream)
+    torch.cuda.synchronize()
+    alg_bytes, sectors, draws = [int(x) for x in acct.cpu().tolist()]
+    head = out[f"rw_{args.mode}"]
+    avg_s = head["ms_per_step"] / 1000.0
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / avg_s / 1e9
+    traffic = ncu_traffic(f"rw_{args.mode}_s{args.scale}_e{args.edge_factor}_W{W}_L{L}")
+
+    # ---- e2e through the host API, pinned buffers, copies inside the region
+    e2e = None
+    if "e2e" in only:
+        h_starts = torch.empty(W, dtype=torch.int32, pin_memory=True)
+        h_starts.copy_(starts.cpu())
+        h_paths = torch.empty(W * (L + 1), dtype=torch.int32, pin_memory=True)
+        hs = h_starts.numpy().view(np.uint32)
+        hp = h_paths.numpy().view(np.uint32).reshape(W, L + 1)
+        gm = graphs[args.mode]
+        p = G.RwParams(L, 0, 7 + rank)
+        import ctypes as C
+        ecnt = C.c_uint64()
+
+        def e2e_call():
+            G._check(G.lib.grass_rw_host(gm.handle, C.byref(p), G._p(hs), W, G._p(hp),
+                                         C.byref(ecnt)))
+        for _ in range(args.warmup):
+            e2e_call()
+        barrier(dist, local)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_call()
+        el = time.perf_counter() - t0
+        barrier(dist, local)
+        el = max_over_ranks(dist, el, torch)
+        e2e = {"value": sum_over_ranks(dist, int(ecnt.value) * args.steps, torch) / el,
+               "unit": UNIT, "h2d_bytes_per_step": W * 4, "d2h_bytes_per_step": W * (L + 1) * 4,
+               "ms_per_step": 1000 * el / args.steps, "api": "grass_rw_host (pinned host buffers)"}
+
+    cpu = None
+    if rank == 0 and "cpu" in only:
+        try:
+            cpu = cpu_baseline(gdir, args.mode, n, L, 7)
+        except Exception as ex:  # the oracle is test infrastructure; report, don't fail
+            cpu = {"error": str(ex)}
+
+    if rank == 0:
+        csr_bytes = (n + 1) * 8 + 4 * E
+        line = {
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+            "data": "synthetic (R-MAT generated on the box, seed 42)",
+            "config": workload_config(args, meta),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": traffic,
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "sector_bytes_per_launch": sectors * 32,
+                         "sector_GBps": sectors * 32 / avg_s / 1e9,
+                         "draws_per_launch": draws},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": head["launches"],
+            "clocks": clk,
+            "results": out,
+            "compressed_vs_csr": ({m: out[f"rw_{m}"]["value"] / out["rw_CSR"]["value"]
+                                   for m in ("LE", "GT")} if "rw_CSR" in out else None),
+            "footprint_bytes": {"CSR": csr_bytes,
+                                **{m: infos[m]["device_bytes"] for m in infos},
+                                **{f"ratio_{m}": csr_bytes / infos[m]["device_bytes"]
+                                   for m in infos}},
+            "load_seconds": {m: infos[m]["upload_seconds"] for m in infos},
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,427 @@
+"""grass_b200 -- B200-native compressed-graph sampling (GraSS hot path).
+
+Python binding over the C ABI in ``include/grass.h`` (``lib/libgrass_b200.so``).
+Everything here calls into the native library; there is no Python or CPU
+fallback for any sampling or decoding operation, and importing the package
+raises if the library has not been built.
+
+Reference interface mirrored (calla212/GraSS):
+  * ``Graph(prefix, mode)``      -- loadGraph + transferToGPUs (GT/src/grass.cu:1126-1233)
+  * ``Graph.rw / khop / mrw``    -- the rw / ks / mrw apps (GT/src/apps/*)
+  * ``Graph.decode_all``         -- GlobalDecoder / BCGVertex::get_vertex (GT/src/bcg.cuh)
+  * ``compress``/``graph_sort``  -- GT|LE/chunk_compress (offline tools)
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libgrass_b200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include", "grass.h")
+
+OK, E_IO, E_FORMAT, E_CUDA, E_OOM, E_BUDGET, E_TIMEOUT, E_ARG, E_DATA = range(9)
+MODE_GT, MODE_LE = 0, 1
+MODES = {"GT": MODE_GT, "LE": MODE_LE, "gt": MODE_GT, "le": MODE_LE, 0: 0, 1: 1}
+INVALID = 0xFFFFFFFF
+LAYOUT_WALK_MAJOR, LAYOUT_STEP_MAJOR = 0, 1
+SELECT_UNIFORM, SELECT_DEGREE = 0, 1
+MAX_HOPS = 8
+
+
+class GrassError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def build() -> None:
+    import subprocess
+    subprocess.check_call(["make", "-s", "-j8", "-C", os.path.join(HERE, "csrc"), "all"])
+
+
+class GraphInfo(C.Structure):
+    _fields_ = [
+        ("n", C.c_uint64), ("n_file", C.c_uint64), ("num_edges", C.c_uint64),
+        ("max_degree", C.c_uint32), ("ubl", C.c_uint32), ("mode", C.c_int32),
+        ("device", C.c_int32), ("graph_file_bytes", C.c_uint64),
+        ("offset_file_bytes", C.c_uint64), ("device_bytes", C.c_uint64),
+        ("read_seconds", C.c_double), ("upload_seconds", C.c_double),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class RwParams(C.Structure):
+    _fields_ = [("length", C.c_uint32), ("layout", C.c_uint32), ("seed", C.c_uint64)]
+
+
+class KhopParams(C.Structure):
+    _fields_ = [("hops", C.c_uint32), ("fanouts", C.c_uint32 * MAX_HOPS), ("seed", C.c_uint64)]
+
+
+class MrwParams(C.Structure):
+    _fields_ = [("walkers", C.c_uint32), ("steps", C.c_uint32), ("select", C.c_uint32),
+                ("reserved", C.c_uint32), ("seed", C.c_uint64)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"grass_b200 native library not built ({LIB_PATH}); run "
+            "`make -C grass_b200/csrc` or __graft_entry__.build()")
+    L = C.CDLL(LIB_PATH)
+    P, u32, u64, i32, d = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_double
+    PP = C.POINTER(C.c_void_p)
+    sig = {
+        "grass_last_error": ([], C.c_char_p),
+        "grass_launch_count": ([], u64),
+        "grass_version": ([], C.c_char_p),
+        "grass_gen_rmat": ([u32, u32, d, d, d, u64, P, P], i32),
+        "grass_gen_chung_lu": ([u64, d, d, u64, u64, u64, P, P], i32),
+        "grass_graph_sort": ([P, P, u64, i32, PP], i32),
+        "grass_host_csr_view": ([P, P, P, PP, PP], i32),
+        "grass_host_csr_free": ([P], None),
+        "grass_compress": ([P, P, u64, i32, P, P, P, P], i32),
+        "grass_compress_to_files": ([P, P, u64, i32, C.c_char_p], i32),
+        "grass_open": ([C.c_char_p, i32, i32, PP], i32),
+        "grass_open_mem": ([P, u64, P, u64, i32, i32, PP], i32),
+        "grass_close": ([P], i32),
+        "grass_get_info": ([P, C.POINTER(GraphInfo)], i32),
+        "grass_device_view": ([P, PP, P, PP], i32),
+        "grass_degrees": ([P, P, P], i32),
+        "grass_decode_all": ([P, P, P, P], i32),
+        "grass_uniform_starts": ([u64, u64, u64, P, P], i32),
+        "grass_rw": ([P, C.POINTER(RwParams), P, u64, P, P, P], i32),
+        "grass_rw_host": ([P, C.POINTER(RwParams), P, u64, P, P], i32),
+        "grass_rw_account": ([P, C.POINTER(RwParams), P, u64, P, P], i32),
+        "grass_khop": ([P, C.POINTER(KhopParams), P, u64, P, P, P], i32),
+        "grass_khop_host": ([P, C.POINTER(KhopParams), P, u64, P, P], i32),
+        "grass_mrw": ([P, C.POINTER(MrwParams), P, u64, P, P, P, P], i32),
+        "grass_mrw_host": ([P, C.POINTER(MrwParams), P, u64, P, P, P], i32),
+        "grass_csr_from_graph": ([P, PP], i32),
+        "grass_csr_from_host": ([P, P, u64, i32, PP], i32),
+        "grass_csr_close": ([P], i32),
+        "grass_csr_info": ([P, P, P, P], i32),
+        "grass_csr_rw": ([P, C.POINTER(RwParams), P, u64, P, P, P], i32),
+        "grass_csr_khop": ([P, C.POINTER(KhopParams), P, u64, P, P, P], i32),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    return L
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    return (lib.grass_last_error() or b"").decode()
+
+
+def launch_count() -> int:
+    return int(lib.grass_launch_count())
+
+
+def _check(rc: int):
+    if rc != OK:
+        raise GrassError(rc, last_error())
+
+
+def _p(a: np.ndarray):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _ptr(x):
+    """Device pointer from an int, a torch tensor or None."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return C.c_void_p(x)
+    return C.c_void_p(x.data_ptr())
+
+
+def _stream(s):
+    if s is None:
+        return None
+    if isinstance(s, int):
+        return C.c_void_p(s)
+    return C.c_void_p(s.cuda_stream)
+
+
+# ---------------------------------------------------------------------------
+# Host graph tools
+
+def gen_rmat(scale: int, edge_factor: int, a=0.57, b=0.19, c=0.19, seed: int = 42):
+    m = edge_factor << scale
+    src = np.empty(m, dtype=np.uint32)
+    dst = np.empty(m, dtype=np.uint32)
+    _check(lib.grass_gen_rmat(scale, edge_factor, a, b, c, seed, _p(src), _p(dst)))
+    return src, dst
+
+
+def gen_chung_lu(n: int, exponent: float, mean_degree: float, max_degree: int, m: int,
+                 seed: int = 42):
+    src = np.empty(m, dtype=np.uint32)
+    dst = np.empty(m, dtype=np.uint32)
+    _check(lib.grass_gen_chung_lu(n, exponent, mean_degree, max_degree, seed, m, _p(src),
+                                  _p(dst)))
+    return src, dst
+
+
+def graph_sort(src: np.ndarray, dst: np.ndarray, directed: bool = False):
+    """graph_sort semantics; returns (rowptr u64[n+1], cols u32[nnz])."""
+    src = np.ascontiguousarray(src, dtype=np.uint32)
+    dst = np.ascontiguousarray(dst, dtype=np.uint32)
+    h = C.c_void_p()
+    _check(lib.grass_graph_sort(_p(src), _p(dst), len(src), int(directed), C.byref(h)))
+    try:
+        n, nnz = C.c_uint64(), C.c_uint64()
+        rp, cp = C.c_void_p(), C.c_void_p()
+        _check(lib.grass_host_csr_view(h, C.byref(n), C.byref(nnz), C.byref(rp), C.byref(cp)))
+        rowptr = np.ctypeslib.as_array(C.cast(rp, C.POINTER(C.c_uint64)),
+                                       shape=(n.value + 1,)).copy()
+        cols = (np.ctypeslib.as_array(C.cast(cp, C.POINTER(C.c_uint32)), shape=(nnz.value,)).copy()
+                if nnz.value else np.zeros(0, np.uint32))
+    finally:
+        lib.grass_host_csr_free(h)
+    return rowptr, cols
+
+
+def compress(rowptr: np.ndarray, cols: np.ndarray, mode) -> tuple[bytes, bytes]:
+    """Encode a sorted CSR in the reference's GT or LE on-disk format."""
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint64)
+    cols = np.ascontiguousarray(cols, dtype=np.uint32)
+    n = len(rowptr) - 1
+    gs, os_ = C.c_uint64(), C.c_uint64()
+    m = MODES[mode]
+    cptr = _p(cols) if len(cols) else None
+    _check(lib.grass_compress(_p(rowptr), cptr, n, m, None, C.byref(gs), None, C.byref(os_)))
+    gb = np.zeros(max(gs.value, 1), np.uint8)
+    ob = np.zeros(os_.value, np.uint8)
+    _check(lib.grass_compress(_p(rowptr), cptr, n, m, _p(gb), C.byref(gs), _p(ob), C.byref(os_)))
+    return gb[: gs.value].tobytes(), ob.tobytes()
+
+
+def compress_to_files(rowptr: np.ndarray, cols: np.ndarray, mode, prefix: str) -> None:
+    rowptr = np.ascontiguousarray(rowptr, dtype=np.uint64)
+    cols = np.ascontiguousarray(cols, dtype=np.uint32)
+    _check(lib.grass_compress_to_files(_p(rowptr), _p(cols) if len(cols) else None,
+                                       len(rowptr) - 1, MODES[mode], prefix.encode()))
+
+
+def rmat_graph(scale: int, edge_factor: int, seed: int = 42, a=0.57, b=0.19, c=0.19):
+    """R-MAT -> graph_sort (undirected) CSR."""
+    src, dst = gen_rmat(scale, edge_factor, a, b, c, seed)
+    return graph_sort(src, dst, directed=False)
+
+
+# ---------------------------------------------------------------------------
+# Device graph
+
+def _khop_params(fanouts, seed):
+    p = KhopParams()
+    fanouts = list(fanouts)
+    if not 1 <= len(fanouts) <= MAX_HOPS:
+        raise ValueError("1..8 hops")
+    p.hops = len(fanouts)
+    for i, f in enumerate(fanouts):
+        p.fanouts[i] = int(f)
+    p.seed = seed
+    return p
+
+
+def hop_widths(fanouts):
+    out, w = [], 1
+    for f in fanouts:
+        w *= int(f)
+        out.append(w)
+    return out
+
+
+class Graph:
+    """A compressed graph resident on one GPU."""
+
+    def __init__(self, prefix: str | None = None, mode="GT", device: int = 0, *,
+                 graph_bytes: bytes | None = None, offset_bytes: bytes | None = None):
+        self._h = C.c_void_p()
+        m = mode if isinstance(mode, int) else MODES[mode]
+        if prefix is not None:
+            _check(lib.grass_open(prefix.encode(), m, device, C.byref(self._h)))
+        else:
+            gb = np.frombuffer(graph_bytes, np.uint8) if graph_bytes else np.zeros(1, np.uint8)
+            ob = np.frombuffer(offset_bytes, np.uint8)
+            _check(lib.grass_open_mem(_p(gb), len(graph_bytes or b""), _p(ob), len(ob), m, device,
+                                      C.byref(self._h)))
+        self.mode = m
+
+    @classmethod
+    def from_bytes(cls, graph_bytes: bytes, offset_bytes: bytes, mode="GT", device: int = 0):
+        return cls(None, mode, device, graph_bytes=graph_bytes, offset_bytes=offset_bytes)
+
+    def close(self):
+        if self._h:
+            lib.grass_close(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self) -> dict:
+        i = GraphInfo()
+        _check(lib.grass_get_info(self._h, C.byref(i)))
+        return i.as_dict()
+
+    @property
+    def n(self) -> int:
+        return int(self.info()["n"])
+
+    # -- host-buffer (end-to-end) calls --
+    def rw(self, starts: np.ndarray, length: int, seed: int, layout: int = LAYOUT_WALK_MAJOR):
+        starts = np.ascontiguousarray(starts, dtype=np.uint32)
+        W = len(starts)
+        p = RwParams(length, layout, seed)
+        shape = (W, length + 1) if layout == LAYOUT_WALK_MAJOR else (length + 1, W)
+        paths = np.zeros(shape, dtype=np.uint32)
+        e = C.c_uint64()
+        _check(lib.grass_rw_host(self._h, C.byref(p), _p(starts), W, _p(paths), C.byref(e)))
+        return paths, int(e.value)
+
+    def khop(self, seeds: np.ndarray, fanouts, seed: int):
+        seeds = np.ascontiguousarray(seeds, dtype=np.uint32)
+        p = _khop_params(fanouts, seed)
+        outs = [np.zeros((len(seeds), w), dtype=np.uint32) for w in hop_widths(fanouts)]
+        arr = (C.c_void_p * len(outs))(*[o.ctypes.data for o in outs])
+        e = C.c_uint64()
+        _check(lib.grass_khop_host(self._h, C.byref(p), _p(seeds), len(seeds),
+                                   C.cast(arr, C.c_void_p), C.byref(e)))
+        return outs, int(e.value)
+
+    def mrw(self, roots: np.ndarray, steps: int, seed: int, select: int = SELECT_UNIFORM):
+        roots = np.array(roots, dtype=np.uint32, order="C", copy=True)
+        S, R = roots.shape
+        p = MrwParams(R, steps, select, 0, seed)
+        src = np.zeros((S, steps), np.uint32)
+        dst = np.zeros((S, steps), np.uint32)
+        e = C.c_uint64()
+        _check(lib.grass_mrw_host(self._h, C.byref(p), _p(roots), S, _p(src), _p(dst),
+                                  C.byref(e)))
+        return src, dst, roots, int(e.value)
+
+    # -- device-buffer calls (torch tensors or raw ints) --
+    def rw_device(self, starts, W: int, length: int, seed: int, paths, edge_count=None,
+                  layout: int = LAYOUT_WALK_MAJOR, stream=None):
+        p = RwParams(length, layout, seed)
+        _check(lib.grass_rw(self._h, C.byref(p), _ptr(starts), W, _ptr(paths), _ptr(edge_count),
+                            _stream(stream)))
+
+    def rw_account(self, starts, W: int, length: int, seed: int, out3, stream=None):
+        """Adds [algorithmic bytes, 32B sectors, draws] of the walk to out3."""
+        p = RwParams(length, 0, seed)
+        _check(lib.grass_rw_account(self._h, C.byref(p), _ptr(starts), W, _ptr(out3),
+                                    _stream(stream)))
+
+    def khop_device(self, seeds, S: int, fanouts, seed: int, hop_out, edge_count=None,
+                    stream=None):
+        p = _khop_params(fanouts, seed)
+        arr = (C.c_void_p * len(hop_out))(*[_ptr(o).value for o in hop_out])
+        _check(lib.grass_khop(self._h, C.byref(p), _ptr(seeds), S, C.cast(arr, C.c_void_p),
+                              _ptr(edge_count), _stream(stream)))
+
+    def mrw_device(self, roots, S: int, walkers: int, steps: int, seed: int, src, dst,
+                   select: int = SELECT_UNIFORM, edge_count=None, stream=None):
+        p = MrwParams(walkers, steps, select, 0, seed)
+        _check(lib.grass_mrw(self._h, C.byref(p), _ptr(roots), S, _ptr(src), _ptr(dst),
+                             _ptr(edge_count), _stream(stream)))
+
+    def decode_all_device(self, rowptr, cols, stream=None):
+        _check(lib.grass_decode_all(self._h, _ptr(rowptr), _ptr(cols), _stream(stream)))
+
+    def degrees_device(self, deg, stream=None):
+        _check(lib.grass_degrees(self._h, _ptr(deg), _stream(stream)))
+
+    def decode_all(self):
+        """Decode every list; returns host (rowptr, cols).  Uses torch for buffers."""
+        import torch
+        inf = self.info()
+        n, E = int(inf["n"]), int(inf["num_edges"])
+        dev = torch.device("cuda", int(inf["device"]))
+        rp = torch.empty(n + 1, dtype=torch.int64, device=dev)
+        cl = torch.empty(max(E, 1), dtype=torch.int32, device=dev)
+        self.decode_all_device(rp, cl)
+        torch.cuda.synchronize(dev)
+        return (rp.cpu().numpy().view(np.uint64).copy(),
+                cl.cpu().numpy().view(np.uint32)[:E].copy())
+
+    def csr(self) -> "Csr":
+        h = C.c_void_p()
+        _check(lib.grass_csr_from_graph(self._h, C.byref(h)))
+        return Csr(h)
+
+
+def uniform_starts_device(n: int, count: int, seed: int, out, stream=None):
+    _check(lib.grass_uniform_starts(n, count, seed, _ptr(out), _stream(stream)))
+
+
+class Csr:
+    """Uncompressed CSR on one GPU (comparison baseline)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def from_host(cls, rowptr: np.ndarray, cols: np.ndarray, device: int = 0):
+        rowptr = np.ascontiguousarray(rowptr, dtype=np.uint64)
+        cols = np.ascontiguousarray(cols, dtype=np.uint32)
+        h = C.c_void_p()
+        _check(lib.grass_csr_from_host(_p(rowptr), _p(cols) if len(cols) else None,
+                                       len(rowptr) - 1, device, C.byref(h)))
+        return cls(h)
+
+    def close(self):
+        if self._h:
+            lib.grass_csr_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self):
+        n, nnz, b = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(lib.grass_csr_info(self._h, C.byref(n), C.byref(nnz), C.byref(b)))
+        return {"n": n.value, "nnz": nnz.value, "device_bytes": b.value}
+
+    def rw_device(self, starts, W: int, length: int, seed: int, paths, edge_count=None,
+                  layout: int = LAYOUT_WALK_MAJOR, stream=None):
+        p = RwParams(length, layout, seed)
+        _check(lib.grass_csr_rw(self._h, C.byref(p), _ptr(starts), W, _ptr(paths),
+                                _ptr(edge_count), _stream(stream)))
+
+    def khop_device(self, seeds, S: int, fanouts, seed: int, hop_out, edge_count=None,
+                    stream=None):
+        p = _khop_params(fanouts, seed)
+        arr = (C.c_void_p * len(hop_out))(*[_ptr(o).value for o in hop_out])
+        _check(lib.grass_csr_khop(self._h, C.byref(p), _ptr(seeds), S, C.cast(arr, C.c_void_p),
+                                  _ptr(edge_count), _stream(stream)))
+
+
+def exported_symbols() -> list[str]:
+    """Function names declared in include/grass.h."""
+    import re
+    txt = open(INCLUDE).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(grass_[a-z0-9_]+)\s*\(", txt)))

@@ -1,0 +1,118 @@
+// graph.h -- host-side handle types and kernel launchers (internal).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+
+#include "device_common.cuh"
+#include "internal.h"
+
+struct grass_graph {
+  int device = 0;
+  int mode = 0;
+  uint32_t *d_words = nullptr;     // n_words + guard words
+  uint64_t n_words = 0;            // stream words (excluding guard words)
+  uint64_t *d_offsets = nullptr;   // n + 1
+  unsigned int *d_err = nullptr;   // device error word (GRASS_E_DATA on bad ids)
+  grass_graph_info info{};
+  grass::DevGraph view() const {
+    grass::DevGraph g;
+    g.words = d_words;
+    g.offsets = d_offsets;
+    g.n = (uint32_t)info.n;
+    g.mode = mode;
+    return g;
+  }
+};
+
+struct grass_csr {
+  int device = 0;
+  uint64_t n = 0, nnz = 0;
+  uint64_t *d_rowptr = nullptr;
+  uint32_t *d_cols = nullptr;
+  grass::DevCsr view() const {
+    grass::DevCsr c;
+    c.rowptr = d_rowptr;
+    c.cols = d_cols;
+    c.n = (uint32_t)n;
+    return c;
+  }
+};
+
+namespace grass {
+
+// Zero words after the stream.  A header read starts at most at the last
+// stream bit and decodes four gamma codes of at most 63 bits through a
+// cursor that reads two words ahead, so reads stay within 10 words past the
+// stream even for a corrupt header; validation runs before any sampling.
+constexpr int kGuardWords = 16;
+
+// RAII device switch.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+int cuda_fail(cudaError_t e, const char *what);
+#define GRASS_CUDA(call)                                   \
+  do {                                                     \
+    cudaError_t _e = (call);                               \
+    if (_e != cudaSuccess) return grass::cuda_fail(_e, #call); \
+  } while (0)
+
+// Streaming SM count of the current device (cached per device).
+int sm_count(int device);
+
+// ---- load path (kernels_load.cu) ----
+// In-place byte swap of n_words words.
+void launch_bswap(uint32_t *w, uint64_t n_words, cudaStream_t s);
+// lens of n ubl-bit fields (payload words already native) -> exclusive scan
+// into out[0..n]; tmp must hold scan_tmp_words(n) u64.
+uint64_t scan_tmp_words(uint64_t n);
+void launch_unpack_scan(const uint32_t *payload, uint64_t n, uint32_t ubl, uint64_t *out,
+                        uint64_t *tmp, cudaStream_t s);
+// u32 counts -> u64 exclusive scan into out[0..n]
+void launch_scan_u32(const uint32_t *counts, uint64_t n, uint64_t *out, uint64_t *tmp,
+                     cudaStream_t s);
+// Header validation: stats[0] = sum of degrees, stats[1] = max degree,
+// stats[2] = first bad vertex + 1 (0 if none). deg may be null.
+void launch_validate(const DevGraph &g, uint32_t *deg, unsigned long long *stats,
+                     cudaStream_t s);
+void launch_degrees(const DevGraph &g, uint32_t *deg, cudaStream_t s);
+void launch_degrees64(const DevGraph &g, uint64_t *deg, cudaStream_t s);
+// In-place exclusive scan of vals[0..n) into vals[0..n]; tmp as above.
+void launch_scan_u64_inplace(uint64_t *vals, uint64_t n, uint64_t *tmp, cudaStream_t s);
+
+// ---- decode (kernels_decode.cu) ----
+void launch_decode_all(const DevGraph &g, const uint64_t *rowptr, uint32_t *cols,
+                       unsigned int *err, cudaStream_t s);
+
+// ---- samplers (kernels_sample.cu) ----
+void launch_uniform_starts(uint64_t n, uint64_t count, uint64_t seed, uint32_t *out,
+                           cudaStream_t s);
+void launch_rw(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts, uint64_t W,
+               uint32_t *paths, unsigned long long *edges, unsigned int *err, cudaStream_t s);
+void launch_rw_account(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts,
+                       uint64_t W, unsigned long long *out, cudaStream_t s);
+void launch_rw_csr(const DevCsr &c, const grass_rw_params &p, const uint32_t *starts,
+                   uint64_t W, uint32_t *paths, unsigned long long *edges, cudaStream_t s);
+void launch_khop(const DevGraph &g, const grass_khop_params &p, const uint32_t *seeds,
+                 uint64_t S, uint32_t *const *hop_out, unsigned long long *edges,
+                 unsigned int *err, cudaStream_t s);
+void launch_khop_csr(const DevCsr &c, const grass_khop_params &p, const uint32_t *seeds,
+                     uint64_t S, uint32_t *const *hop_out, unsigned long long *edges,
+                     cudaStream_t s);
+int launch_mrw(const DevGraph &g, const grass_mrw_params &p, uint32_t *roots, uint64_t S,
+               uint32_t *src, uint32_t *dst, unsigned long long *edges, unsigned int *err,
+               cudaStream_t s);
+
+}  // namespace grass

@@ -1,0 +1,261 @@
+// kernels_load.cu -- device side of graph loading.
+//
+// Replaces copyPartitionToGPU (GT/src/utils.hpp:360-386): the reference
+// expands the packed .offset lengths with decode_offset (GT/src/bcg.cuh:
+// 368-412, one thread per vertex, grid min(8192, n/256) -- zero blocks when
+// n < 256) and then runs cub::DeviceScan::ExclusiveSum.  Here the unpack is
+// fused into a reduce-then-scan over 4096-vertex tiles, and a validation pass
+// checks every header against its length field once, so sampling kernels can
+// trust headers without per-draw bounds checks.
+#include <cub/block/block_reduce.cuh>
+#include <cub/block/block_scan.cuh>
+
+#include "graph.h"
+
+namespace grass {
+
+namespace {
+
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 16;
+constexpr int kTile = kScanThreads * kScanItems;
+
+__global__ void bswap_kernel(uint32_t *w, uint64_t n_words) {
+  uint64_t n4 = n_words / 4;
+  uint4 *w4 = reinterpret_cast<uint4 *>(w);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    uint4 x = w4[i];
+    x.x = __byte_perm(x.x, 0, 0x0123);
+    x.y = __byte_perm(x.y, 0, 0x0123);
+    x.z = __byte_perm(x.z, 0, 0x0123);
+    x.w = __byte_perm(x.w, 0, 0x0123);
+    w4[i] = x;
+  }
+  uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (t < n_words - n4 * 4) w[n4 * 4 + t] = __byte_perm(w[n4 * 4 + t], 0, 0x0123);
+}
+
+struct FieldLoader {  // n ubl-bit big-endian fields, ubl in [1, 64]
+  const uint32_t *payload;
+  uint32_t ubl;
+  __device__ __forceinline__ uint64_t operator()(uint64_t u) const {
+    const uint64_t bit = u * ubl;
+    if (ubl <= 32) return read_field(payload, bit, (int)ubl);
+    uint64_t hi = read_field(payload, bit, (int)ubl - 32);
+    return (hi << 32) | read_field(payload, bit + ubl - 32, 32);
+  }
+};
+
+struct CountLoader {
+  const uint32_t *counts;
+  __device__ __forceinline__ uint64_t operator()(uint64_t u) const { return counts[u]; }
+};
+
+// Reads u64 values that tile_scan may overwrite in place: every CTA reads its
+// whole tile before its block scan and writes only after it.
+struct U64Loader {
+  const uint64_t *vals;
+  __device__ __forceinline__ uint64_t operator()(uint64_t u) const { return vals[u]; }
+};
+
+template <class Loader>
+__global__ void __launch_bounds__(kScanThreads) tile_reduce(Loader ld, uint64_t n,
+                                                              uint64_t *tile_sums) {
+  using BR = cub::BlockReduce<uint64_t, kScanThreads>;
+  __shared__ typename BR::TempStorage tmp;
+  const uint64_t base = (uint64_t)blockIdx.x * kTile;
+  uint64_t sum = 0;
+#pragma unroll 4
+  for (int k = 0; k < kScanItems; k++) {
+    uint64_t u = base + (uint64_t)k * kScanThreads + threadIdx.x;
+    if (u < n) sum += ld(u);
+  }
+  uint64_t tot = BR(tmp).Sum(sum);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = tot;
+}
+
+// Exclusive scan of T tile sums in place by one CTA; tile_sums[T] = total.
+__global__ void __launch_bounds__(1024) scan_tile_sums(uint64_t *ts, uint64_t T) {
+  using BS = cub::BlockScan<uint64_t, 1024>;
+  __shared__ typename BS::TempStorage tmp;
+  const uint64_t per = (T + 1023) / 1024;
+  const uint64_t b = threadIdx.x * per, e = min(T, b + per);
+  uint64_t local = 0;
+  for (uint64_t i = b; i < e; i++) local += ts[i];
+  uint64_t excl, total;
+  BS(tmp).ExclusiveSum(local, excl, total);
+  for (uint64_t i = b; i < e; i++) {
+    uint64_t x = ts[i];
+    ts[i] = excl;
+    excl += x;
+  }
+  if (threadIdx.x == 0) ts[T] = total;
+}
+
+template <class Loader>
+__global__ void __launch_bounds__(kScanThreads) tile_scan(Loader ld, uint64_t n,
+                                                            const uint64_t *tile_sums,
+                                                            uint64_t *out) {
+  using BS = cub::BlockScan<uint64_t, kScanThreads>;
+  __shared__ typename BS::TempStorage tmp;
+  const uint64_t base = (uint64_t)blockIdx.x * kTile + (uint64_t)threadIdx.x * kScanItems;
+  uint64_t vals[kScanItems];
+  uint64_t sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    uint64_t u = base + k;
+    vals[k] = u < n ? ld(u) : 0;
+    sum += vals[k];
+  }
+  uint64_t excl;
+  BS(tmp).ExclusiveSum(sum, excl);
+  excl += tile_sums[blockIdx.x];
+#pragma unroll
+  for (int k = 0; k < kScanItems; k++) {
+    uint64_t u = base + k;
+    if (u < n) out[u] = excl;
+    excl += vals[k];
+  }
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+    const uint64_t T = gridDim.x;
+    out[n] = tile_sums[T];
+  }
+}
+
+template <class Loader>
+void scan_impl(Loader ld, uint64_t n, uint64_t *out, uint64_t *tmp, cudaStream_t s) {
+  const uint64_t T = (n + kTile - 1) / kTile;
+  if (T == 0) {
+    cudaMemsetAsync(out, 0, sizeof(uint64_t), s);
+    return;
+  }
+  tile_reduce<<<(unsigned)T, kScanThreads, 0, s>>>(ld, n, tmp);
+  scan_tile_sums<<<1, 1024, 0, s>>>(tmp, T);
+  tile_scan<<<(unsigned)T, kScanThreads, 0, s>>>(ld, n, tmp, out);
+  count_launch(3);
+}
+
+template <int MODE>
+__global__ void validate_kernel(DevGraph g, uint32_t *deg, unsigned long long *stats) {
+  using BR = cub::BlockReduce<unsigned long long, 256>;
+  __shared__ typename BR::TempStorage tmp;
+  unsigned long long sum = 0, mx = 0, bad = ~0ull;
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < g.n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t o0 = g.offsets[v], o1 = g.offsets[v + 1];
+    BitCur c;
+    c.init(g.words, o0);
+    uint32_t d = c.gamma();
+    bool ok = true;
+    uint64_t end = 0;
+    if (MODE == 0) {
+      uint32_t hb = c.gamma(), bb = c.gamma(), fp = c.gamma();
+      VHdr h = gt_header(g, (uint32_t)v);
+      ok = hb >= (d ? 1u : 0u) && hb <= 32 && bb <= 32 && fp <= h.bn + 1 && d < 0x7FFFFFFFu;
+      end = ok ? payload_end<0>(g, h) : 0;
+    } else {
+      if (d == 0) {
+        end = c.pos(g.words);
+      } else if (d == 1) {
+        uint32_t nb = c.gamma();
+        ok = nb < g.n;
+        end = c.pos(g.words);
+      } else {
+        uint32_t rb = c.gamma(), sb = c.gamma(), fp = c.gamma();
+        VHdr h = le_header(g, (uint32_t)v);
+        ok = rb >= 1 && rb <= 32 && sb <= 31 && fp <= h.bn + 2 && d < 0x7FFFFFFFu;
+        end = ok ? payload_end<1>(g, h) : 0;
+      }
+    }
+    ok = ok && end == o1;
+    if (!ok) bad = min(bad, (unsigned long long)v);
+    if (deg) deg[v] = ok ? d : 0;
+    if (ok) {
+      sum += d;
+      mx = max(mx, (unsigned long long)d);
+    }
+  }
+  unsigned long long s = BR(tmp).Sum(sum);
+  __syncthreads();
+  unsigned long long m = BR(tmp).Reduce(mx, cub::Max());
+  __syncthreads();
+  unsigned long long b = BR(tmp).Reduce(bad, cub::Min());
+  if (threadIdx.x == 0) {
+    atomicAdd(&stats[0], s);
+    atomicMax(&stats[1], m);
+    if (b != ~0ull) atomicMin(&stats[2], b);
+  }
+}
+
+template <int MODE, class T>
+__global__ void degrees_kernel(DevGraph g, T *deg) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < g.n;
+       v += (uint64_t)gridDim.x * blockDim.x) {
+    BitCur c;
+    c.init(g.words, g.offsets[v]);
+    deg[v] = (T)c.gamma();
+  }
+}
+
+unsigned grid_for(uint64_t items, int threads, int device) {
+  uint64_t blocks = (items + threads - 1) / threads;
+  uint64_t cap = (uint64_t)sm_count(device) * 16;
+  return (unsigned)std::max<uint64_t>(1, std::min(blocks, cap));
+}
+
+}  // namespace
+
+void launch_bswap(uint32_t *w, uint64_t n_words, cudaStream_t s) {
+  if (!n_words) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  bswap_kernel<<<grid_for(n_words / 4 + 1, 256, dev), 256, 0, s>>>(w, n_words);
+  count_launch();
+}
+
+uint64_t scan_tmp_words(uint64_t n) { return (n + kTile - 1) / kTile + 1; }
+
+void launch_unpack_scan(const uint32_t *payload, uint64_t n, uint32_t ubl, uint64_t *out,
+                        uint64_t *tmp, cudaStream_t s) {
+  scan_impl(FieldLoader{payload, ubl}, n, out, tmp, s);
+}
+
+void launch_scan_u32(const uint32_t *counts, uint64_t n, uint64_t *out, uint64_t *tmp,
+                     cudaStream_t s) {
+  scan_impl(CountLoader{counts}, n, out, tmp, s);
+}
+
+void launch_validate(const DevGraph &g, uint32_t *deg, unsigned long long *stats,
+                     cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  unsigned grid = grid_for(g.n, 256, dev);
+  if (g.mode == GRASS_MODE_GT) validate_kernel<0><<<grid, 256, 0, s>>>(g, deg, stats);
+  else validate_kernel<1><<<grid, 256, 0, s>>>(g, deg, stats);
+  count_launch();
+}
+
+void launch_degrees(const DevGraph &g, uint32_t *deg, cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  unsigned grid = grid_for(g.n, 256, dev);
+  if (g.mode == GRASS_MODE_GT) degrees_kernel<0, uint32_t><<<grid, 256, 0, s>>>(g, deg);
+  else degrees_kernel<1, uint32_t><<<grid, 256, 0, s>>>(g, deg);
+  count_launch();
+}
+
+void launch_degrees64(const DevGraph &g, uint64_t *deg, cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  unsigned grid = grid_for(g.n, 256, dev);
+  if (g.mode == GRASS_MODE_GT) degrees_kernel<0, uint64_t><<<grid, 256, 0, s>>>(g, deg);
+  else degrees_kernel<1, uint64_t><<<grid, 256, 0, s>>>(g, deg);
+  count_launch();
+}
+
+void launch_scan_u64_inplace(uint64_t *vals, uint64_t n, uint64_t *tmp, cudaStream_t s) {
+  scan_impl(U64Loader{vals}, n, vals, tmp, s);
+}
+
+}  // namespace grass

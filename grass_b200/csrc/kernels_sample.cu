@@ -1,0 +1,593 @@
+// kernels_sample.cu -- random walk, k-hop and multi-RW kernels over the
+// compressed graph, plus the uncompressed-CSR baselines with the same RNG.
+//
+// The reference runs every app step as a separate transit-parallel pass:
+// sample kernel, then a global radix sort inverting sample->transit, run-
+// length encoding, a scan and a kernel-type partition, with blocking syncs in
+// between (GT/src/grass.cu:1573-1998).  For fanout-1 walks nothing is shared
+// between walkers on the same transit, so here one launch runs all steps:
+// each thread owns DEPTH walkers and interleaves them, which keeps DEPTH
+// independent decode chains in flight per thread.
+#include "graph.h"
+
+namespace grass {
+
+namespace {
+
+__device__ __forceinline__ void store_path(uint32_t *paths, int layout, uint64_t W, uint32_t L,
+                                           uint64_t w, uint32_t s, uint32_t v) {
+  if (layout == GRASS_LAYOUT_WALK_MAJOR) paths[w * (uint64_t)(L + 1) + s] = v;
+  else paths[(uint64_t)s * W + w] = v;
+}
+
+template <int MODE, int DEPTH>
+__global__ void __launch_bounds__(256) rw_kernel(DevGraph g, const uint32_t *__restrict__ starts,
+                                                 uint64_t W, uint32_t L, uint64_t seed,
+                                                 int layout, uint32_t *__restrict__ paths,
+                                                 unsigned long long *edges, unsigned int *err) {
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t cnt = 0;
+  bool bad = false;
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; base < W;
+       base += nthreads * DEPTH) {
+    uint32_t v[DEPTH];
+    u32x4 r[DEPTH];
+#pragma unroll
+    for (int k = 0; k < DEPTH; k++) {
+      const uint64_t w = base + k * nthreads;
+      v[k] = INVALID_VERTEX;
+      r[k] = u32x4{0, 0, 0, 0};
+      if (w < W) {
+        const uint32_t s0 = starts[w];
+        store_path(paths, layout, W, L, w, 0, s0);
+        v[k] = s0 < g.n ? s0 : INVALID_VERTEX;
+      }
+    }
+    for (uint32_t s = 0; s < L; s++) {
+#pragma unroll
+      for (int k = 0; k < DEPTH; k++) {
+        const uint64_t w = base + k * nthreads;
+        if ((s & 3) == 0)
+          r[k] = philox4x32_10(seed, s >> 2, (uint32_t)w, (uint32_t)(w >> 32), TAG_RW);
+        if (v[k] != INVALID_VERTEX) {
+          const VHdr h = header<MODE>(g, v[k]);
+          if (h.d == 0) {
+            v[k] = INVALID_VERTEX;
+          } else {
+            const uint32_t nv = neighbor<MODE>(g, h, mulhi_u32(pick(r[k], s & 3), h.d));
+            if (nv >= g.n) {
+              bad = true;
+              v[k] = INVALID_VERTEX;
+            } else {
+              v[k] = nv;
+              cnt++;
+            }
+          }
+        }
+        if (w < W) store_path(paths, layout, W, L, w, s + 1, v[k]);
+      }
+    }
+  }
+  warp_add_u64(edges, cnt);
+  if (bad && err) atomicOr(err, 1u);
+}
+
+// Bits a draw of neighbor i reads from the stream, and the 32-byte sectors
+// those reads span (header range plus payload ranges, in stream order).
+template <int MODE>
+__device__ __forceinline__ void draw_footprint(const DevGraph &g, const VHdr &h, uint32_t i,
+                                               uint64_t &bits, uint64_t &sectors) {
+  const uint64_t o0 = g.offsets[h.v];
+  uint64_t r0[3], r1[3];  // half-open bit ranges
+  int nr = 0;
+  uint64_t hdr_end = h.P;
+  if (MODE == 1 && h.d == 1) {  // LE degree 1: the neighbor is the second header field
+    BitCur c;
+    c.init(g.words, o0);
+    c.gamma();
+    c.gamma();
+    hdr_end = c.pos(g.words);
+  }
+  r0[nr] = o0;
+  r1[nr++] = hdr_end;
+  if (MODE == 0) {
+    const uint32_t split = (h.bl + 1) * h.om;
+    const bool flag = i < split;
+    const uint32_t j = flag ? i : i - split;
+    const uint32_t len = h.bl + (flag ? 1u : 0u);
+    uint32_t blk = j / len;
+    const uint32_t id = j - blk * len;
+    if (!flag) blk += h.om;
+    const uint64_t pos = h.P + (uint64_t)blk * (uint64_t)(h.a + (h.bl - 1) * h.b) +
+                         (uint64_t)min(blk, h.om) * (uint64_t)h.b;
+    r0[nr] = pos;
+    r1[nr++] = pos + h.a + (uint64_t)id * h.b;
+  } else if (h.d > 1) {
+    uint32_t tl = h.bl + 1;
+    const uint32_t split = h.om * tl;
+    const bool flag = i >= split;
+    const uint32_t j = flag ? i - split : i;
+    if (flag) tl -= 1;
+    uint32_t c = j / tl;
+    const uint32_t id = j - c * tl;
+    if (flag) c += h.om;
+    const uint64_t rp = h.P + (uint64_t)c * h.a;
+    r0[nr] = rp;
+    r1[nr++] = rp + (id ? 2u : 1u) * (uint64_t)h.a;
+    if (id) {
+      const uint64_t spos =
+          h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a +
+          ((uint64_t)(h.bl - 1) * c + min(h.om, c) + id - 1) * (uint64_t)(h.b + 1);
+      r0[nr] = spos;
+      r1[nr++] = spos + h.b + 1;
+    }
+  }
+  bits = 0;
+  sectors = 0;
+  uint64_t last = ~0ull;
+  for (int k = 0; k < nr; k++) {
+    if (r1[k] <= r0[k]) continue;
+    bits += r1[k] - r0[k];
+    const uint64_t s0 = r0[k] >> 8, s1 = (r1[k] - 1) >> 8;
+    sectors += s1 - s0 + 1 - (s0 == last ? 1 : 0);
+    last = s1;
+  }
+}
+
+// Replays a walk (same stream as rw_kernel) and sums, per draw, the
+// algorithmic bytes 8 (offset) + ceil(stream bits read / 8) + 4 (path entry)
+// and the 32-byte sectors those reads span (+1 for the offset).  out[0] =
+// bytes, out[1] = sectors, out[2] = draws.  Start entries add 4 bytes each.
+template <int MODE>
+__global__ void __launch_bounds__(256) rw_account_kernel(DevGraph g,
+                                                         const uint32_t *__restrict__ starts,
+                                                         uint64_t W, uint32_t L, uint64_t seed,
+                                                         unsigned long long *out) {
+  uint64_t bytes = 0, sect = 0, draws = 0;
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < W;
+       w += (uint64_t)gridDim.x * blockDim.x) {
+    uint32_t v = starts[w];
+    bytes += 4;
+    if (v >= g.n) v = INVALID_VERTEX;
+    u32x4 r{0, 0, 0, 0};
+    for (uint32_t s = 0; s < L; s++) {
+      if ((s & 3) == 0) r = philox4x32_10(seed, s >> 2, (uint32_t)w, (uint32_t)(w >> 32), TAG_RW);
+      bytes += 4;
+      if (v == INVALID_VERTEX) continue;
+      const VHdr h = header<MODE>(g, v);
+      if (h.d == 0) {
+        v = INVALID_VERTEX;
+        continue;
+      }
+      const uint32_t i = mulhi_u32(pick(r, s & 3), h.d);
+      uint64_t b, sc;
+      draw_footprint<MODE>(g, h, i, b, sc);
+      bytes += 8 + (b + 7) / 8;
+      sect += 1 + sc;
+      draws++;
+      const uint32_t nv = neighbor<MODE>(g, h, i);
+      v = nv < g.n ? nv : INVALID_VERTEX;
+    }
+  }
+  warp_add_u64(&out[0], bytes);
+  warp_add_u64(&out[1], sect);
+  warp_add_u64(&out[2], draws);
+}
+
+template <int DEPTH>
+__global__ void __launch_bounds__(256) rw_csr_kernel(DevCsr c, const uint32_t *__restrict__ starts,
+                                                     uint64_t W, uint32_t L, uint64_t seed,
+                                                     int layout, uint32_t *__restrict__ paths,
+                                                     unsigned long long *edges) {
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t cnt = 0;
+  for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; base < W;
+       base += nthreads * DEPTH) {
+    uint32_t v[DEPTH];
+    u32x4 r[DEPTH];
+#pragma unroll
+    for (int k = 0; k < DEPTH; k++) {
+      const uint64_t w = base + k * nthreads;
+      v[k] = INVALID_VERTEX;
+      r[k] = u32x4{0, 0, 0, 0};
+      if (w < W) {
+        const uint32_t s0 = starts[w];
+        store_path(paths, layout, W, L, w, 0, s0);
+        v[k] = s0 < c.n ? s0 : INVALID_VERTEX;
+      }
+    }
+    for (uint32_t s = 0; s < L; s++) {
+#pragma unroll
+      for (int k = 0; k < DEPTH; k++) {
+        const uint64_t w = base + k * nthreads;
+        if ((s & 3) == 0)
+          r[k] = philox4x32_10(seed, s >> 2, (uint32_t)w, (uint32_t)(w >> 32), TAG_RW);
+        if (v[k] != INVALID_VERTEX) {
+          const uint64_t b = __ldg(c.rowptr + v[k]);
+          const uint64_t d = __ldg(c.rowptr + v[k] + 1) - b;
+          if (d == 0) {
+            v[k] = INVALID_VERTEX;
+          } else {
+            v[k] = __ldg(c.cols + b + mulhi_u32(pick(r[k], s & 3), (uint32_t)d));
+            cnt++;
+          }
+        }
+        if (w < W) store_path(paths, layout, W, L, w, s + 1, v[k]);
+      }
+    }
+  }
+  warp_add_u64(edges, cnt);
+}
+
+// ---------------------------------------------------------------------------
+// k-hop.  One warp per sample.  For each hop, the frontier is taken in
+// chunks of 32 transits: lane p decodes the header of transit p into shared
+// memory, then the chunk's f*32 draws are spread over the lanes.
+
+struct KhopArgs {
+  uint32_t hops;
+  uint32_t fan[GRASS_MAX_HOPS];
+  uint64_t width[GRASS_MAX_HOPS];  // prod_{j<=h} fan[j]
+  uint32_t *out[GRASS_MAX_HOPS];
+  uint64_t seed;
+};
+
+struct SmemHdr {
+  uint64_t P[32];
+  uint32_t v[32], d[32], bn[32], bl[32], om[32], fp[32];
+  int a[32], b[32];
+  __device__ __forceinline__ void put(int i, const VHdr &h) {
+    P[i] = h.P; v[i] = h.v; d[i] = h.d; bn[i] = h.bn; bl[i] = h.bl; om[i] = h.om; fp[i] = h.fp;
+    a[i] = h.a; b[i] = h.b;
+  }
+  __device__ __forceinline__ VHdr get(int i) const {
+    VHdr h;
+    h.P = P[i]; h.v = v[i]; h.d = d[i]; h.bn = bn[i]; h.bl = bl[i]; h.om = om[i]; h.fp = fp[i];
+    h.a = a[i]; h.b = b[i];
+    return h;
+  }
+};
+
+template <int MODE>
+__global__ void __launch_bounds__(256) khop_kernel(DevGraph g, const uint32_t *__restrict__ seeds,
+                                                   uint64_t S, KhopArgs A,
+                                                   unsigned long long *edges, unsigned int *err) {
+  __shared__ SmemHdr sh[8];
+  const int lane = threadIdx.x & 31;
+  SmemHdr &my = sh[threadIdx.x >> 5];
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  uint64_t cnt = 0;
+  bool bad = false;
+  for (uint64_t s = warp; s < S; s += nwarps) {
+    for (uint32_t hop = 0; hop < A.hops; hop++) {
+      const uint32_t f = A.fan[hop];
+      const uint64_t P = hop ? A.width[hop - 1] : 1;
+      uint32_t *out = A.out[hop] + s * A.width[hop];
+      const uint32_t *prev = hop ? A.out[hop - 1] + s * A.width[hop - 1] : nullptr;
+      for (uint64_t pc = 0; pc < P; pc += 32) {
+        const uint64_t p = pc + lane;
+        uint32_t t = INVALID_VERTEX;
+        if (p < P) t = hop ? prev[p] : seeds[s];
+        VHdr h;
+        if (t < g.n) {
+          h = header<MODE>(g, t);
+        } else {
+          h.d = 0;
+          h.P = 0;
+          h.v = t;
+          h.bn = h.bl = h.om = h.fp = 0;
+          h.a = h.b = 0;
+        }
+        my.put(lane, h);
+        __syncwarp();
+        const uint64_t nP = min((uint64_t)32, P - pc);
+        const uint64_t total = nP * f;
+        for (uint64_t j0 = 0; j0 < total; j0 += 32) {
+          const uint64_t j = j0 + lane;
+          if (j < total) {
+            const uint32_t pl = (uint32_t)(j / f);
+            const uint64_t slot = pc * f + j;
+            const VHdr hk = my.get(pl);
+            uint32_t nv = INVALID_VERTEX;
+            if (hk.d) {
+              const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(slot >> 2), (uint32_t)s,
+                                             (uint32_t)(s >> 32), TAG_KHOP | hop);
+              nv = neighbor<MODE>(g, hk, mulhi_u32(pick(rr, (int)(slot & 3)), hk.d));
+              if (nv >= g.n) {
+                bad = true;
+                nv = INVALID_VERTEX;
+              } else {
+                cnt++;
+              }
+            }
+            out[slot] = nv;
+          }
+        }
+        __syncwarp();
+      }
+    }
+  }
+  warp_add_u64(edges, cnt);
+  if (bad && err) atomicOr(err, 1u);
+}
+
+__global__ void __launch_bounds__(256) khop_csr_kernel(DevCsr c, const uint32_t *__restrict__ seeds,
+                                                       uint64_t S, KhopArgs A,
+                                                       unsigned long long *edges) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  uint64_t cnt = 0;
+  for (uint64_t s = warp; s < S; s += nwarps) {
+    for (uint32_t hop = 0; hop < A.hops; hop++) {
+      const uint32_t f = A.fan[hop];
+      const uint64_t P = hop ? A.width[hop - 1] : 1;
+      uint32_t *out = A.out[hop] + s * A.width[hop];
+      const uint32_t *prev = hop ? A.out[hop - 1] + s * A.width[hop - 1] : nullptr;
+      const uint64_t total = P * f;
+      for (uint64_t j = lane; j < total; j += 32) {
+        const uint64_t p = j / f;
+        const uint32_t t = hop ? prev[p] : seeds[s];
+        uint32_t nv = INVALID_VERTEX;
+        if (t < c.n) {
+          const uint64_t b = c.rowptr[t], d = c.rowptr[t + 1] - b;
+          if (d) {
+            const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(j >> 2), (uint32_t)s,
+                                           (uint32_t)(s >> 32), TAG_KHOP | hop);
+            nv = c.cols[b + mulhi_u32(pick(rr, (int)(j & 3)), (uint32_t)d)];
+            cnt++;
+          }
+        }
+        out[j] = nv;
+      }
+      __syncwarp();
+    }
+  }
+  warp_add_u64(edges, cnt);
+}
+
+// ---------------------------------------------------------------------------
+// Multi random walk.  One warp per sample; the walkers' vertices, degrees and
+// a Fenwick tree of degrees (degree-proportional selection) live in shared
+// memory; lane 0 runs the step chain, which is sequential by definition.
+
+struct MrwLayout {
+  uint32_t R;
+  __host__ __device__ size_t bytes_per_warp() const {
+    return ((size_t)R * 4 + 15) / 16 * 16 * 2 + ((size_t)R + 1) * 8;
+  }
+};
+
+__device__ __forceinline__ void fen_add(uint64_t *fen, uint32_t R, uint32_t i, int64_t delta) {
+  for (uint32_t k = i + 1; k <= R; k += k & (0u - k)) fen[k] += (uint64_t)delta;
+}
+
+// largest k with prefix(k) <= u; the selected walker is k (0-based).
+__device__ __forceinline__ uint32_t fen_find(const uint64_t *fen, uint32_t R, uint32_t logR,
+                                             uint64_t u) {
+  uint32_t k = 0;
+  for (uint32_t step = 1u << logR; step; step >>= 1) {
+    const uint32_t nk = k + step;
+    if (nk <= R && fen[nk] <= u) {
+      k = nk;
+      u -= fen[nk];
+    }
+  }
+  return k;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) mrw_kernel(DevGraph g, uint32_t *__restrict__ roots,
+                                                  uint64_t S, uint32_t R, uint32_t T, int select,
+                                                  uint64_t seed, uint32_t *__restrict__ src,
+                                                  uint32_t *__restrict__ dst,
+                                                  unsigned long long *edges, unsigned int *err) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const MrwLayout lay{R};
+  const int lane = threadIdx.x & 31;
+  unsigned char *base = smem + (threadIdx.x >> 5) * lay.bytes_per_warp();
+  const size_t rbytes = ((size_t)R * 4 + 15) / 16 * 16;
+  uint32_t *rv = reinterpret_cast<uint32_t *>(base);
+  uint32_t *rd = reinterpret_cast<uint32_t *>(base + rbytes);
+  uint64_t *fen = reinterpret_cast<uint64_t *>(base + 2 * rbytes);
+  uint32_t logR = 0;
+  while ((1u << (logR + 1)) <= R) logR++;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  uint64_t cnt = 0;
+  bool bad = false;
+  for (uint64_t s = warp; s < S; s += nwarps) {
+    uint32_t *rt = roots + s * R;
+    for (uint32_t i = lane; i < R; i += 32) {
+      const uint32_t x = rt[i];
+      rv[i] = x;
+      uint32_t d = 0;
+      if (x < g.n) d = header<MODE>(g, x).d;
+      rd[i] = d;
+    }
+    __syncwarp();
+    if (lane == 0) {
+      uint64_t wsum = 0;
+      if (select == GRASS_SELECT_DEGREE) {
+        for (uint32_t k = 0; k <= R; k++) fen[k] = 0;
+        for (uint32_t i = 0; i < R; i++) {
+          fen_add(fen, R, i, rd[i]);
+          wsum += rd[i];
+        }
+      }
+      for (uint32_t t = 0; t < T; t++) {
+        const u32x4 rr = philox4x32_10(seed, t, (uint32_t)s, (uint32_t)(s >> 32), TAG_MRW);
+        const uint64_t io = s * T + t;
+        uint32_t x;
+        if (select == GRASS_SELECT_DEGREE) {
+          if (wsum == 0) {
+            src[io] = INVALID_VERTEX;
+            dst[io] = INVALID_VERTEX;
+            continue;
+          }
+          const uint64_t r64 = ((uint64_t)rr.z << 32) | rr.x;
+          x = fen_find(fen, R, logR, mulhi_u64(r64, wsum));
+        } else {
+          x = mulhi_u32(rr.x, R);
+        }
+        const uint32_t v = rv[x];
+        src[io] = v;
+        if (rd[x] == 0) {
+          dst[io] = INVALID_VERTEX;
+          continue;
+        }
+        const VHdr h = header<MODE>(g, v);
+        uint32_t nv = neighbor<MODE>(g, h, mulhi_u32(rr.y, h.d));
+        if (nv >= g.n) {
+          bad = true;
+          dst[io] = INVALID_VERTEX;
+          continue;
+        }
+        dst[io] = nv;
+        cnt++;
+        rv[x] = nv;
+        const uint32_t nd = header<MODE>(g, nv).d;
+        if (select == GRASS_SELECT_DEGREE) {
+          fen_add(fen, R, x, (int64_t)nd - (int64_t)rd[x]);
+          wsum = wsum - rd[x] + nd;
+        }
+        rd[x] = nd;
+      }
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < R; i += 32) rt[i] = rv[i];
+    __syncwarp();
+  }
+  warp_add_u64(edges, cnt);
+  if (bad && err) atomicOr(err, 1u);
+}
+
+__global__ void starts_kernel(uint64_t n, uint64_t count, uint64_t seed, uint32_t tag,
+                              uint32_t *out) {
+  const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t q = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; q * 4 < count; q += nt) {
+    const u32x4 r = philox4x32_10(seed, (uint32_t)q, 0, 0, tag);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint64_t i = q * 4 + k;
+      if (i < count) out[i] = mulhi_u32(pick(r, k), (uint32_t)n);
+    }
+  }
+}
+
+unsigned grid_warps(uint64_t units, int units_per_block, int device, int per_sm) {
+  const uint64_t need = (units + units_per_block - 1) / units_per_block;
+  const uint64_t cap = (uint64_t)sm_count(device) * per_sm;
+  return (unsigned)std::max<uint64_t>(1, std::min(need, cap));
+}
+
+int cur_dev() {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d;
+}
+
+}  // namespace
+
+void launch_uniform_starts(uint64_t n, uint64_t count, uint64_t seed, uint32_t *out,
+                           cudaStream_t s) {
+  if (!count) return;
+  starts_kernel<<<grid_warps((count + 3) / 4, 256, cur_dev(), 8), 256, 0, s>>>(n, count, seed,
+                                                                              TAG_START, out);
+  count_launch();
+}
+
+void launch_rw(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts, uint64_t W,
+               uint32_t *paths, unsigned long long *edges, unsigned int *err, cudaStream_t s) {
+  if (!W) return;
+  constexpr int DEPTH = 2;
+  const unsigned grid = grid_warps((W + DEPTH - 1) / DEPTH, 256, cur_dev(), 8);
+  if (g.mode == GRASS_MODE_GT)
+    rw_kernel<0, DEPTH><<<grid, 256, 0, s>>>(g, starts, W, p.length, p.seed, (int)p.layout,
+                                             paths, edges, err);
+  else
+    rw_kernel<1, DEPTH><<<grid, 256, 0, s>>>(g, starts, W, p.length, p.seed, (int)p.layout,
+                                             paths, edges, err);
+  count_launch();
+}
+
+void launch_rw_account(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts,
+                       uint64_t W, unsigned long long *out, cudaStream_t s) {
+  if (!W) return;
+  const unsigned grid = grid_warps(W, 256, cur_dev(), 8);
+  if (g.mode == GRASS_MODE_GT)
+    rw_account_kernel<0><<<grid, 256, 0, s>>>(g, starts, W, p.length, p.seed, out);
+  else
+    rw_account_kernel<1><<<grid, 256, 0, s>>>(g, starts, W, p.length, p.seed, out);
+  count_launch();
+}
+
+void launch_rw_csr(const DevCsr &c, const grass_rw_params &p, const uint32_t *starts,
+                   uint64_t W, uint32_t *paths, unsigned long long *edges, cudaStream_t s) {
+  if (!W) return;
+  constexpr int DEPTH = 2;
+  const unsigned grid = grid_warps((W + DEPTH - 1) / DEPTH, 256, cur_dev(), 8);
+  rw_csr_kernel<DEPTH><<<grid, 256, 0, s>>>(c, starts, W, p.length, p.seed, (int)p.layout,
+                                            paths, edges);
+  count_launch();
+}
+
+static KhopArgs khop_args(const grass_khop_params &p, uint32_t *const *hop_out) {
+  KhopArgs A{};
+  A.hops = p.hops;
+  uint64_t w = 1;
+  for (uint32_t h = 0; h < p.hops; h++) {
+    A.fan[h] = p.fanouts[h];
+    w *= p.fanouts[h];
+    A.width[h] = w;
+    A.out[h] = hop_out[h];
+  }
+  A.seed = p.seed;
+  return A;
+}
+
+void launch_khop(const DevGraph &g, const grass_khop_params &p, const uint32_t *seeds,
+                 uint64_t S, uint32_t *const *hop_out, unsigned long long *edges,
+                 unsigned int *err, cudaStream_t s) {
+  if (!S) return;
+  const KhopArgs A = khop_args(p, hop_out);
+  const unsigned grid = grid_warps(S, 8, cur_dev(), 8);
+  if (g.mode == GRASS_MODE_GT)
+    khop_kernel<0><<<grid, 256, 0, s>>>(g, seeds, S, A, edges, err);
+  else
+    khop_kernel<1><<<grid, 256, 0, s>>>(g, seeds, S, A, edges, err);
+  count_launch();
+}
+
+void launch_khop_csr(const DevCsr &c, const grass_khop_params &p, const uint32_t *seeds,
+                     uint64_t S, uint32_t *const *hop_out, unsigned long long *edges,
+                     cudaStream_t s) {
+  if (!S) return;
+  const KhopArgs A = khop_args(p, hop_out);
+  khop_csr_kernel<<<grid_warps(S, 8, cur_dev(), 8), 256, 0, s>>>(c, seeds, S, A, edges);
+  count_launch();
+}
+
+int launch_mrw(const DevGraph &g, const grass_mrw_params &p, uint32_t *roots, uint64_t S,
+               uint32_t *src, uint32_t *dst, unsigned long long *edges, unsigned int *err,
+               cudaStream_t s) {
+  if (!S || !p.steps) return GRASS_OK;
+  const MrwLayout lay{p.walkers};
+  const size_t per_warp = lay.bytes_per_warp();
+  const size_t budget = 200 * 1024;
+  int warps = (int)std::min<size_t>(8, budget / per_warp);
+  if (warps < 1) return set_error(GRASS_E_ARG, "multi-RW: %u walkers exceed shared memory",
+                                  p.walkers);
+  const size_t smem = per_warp * warps;
+  auto kern = g.mode == GRASS_MODE_GT ? mrw_kernel<0> : mrw_kernel<1>;
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const unsigned grid = grid_warps(S, warps, cur_dev(), 8);
+  kern<<<grid, warps * 32, smem, s>>>(g, roots, S, p.walkers, p.steps, (int)p.select, p.seed,
+                                       src, dst, edges, err);
+  count_launch();
+  return GRASS_OK;
+}
+
+}  // namespace grass

@@ -1,0 +1,231 @@
+/*
+ * grass.h -- C ABI of the B200-native compressed-graph sampler.
+ *
+ * Plain C: opaque handles, plain pointers and sizes, int status codes, no
+ * exceptions or aborts across the boundary.  Device-pointer entry points are
+ * asynchronous on the given CUDA stream (NULL = legacy default stream);
+ * "_host" entry points take host buffers, copy in and out inside the call
+ * and return when the results are in host memory.
+ *
+ * Each entry point names the reference (calla212/GraSS) interface it replaces,
+ * by file:line within that project.  The reference exposes its hot path as a
+ * compile-time App template run by nextdoor<SampleType, App>(graph_file,
+ * nruns) (GT/src/grass.cu:2066-2135); here the app becomes a runtime
+ * parameter block and the graph a handle that outlives one run.
+ */
+#ifndef GRASS_B200_H
+#define GRASS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (replace CHK_CU's print-and-assert, GT/src/utils.hpp:17) ---- */
+#define GRASS_OK 0
+#define GRASS_E_IO 1          /* file missing or unreadable */
+#define GRASS_E_FORMAT 2      /* malformed .graph/.offset content */
+#define GRASS_E_CUDA 3        /* a CUDA runtime call failed */
+#define GRASS_E_OOM 4         /* host or device allocation failed */
+#define GRASS_E_BUDGET 5      /* request exceeds the scratch budget */
+#define GRASS_E_TIMEOUT 6     /* a bounded wait ran out */
+#define GRASS_E_ARG 7         /* invalid argument */
+#define GRASS_E_DATA 8        /* decoded vertex id out of range (corrupt payload) */
+
+/* ---- decode modes: the reference's two source trees / file formats ---- */
+#define GRASS_MODE_GT 0 /* GT/: gamma header + per-block head and gaps   */
+#define GRASS_MODE_LE 1 /* LE/: gamma header + rocks and signed seas     */
+
+#define GRASS_INVALID_VERTEX 0xFFFFFFFFu
+
+/* Output layouts of random-walk paths. */
+#define GRASS_LAYOUT_WALK_MAJOR 0 /* paths[w * (L+1) + s] */
+#define GRASS_LAYOUT_STEP_MAJOR 1 /* paths[s * W + w]     */
+
+/* Multi-RW walker selection. */
+#define GRASS_SELECT_UNIFORM 0 /* reference: MultiRWApp::stepTransits, GT/src/apps/multiRW/multiRW.cu:93-101 */
+#define GRASS_SELECT_DEGREE 1  /* frontier sampling: proportional to current degree */
+
+/* Thread-local message for the last failing call on this thread. */
+const char *grass_last_error(void);
+/* Number of CUDA kernels this library has launched in this process. */
+uint64_t grass_launch_count(void);
+/* Library version string. */
+const char *grass_version(void);
+
+/* =========================================================================
+ * Host graph tools.  Replace the offline pipeline GT/chunk_compress/
+ * (graph_sort.cpp:22-82, compressor.hpp:24-490, compress.cpp:6-28).
+ * ========================================================================= */
+
+/* R-MAT edge generator: m = edge_factor << scale edges into src[m], dst[m].
+ * Edge k takes its quadrant choices from Philox(seed; k, 0, 0, TAG_GEN).
+ * No reference counterpart (the reference ships no generator). */
+int grass_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c,
+                   uint64_t seed, uint32_t *src, uint32_t *dst);
+
+/* Chung-Lu power-law generator: m edges between n vertices whose expected
+ * degrees follow w_i ~ (i + i0)^(-1/(exponent-1)), scaled to mean_degree and
+ * capped at max_degree.  No reference counterpart. */
+int grass_gen_chung_lu(uint64_t n, double exponent, double mean_degree, uint64_t max_degree,
+                       uint64_t seed, uint64_t m, uint32_t *src, uint32_t *dst);
+
+/* Host CSR produced by grass_graph_sort. */
+typedef struct grass_host_csr grass_host_csr;
+
+/* graph_sort semantics (GT/chunk_compress/graph_sort.cpp:47-72): relabel
+ * vertices by first appearance, drop self-loops, dedupe, and (directed == 0)
+ * symmetrize.  Rows come out sorted. */
+int grass_graph_sort(const uint32_t *src, const uint32_t *dst, uint64_t m, int directed,
+                     grass_host_csr **out);
+int grass_host_csr_view(const grass_host_csr *csr, uint64_t *n, uint64_t *nnz,
+                        const uint64_t **rowptr, const uint32_t **cols);
+void grass_host_csr_free(grass_host_csr *csr);
+
+/* Compress a sorted CSR into the reference's on-disk format, byte-identical
+ * to Compressor::compress + write_cgr (GT/chunk_compress/compressor.hpp:
+ * 120-243, 245-362, 422-447; LE/chunk_compress/compressor.hpp:130-187,
+ * 217-285, 288-403, 479-502).  Two-call pattern: with NULL buffers, the
+ * sizes are returned in *graph_size and *offset_size; then call again with
+ * buffers of those sizes. */
+int grass_compress(const uint64_t *rowptr, const uint32_t *cols, uint64_t n, int mode,
+                   uint8_t *graph_buf, uint64_t *graph_size, uint8_t *offset_buf,
+                   uint64_t *offset_size);
+/* Same, writing <prefix>.graph and <prefix>.offset. */
+int grass_compress_to_files(const uint64_t *rowptr, const uint32_t *cols, uint64_t n, int mode,
+                            const char *prefix);
+
+/* =========================================================================
+ * Device graph.  Replaces loadGraph (GT/src/grass.cu:1126-1215),
+ * transferToGPUs (GT/src/grass.cu:1217-1233) and copyPartitionToGPU +
+ * decode_offset + the offset scan (GT/src/utils.hpp:360-386,
+ * GT/src/bcg.cuh:368-412).  Unlike the reference's __constant__ partition
+ * (GT/src/grass.cu:59), several graphs may be open at once.
+ * ========================================================================= */
+typedef struct grass_graph grass_graph;
+
+typedef struct {
+  uint64_t n;                 /* vertices (byte-padding fields trimmed)   */
+  uint64_t n_file;            /* the reference's count (size-1)*8/ubl     */
+  uint64_t num_edges;         /* sum of degrees                           */
+  uint32_t max_degree;
+  uint32_t ubl;               /* width of one .offset length field        */
+  int32_t mode;               /* GRASS_MODE_GT or GRASS_MODE_LE           */
+  int32_t device;
+  uint64_t graph_file_bytes;  /* .graph size                              */
+  uint64_t offset_file_bytes; /* .offset size                             */
+  uint64_t device_bytes;      /* resident: stream words + offset index    */
+  double read_seconds;        /* file read into pinned memory             */
+  double upload_seconds;      /* copies + device index build              */
+} grass_graph_info;
+
+/* Load <prefix>.graph / <prefix>.offset onto `device`. */
+int grass_open(const char *prefix, int mode, int device, grass_graph **out);
+/* Same from in-memory file images. */
+int grass_open_mem(const void *graph_bytes, uint64_t graph_size, const void *offset_bytes,
+                   uint64_t offset_size, int mode, int device, grass_graph **out);
+int grass_close(grass_graph *g);
+int grass_get_info(const grass_graph *g, grass_graph_info *info);
+/* Device view of the resident graph (for callers that launch their own
+ * kernels): stream words (n_words + guard words), bit offsets u64[n+1]. */
+int grass_device_view(const grass_graph *g, const uint32_t **words, uint64_t *n_words,
+                      const uint64_t **offsets);
+
+/* Per-vertex degree (BCGVertex::outd, GT/src/bcg.cuh:113 / LE/src/bcg.cuh:132). */
+int grass_degrees(const grass_graph *g, uint32_t *d_deg, void *stream);
+
+/* Decode-only sweep: every neighbor list into a device CSR.  d_rowptr has
+ * n+1 entries, d_cols num_edges entries.  Replaces the block-cooperative
+ * GlobalDecoder (GT/src/bcg.cuh:171-345) and per-index BCGVertex::get_vertex
+ * (GT/src/bcg.cuh:153-168, LE/src/bcg.cuh:195-261). */
+int grass_decode_all(const grass_graph *g, uint64_t *d_rowptr, uint32_t *d_cols, void *stream);
+
+/* Uniform start vertices on the device (Philox TAG_START stream). */
+int grass_uniform_starts(uint64_t n, uint64_t count, uint64_t seed, uint32_t *d_out,
+                         void *stream);
+
+/* =========================================================================
+ * Samplers.  Replace the App plugins run through doTransitParallelSampling
+ * (GT/src/grass.cu:1417-2037) with the per-step sort/RLE/partition engine
+ * removed: one launch runs all steps.
+ * ========================================================================= */
+
+typedef struct {
+  uint32_t length;  /* steps per walk; reference RandomWalkApp::steps() = 80 */
+  uint32_t layout;  /* GRASS_LAYOUT_*                                        */
+  uint64_t seed;    /* Philox key                                            */
+} grass_rw_params;
+
+/* Random walk (DeepWalkApp, GT/src/apps/randomwalk/randomWalks.cu:49-81).
+ * paths holds W*(L+1) vertices, column 0 the start; a walk that reaches a
+ * vertex with no edges continues as GRASS_INVALID_VERTEX.  If d_edge_count
+ * is not NULL, the number of sampled edges is added to it. */
+int grass_rw(const grass_graph *g, const grass_rw_params *p, const uint32_t *d_starts,
+             uint64_t W, uint32_t *d_paths, unsigned long long *d_edge_count, void *stream);
+int grass_rw_host(const grass_graph *g, const grass_rw_params *p, const uint32_t *h_starts,
+                  uint64_t W, uint32_t *h_paths, uint64_t *edges_out);
+/* Traffic accounting for a walk (no reference counterpart; the reference
+ * reports only wall times, GT/src/grass.cu:2127-2130).  Replays the walk of
+ * grass_rw without writing paths and adds to d_out[0] the algorithmic bytes
+ * (per draw: 8 offset + ceil(stream bits read / 8) + 4 path entry; 4 per
+ * start entry), to d_out[1] the 32-byte sectors the reads span (+1 per draw
+ * for the offset) and to d_out[2] the number of draws. */
+int grass_rw_account(const grass_graph *g, const grass_rw_params *p, const uint32_t *d_starts,
+                     uint64_t W, unsigned long long *d_out, void *stream);
+
+#define GRASS_MAX_HOPS 8
+typedef struct {
+  uint32_t hops;                    /* number of hops (reference: 2)       */
+  uint32_t fanouts[GRASS_MAX_HOPS]; /* draws per transit per hop (10, 25)  */
+  uint64_t seed;
+} grass_khop_params;
+
+/* k-hop with replacement (KHopApp, GT/src/apps/khop/khop.cu:1-79).  Hop h
+ * output d_hop_out[h] is [S][prod_{j<=h} fanouts[j]]; slot p*f_h + k holds
+ * draw k from entry p of the previous hop. */
+int grass_khop(const grass_graph *g, const grass_khop_params *p, const uint32_t *d_seeds,
+               uint64_t S, uint32_t *const *d_hop_out, unsigned long long *d_edge_count,
+               void *stream);
+int grass_khop_host(const grass_graph *g, const grass_khop_params *p, const uint32_t *h_seeds,
+                    uint64_t S, uint32_t *const *h_hop_out, uint64_t *edges_out);
+
+typedef struct {
+  uint32_t walkers; /* R, walkers per sample (reference NUM_ROOT_VERTICES = 80) */
+  uint32_t steps;   /* T (reference MultiRWApp::steps() = 100)                 */
+  uint32_t select;  /* GRASS_SELECT_*                                          */
+  uint32_t reserved;
+  uint64_t seed;
+} grass_mrw_params;
+
+/* Multi random walk (MultiRWApp, GT/src/apps/multiRW/multiRW.cu:3-112).
+ * d_roots [S][R] holds the walkers' start vertices and is updated in place
+ * to their final positions; d_src/d_dst [S][T] receive the edge taken at each
+ * step (GRASS_INVALID_VERTEX as dst when the walker's vertex has no edges). */
+int grass_mrw(const grass_graph *g, const grass_mrw_params *p, uint32_t *d_roots, uint64_t S,
+              uint32_t *d_src, uint32_t *d_dst, unsigned long long *d_edge_count, void *stream);
+int grass_mrw_host(const grass_graph *g, const grass_mrw_params *p, uint32_t *h_roots,
+                   uint64_t S, uint32_t *h_src, uint32_t *h_dst, uint64_t *edges_out);
+
+/* =========================================================================
+ * Uncompressed-CSR baseline with the same RNG streams (no reference
+ * counterpart: the reference's NextDoor CSR loaders, GT/src/graph.hpp, are
+ * never called).  Produces the same walks as the compressed sampler.
+ * ========================================================================= */
+typedef struct grass_csr grass_csr;
+int grass_csr_from_graph(const grass_graph *g, grass_csr **out);
+int grass_csr_from_host(const uint64_t *rowptr, const uint32_t *cols, uint64_t n, int device,
+                        grass_csr **out);
+int grass_csr_close(grass_csr *c);
+int grass_csr_info(const grass_csr *c, uint64_t *n, uint64_t *nnz, uint64_t *device_bytes);
+int grass_csr_rw(const grass_csr *c, const grass_rw_params *p, const uint32_t *d_starts,
+                 uint64_t W, uint32_t *d_paths, unsigned long long *d_edge_count, void *stream);
+int grass_csr_khop(const grass_csr *c, const grass_khop_params *p, const uint32_t *d_seeds,
+                   uint64_t S, uint32_t *const *d_hop_out, unsigned long long *d_edge_count,
+                   void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRASS_B200_H */
