@@ -396,6 +396,14 @@ int grass_uniform_starts(uint64_t n, uint64_t count, uint64_t seed, uint32_t *d_
   return check_launch();
 }
 
+int grass_mrw_roots(uint64_t n, uint64_t S, uint32_t R, uint64_t seed, uint32_t *d_roots,
+                    void *stream) {
+  clear_error();
+  if (!n || n > 0xFFFFFFFFull || (S && R && !d_roots)) return set_error(GRASS_E_ARG, "bad arguments");
+  launch_uniform_starts(n, S * (uint64_t)R, seed, d_roots, as_stream(stream), true);
+  return check_launch();
+}
+
 int grass_rw(const grass_graph *g, const grass_rw_params *p, const uint32_t *d_starts,
              uint64_t W, uint32_t *d_paths, unsigned long long *d_edge_count, void *stream) {
   clear_error();

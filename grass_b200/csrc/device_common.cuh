@@ -188,17 +188,27 @@ __device__ __forceinline__ uint32_t le_neighbor(const DevGraph &g, const VHdr &h
   uint32_t c = j / tl;
   const uint32_t id = j - c * tl;
   if (flag) c += h.om;
-  BitCur cur;
-  cur.init(g.words, h.P + (uint64_t)c * (uint64_t)h.a);
-  const uint32_t r1m = cur.get(h.a);
-  const uint32_t r1 = (c < h.fp) ? h.v - r1m : h.v + r1m;
-  if (id == 0) return r1;
-  const uint32_t r2m = cur.get(h.a);
-  const uint32_t r2 = (c + 1 < h.fp) ? h.v - r2m : h.v + r2m;
+  // The sea's position depends only on the header, so its load is issued
+  // together with the rocks' (for id == 0 it re-reads the first sea, which
+  // is in bounds and unused).
   const uint64_t spos =
       h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a +
-      ((uint64_t)(h.bl - 1) * c + min(h.om, c) + id - 1) * (uint64_t)(h.b + 1);
-  const uint32_t raw = read_field(g.words, spos, h.b + 1);
+      ((uint64_t)(h.bl - 1) * c + min(h.om, c) + (id ? id - 1 : 0)) * (uint64_t)(h.b + 1);
+  const uint64_t rpos = h.P + (uint64_t)c * (uint64_t)h.a;
+  const uint32_t *rq = g.words + (rpos >> 5);
+  const uint32_t *sq = g.words + (spos >> 5);
+  const uint32_t rw0 = ldw(rq), rw1 = ldw(rq + 1), rw2 = ldw(rq + 2);
+  const uint32_t sw0 = ldw(sq), sw1 = ldw(sq + 1);
+  // rocks c and c+1: 2*a <= 64 bits starting at bit (rpos & 31) of rw0
+  const uint32_t rs = (uint32_t)rpos & 31u;
+  const uint64_t rwin = ((((uint64_t)rw0 << 32) | rw1) << rs) | (rs ? ((uint64_t)rw2 << rs) >> 32 : 0);
+  const uint32_t r1m = (uint32_t)(rwin >> (64 - h.a));
+  const uint32_t r1 = (c < h.fp) ? h.v - r1m : h.v + r1m;
+  if (id == 0) return r1;
+  const uint32_t r2m = (uint32_t)((rwin << h.a) >> (64 - h.a));
+  const uint32_t r2 = (c + 1 < h.fp) ? h.v - r2m : h.v + r2m;
+  const uint32_t swin = __funnelshift_l(sw1, sw0, (uint32_t)spos & 31u);
+  const uint32_t raw = swin >> (31 - h.b);
   const uint32_t mag = raw >> 1;
   // (r2 - r1) >= 0 for sorted rows: unsigned division is the compressor's.
   return ((r2 - r1) / tl) * id + r1 + ((raw & 1u) ? 0u - mag : mag);

@@ -98,7 +98,7 @@ void launch_decode_all(const DevGraph &g, const uint64_t *rowptr, uint32_t *cols
 
 // ---- samplers (kernels_sample.cu) ----
 void launch_uniform_starts(uint64_t n, uint64_t count, uint64_t seed, uint32_t *out,
-                           cudaStream_t s);
+                           cudaStream_t s, bool mrw_roots = false);
 void launch_rw(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts, uint64_t W,
                uint32_t *paths, unsigned long long *edges, unsigned int *err, cudaStream_t s);
 void launch_rw_account(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts,

@@ -491,10 +491,10 @@ int cur_dev() {
 }  // namespace
 
 void launch_uniform_starts(uint64_t n, uint64_t count, uint64_t seed, uint32_t *out,
-                           cudaStream_t s) {
+                           cudaStream_t s, bool mrw_roots) {
   if (!count) return;
-  starts_kernel<<<grid_warps((count + 3) / 4, 256, cur_dev(), 8), 256, 0, s>>>(n, count, seed,
-                                                                              TAG_START, out);
+  starts_kernel<<<grid_warps((count + 3) / 4, 256, cur_dev(), 8), 256, 0, s>>>(
+      n, count, seed, mrw_roots ? TAG_MRW_ROOT : TAG_START, out);
   count_launch();
 }
 

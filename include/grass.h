@@ -207,6 +207,11 @@ int grass_mrw(const grass_graph *g, const grass_mrw_params *p, uint32_t *d_roots
               uint32_t *d_src, uint32_t *d_dst, unsigned long long *d_edge_count, void *stream);
 int grass_mrw_host(const grass_graph *g, const grass_mrw_params *p, uint32_t *h_roots,
                    uint64_t S, uint32_t *h_src, uint32_t *h_dst, uint64_t *edges_out);
+/* Initial walker vertices for S samples of R walkers, uniform over n from the
+ * Philox TAG_MRW_ROOT stream (replaces MultiRWApp::initializeSample's
+ * unseeded rand() % n, GT/src/apps/multiRW/multiRW.cu:103-111). */
+int grass_mrw_roots(uint64_t n, uint64_t S, uint32_t R, uint64_t seed, uint32_t *d_roots,
+                    void *stream);
 
 /* =========================================================================
  * Uncompressed-CSR baseline with the same RNG streams (no reference
