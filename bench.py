@@ -39,6 +39,7 @@ sys.path.insert(0, ROOT)
 METRIC = "sampled edges/s (random walk, compressed graph)"
 UNIT = "edges/s"
 CACHE = os.path.join(tempfile.gettempdir(), "grass_bench_cache")
+LAYOUT = 1  # GRASS_LAYOUT_STEP_MAJOR: coalesced path stores in every arm
 
 
 def parse():
@@ -305,6 +306,7 @@ def workload_config(args, meta):
         "vertices": meta["n"], "directed_edges": meta["num_edges"],
         "walkers": args.walkers, "length": args.length, "philox_seed": 7,
         "decode_mode": args.mode, "l2": "flushed (256 MiB write) between timed steps",
+        "path_layout": "step-major [L+1][W] (both compressed and CSR arms)",
     }
 
 
@@ -343,14 +345,15 @@ def main():
     out = {}
 
     def rw_fn(obj):
-        return lambda: obj.rw_device(starts, W, L, 7 + rank, paths, ecount, stream=stream)
+        return lambda: obj.rw_device(starts, W, L, 7 + rank, paths, ecount, layout=LAYOUT,
+                                     stream=stream)
 
     # ---- (a) random walk: headline mode first
     order = [args.mode] + [m for m in ("LE", "GT") if m != args.mode]
     launches0 = G.launch_count()
     for m in order:
         ecount.zero_()
-        graphs[m].rw_device(starts, W, L, 7 + rank, paths, ecount, stream=stream)
+        graphs[m].rw_device(starts, W, L, 7 + rank, paths, ecount, layout=LAYOUT, stream=stream)
         torch.cuda.synchronize()
         edges_per_step = int(ecount.item())
         lc0 = G.launch_count()
@@ -362,7 +365,7 @@ def main():
                           "ms_min": min(ms), "ms_max": max(ms)}
     if "csr" in only and csr is not None:
         ecount.zero_()
-        csr.rw_device(starts, W, L, 7 + rank, paths, ecount, stream=stream)
+        csr.rw_device(starts, W, L, 7 + rank, paths, ecount, layout=LAYOUT, stream=stream)
         torch.cuda.synchronize()
         e1 = int(ecount.item())
         ms, tot = timed(torch, rw_fn(csr), args.steps, args.warmup, flush, dist, local)
@@ -426,7 +429,7 @@ def main():
         hs = h_starts.numpy().view(np.uint32)
         hp = h_paths.numpy().view(np.uint32).reshape(W, L + 1)
         gm = graphs[args.mode]
-        p = G.RwParams(L, 0, 7 + rank)
+        p = G.RwParams(L, LAYOUT, 7 + rank)
         import ctypes as C
         ecnt = C.c_uint64()
 

@@ -19,7 +19,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libgrass_b200.so")
+# GRASS_LIB_PATH selects an alternative build of the same library (e.g. a
+# build with other compile-time options); the default is the in-tree build.
+LIB_PATH = os.environ.get("GRASS_LIB_PATH") or os.path.join(HERE, "lib", "libgrass_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include", "grass.h")
 
 OK, E_IO, E_FORMAT, E_CUDA, E_OOM, E_BUDGET, E_TIMEOUT, E_ARG, E_DATA = range(9)
@@ -63,6 +65,12 @@ class KhopParams(C.Structure):
     _fields_ = [("hops", C.c_uint32), ("fanouts", C.c_uint32 * MAX_HOPS), ("seed", C.c_uint64)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("rw_depth", C.c_uint32), ("rw_threads", C.c_uint32),
+                ("rw_blocks_per_sm", C.c_uint32), ("l2_persist", C.c_uint32),
+                ("l2_fetch_bytes", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+
+
 class MrwParams(C.Structure):
     _fields_ = [("walkers", C.c_uint32), ("steps", C.c_uint32), ("select", C.c_uint32),
                 ("reserved", C.c_uint32), ("seed", C.c_uint64)]
@@ -92,6 +100,9 @@ def _load():
         "grass_close": ([P], i32),
         "grass_get_info": ([P, C.POINTER(GraphInfo)], i32),
         "grass_device_view": ([P, PP, P, PP], i32),
+        "grass_set_tuning": ([P, C.POINTER(Tuning)], i32),
+        "grass_get_tuning": ([P, C.POINTER(Tuning)], i32),
+        "grass_csr_set_tuning": ([P, C.POINTER(Tuning)], i32),
         "grass_degrees": ([P, P, P], i32),
         "grass_decode_all": ([P, P, P, P], i32),
         "grass_uniform_starts": ([u64, u64, u64, P, P], i32),
@@ -287,6 +298,16 @@ class Graph:
     def n(self) -> int:
         return int(self.info()["n"])
 
+    def set_tuning(self, rw_depth=0, rw_threads=0, rw_blocks_per_sm=0, l2_persist=0,
+                   l2_fetch_bytes=0):
+        t = Tuning(rw_depth, rw_threads, rw_blocks_per_sm, l2_persist, l2_fetch_bytes)
+        _check(lib.grass_set_tuning(self._h, C.byref(t)))
+
+    def tuning(self) -> dict:
+        t = Tuning()
+        _check(lib.grass_get_tuning(self._h, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in Tuning._fields_ if k != "reserved"}
+
     # -- host-buffer (end-to-end) calls --
     def rw(self, starts: np.ndarray, length: int, seed: int, layout: int = LAYOUT_WALK_MAJOR):
         starts = np.ascontiguousarray(starts, dtype=np.uint32)
@@ -399,6 +420,11 @@ class Csr:
             self.close()
         except Exception:
             pass
+
+    def set_tuning(self, rw_depth=0, rw_threads=0, rw_blocks_per_sm=0, l2_persist=0,
+                   l2_fetch_bytes=0):
+        t = Tuning(rw_depth, rw_threads, rw_blocks_per_sm, l2_persist, l2_fetch_bytes)
+        _check(lib.grass_csr_set_tuning(self._h, C.byref(t)))
 
     def info(self):
         n, nnz, b = C.c_uint64(), C.c_uint64(), C.c_uint64()

@@ -129,6 +129,7 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
       if (g) {
         cudaFree(g->d_words);
         cudaFree(g->d_offsets);
+        cudaFree(g->d_recs);
         cudaFree(g->d_err);
         delete g;
       }
@@ -138,7 +139,9 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
   g->mode = mode;
   const uint64_t gsize = src.size;
   g->n_words = (gsize + 3) / 4;
-  const uint64_t alloc_words = (g->n_words + kGuardWords + 3) / 4 * 4;
+  // whole 32-byte sectors, at least one full zero sector past the stream
+  // (sector loads may touch the sector after the one holding a field start)
+  const uint64_t alloc_words = (g->n_words + kGuardWords + 7) / 8 * 8;
   GRASS_CUDA(cudaMalloc(&g->d_words, alloc_words * 4));
   GRASS_CUDA(cudaMalloc(&g->d_offsets, (n + 1) * sizeof(uint64_t)));
   GRASS_CUDA(cudaMalloc(&g->d_err, sizeof(unsigned int)));
@@ -217,6 +220,14 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
                      "corrupt file?)",
                      stats[2]);
 
+  // Vertex records replace the bit-offset table for everything after load.
+  GRASS_CUDA(cudaMalloc(&g->d_recs, n * sizeof(uint4)));
+  launch_build_records(g->view(), g->d_recs, st);
+  GRASS_CUDA(cudaStreamSynchronize(st));
+  GRASS_CUDA(cudaGetLastError());
+  cudaFree(g->d_offsets);
+  g->d_offsets = nullptr;
+
   g->info.n_file = n_file;
   g->info.num_edges = stats[0];
   g->info.max_degree = (uint32_t)stats[1];
@@ -225,7 +236,7 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
   g->info.device = device;
   g->info.graph_file_bytes = gsize;
   g->info.offset_file_bytes = osize;
-  g->info.device_bytes = alloc_words * 4 + (n + 1) * sizeof(uint64_t);
+  g->info.device_bytes = alloc_words * 4 + n * sizeof(uint4);
   g->info.read_seconds = src.read_s;
   g->info.upload_seconds = now_s() - t0;
   *out = g;
@@ -246,6 +257,10 @@ bool read_whole(const std::string &path, std::vector<uint8_t> &buf) {
 }
 
 cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// CSR row pointers are read a 32-byte sector at a time (csr_row): whole
+// sectors plus one spare.
+size_t csr_rowptr_bytes(uint64_t n) { return ((n + 1 + 3) / 4 * 4 + 4) * sizeof(uint64_t); }
 
 int check_launch() {
   cudaError_t e = cudaGetLastError();
@@ -341,6 +356,7 @@ int grass_close(grass_graph *g) {
   DeviceGuard dg(g->device);
   cudaFree(g->d_words);
   cudaFree(g->d_offsets);
+  cudaFree(g->d_recs);
   cudaFree(g->d_err);
   delete g;
   return GRASS_OK;
@@ -353,11 +369,30 @@ int grass_get_info(const grass_graph *g, grass_graph_info *info) {
 }
 
 int grass_device_view(const grass_graph *g, const uint32_t **words, uint64_t *n_words,
-                      const uint64_t **offsets) {
+                      const void **records) {
   if (!g) return set_error(GRASS_E_ARG, "null graph");
   if (words) *words = g->d_words;
   if (n_words) *n_words = g->n_words;
-  if (offsets) *offsets = g->d_offsets;
+  if (records) *records = g->d_recs;
+  return GRASS_OK;
+}
+
+int grass_set_tuning(grass_graph *g, const grass_tuning *t) {
+  if (!g || !t) return set_error(GRASS_E_ARG, "null argument");
+  if (t->rw_depth && t->rw_depth != 1 && t->rw_depth != 2 && t->rw_depth != 4)
+    return set_error(GRASS_E_ARG, "rw_depth must be 1, 2 or 4");
+  if (t->rw_threads && (t->rw_threads % 32 || t->rw_threads > 512))
+    return set_error(GRASS_E_ARG, "rw_threads must be a multiple of 32 up to 512");
+  DeviceGuard dg(g->device);
+  if (int rc = apply_tuning(g->device, *t, g->d_recs, g->info.n * sizeof(uint4), g->l2win))
+    return rc;
+  g->tuning = *t;
+  return GRASS_OK;
+}
+
+int grass_get_tuning(const grass_graph *g, grass_tuning *t) {
+  if (!g || !t) return set_error(GRASS_E_ARG, "null argument");
+  *t = resolve_tuning(g->tuning, g->mode);
   return GRASS_OK;
 }
 
@@ -411,7 +446,8 @@ int grass_rw(const grass_graph *g, const grass_rw_params *p, const uint32_t *d_s
   if (!p || p->layout > 1 || (W && (!d_starts || !d_paths)))
     return set_error(GRASS_E_ARG, "random walk: bad arguments");
   DeviceGuard dg(g->device);
-  launch_rw(g->view(), *p, d_starts, W, d_paths, d_edge_count, g->d_err, as_stream(stream));
+  launch_rw(g->view(), *p, d_starts, W, d_paths, d_edge_count, g->d_err, as_stream(stream),
+            g->tuning, g->l2win);
   return check_launch();
 }
 
@@ -441,7 +477,7 @@ int grass_rw_host(const grass_graph *g, const grass_rw_params *p, const uint32_t
   GRASS_CUDA(cudaMemsetAsync(de.p, 0, 8, st));
   GRASS_CUDA(cudaMemcpyAsync(ds.p, h_starts, W * 4, cudaMemcpyHostToDevice, st));
   launch_rw(g->view(), *p, (uint32_t *)ds.p, W, (uint32_t *)dp.p, (unsigned long long *)de.p,
-            g->d_err, st);
+            g->d_err, st, g->tuning, g->l2win);
   if (int rc = check_launch()) return rc;
   GRASS_CUDA(cudaMemcpyAsync(h_paths, dp.p, path_n * 4, cudaMemcpyDeviceToHost, st));
   unsigned long long e = 0;
@@ -552,7 +588,7 @@ int grass_csr_from_graph(const grass_graph *g, grass_csr **out) {
   c->device = g->device;
   c->n = g->info.n;
   c->nnz = g->info.num_edges;
-  cudaError_t e1 = cudaMalloc(&c->d_rowptr, (c->n + 1) * 8);
+  cudaError_t e1 = cudaMalloc(&c->d_rowptr, csr_rowptr_bytes(c->n));
   cudaError_t e2 = cudaMalloc(&c->d_cols, std::max<uint64_t>(c->nnz, 1) * 4);
   if (e1 != cudaSuccess || e2 != cudaSuccess) {
     grass_csr_close(c);
@@ -583,7 +619,7 @@ int grass_csr_from_host(const uint64_t *rowptr, const uint32_t *cols, uint64_t n
     delete c;
     return set_error(GRASS_E_ARG, "null cols");
   }
-  cudaError_t e1 = cudaMalloc(&c->d_rowptr, (n + 1) * 8);
+  cudaError_t e1 = cudaMalloc(&c->d_rowptr, csr_rowptr_bytes(n));
   cudaError_t e2 = cudaMalloc(&c->d_cols, std::max<uint64_t>(c->nnz, 1) * 4);
   if (e1 != cudaSuccess || e2 != cudaSuccess) {
     grass_csr_close(c);
@@ -617,13 +653,23 @@ int grass_csr_info(const grass_csr *c, uint64_t *n, uint64_t *nnz, uint64_t *dev
   return GRASS_OK;
 }
 
+int grass_csr_set_tuning(grass_csr *c, const grass_tuning *t) {
+  if (!c || !t) return set_error(GRASS_E_ARG, "null argument");
+  DeviceGuard dg(c->device);
+  if (int rc = apply_tuning(c->device, *t, c->d_rowptr, (c->n + 1) * sizeof(uint64_t), c->l2win))
+    return rc;
+  c->tuning = *t;
+  return GRASS_OK;
+}
+
 int grass_csr_rw(const grass_csr *c, const grass_rw_params *p, const uint32_t *d_starts,
                  uint64_t W, uint32_t *d_paths, unsigned long long *d_edge_count, void *stream) {
   clear_error();
   if (!c || !p || p->layout > 1 || (W && (!d_starts || !d_paths)))
     return set_error(GRASS_E_ARG, "CSR random walk: bad arguments");
   DeviceGuard dg(c->device);
-  launch_rw_csr(c->view(), *p, d_starts, W, d_paths, d_edge_count, as_stream(stream));
+  launch_rw_csr(c->view(), *p, d_starts, W, d_paths, d_edge_count, as_stream(stream),
+                c->tuning, c->l2win);
   return check_launch();
 }
 

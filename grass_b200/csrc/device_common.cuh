@@ -14,9 +14,19 @@ namespace grass {
 
 constexpr uint32_t INVALID_VERTEX = 0xFFFFFFFFu;
 
+// Vertex record: the decoded gamma header of one vertex, 16 bytes, built once
+// at load from the .offset lengths and the stream headers.  Samplers read
+// one aligned record (one 32-byte sector, L2-resident for graphs of tens of
+// millions of vertices) instead of an 8-byte bit offset followed by a
+// dependent header read from the stream.
+//   x = payload bit offset P, low 32 bits
+//   y = P bits 32..47 | a << 16 (6 bits) | b << 22 (6 bits)
+//   z = degree d
+//   w = first_pos, or for LE degree 1 the single neighbor
 struct DevGraph {
   const uint32_t *__restrict__ words;
-  const uint64_t *__restrict__ offsets;  // n + 1 bit offsets
+  const uint4 *__restrict__ recs;        // n vertex records (sampling, decode)
+  const uint64_t *__restrict__ offsets;  // n + 1 bit offsets (load time only)
   uint32_t n;
   int32_t mode;
 };
@@ -84,6 +94,110 @@ struct BitCur {
   }
 };
 
+// One 32-byte sector of the stream as four 64-bit words in stream order (the
+// first word holds stream bits 0..63 of the sector, MSB first).  A single
+// 256-bit load is one L2 request; separate 32-bit loads of the same sector
+// issued back to back each miss L1 and become separate L2 requests.
+struct Sec {
+  uint64_t q0, q1, q2, q3;
+};
+
+__device__ __forceinline__ uint64_t swap_halves(uint64_t x) { return (x << 32) | (x >> 32); }
+
+// L2 eviction priorities.  Every draw reads one entry of a small hot table
+// (vertex records, or the CSR's row pointers: tens of MB, i.e. L2-sized)
+// and one or two random sectors of a large cold array (the stream, or CSR
+// columns: far larger than L2).  Without hints the cold reads evict the hot
+// table between its uses and every draw pays a DRAM access for it.
+//   hot table  -> evict_last
+//   cold reads -> GRASS_COLD_POLICY (0: normal, 1: evict_first)
+//   path/frontier stores -> GRASS_ST_POLICY (0: normal, 1: evict_first)
+#ifndef GRASS_HOT_POLICY
+#define GRASS_HOT_POLICY 1
+#endif
+#ifndef GRASS_COLD_POLICY
+#define GRASS_COLD_POLICY 0
+#endif
+#ifndef GRASS_ST_POLICY
+#define GRASS_ST_POLICY 1
+#endif
+
+__device__ __forceinline__ uint64_t policy_evict_last() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+__device__ __forceinline__ uint64_t policy_evict_first() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+__device__ __forceinline__ uint4 load_record(const uint4 *p) {
+  uint4 r;
+#if GRASS_HOT_POLICY
+  asm("ld.global.nc.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+      : "l"(p), "l"(policy_evict_last()));
+#else
+  asm("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
+      : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+      : "l"(p));
+#endif
+  return r;
+}
+
+// A 4-byte cold read (CSR column).
+__device__ __forceinline__ uint32_t load_cold_u32(const uint32_t *p) {
+#if GRASS_COLD_POLICY
+  uint32_t v;
+  asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy_evict_first()));
+  return v;
+#else
+  return __ldg(p);
+#endif
+}
+
+// Store of an output entry that is not read again by the kernel.
+__device__ __forceinline__ void store_out_u32(uint32_t *p, uint32_t v) {
+#if GRASS_ST_POLICY
+  asm volatile("st.global.L2::cache_hint.u32 [%0], %1, %2;" ::"l"(p), "r"(v),
+               "l"(policy_evict_first())
+               : "memory");
+#else
+  *p = v;
+#endif
+}
+
+__device__ __forceinline__ Sec load_sector(const uint32_t *words, uint64_t sector) {
+  const uint64_t *p = reinterpret_cast<const uint64_t *>(words) + sector * 4;
+  uint64_t a0, a1, a2, a3;
+#if GRASS_COLD_POLICY
+  asm("ld.global.nc.L2::evict_first.v4.b64 {%0,%1,%2,%3}, [%4];"
+      : "=l"(a0), "=l"(a1), "=l"(a2), "=l"(a3)
+      : "l"(p));
+#else
+  asm("ld.global.nc.v4.b64 {%0,%1,%2,%3}, [%4];"
+      : "=l"(a0), "=l"(a1), "=l"(a2), "=l"(a3)
+      : "l"(p));
+#endif
+  // little-endian u64 = (word 2i+1 << 32) | word 2i; stream order wants word 2i high
+  return Sec{swap_halves(a0), swap_halves(a1), swap_halves(a2), swap_halves(a3)};
+}
+
+__device__ __forceinline__ uint64_t sec_word(const Sec &s, uint32_t k) {
+  return k == 0 ? s.q0 : k == 1 ? s.q1 : k == 2 ? s.q2 : s.q3;
+}
+
+// The 64 stream bits starting at bit `off` (0..255) of sector a, continuing
+// into sector b when they cross its end.
+__device__ __forceinline__ uint64_t sec_window(const Sec &a, const Sec &b, uint32_t off) {
+  const uint32_t k = off >> 6, s = off & 63u;
+  const uint64_t x = sec_word(a, k);
+  const uint64_t y = k == 3 ? b.q0 : sec_word(a, k + 1);
+  return s ? (x << s) | (y >> (64 - s)) : x;
+}
+
 __device__ __forceinline__ uint32_t isqrt_u32(uint32_t x) {
   uint32_t r = (uint32_t)__fsqrt_rn((float)x);
   if ((uint64_t)r * r > x) r--;
@@ -137,12 +251,135 @@ __device__ __forceinline__ uint32_t gt_neighbor(const DevGraph &g, const VHdr &h
   if (!flag) blk += h.om;
   const uint64_t pos = h.P + (uint64_t)blk * (uint64_t)(h.a + (h.bl - 1) * h.b) +
                        (uint64_t)min(blk, h.om) * (uint64_t)h.b;
+  const uint32_t off = (uint32_t)pos & 255u;
+  const uint64_t span = (uint64_t)h.a + (uint64_t)id * (uint64_t)h.b;
+  if (off + span <= 512u) {
+    // Head and gaps lie in at most two sectors: two vector loads, then the
+    // fields are pulled from registers through a 128-bit shift window
+    // (buf holds nb valid bits at the top, nxt the next 64 stream bits).
+    const Sec zero{0, 0, 0, 0};
+    const uint64_t s0 = pos >> 8;
+    const Sec A = load_sector(g.words, s0);
+    const Sec B = off + span > 256u ? load_sector(g.words, s0 + 1) : zero;
+    uint32_t k = off >> 6;
+    auto word = [&](uint32_t i) -> uint64_t {
+      return i < 4 ? sec_word(A, i) : i < 8 ? sec_word(B, i - 4) : 0ull;
+    };
+    const uint32_t sh = off & 63u;
+    uint64_t buf = word(k) << sh;
+    int nb = 64 - (int)sh;
+    uint64_t nxt = word(++k);
+    auto get = [&](int w) -> uint32_t {  // w in [1, 32]
+      uint32_t v;
+      if (nb >= w) {
+        v = (uint32_t)(buf >> (64 - w));
+        buf = w == 64 ? 0 : buf << w;
+        nb -= w;
+      } else {
+        const int r = w - nb;  // bits taken from nxt, 1..32
+        v = (uint32_t)(((nb ? buf >> (64 - nb) : 0ull) << r) | (nxt >> (64 - r)));
+        buf = nxt << r;
+        nb = 64 - r;
+        nxt = word(++k);
+      }
+      return v;
+    };
+    const uint32_t head = get(h.a);
+    uint32_t cur = (blk >= h.fp) ? h.v + head + 1u : h.v - head - 1u;
+    for (uint32_t j = 0; j < id; j++) cur += get(h.b) + 1u;
+    return cur;
+  }
+  // Long runs (hub vertices): prefetch every sector of the run into L1 so
+  // the sequential cursor below waits on one memory round trip, not one per
+  // word.
+  const uint64_t l_first = pos >> 10, l_last = (pos + span - 1) >> 10;  // 128-byte lines
+  for (uint64_t l = l_first; l <= l_last; l++)
+    asm volatile("prefetch.global.L1 [%0];" ::"l"(g.words + l * 32));
   BitCur c;
   c.init(g.words, pos);
   uint32_t head = c.get(h.a);
   uint32_t cur = (blk >= h.fp) ? h.v + head + 1u : h.v - head - 1u;
   for (uint32_t k = 0; k < id; k++) cur += c.get(h.b) + 1u;
   return cur;
+}
+
+// GT draw of neighbor i, located but not decoded: the bit offset of the
+// block's head, how many gaps follow it to reach neighbor i, and the head's
+// sign (GT/src/bcg.cuh:153-163).
+struct GtRun {
+  uint64_t pos;   // bit offset of the head field
+  uint32_t gaps;  // gaps to add after the head (neighbor_id)
+  bool up;        // head counts upward from v (block >= first_pos)
+};
+
+__device__ __forceinline__ GtRun gt_locate(const VHdr &h, uint32_t i) {
+  const uint32_t split = (h.bl + 1) * h.om;
+  const bool flag = i < split;
+  const uint32_t j = flag ? i : i - split;
+  const uint32_t len = h.bl + (flag ? 1u : 0u);
+  uint32_t blk = j / len;
+  const uint32_t id = j - blk * len;
+  if (!flag) blk += h.om;
+  GtRun r;
+  r.pos = h.P + (uint64_t)blk * (uint64_t)(h.a + (h.bl - 1) * h.b) +
+          (uint64_t)min(blk, h.om) * (uint64_t)h.b;
+  r.gaps = id;
+  r.up = blk >= h.fp;
+  return r;
+}
+
+// Sum of (field + 1) over `n` consecutive b-bit fields starting at bit pos,
+// through a sequential cursor (the first load is one memory round trip, the
+// rest hit L1).
+__device__ __forceinline__ uint32_t gap_sum(const uint32_t *words, uint64_t pos, uint32_t n,
+                                            int b) {
+  if (!n) return 0;
+  BitCur c;
+  c.init(words, pos);
+  uint32_t s = n;
+  for (uint32_t k = 0; k < n; k++) s += c.get(b);
+  return s;
+}
+
+// Gap runs longer than this are decoded by the whole warp.
+constexpr uint32_t kGtLongRun = 24;
+
+// Warp-cooperative GT draw: lane L may hold one draw (active) whose value is
+// v +/- (head + 1) + sum(gap + 1) over run.gaps gaps.  Short runs are decoded
+// by their own lane.  Each long run (a hub vertex's block holds hundreds of
+// gaps) is split into 32 contiguous sub-ranges, one per lane, each summed by
+// its own cursor, and combined with __reduce_add_sync -- one memory round
+// trip and gaps/32 L1 reads per lane instead of one lane walking all gaps
+// while the rest of the warp waits.  All 32 lanes must call this together.
+__device__ __forceinline__ uint32_t gt_warp_neighbor(const uint32_t *words, bool active,
+                                                     uint32_t v, const GtRun &run, int a, int b,
+                                                     uint32_t * /* unused */) {
+  const unsigned FULLM = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  const bool lng = active && run.gaps > kGtLongRun;
+  uint32_t cur = 0;
+  if (active && !lng) {
+    const uint32_t hv = read_field(words, run.pos, a) + 1u;
+    cur = (run.up ? v + hv : v - hv) + gap_sum(words, run.pos + (uint64_t)a, run.gaps, b);
+  }
+  unsigned mask = __ballot_sync(FULLM, lng);
+  while (mask) {
+    const int L = __ffs(mask) - 1;
+    mask &= mask - 1;
+    const uint64_t pos = __shfl_sync(FULLM, run.pos, L);
+    const uint32_t gaps = __shfl_sync(FULLM, run.gaps, L);
+    const int aL = __shfl_sync(FULLM, a, L);
+    const int bL = __shfl_sync(FULLM, b, L);
+    const uint32_t m = (gaps + 31) / 32;
+    const uint32_t g0 = min(gaps, (uint32_t)lane * m), g1 = min(gaps, g0 + m);
+    uint32_t s = gap_sum(words, pos + (uint64_t)aL + (uint64_t)g0 * (uint64_t)bL, g1 - g0, bL);
+    s = __reduce_add_sync(FULLM, s);
+    if (lane == L) {
+      const uint32_t hv = read_field(words, run.pos, a) + 1u;
+      cur = (run.up ? v + hv : v - hv) + s;
+    }
+  }
+  return active ? cur : v;
 }
 
 // LE header: BCGVertex ctor, LE/src/bcg.cuh:130-152.
@@ -188,36 +425,133 @@ __device__ __forceinline__ uint32_t le_neighbor(const DevGraph &g, const VHdr &h
   uint32_t c = j / tl;
   const uint32_t id = j - c * tl;
   if (flag) c += h.om;
-  // The sea's position depends only on the header, so its load is issued
-  // together with the rocks' (for id == 0 it re-reads the first sea, which
-  // is in bounds and unused).
+  // Rocks c and c+1 (2a <= 64 bits) and the sea (b+1 <= 32 bits) are read
+  // with one 32-byte sector load each, plus the next sector only when a
+  // field crosses a sector end; the sea's position depends only on the
+  // header, so both loads are in flight together.
+  const uint64_t rpos = h.P + (uint64_t)c * (uint64_t)h.a;
+  const uint64_t rsec = rpos >> 8;
+  const uint32_t roff = (uint32_t)rpos & 255u;
+  const Sec zero{0, 0, 0, 0};
+  if (id == 0) {  // the chunk's left rock itself
+    const bool cross = roff + (uint32_t)h.a > 256u;
+    const Sec A = load_sector(g.words, rsec);
+    const Sec A2 = cross ? load_sector(g.words, rsec + 1) : zero;
+    const uint32_t r1m = (uint32_t)(sec_window(A, A2, roff) >> (64 - h.a));
+    return (c < h.fp) ? h.v - r1m : h.v + r1m;
+  }
+  const bool rcross = roff + 2u * (uint32_t)h.a > 256u;
   const uint64_t spos =
       h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a +
-      ((uint64_t)(h.bl - 1) * c + min(h.om, c) + (id ? id - 1 : 0)) * (uint64_t)(h.b + 1);
-  const uint64_t rpos = h.P + (uint64_t)c * (uint64_t)h.a;
-  const uint32_t *rq = g.words + (rpos >> 5);
-  const uint32_t *sq = g.words + (spos >> 5);
-  const uint32_t rw0 = ldw(rq), rw1 = ldw(rq + 1), rw2 = ldw(rq + 2);
-  const uint32_t sw0 = ldw(sq), sw1 = ldw(sq + 1);
-  // rocks c and c+1: 2*a <= 64 bits starting at bit (rpos & 31) of rw0
-  const uint32_t rs = (uint32_t)rpos & 31u;
-  const uint64_t rwin = ((((uint64_t)rw0 << 32) | rw1) << rs) | (rs ? ((uint64_t)rw2 << rs) >> 32 : 0);
+      ((uint64_t)(h.bl - 1) * c + min(h.om, c) + id - 1) * (uint64_t)(h.b + 1);
+  const uint64_t ssec = spos >> 8;
+  const uint32_t soff = (uint32_t)spos & 255u;
+  const bool scross = soff + (uint32_t)h.b + 1u > 256u;
+  // seas follow the rocks, so ssec >= rsec; sectors already requested are reused
+  const bool s_is_a = ssec == rsec, s_is_a2 = rcross && ssec == rsec + 1;
+  const bool s2_is_a2 = rcross && s_is_a;
+  const Sec A = load_sector(g.words, rsec);
+  const Sec A2 = rcross ? load_sector(g.words, rsec + 1) : zero;
+  const Sec Bl = (s_is_a || s_is_a2) ? zero : load_sector(g.words, ssec);
+  const Sec B2l = (!scross || s2_is_a2) ? zero : load_sector(g.words, ssec + 1);
+  const Sec B = s_is_a ? A : s_is_a2 ? A2 : Bl;
+  const Sec B2 = s2_is_a2 ? A2 : B2l;
+  const uint64_t rwin = sec_window(A, A2, roff);
   const uint32_t r1m = (uint32_t)(rwin >> (64 - h.a));
   const uint32_t r1 = (c < h.fp) ? h.v - r1m : h.v + r1m;
-  if (id == 0) return r1;
   const uint32_t r2m = (uint32_t)((rwin << h.a) >> (64 - h.a));
   const uint32_t r2 = (c + 1 < h.fp) ? h.v - r2m : h.v + r2m;
-  const uint32_t swin = __funnelshift_l(sw1, sw0, (uint32_t)spos & 31u);
-  const uint32_t raw = swin >> (31 - h.b);
+  const uint32_t raw = (uint32_t)(sec_window(B, B2, soff) >> (63 - h.b));
   const uint32_t mag = raw >> 1;
   // (r2 - r1) >= 0 for sorted rows: unsigned division is the compressor's.
   return ((r2 - r1) / tl) * id + r1 + ((raw & 1u) ? 0u - mag : mag);
 }
 
+// Stream headers (gamma decode at offsets[v]); used at load time only.
 template <int MODE>
-__device__ __forceinline__ VHdr header(const DevGraph &g, uint32_t v) {
+__device__ __forceinline__ VHdr stream_header(const DevGraph &g, uint32_t v) {
   if constexpr (MODE == 0) return gt_header(g, v);
   else return le_header(g, v);
+}
+
+__device__ __forceinline__ uint4 pack_record(const VHdr &h) {
+  uint4 r;
+  r.x = (uint32_t)h.P;
+  r.y = ((uint32_t)(h.P >> 32) & 0xFFFFu) | ((uint32_t)h.a & 63u) << 16 |
+        ((uint32_t)h.b & 63u) << 22;
+  r.z = h.d;
+  r.w = h.fp;
+  return r;
+}
+
+// Header from a vertex record: the same fields gt_header/le_header decode,
+// with the block/chunk geometry recomputed from the degree.
+template <int MODE>
+__device__ __forceinline__ VHdr record_header(const uint4 r, uint32_t v) {
+  VHdr h;
+  h.v = v;
+  h.P = (uint64_t)r.x | ((uint64_t)(r.y & 0xFFFFu) << 32);
+  h.a = (int)((r.y >> 16) & 63u);
+  h.b = (int)((r.y >> 22) & 63u);
+  h.d = r.z;
+  h.fp = r.w;
+  if constexpr (MODE == 0) {
+    const uint32_t s = isqrt_u32(h.d);
+    if (s * s == h.d) {
+      h.bn = h.bl = s;
+      h.om = 0;
+    } else {
+      h.bn = s + 1;
+      h.bl = h.d / h.bn;
+      h.om = h.d - h.bn * h.bl;
+    }
+  } else {
+    h.bn = h.bl = h.om = 0;
+    if (h.d > 1) {
+      const uint32_t D = h.d - 1;
+      const uint32_t s = isqrt_u32(D);
+      const uint32_t om = D - s * s;
+      h.bn = s + (om > s ? 1u : 0u);
+      h.bl = D / h.bn;
+      h.om = D - h.bn * h.bl;
+    }
+  }
+  return h;
+}
+
+// [rowptr[v], rowptr[v+1]) of a CSR with one 32-byte load (two when the pair
+// straddles a sector, v % 4 == 3).  rowptr must be allocated in whole
+// sectors with one spare sector (see grass_csr allocation).
+__device__ __forceinline__ void csr_row(const uint64_t *rowptr, uint32_t v, uint64_t &b,
+                                        uint64_t &e) {
+  const uint64_t *p = rowptr + (v & ~3u);
+  uint64_t a0, a1, a2, a3;
+#if GRASS_HOT_POLICY
+  asm("ld.global.nc.L2::evict_last.v4.b64 {%0,%1,%2,%3}, [%4];"
+      : "=l"(a0), "=l"(a1), "=l"(a2), "=l"(a3)
+      : "l"(p));
+#else
+  asm("ld.global.nc.v4.b64 {%0,%1,%2,%3}, [%4];"
+      : "=l"(a0), "=l"(a1), "=l"(a2), "=l"(a3)
+      : "l"(p));
+#endif
+  const uint32_t k = v & 3u;
+  b = k == 0 ? a0 : k == 1 ? a1 : k == 2 ? a2 : a3;
+  e = k == 0 ? a1 : k == 1 ? a2 : k == 2 ? a3 : __ldg(p + 4);
+}
+
+template <int MODE>
+__device__ __forceinline__ VHdr header(const DevGraph &g, uint32_t v) {
+  return record_header<MODE>(load_record(g.recs + v), v);
+}
+
+__device__ __forceinline__ uint32_t record_degree(const DevGraph &g, uint32_t v) {
+  return __ldg(&g.recs[v].z);
+}
+
+// Length of gamma(x): 2 floor(log2(x+1)) + 1.
+__device__ __forceinline__ uint32_t gamma_len(uint32_t x) {
+  return 2u * (31u - __clz(x + 1u)) + 1u;
 }
 
 template <int MODE>

@@ -8,17 +8,33 @@
 #include "device_common.cuh"
 #include "internal.h"
 
+namespace grass {
+// Per-launch L2 access-policy window (cudaLaunchAttributeAccessPolicyWindow):
+// marks the hot per-vertex table persisting so the random payload reads do
+// not evict it between uses.
+struct L2Window {
+  const void *base = nullptr;
+  size_t bytes = 0;
+  float hit_ratio = 0.f;
+  bool on() const { return base && bytes && hit_ratio > 0.f; }
+};
+}  // namespace grass
+
 struct grass_graph {
+  grass::L2Window l2win;
   int device = 0;
   int mode = 0;
   uint32_t *d_words = nullptr;     // n_words + guard words
   uint64_t n_words = 0;            // stream words (excluding guard words)
-  uint64_t *d_offsets = nullptr;   // n + 1
+  uint64_t *d_offsets = nullptr;   // n + 1 bit offsets; freed once records exist
+  uint4 *d_recs = nullptr;         // n vertex records
   unsigned int *d_err = nullptr;   // device error word (GRASS_E_DATA on bad ids)
   grass_graph_info info{};
+  grass_tuning tuning{};
   grass::DevGraph view() const {
     grass::DevGraph g;
     g.words = d_words;
+    g.recs = d_recs;
     g.offsets = d_offsets;
     g.n = (uint32_t)info.n;
     g.mode = mode;
@@ -27,7 +43,9 @@ struct grass_graph {
 };
 
 struct grass_csr {
+  grass::L2Window l2win;
   int device = 0;
+  grass_tuning tuning{};
   uint64_t n = 0, nnz = 0;
   uint64_t *d_rowptr = nullptr;
   uint32_t *d_cols = nullptr;
@@ -87,6 +105,7 @@ void launch_scan_u32(const uint32_t *counts, uint64_t n, uint64_t *out, uint64_t
 // stats[2] = first bad vertex + 1 (0 if none). deg may be null.
 void launch_validate(const DevGraph &g, uint32_t *deg, unsigned long long *stats,
                      cudaStream_t s);
+void launch_build_records(const DevGraph &g, uint4 *recs, cudaStream_t s);
 void launch_degrees(const DevGraph &g, uint32_t *deg, cudaStream_t s);
 void launch_degrees64(const DevGraph &g, uint64_t *deg, cudaStream_t s);
 // In-place exclusive scan of vals[0..n) into vals[0..n]; tmp as above.
@@ -100,11 +119,21 @@ void launch_decode_all(const DevGraph &g, const uint64_t *rowptr, uint32_t *cols
 void launch_uniform_starts(uint64_t n, uint64_t count, uint64_t seed, uint32_t *out,
                            cudaStream_t s, bool mrw_roots = false);
 void launch_rw(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts, uint64_t W,
-               uint32_t *paths, unsigned long long *edges, unsigned int *err, cudaStream_t s);
+               uint32_t *paths, unsigned long long *edges, unsigned int *err, cudaStream_t s,
+               const grass_tuning &t, const L2Window &win = L2Window());
+// Applies the process-wide parts of a tuning block (L2 fetch granularity,
+// persisting-L2 carve-out) on `device` and computes the access window for a
+// hot table of `bytes` at `base`.
+int apply_tuning(int device, const grass_tuning &t, const void *base, size_t bytes,
+                 L2Window &win);
 void launch_rw_account(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts,
                        uint64_t W, unsigned long long *out, cudaStream_t s);
 void launch_rw_csr(const DevCsr &c, const grass_rw_params &p, const uint32_t *starts,
-                   uint64_t W, uint32_t *paths, unsigned long long *edges, cudaStream_t s);
+                   uint64_t W, uint32_t *paths, unsigned long long *edges, cudaStream_t s,
+                   const grass_tuning &t, const L2Window &win = L2Window());
+// Fills unset (zero) fields of a tuning block with the defaults.
+// kind: GRASS_MODE_GT, GRASS_MODE_LE or 2 (uncompressed CSR).
+grass_tuning resolve_tuning(const grass_tuning &t, int kind);
 void launch_khop(const DevGraph &g, const grass_khop_params &p, const uint32_t *seeds,
                  uint64_t S, uint32_t *const *hop_out, unsigned long long *edges,
                  unsigned int *err, cudaStream_t s);

@@ -191,11 +191,16 @@ __global__ void validate_kernel(DevGraph g, uint32_t *deg, unsigned long long *s
 template <int MODE, class T>
 __global__ void degrees_kernel(DevGraph g, T *deg) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < g.n;
-       v += (uint64_t)gridDim.x * blockDim.x) {
-    BitCur c;
-    c.init(g.words, g.offsets[v]);
-    deg[v] = (T)c.gamma();
-  }
+       v += (uint64_t)gridDim.x * blockDim.x)
+    deg[v] = (T)record_degree(g, (uint32_t)v);
+}
+
+// One record per vertex from its stream header (run once, after validation).
+template <int MODE>
+__global__ void build_records_kernel(DevGraph g, uint4 *recs) {
+  for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < g.n;
+       v += (uint64_t)gridDim.x * blockDim.x)
+    recs[v] = pack_record(stream_header<MODE>(g, (uint32_t)v));
 }
 
 unsigned grid_for(uint64_t items, int threads, int device) {
@@ -233,6 +238,15 @@ void launch_validate(const DevGraph &g, uint32_t *deg, unsigned long long *stats
   unsigned grid = grid_for(g.n, 256, dev);
   if (g.mode == GRASS_MODE_GT) validate_kernel<0><<<grid, 256, 0, s>>>(g, deg, stats);
   else validate_kernel<1><<<grid, 256, 0, s>>>(g, deg, stats);
+  count_launch();
+}
+
+void launch_build_records(const DevGraph &g, uint4 *recs, cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  unsigned grid = grid_for(g.n, 256, dev);
+  if (g.mode == GRASS_MODE_GT) build_records_kernel<0><<<grid, 256, 0, s>>>(g, recs);
+  else build_records_kernel<1><<<grid, 256, 0, s>>>(g, recs);
   count_launch();
 }
 

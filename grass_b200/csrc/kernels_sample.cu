@@ -16,12 +16,12 @@ namespace {
 
 __device__ __forceinline__ void store_path(uint32_t *paths, int layout, uint64_t W, uint32_t L,
                                            uint64_t w, uint32_t s, uint32_t v) {
-  if (layout == GRASS_LAYOUT_WALK_MAJOR) paths[w * (uint64_t)(L + 1) + s] = v;
-  else paths[(uint64_t)s * W + w] = v;
+  if (layout == GRASS_LAYOUT_WALK_MAJOR) store_out_u32(paths + w * (uint64_t)(L + 1) + s, v);
+  else store_out_u32(paths + (uint64_t)s * W + w, v);
 }
 
 template <int MODE, int DEPTH>
-__global__ void __launch_bounds__(256) rw_kernel(DevGraph g, const uint32_t *__restrict__ starts,
+__global__ void __launch_bounds__(512) rw_kernel(DevGraph g, const uint32_t *__restrict__ starts,
                                                  uint64_t W, uint32_t L, uint64_t seed,
                                                  int layout, uint32_t *__restrict__ paths,
                                                  unsigned long long *edges, unsigned int *err) {
@@ -72,24 +72,84 @@ __global__ void __launch_bounds__(256) rw_kernel(DevGraph g, const uint32_t *__r
   if (bad && err) atomicOr(err, 1u);
 }
 
-// Bits a draw of neighbor i reads from the stream, and the 32-byte sectors
-// those reads span (header range plus payload ranges, in stream order).
+// GT random walk.  A warp owns 32*DEPTH consecutive walkers and every step is
+// warp-synchronous, so the gap runs of all lanes are decoded cooperatively
+// (gt_warp_neighbor): on power-law graphs walks keep returning to hub
+// vertices whose blocks hold hundreds of gaps, which a per-lane loop would
+// serialise across the whole warp.
+template <int DEPTH>
+__global__ void __launch_bounds__(512) rw_gt_kernel(DevGraph g,
+                                                    const uint32_t *__restrict__ starts,
+                                                    uint64_t W, uint32_t L, uint64_t seed,
+                                                    int layout, uint32_t *__restrict__ paths,
+                                                    unsigned long long *edges,
+                                                    unsigned int *err) {
+  __shared__ uint32_t sh_all[16][32];
+  uint32_t *sh = sh_all[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const uint64_t gwarp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  uint64_t cnt = 0;
+  bool bad = false;
+  for (uint64_t wb = gwarp * 32 * DEPTH; wb < W; wb += nwarps * 32 * DEPTH) {
+    uint32_t v[DEPTH];
+    u32x4 r[DEPTH];
+#pragma unroll
+    for (int k = 0; k < DEPTH; k++) {
+      const uint64_t w = wb + (uint64_t)k * 32 + lane;
+      v[k] = INVALID_VERTEX;
+      r[k] = u32x4{0, 0, 0, 0};
+      if (w < W) {
+        const uint32_t s0 = starts[w];
+        store_path(paths, layout, W, L, w, 0, s0);
+        v[k] = s0 < g.n ? s0 : INVALID_VERTEX;
+      }
+    }
+    for (uint32_t s = 0; s < L; s++) {
+#pragma unroll
+      for (int k = 0; k < DEPTH; k++) {
+        const uint64_t w = wb + (uint64_t)k * 32 + lane;
+        if ((s & 3) == 0)
+          r[k] = philox4x32_10(seed, s >> 2, (uint32_t)w, (uint32_t)(w >> 32), TAG_RW);
+        bool active = v[k] != INVALID_VERTEX;
+        GtRun run{0, 0, false};
+        int a = 0, b = 0;
+        if (active) {
+          const VHdr h = header<0>(g, v[k]);
+          if (h.d == 0) {
+            active = false;
+            v[k] = INVALID_VERTEX;
+          } else {
+            run = gt_locate(h, mulhi_u32(pick(r[k], s & 3), h.d));
+            a = h.a;
+            b = h.b;
+          }
+        }
+        const uint32_t nv = gt_warp_neighbor(g.words, active, v[k], run, a, b, sh);
+        if (active) {
+          if (nv >= g.n) {
+            bad = true;
+            v[k] = INVALID_VERTEX;
+          } else {
+            v[k] = nv;
+            cnt++;
+          }
+        }
+        if (w < W) store_path(paths, layout, W, L, w, s + 1, v[k]);
+      }
+    }
+  }
+  warp_add_u64(edges, cnt);
+  if (bad && err) atomicOr(err, 1u);
+}
+
+// Stream bits a draw of neighbor i reads (the payload fields; the header is
+// in the vertex record), and the 32-byte sectors those reads span.
 template <int MODE>
 __device__ __forceinline__ void draw_footprint(const DevGraph &g, const VHdr &h, uint32_t i,
                                                uint64_t &bits, uint64_t &sectors) {
-  const uint64_t o0 = g.offsets[h.v];
-  uint64_t r0[3], r1[3];  // half-open bit ranges
+  uint64_t r0[3], r1[3];  // half-open bit ranges, in stream order
   int nr = 0;
-  uint64_t hdr_end = h.P;
-  if (MODE == 1 && h.d == 1) {  // LE degree 1: the neighbor is the second header field
-    BitCur c;
-    c.init(g.words, o0);
-    c.gamma();
-    c.gamma();
-    hdr_end = c.pos(g.words);
-  }
-  r0[nr] = o0;
-  r1[nr++] = hdr_end;
   if (MODE == 0) {
     const uint32_t split = (h.bl + 1) * h.om;
     const bool flag = i < split;
@@ -135,9 +195,10 @@ __device__ __forceinline__ void draw_footprint(const DevGraph &g, const VHdr &h,
 }
 
 // Replays a walk (same stream as rw_kernel) and sums, per draw, the
-// algorithmic bytes 8 (offset) + ceil(stream bits read / 8) + 4 (path entry)
-// and the 32-byte sectors those reads span (+1 for the offset).  out[0] =
-// bytes, out[1] = sectors, out[2] = draws.  Start entries add 4 bytes each.
+// algorithmic bytes 16 (vertex record) + ceil(payload bits read / 8) + 4
+// (path entry) and the 32-byte sectors the reads span (+1 for the record).
+// out[0] = bytes, out[1] = sectors, out[2] = draws.  Start entries add 4
+// bytes each.
 template <int MODE>
 __global__ void __launch_bounds__(256) rw_account_kernel(DevGraph g,
                                                          const uint32_t *__restrict__ starts,
@@ -162,7 +223,7 @@ __global__ void __launch_bounds__(256) rw_account_kernel(DevGraph g,
       const uint32_t i = mulhi_u32(pick(r, s & 3), h.d);
       uint64_t b, sc;
       draw_footprint<MODE>(g, h, i, b, sc);
-      bytes += 8 + (b + 7) / 8;
+      bytes += 16 + (b + 7) / 8;
       sect += 1 + sc;
       draws++;
       const uint32_t nv = neighbor<MODE>(g, h, i);
@@ -175,7 +236,7 @@ __global__ void __launch_bounds__(256) rw_account_kernel(DevGraph g,
 }
 
 template <int DEPTH>
-__global__ void __launch_bounds__(256) rw_csr_kernel(DevCsr c, const uint32_t *__restrict__ starts,
+__global__ void __launch_bounds__(512) rw_csr_kernel(DevCsr c, const uint32_t *__restrict__ starts,
                                                      uint64_t W, uint32_t L, uint64_t seed,
                                                      int layout, uint32_t *__restrict__ paths,
                                                      unsigned long long *edges) {
@@ -203,12 +264,13 @@ __global__ void __launch_bounds__(256) rw_csr_kernel(DevCsr c, const uint32_t *_
         if ((s & 3) == 0)
           r[k] = philox4x32_10(seed, s >> 2, (uint32_t)w, (uint32_t)(w >> 32), TAG_RW);
         if (v[k] != INVALID_VERTEX) {
-          const uint64_t b = __ldg(c.rowptr + v[k]);
-          const uint64_t d = __ldg(c.rowptr + v[k] + 1) - b;
+          uint64_t b, e;
+          csr_row(c.rowptr, v[k], b, e);
+          const uint64_t d = e - b;
           if (d == 0) {
             v[k] = INVALID_VERTEX;
           } else {
-            v[k] = __ldg(c.cols + b + mulhi_u32(pick(r[k], s & 3), (uint32_t)d));
+            v[k] = load_cold_u32(c.cols + b + mulhi_u32(pick(r[k], s & 3), (uint32_t)d));
             cnt++;
           }
         }
@@ -253,6 +315,7 @@ __global__ void __launch_bounds__(256) khop_kernel(DevGraph g, const uint32_t *_
                                                    uint64_t S, KhopArgs A,
                                                    unsigned long long *edges, unsigned int *err) {
   __shared__ SmemHdr sh[8];
+  __shared__ uint32_t gt_sh[8][32];
   const int lane = threadIdx.x & 31;
   SmemHdr &my = sh[threadIdx.x >> 5];
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -283,17 +346,40 @@ __global__ void __launch_bounds__(256) khop_kernel(DevGraph g, const uint32_t *_
         __syncwarp();
         const uint64_t nP = min((uint64_t)32, P - pc);
         const uint64_t total = nP * f;
-        for (uint64_t j0 = 0; j0 < total; j0 += 32) {
+        for (uint64_t j0 = 0; j0 < total; j0 += 32) {  // warp-uniform
           const uint64_t j = j0 + lane;
-          if (j < total) {
+          const bool act = j < total;
+          uint64_t slot = 0;
+          bool draw = false;
+          uint32_t nv = INVALID_VERTEX, tv = 0;
+          GtRun run{0, 0, false};
+          int ra = 0, rb = 0;
+          if (act) {
             const uint32_t pl = (uint32_t)(j / f);
-            const uint64_t slot = pc * f + j;
+            slot = pc * f + j;
             const VHdr hk = my.get(pl);
-            uint32_t nv = INVALID_VERTEX;
             if (hk.d) {
+              draw = true;
               const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(slot >> 2), (uint32_t)s,
                                              (uint32_t)(s >> 32), TAG_KHOP | hop);
-              nv = neighbor<MODE>(g, hk, mulhi_u32(pick(rr, (int)(slot & 3)), hk.d));
+              const uint32_t idx = mulhi_u32(pick(rr, (int)(slot & 3)), hk.d);
+              if (MODE == 0) {
+                run = gt_locate(hk, idx);
+                tv = hk.v;
+                ra = hk.a;
+                rb = hk.b;
+              } else {
+                nv = le_neighbor(g, hk, idx);
+              }
+            }
+          }
+          if (MODE == 0) {
+            const uint32_t x = gt_warp_neighbor(g.words, draw, tv, run, ra, rb,
+                                                gt_sh[threadIdx.x >> 5]);
+            if (draw) nv = x;
+          }
+          if (act) {
+            if (draw) {
               if (nv >= g.n) {
                 bad = true;
                 nv = INVALID_VERTEX;
@@ -331,7 +417,9 @@ __global__ void __launch_bounds__(256) khop_csr_kernel(DevCsr c, const uint32_t 
         const uint32_t t = hop ? prev[p] : seeds[s];
         uint32_t nv = INVALID_VERTEX;
         if (t < c.n) {
-          const uint64_t b = c.rowptr[t], d = c.rowptr[t + 1] - b;
+          uint64_t b, e;
+          csr_row(c.rowptr, t, b, e);
+          const uint64_t d = e - b;
           if (d) {
             const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(j >> 2), (uint32_t)s,
                                            (uint32_t)(s >> 32), TAG_KHOP | hop);
@@ -403,7 +491,7 @@ __global__ void __launch_bounds__(256) mrw_kernel(DevGraph g, uint32_t *__restri
       const uint32_t x = rt[i];
       rv[i] = x;
       uint32_t d = 0;
-      if (x < g.n) d = header<MODE>(g, x).d;
+      if (x < g.n) d = record_degree(g, x);
       rd[i] = d;
     }
     __syncwarp();
@@ -447,7 +535,7 @@ __global__ void __launch_bounds__(256) mrw_kernel(DevGraph g, uint32_t *__restri
         dst[io] = nv;
         cnt++;
         rv[x] = nv;
-        const uint32_t nd = header<MODE>(g, nv).d;
+        const uint32_t nd = record_degree(g, nv);
         if (select == GRASS_SELECT_DEGREE) {
           fen_add(fen, R, x, (int64_t)nd - (int64_t)rd[x]);
           wsum = wsum - rd[x] + nd;
@@ -498,17 +586,113 @@ void launch_uniform_starts(uint64_t n, uint64_t count, uint64_t seed, uint32_t *
   count_launch();
 }
 
+// Launch through cudaLaunchKernelEx so the L2 window is a per-launch
+// attribute: the caller's stream keeps its own access policy.
+template <class... ExpTypes, class... ActTypes>
+static void launch_with_window(void (*kern)(ExpTypes...), unsigned grid, unsigned block,
+                               cudaStream_t s, const L2Window &win, ActTypes &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  if (win.on()) {
+    attr[0].id = cudaLaunchAttributeAccessPolicyWindow;
+    attr[0].val.accessPolicyWindow.base_ptr = const_cast<void *>(win.base);
+    attr[0].val.accessPolicyWindow.num_bytes = win.bytes;
+    attr[0].val.accessPolicyWindow.hitRatio = win.hit_ratio;
+    attr[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+  }
+  cudaLaunchKernelEx(&cfg, kern, std::forward<ActTypes>(args)...);
+}
+
+int apply_tuning(int device, const grass_tuning &t, const void *base, size_t bytes,
+                 L2Window &win) {
+  win = L2Window();
+  if (t.l2_fetch_bytes) {
+    cudaError_t e = cudaDeviceSetLimit(cudaLimitMaxL2FetchGranularity, t.l2_fetch_bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaLimitMaxL2FetchGranularity");
+  }
+  if (t.l2_persist && base && bytes) {
+    int max_persist = 0, max_window = 0;
+    cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, device);
+    cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, device);
+    if (max_persist > 0 && max_window > 0) {
+      const size_t carve = std::min<size_t>((size_t)max_persist, bytes);
+      cudaError_t e = cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, carve);
+      if (e != cudaSuccess) return cuda_fail(e, "cudaLimitPersistingL2CacheSize");
+      size_t got = 0;
+      cudaDeviceGetLimit(&got, cudaLimitPersistingL2CacheSize);
+      win.base = base;
+      win.bytes = std::min<size_t>(bytes, (size_t)max_window);
+      win.hit_ratio = (float)std::min(1.0, (double)got / (double)win.bytes);
+    }
+  }
+  return GRASS_OK;
+}
+
+// Defaults measured on B200 (R-MAT s22 ef32, 1M walkers x 80): LE and CSR
+// gain from four interleaved walkers per thread; GT, whose warps synchronise
+// every step, is fastest with one.
+grass_tuning resolve_tuning(const grass_tuning &t, int kind) {
+  grass_tuning r = t;
+  if (!r.rw_depth) r.rw_depth = kind == GRASS_MODE_GT ? 1 : 4;
+  if (!r.rw_threads) r.rw_threads = 256;
+  return r;  // rw_blocks_per_sm == 0: as many as are resident
+}
+
+// Grid for a grid-stride kernel: the requested blocks per SM, capped by
+// what the occupancy calculator says is resident, times the SM count, and
+// no more blocks than there is work for.
+template <class K>
+static unsigned resident_grid(K kern, int threads, uint32_t want_per_sm, uint64_t units,
+                              uint64_t units_per_block) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0);
+  if (per_sm < 1) per_sm = 1;
+  if (want_per_sm && (int)want_per_sm < per_sm) per_sm = (int)want_per_sm;
+  const uint64_t need = (units + units_per_block - 1) / units_per_block;
+  const uint64_t cap = (uint64_t)sm_count(cur_dev()) * per_sm;
+  return (unsigned)std::max<uint64_t>(1, std::min(need, cap));
+}
+
+template <int MODE, int DEPTH>
+static void rw_launch_depth(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts,
+                            uint64_t W, uint32_t *paths, unsigned long long *edges,
+                            unsigned int *err, cudaStream_t s, const grass_tuning &t,
+                            const L2Window &win) {
+  // GT: warp-synchronous kernel with cooperative gap decoding; LE: one
+  // independent O(1) decode per lane.
+  auto kern = MODE == 0 ? rw_gt_kernel<DEPTH> : rw_kernel<MODE, DEPTH>;
+  const unsigned grid =
+      resident_grid(kern, (int)t.rw_threads, t.rw_blocks_per_sm, W, (uint64_t)t.rw_threads * DEPTH);
+  launch_with_window(kern, grid, t.rw_threads, s, win, g, starts, W, p.length, p.seed,
+                     (int)p.layout, paths, edges, err);
+}
+
+template <int MODE>
+static void rw_dispatch(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts,
+                        uint64_t W, uint32_t *paths, unsigned long long *edges,
+                        unsigned int *err, cudaStream_t s, const grass_tuning &t,
+                        const L2Window &win) {
+  switch (t.rw_depth) {
+    case 1: rw_launch_depth<MODE, 1>(g, p, starts, W, paths, edges, err, s, t, win); break;
+    case 4: rw_launch_depth<MODE, 4>(g, p, starts, W, paths, edges, err, s, t, win); break;
+    default: rw_launch_depth<MODE, 2>(g, p, starts, W, paths, edges, err, s, t, win);
+  }
+}
+
 void launch_rw(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts, uint64_t W,
-               uint32_t *paths, unsigned long long *edges, unsigned int *err, cudaStream_t s) {
+               uint32_t *paths, unsigned long long *edges, unsigned int *err, cudaStream_t s,
+               const grass_tuning &tin, const L2Window &win) {
   if (!W) return;
-  constexpr int DEPTH = 2;
-  const unsigned grid = grid_warps((W + DEPTH - 1) / DEPTH, 256, cur_dev(), 8);
-  if (g.mode == GRASS_MODE_GT)
-    rw_kernel<0, DEPTH><<<grid, 256, 0, s>>>(g, starts, W, p.length, p.seed, (int)p.layout,
-                                             paths, edges, err);
-  else
-    rw_kernel<1, DEPTH><<<grid, 256, 0, s>>>(g, starts, W, p.length, p.seed, (int)p.layout,
-                                             paths, edges, err);
+  const grass_tuning t = resolve_tuning(tin, g.mode);
+  if (g.mode == GRASS_MODE_GT) rw_dispatch<0>(g, p, starts, W, paths, edges, err, s, t, win);
+  else rw_dispatch<1>(g, p, starts, W, paths, edges, err, s, t, win);
   count_launch();
 }
 
@@ -524,12 +708,32 @@ void launch_rw_account(const DevGraph &g, const grass_rw_params &p, const uint32
 }
 
 void launch_rw_csr(const DevCsr &c, const grass_rw_params &p, const uint32_t *starts,
-                   uint64_t W, uint32_t *paths, unsigned long long *edges, cudaStream_t s) {
+                   uint64_t W, uint32_t *paths, unsigned long long *edges, cudaStream_t s,
+                   const grass_tuning &tin, const L2Window &win) {
   if (!W) return;
-  constexpr int DEPTH = 2;
-  const unsigned grid = grid_warps((W + DEPTH - 1) / DEPTH, 256, cur_dev(), 8);
-  rw_csr_kernel<DEPTH><<<grid, 256, 0, s>>>(c, starts, W, p.length, p.seed, (int)p.layout,
-                                            paths, edges);
+  const grass_tuning t = resolve_tuning(tin, 2);
+  const uint32_t L = p.length;
+  const int lay = (int)p.layout;
+  const int T = (int)t.rw_threads;
+  switch (t.rw_depth) {
+    case 1: {
+      const unsigned grid = resident_grid(rw_csr_kernel<1>, T, t.rw_blocks_per_sm, W, T);
+      launch_with_window(rw_csr_kernel<1>, grid, T, s, win, c, starts, W, L, p.seed, lay, paths,
+                         edges);
+      break;
+    }
+    case 4: {
+      const unsigned grid = resident_grid(rw_csr_kernel<4>, T, t.rw_blocks_per_sm, W, T * 4);
+      launch_with_window(rw_csr_kernel<4>, grid, T, s, win, c, starts, W, L, p.seed, lay, paths,
+                         edges);
+      break;
+    }
+    default: {
+      const unsigned grid = resident_grid(rw_csr_kernel<2>, T, t.rw_blocks_per_sm, W, T * 2);
+      launch_with_window(rw_csr_kernel<2>, grid, T, s, win, c, starts, W, L, p.seed, lay, paths,
+                         edges);
+    }
+  }
   count_launch();
 }
 

@@ -129,9 +129,33 @@ int grass_open_mem(const void *graph_bytes, uint64_t graph_size, const void *off
 int grass_close(grass_graph *g);
 int grass_get_info(const grass_graph *g, grass_graph_info *info);
 /* Device view of the resident graph (for callers that launch their own
- * kernels): stream words (n_words + guard words), bit offsets u64[n+1]. */
+ * kernels): the stream words (n_words + 16 zero guard words, each word the
+ * next 32 stream bits MSB-first) and the n vertex records, 16 bytes each:
+ * {P low 32 bits, P bits 32..47 | a << 16 | b << 22, degree, first_pos},
+ * where P is the bit offset of the vertex's payload after its gamma header,
+ * a/b are the GT head/body or LE rock/sea widths and, for an LE vertex of
+ * degree 1, first_pos holds its neighbor.  The records replace the
+ * reference's uint64 bit-offset table (GT/src/utils.hpp:363). */
 int grass_device_view(const grass_graph *g, const uint32_t **words, uint64_t *n_words,
-                      const uint64_t **offsets);
+                      const void **records);
+
+/* Launch shape of the samplers (no reference counterpart: the reference's
+ * launch shapes are compile-time constants, GT/src/grass.cu:46-49, 1845,
+ * 1886).  Zero fields take the defaults; grass_autotune picks values. */
+typedef struct {
+  uint32_t rw_depth;          /* walkers interleaved per thread: 1, 2, 4
+                                 (default 4 for LE and CSR, 1 for GT)                */
+  uint32_t rw_threads;        /* threads per block for walks (default 256)           */
+  uint32_t rw_blocks_per_sm;  /* resident blocks per SM for walks (0 = all resident) */
+  uint32_t l2_persist;        /* 1: launches mark the vertex records (or CSR row
+                                 pointers) persisting in L2 through a per-launch
+                                 access-policy window                               */
+  uint32_t l2_fetch_bytes;    /* 0 = leave as is; 32/64/128: this process's
+                                 cudaLimitMaxL2FetchGranularity hint                 */
+  uint32_t reserved[3];
+} grass_tuning;
+int grass_set_tuning(grass_graph *g, const grass_tuning *t);
+int grass_get_tuning(const grass_graph *g, grass_tuning *t);
 
 /* Per-vertex degree (BCGVertex::outd, GT/src/bcg.cuh:113 / LE/src/bcg.cuh:132). */
 int grass_degrees(const grass_graph *g, uint32_t *d_deg, void *stream);
@@ -224,6 +248,7 @@ int grass_csr_from_host(const uint64_t *rowptr, const uint32_t *cols, uint64_t n
                         grass_csr **out);
 int grass_csr_close(grass_csr *c);
 int grass_csr_info(const grass_csr *c, uint64_t *n, uint64_t *nnz, uint64_t *device_bytes);
+int grass_csr_set_tuning(grass_csr *c, const grass_tuning *t);
 int grass_csr_rw(const grass_csr *c, const grass_rw_params *p, const uint32_t *d_starts,
                  uint64_t W, uint32_t *d_paths, unsigned long long *d_edge_count, void *stream);
 int grass_csr_khop(const grass_csr *c, const grass_khop_params *p, const uint32_t *d_seeds,
