@@ -105,6 +105,7 @@ def _load():
         "grass_csr_set_tuning": ([P, C.POINTER(Tuning)], i32),
         "grass_degrees": ([P, P, P], i32),
         "grass_decode_all": ([P, P, P, P], i32),
+        "grass_decode_all_noalloc": ([P, P, P, P], i32),
         "grass_uniform_starts": ([u64, u64, u64, P, P], i32),
         "grass_rw": ([P, C.POINTER(RwParams), P, u64, P, P, P], i32),
         "grass_rw_host": ([P, C.POINTER(RwParams), P, u64, P, P], i32),

@@ -166,6 +166,19 @@ int grass_degrees(const grass_graph *g, uint32_t *d_deg, void *stream);
  * (GT/src/bcg.cuh:153-168, LE/src/bcg.cuh:195-261). */
 int grass_decode_all(const grass_graph *g, uint64_t *d_rowptr, uint32_t *d_cols, void *stream);
 
+/* Same as grass_decode_all, but allocates no device memory.  No counterpart
+ * in the reference.  For callers that cannot allocate when they decode:
+ * applications that reserve the whole device for their own memory pool, and
+ * loops that must not pay for allocator calls or the device-wide
+ * synchronisation cudaFree implies.  The scan scratch comes from a fixed
+ * 512 KiB array that every GPU loading this library holds until exit, which
+ * limits graphs to 268,435,456 vertices (larger ones return GRASS_E_ARG).
+ * The first call on a device looks up the array's device address, so make it
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU race. */
+int grass_decode_all_noalloc(const grass_graph *g, uint64_t *d_rowptr, uint32_t *d_cols,
+                             void *stream);
+
 /* Uniform start vertices on the device (Philox TAG_START stream). */
 int grass_uniform_starts(uint64_t n, uint64_t count, uint64_t seed, uint32_t *d_out,
                          void *stream);
