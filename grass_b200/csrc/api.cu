@@ -418,7 +418,7 @@ int grass_decode_all(const grass_graph *g, uint64_t *d_rowptr, uint32_t *d_cols,
   GRASS_CUDA(cudaMallocAsync(&scan_tmp, (scan_tmp_words(n) + 1) * sizeof(uint64_t), st));
   launch_degrees64(g->view(), d_rowptr, st);
   launch_scan_u64_inplace(d_rowptr, n, scan_tmp, st);
-  launch_decode_all(g->view(), d_rowptr, d_cols, g->d_err, st);
+  launch_decode_all(g->view(), d_rowptr, d_cols, g->info.num_edges, g->d_err, st);
   cudaFreeAsync(scan_tmp, st);
   return check_launch();
 }

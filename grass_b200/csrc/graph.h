@@ -112,7 +112,8 @@ void launch_degrees64(const DevGraph &g, uint64_t *deg, cudaStream_t s);
 void launch_scan_u64_inplace(uint64_t *vals, uint64_t n, uint64_t *tmp, cudaStream_t s);
 
 // ---- decode (kernels_decode.cu) ----
-void launch_decode_all(const DevGraph &g, const uint64_t *rowptr, uint32_t *cols,
+// E = rowptr[n] (the number of edges, known from load-time validation).
+void launch_decode_all(const DevGraph &g, const uint64_t *rowptr, uint32_t *cols, uint64_t E,
                        unsigned int *err, cudaStream_t s);
 
 // ---- samplers (kernels_sample.cu) ----

@@ -5,16 +5,21 @@
 // kernels at GT/src/grass.cu:529-553, 762-786) and repeated
 // BCGVertex::get_vertex calls (LE/src/bcg.cuh:195-261).
 //
-// Layout of the work: one warp takes a tile of 32 consecutive vertices.
-//  1. Each lane decodes the gamma header of one vertex (variable-length codes,
-//     so lanes work on independent vertices).
-//  2. A warp prefix sum of the degrees maps the tile's neighbor lists onto
-//     one contiguous index space; each round, lane j takes neighbor r*32+j,
-//     finds its vertex by a shuffle binary search and reads its own field.
-//  3. GT: the fields are heads and gaps, so a segmented warp scan (segments =
-//     blocks; a carry crosses rounds) turns gaps into ids.  LE: each neighbor
-//     is two rocks plus one signed sea, no scan.
-//  4. Stores are coalesced: the tile's output is contiguous in cols.
+// Work is split over the neighbor index space, not over vertices: task t
+// covers neighbors [t*C, (t+1)*C) of the CSR being written, whatever
+// vertices they belong to, so a hub vertex with 10^5 neighbors is spread over
+// many warps instead of serialising one.  Per task a warp
+//  1. finds the vertex holding the first neighbor with a 32-ary search of
+//     rowptr (one coalesced probe per level);
+//  2. for each round of 32 consecutive neighbors, loads the row ends and
+//     records of a window of 32 vertices (coalesced), maps every lane to its
+//     vertex by a shuffle binary search and takes the header by shuffle;
+//  3. decodes: LE -- each neighbor is two rocks and one signed sea
+//     (independent); GT -- each lane reads its own field (block head or gap)
+//     and a segmented warp scan turns gaps into ids, with the running value
+//     carried from round to round (and, at a task start inside a block,
+//     decoded once by lane 0);
+//  4. writes its 32 ids with one coalesced store.
 #include "graph.h"
 
 namespace grass {
@@ -22,6 +27,7 @@ namespace grass {
 namespace {
 
 constexpr unsigned FULL = 0xFFFFFFFFu;
+constexpr uint32_t kTaskNeighbors = 2048;  // multiple of 32
 
 __device__ __forceinline__ VHdr shfl_hdr(const VHdr &h, int src) {
   VHdr o;
@@ -37,83 +43,122 @@ __device__ __forceinline__ VHdr shfl_hdr(const VHdr &h, int src) {
   return o;
 }
 
+// Largest v in [0, n) with rowptr[v] <= x, for x < rowptr[n].
+__device__ __forceinline__ uint32_t warp_row_of(const uint64_t *rowptr, uint32_t n, uint64_t x) {
+  const int lane = threadIdx.x & 31;
+  uint64_t lo = 0, hi = n;  // rowptr[lo] <= x < rowptr[hi]
+  while (hi - lo > 1) {
+    const uint64_t step = (hi - lo + 31) / 32;
+    const uint64_t p = lo + (uint64_t)(lane + 1) * step;
+    const bool le = p < hi && rowptr[p] <= x;
+    const uint32_t c = __popc(__ballot_sync(FULL, le));
+    const uint64_t nlo = lo + (uint64_t)c * step;
+    hi = min(hi, lo + (uint64_t)(c + 1) * step);
+    lo = nlo;
+  }
+  return (uint32_t)lo;
+}
+
+// Largest v in [lo, n) with rowptr[v] <= x, one thread (rare fallback).
+__device__ __forceinline__ uint32_t row_of_serial(const uint64_t *rowptr, uint32_t lo, uint32_t n,
+                                                  uint64_t x) {
+  uint32_t hi = n;
+  while (hi - lo > 1) {
+    const uint32_t mid = lo + (hi - lo) / 2;
+    if (rowptr[mid] <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint64_t *rowptr,
-                                                           uint32_t *cols, unsigned int *err) {
+                                                           uint32_t *cols, uint64_t E,
+                                                           unsigned int *err) {
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  const uint64_t tiles = ((uint64_t)g.n + 31) / 32;
+  const uint64_t tasks = (E + kTaskNeighbors - 1) / kTaskNeighbors;
   bool bad = false;
-  for (uint64_t t = warp; t < tiles; t += nwarps) {
-    const uint64_t v = t * 32 + lane;
-    VHdr h;
-    if (v < g.n) {
-      h = header<MODE>(g, (uint32_t)v);
-    } else {
-      h.d = 0;
-      h.P = 0;
-      h.v = 0;
-      h.bn = h.bl = h.om = h.fp = 0;
-      h.a = h.b = 0;
-    }
-    // exclusive prefix of degrees across the tile
-    uint32_t incl = h.d;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      uint32_t y = __shfl_up_sync(FULL, incl, o);
-      if (lane >= o) incl += y;
-    }
-    const uint32_t excl = incl - h.d;
-    const uint32_t total = __shfl_sync(FULL, incl, 31);
-    const uint64_t out0 = rowptr[t * 32];
+  for (uint64_t t = warp; t < tasks; t += nwarps) {
+    const uint64_t g0 = t * kTaskNeighbors;
+    const uint64_t g1 = min(E, g0 + kTaskNeighbors);
+    uint32_t vr = warp_row_of(rowptr, g.n, g0);
     uint32_t carry = 0;
-    for (uint32_t r = 0; r < total; r += 32) {
-      const uint32_t gi = r + lane;
-      const bool active = gi < total;
-      // largest k with excl[k] <= gi (a non-empty list when gi < total)
+    if (MODE == 0) {
+      // a task that starts inside a block needs the value of neighbor g0-1
+      const uint32_t i0 = (uint32_t)(g0 - rowptr[vr]);
+      if (i0 > 0) {
+        uint32_t c = 0;
+        if (lane == 0) {
+          const VHdr h0 = header<0>(g, vr);
+          if (gt_locate(h0, i0).gaps > 0) c = gt_neighbor(g, h0, i0 - 1);
+        }
+        carry = __shfl_sync(FULL, c, 0);
+      }
+    }
+    for (uint64_t r = g0; r < g1; r += 32) {  // warp-uniform
+      const uint64_t gl = r + lane;
+      const bool act = gl < g1;
+      // window of vertices [vr, vr + 32): row ends and headers, one per lane
+      const uint32_t wv = vr + lane;
+      const uint64_t base = rowptr[vr];
+      const uint64_t e = wv < g.n ? rowptr[wv + 1] : ~0ull;
+      VHdr hw;
+      if (wv < g.n) {
+        hw = header<MODE>(g, wv);
+      } else {
+        hw.d = 0; hw.P = 0; hw.v = 0; hw.bn = hw.bl = hw.om = hw.fp = 0; hw.a = hw.b = 0;
+      }
+      // owner lane k: number of window rows that end at or before gl
+      // (binary lifting over 31 probes gives the exact count when it is
+      // below 32)
       int k = 0;
 #pragma unroll
       for (int step = 16; step > 0; step >>= 1) {
-        uint32_t e = __shfl_sync(FULL, excl, k + step);
-        if (e <= gi) k += step;
+        const uint64_t ek = __shfl_sync(FULL, e, k + step - 1);
+        if (ek <= gl) k += step;
       }
-      const VHdr hk = shfl_hdr(h, k);
-      const uint32_t i = gi - __shfl_sync(FULL, excl, k);
+      // a count of 32 means gl lies beyond the window (a run of >= 32 empty
+      // rows); those lanes resolve their vertex and header on their own.
+      const uint64_t e31 = __shfl_sync(FULL, e, 31);
+      const bool far = act && e31 <= gl;
+      const int src = far ? 0 : k;
+      const uint64_t prev_e = __shfl_sync(FULL, e, src > 0 ? src - 1 : 0);
+      VHdr hk = shfl_hdr(hw, src);
+      uint64_t startv = src == 0 ? base : prev_e;
+      if (far) {
+        const uint32_t v = row_of_serial(rowptr, vr + 32, g.n, gl);
+        hk = header<MODE>(g, v);
+        startv = rowptr[v];
+      }
+      const uint32_t i = (uint32_t)(gl - startv);
       uint32_t val = 0;
       if (MODE == 1) {
-        if (active) val = le_neighbor(g, hk, i);
+        if (act) val = le_neighbor(g, hk, i);
       } else {
-        // field of neighbor i: the block head (id == 0) or a gap
         bool head = true;
         uint32_t x = 0;
-        if (active) {
-          const uint32_t split = (hk.bl + 1) * hk.om;
-          const bool flag = i < split;
-          const uint32_t j = flag ? i : i - split;
-          const uint32_t len = hk.bl + (flag ? 1u : 0u);
-          uint32_t blk = j / len;
-          const uint32_t id = j - blk * len;
-          if (!flag) blk += hk.om;
-          const uint64_t bpos = hk.P + (uint64_t)blk * (uint64_t)(hk.a + (hk.bl - 1) * hk.b) +
-                                (uint64_t)min(blk, hk.om) * (uint64_t)hk.b;
-          if (id == 0) {
-            const uint32_t hv = read_field(g.words, bpos, hk.a);
-            x = (blk >= hk.fp) ? hk.v + hv + 1u : hk.v - hv - 1u;
+        if (act) {
+          const GtRun run = gt_locate(hk, i);
+          if (far) {
+            x = gt_neighbor(g, hk, i);  // complete value; starts its own segment
+          } else if (run.gaps == 0) {
+            const uint32_t hv = read_field(g.words, run.pos, hk.a) + 1u;
+            x = run.up ? hk.v + hv : hk.v - hv;
           } else {
             head = false;
-            x = read_field(g.words, bpos + hk.a + (uint64_t)(id - 1) * hk.b, hk.b) + 1u;
+            x = read_field(g.words, run.pos + hk.a + (uint64_t)(run.gaps - 1) * hk.b, hk.b) + 1u;
           }
         }
         if (lane == 0 && !head) {
           x += carry;
           head = true;
         }
-        // segmented inclusive scan (segments start at heads)
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          uint32_t y = __shfl_up_sync(FULL, x, o);
-          int f = __shfl_up_sync(FULL, (int)head, o);
+        for (int o = 1; o < 32; o <<= 1) {  // segmented inclusive scan
+          const uint32_t y = __shfl_up_sync(FULL, x, o);
+          const int f = __shfl_up_sync(FULL, (int)head, o);
           if (lane >= o && !head) {
             x += y;
             head = f;
@@ -122,9 +167,17 @@ __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint6
         carry = __shfl_sync(FULL, x, 31);
         val = x;
       }
-      if (active) {
+      if (act) {
         if (val >= g.n) bad = true;
-        cols[out0 + gi] = val;
+        cols[gl] = val;
+      }
+      // next window starts at the vertex of the round's last neighbor
+      const uint32_t vlast = __shfl_sync(FULL, far ? 0xFFFFFFFFu : vr + (uint32_t)k, 31);
+      if (vlast != 0xFFFFFFFFu) {
+        vr = vlast;
+      } else {
+        const uint64_t gl31 = r + 31;
+        vr = gl31 < g1 ? warp_row_of(rowptr, g.n, gl31) : vr;
       }
     }
   }
@@ -133,16 +186,19 @@ __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint6
 
 }  // namespace
 
-void launch_decode_all(const DevGraph &g, const uint64_t *rowptr, uint32_t *cols,
+void launch_decode_all(const DevGraph &g, const uint64_t *rowptr, uint32_t *cols, uint64_t E,
                        unsigned int *err, cudaStream_t s) {
   int dev = 0;
   cudaGetDevice(&dev);
-  const uint64_t tiles = ((uint64_t)g.n + 31) / 32;
-  const uint64_t blocks_needed = (tiles + 7) / 8;
+  if (!E) return;
+  const uint64_t tasks = (E + kTaskNeighbors - 1) / kTaskNeighbors;
+  const uint64_t blocks_needed = (tasks + 7) / 8;
   const unsigned grid = (unsigned)std::max<uint64_t>(
       1, std::min<uint64_t>(blocks_needed, (uint64_t)sm_count(dev) * 8));
-  if (g.mode == GRASS_MODE_GT) decode_all_kernel<0><<<grid, 256, 0, s>>>(g, rowptr, cols, err);
-  else decode_all_kernel<1><<<grid, 256, 0, s>>>(g, rowptr, cols, err);
+  if (g.mode == GRASS_MODE_GT)
+    decode_all_kernel<0><<<grid, 256, 0, s>>>(g, rowptr, cols, E, err);
+  else
+    decode_all_kernel<1><<<grid, 256, 0, s>>>(g, rowptr, cols, E, err);
   count_launch();
 }
 

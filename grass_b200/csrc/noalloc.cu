@@ -64,7 +64,7 @@ extern "C" int grass_decode_all_noalloc(const grass_graph *g, uint64_t *d_rowptr
   // the GPU (other streams, other threads) race on it.
   launch_degrees64(g->view(), d_rowptr, st);
   launch_scan_u64_inplace(d_rowptr, n, scratch, st);
-  launch_decode_all(g->view(), d_rowptr, d_cols, g->d_err, st);
+  launch_decode_all(g->view(), d_rowptr, d_cols, g->info.num_edges, g->d_err, st);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "kernel launch");
 }
