@@ -354,6 +354,7 @@ int grass_open_mem(const void *graph_bytes, uint64_t graph_size, const void *off
 int grass_close(grass_graph *g) {
   if (!g) return GRASS_OK;
   DeviceGuard dg(g->device);
+  delete g->pipe;
   cudaFree(g->d_words);
   cudaFree(g->d_offsets);
   cudaFree(g->d_recs);
@@ -468,21 +469,64 @@ int grass_rw_host(const grass_graph *g, const grass_rw_params *p, const uint32_t
   if (!p || p->layout > 1 || (W && (!h_starts || !h_paths)))
     return set_error(GRASS_E_ARG, "random walk: bad arguments");
   DeviceGuard dg(g->device);
-  const uint64_t path_n = W * (uint64_t)(p->length + 1);
-  DevBuf ds, dp, de;
-  GRASS_CUDA(cudaMalloc(&ds.p, std::max<uint64_t>(W, 1) * 4));
-  GRASS_CUDA(cudaMalloc(&dp.p, std::max<uint64_t>(path_n, 1) * 4));
-  GRASS_CUDA(cudaMalloc(&de.p, 8));
-  cudaStream_t st = 0;
-  GRASS_CUDA(cudaMemsetAsync(de.p, 0, 8, st));
-  GRASS_CUDA(cudaMemcpyAsync(ds.p, h_starts, W * 4, cudaMemcpyHostToDevice, st));
-  launch_rw(g->view(), *p, (uint32_t *)ds.p, W, (uint32_t *)dp.p, (unsigned long long *)de.p,
-            g->d_err, st, g->tuning, g->l2win);
-  if (int rc = check_launch()) return rc;
-  GRASS_CUDA(cudaMemcpyAsync(h_paths, dp.p, path_n * 4, cudaMemcpyDeviceToHost, st));
+  auto *gm = const_cast<grass_graph *>(g);
+  if (!gm->pipe) {
+    static std::mutex create_mu;
+    std::lock_guard<std::mutex> lk(create_mu);
+    if (!gm->pipe) gm->pipe = new (std::nothrow) HostPipe();
+    if (!gm->pipe) return set_error(GRASS_E_OOM, "host allocation failed");
+  }
+  HostPipe &hp = *gm->pipe;
+  std::lock_guard<std::mutex> lk(hp.mu);
+  if (!hp.st[0]) {
+    for (int i = 0; i < 2; i++)
+      GRASS_CUDA(cudaStreamCreateWithFlags(&hp.st[i], cudaStreamNonBlocking));
+    GRASS_CUDA(cudaEventCreateWithFlags(&hp.ev, cudaEventDisableTiming));
+    GRASS_CUDA(cudaMalloc(&hp.d_edges, sizeof(unsigned long long)));
+  }
+  // Chunks of walkers alternate between two streams: while one chunk's paths
+  // are copied out, the next chunk is copied in and walked.  Walker ids stay
+  // global (w0 = chunk base), so the walks equal one launch over all W.
+  const uint64_t L1 = (uint64_t)p->length + 1;
+  const uint64_t chunk = std::min<uint64_t>(std::max<uint64_t>(W, 1), 1u << 17);
+  if (hp.cap_starts < chunk || hp.cap_paths < chunk * L1) {
+    for (int i = 0; i < 2; i++) {
+      cudaFree(hp.d_starts[i]);
+      cudaFree(hp.d_paths[i]);
+      hp.d_starts[i] = nullptr;
+      hp.d_paths[i] = nullptr;
+    }
+    hp.cap_starts = hp.cap_paths = 0;
+    for (int i = 0; i < 2; i++) {
+      GRASS_CUDA(cudaMalloc(&hp.d_starts[i], chunk * 4));
+      GRASS_CUDA(cudaMalloc(&hp.d_paths[i], chunk * L1 * 4));
+    }
+    hp.cap_starts = chunk;
+    hp.cap_paths = chunk * L1;
+  }
+  GRASS_CUDA(cudaMemsetAsync(hp.d_edges, 0, sizeof(unsigned long long), hp.st[0]));
+  GRASS_CUDA(cudaEventRecord(hp.ev, hp.st[0]));
+  GRASS_CUDA(cudaStreamWaitEvent(hp.st[1], hp.ev, 0));
+  for (uint64_t base = 0, c = 0; base < W; base += chunk, c++) {
+    const int k = (int)(c & 1);
+    cudaStream_t s = hp.st[k];
+    const uint64_t nc = std::min(chunk, W - base);
+    GRASS_CUDA(cudaMemcpyAsync(hp.d_starts[k], h_starts + base, nc * 4, cudaMemcpyHostToDevice, s));
+    launch_rw(g->view(), *p, hp.d_starts[k], nc, hp.d_paths[k], hp.d_edges, g->d_err, s,
+              g->tuning, g->l2win, base);
+    if (int rc = check_launch()) return rc;
+    if (p->layout == GRASS_LAYOUT_WALK_MAJOR)
+      GRASS_CUDA(cudaMemcpyAsync(h_paths + base * L1, hp.d_paths[k], nc * L1 * 4,
+                                 cudaMemcpyDeviceToHost, s));
+    else
+      GRASS_CUDA(cudaMemcpy2DAsync(h_paths + base, W * 4, hp.d_paths[k], nc * 4, nc * 4, L1,
+                                   cudaMemcpyDeviceToHost, s));
+  }
+  GRASS_CUDA(cudaEventRecord(hp.ev, hp.st[1]));
+  GRASS_CUDA(cudaStreamWaitEvent(hp.st[0], hp.ev, 0));
   unsigned long long e = 0;
-  GRASS_CUDA(cudaMemcpyAsync(&e, de.p, 8, cudaMemcpyDeviceToHost, st));
-  if (int rc = read_err_flag(g, st)) return rc;
+  GRASS_CUDA(cudaMemcpyAsync(&e, hp.d_edges, sizeof e, cudaMemcpyDeviceToHost, hp.st[0]));
+  if (int rc = read_err_flag(g, hp.st[0])) return rc;
   if (edges_out) *edges_out = e;
   return GRASS_OK;
 }

@@ -9,6 +9,29 @@
 #include "internal.h"
 
 namespace grass {
+// Workspace of the host-buffer walk (grass_rw_host): two streams and two
+// chunk-sized buffer sets, kept across calls so that steady-state calls
+// allocate nothing; chunk i+1 is copied in and walked while chunk i is copied
+// out.
+struct HostPipe {
+  std::mutex mu;
+  cudaStream_t st[2] = {nullptr, nullptr};
+  cudaEvent_t ev = nullptr;
+  uint32_t *d_starts[2] = {nullptr, nullptr};
+  uint32_t *d_paths[2] = {nullptr, nullptr};
+  size_t cap_starts = 0, cap_paths = 0;  // elements per slot
+  unsigned long long *d_edges = nullptr;
+  ~HostPipe() {
+    for (int i = 0; i < 2; i++) {
+      cudaFree(d_starts[i]);
+      cudaFree(d_paths[i]);
+      if (st[i]) cudaStreamDestroy(st[i]);
+    }
+    cudaFree(d_edges);
+    if (ev) cudaEventDestroy(ev);
+  }
+};
+
 // Per-launch L2 access-policy window (cudaLaunchAttributeAccessPolicyWindow):
 // marks the hot per-vertex table persisting so the random payload reads do
 // not evict it between uses.
@@ -22,6 +45,7 @@ struct L2Window {
 
 struct grass_graph {
   grass::L2Window l2win;
+  grass::HostPipe *pipe = nullptr;  // created by the first grass_rw_host call
   int device = 0;
   int mode = 0;
   uint32_t *d_words = nullptr;     // n_words + guard words
@@ -119,9 +143,10 @@ void launch_decode_all(const DevGraph &g, const uint64_t *rowptr, uint32_t *cols
 // ---- samplers (kernels_sample.cu) ----
 void launch_uniform_starts(uint64_t n, uint64_t count, uint64_t seed, uint32_t *out,
                            cudaStream_t s, bool mrw_roots = false);
+// w0: walker id of starts[0] (a chunk of a larger batch draws as walkers w0 + w).
 void launch_rw(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts, uint64_t W,
                uint32_t *paths, unsigned long long *edges, unsigned int *err, cudaStream_t s,
-               const grass_tuning &t, const L2Window &win = L2Window());
+               const grass_tuning &t, const L2Window &win = L2Window(), uint64_t w0 = 0);
 // Applies the process-wide parts of a tuning block (L2 fetch granularity,
 // persisting-L2 carve-out) on `device` and computes the access window for a
 // hot table of `bytes` at `base`.
@@ -131,7 +156,7 @@ void launch_rw_account(const DevGraph &g, const grass_rw_params &p, const uint32
                        uint64_t W, unsigned long long *out, cudaStream_t s);
 void launch_rw_csr(const DevCsr &c, const grass_rw_params &p, const uint32_t *starts,
                    uint64_t W, uint32_t *paths, unsigned long long *edges, cudaStream_t s,
-                   const grass_tuning &t, const L2Window &win = L2Window());
+                   const grass_tuning &t, const L2Window &win = L2Window(), uint64_t w0 = 0);
 // Fills unset (zero) fields of a tuning block with the defaults.
 // kind: GRASS_MODE_GT, GRASS_MODE_LE or 2 (uncompressed CSR).
 grass_tuning resolve_tuning(const grass_tuning &t, int kind);

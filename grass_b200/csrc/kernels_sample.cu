@@ -20,10 +20,13 @@ __device__ __forceinline__ void store_path(uint32_t *paths, int layout, uint64_t
   else store_out_u32(paths + (uint64_t)s * W + w, v);
 }
 
+// w0: walker id of starts[0] -- draws use walker id w0 + w, so a batch split
+// into chunks produces the same walks as one launch.
 template <int MODE, int DEPTH>
 __global__ void __launch_bounds__(512) rw_kernel(DevGraph g, const uint32_t *__restrict__ starts,
                                                  uint64_t W, uint32_t L, uint64_t seed,
-                                                 int layout, uint32_t *__restrict__ paths,
+                                                 uint64_t w0, int layout,
+                                                 uint32_t *__restrict__ paths,
                                                  unsigned long long *edges, unsigned int *err) {
   const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
   uint64_t cnt = 0;
@@ -47,8 +50,10 @@ __global__ void __launch_bounds__(512) rw_kernel(DevGraph g, const uint32_t *__r
 #pragma unroll
       for (int k = 0; k < DEPTH; k++) {
         const uint64_t w = base + k * nthreads;
-        if ((s & 3) == 0)
-          r[k] = philox4x32_10(seed, s >> 2, (uint32_t)w, (uint32_t)(w >> 32), TAG_RW);
+        if ((s & 3) == 0) {
+          const uint64_t id = w0 + w;
+          r[k] = philox4x32_10(seed, s >> 2, (uint32_t)id, (uint32_t)(id >> 32), TAG_RW);
+        }
         if (v[k] != INVALID_VERTEX) {
           const VHdr h = header<MODE>(g, v[k]);
           if (h.d == 0) {
@@ -81,7 +86,8 @@ template <int DEPTH>
 __global__ void __launch_bounds__(512) rw_gt_kernel(DevGraph g,
                                                     const uint32_t *__restrict__ starts,
                                                     uint64_t W, uint32_t L, uint64_t seed,
-                                                    int layout, uint32_t *__restrict__ paths,
+                                                    uint64_t w0, int layout,
+                                                    uint32_t *__restrict__ paths,
                                                     unsigned long long *edges,
                                                     unsigned int *err) {
   __shared__ uint32_t sh_all[16][32];
@@ -109,8 +115,10 @@ __global__ void __launch_bounds__(512) rw_gt_kernel(DevGraph g,
 #pragma unroll
       for (int k = 0; k < DEPTH; k++) {
         const uint64_t w = wb + (uint64_t)k * 32 + lane;
-        if ((s & 3) == 0)
-          r[k] = philox4x32_10(seed, s >> 2, (uint32_t)w, (uint32_t)(w >> 32), TAG_RW);
+        if ((s & 3) == 0) {
+          const uint64_t id = w0 + w;
+          r[k] = philox4x32_10(seed, s >> 2, (uint32_t)id, (uint32_t)(id >> 32), TAG_RW);
+        }
         bool active = v[k] != INVALID_VERTEX;
         GtRun run{0, 0, false};
         int a = 0, b = 0;
@@ -238,7 +246,8 @@ __global__ void __launch_bounds__(256) rw_account_kernel(DevGraph g,
 template <int DEPTH>
 __global__ void __launch_bounds__(512) rw_csr_kernel(DevCsr c, const uint32_t *__restrict__ starts,
                                                      uint64_t W, uint32_t L, uint64_t seed,
-                                                     int layout, uint32_t *__restrict__ paths,
+                                                     uint64_t w0, int layout,
+                                                     uint32_t *__restrict__ paths,
                                                      unsigned long long *edges) {
   const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
   uint64_t cnt = 0;
@@ -261,8 +270,10 @@ __global__ void __launch_bounds__(512) rw_csr_kernel(DevCsr c, const uint32_t *_
 #pragma unroll
       for (int k = 0; k < DEPTH; k++) {
         const uint64_t w = base + k * nthreads;
-        if ((s & 3) == 0)
-          r[k] = philox4x32_10(seed, s >> 2, (uint32_t)w, (uint32_t)(w >> 32), TAG_RW);
+        if ((s & 3) == 0) {
+          const uint64_t id = w0 + w;
+          r[k] = philox4x32_10(seed, s >> 2, (uint32_t)id, (uint32_t)(id >> 32), TAG_RW);
+        }
         if (v[k] != INVALID_VERTEX) {
           uint64_t b, e;
           csr_row(c.rowptr, v[k], b, e);
@@ -664,13 +675,13 @@ template <int MODE, int DEPTH>
 static void rw_launch_depth(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts,
                             uint64_t W, uint32_t *paths, unsigned long long *edges,
                             unsigned int *err, cudaStream_t s, const grass_tuning &t,
-                            const L2Window &win) {
+                            const L2Window &win, uint64_t w0) {
   // GT: warp-synchronous kernel with cooperative gap decoding; LE: one
   // independent O(1) decode per lane.
   auto kern = MODE == 0 ? rw_gt_kernel<DEPTH> : rw_kernel<MODE, DEPTH>;
   const unsigned grid =
       resident_grid(kern, (int)t.rw_threads, t.rw_blocks_per_sm, W, (uint64_t)t.rw_threads * DEPTH);
-  launch_with_window(kern, grid, t.rw_threads, s, win, g, starts, W, p.length, p.seed,
+  launch_with_window(kern, grid, t.rw_threads, s, win, g, starts, W, p.length, p.seed, w0,
                      (int)p.layout, paths, edges, err);
 }
 
@@ -678,21 +689,21 @@ template <int MODE>
 static void rw_dispatch(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts,
                         uint64_t W, uint32_t *paths, unsigned long long *edges,
                         unsigned int *err, cudaStream_t s, const grass_tuning &t,
-                        const L2Window &win) {
+                        const L2Window &win, uint64_t w0) {
   switch (t.rw_depth) {
-    case 1: rw_launch_depth<MODE, 1>(g, p, starts, W, paths, edges, err, s, t, win); break;
-    case 4: rw_launch_depth<MODE, 4>(g, p, starts, W, paths, edges, err, s, t, win); break;
-    default: rw_launch_depth<MODE, 2>(g, p, starts, W, paths, edges, err, s, t, win);
+    case 1: rw_launch_depth<MODE, 1>(g, p, starts, W, paths, edges, err, s, t, win, w0); break;
+    case 4: rw_launch_depth<MODE, 4>(g, p, starts, W, paths, edges, err, s, t, win, w0); break;
+    default: rw_launch_depth<MODE, 2>(g, p, starts, W, paths, edges, err, s, t, win, w0);
   }
 }
 
 void launch_rw(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts, uint64_t W,
                uint32_t *paths, unsigned long long *edges, unsigned int *err, cudaStream_t s,
-               const grass_tuning &tin, const L2Window &win) {
+               const grass_tuning &tin, const L2Window &win, uint64_t w0) {
   if (!W) return;
   const grass_tuning t = resolve_tuning(tin, g.mode);
-  if (g.mode == GRASS_MODE_GT) rw_dispatch<0>(g, p, starts, W, paths, edges, err, s, t, win);
-  else rw_dispatch<1>(g, p, starts, W, paths, edges, err, s, t, win);
+  if (g.mode == GRASS_MODE_GT) rw_dispatch<0>(g, p, starts, W, paths, edges, err, s, t, win, w0);
+  else rw_dispatch<1>(g, p, starts, W, paths, edges, err, s, t, win, w0);
   count_launch();
 }
 
@@ -709,7 +720,7 @@ void launch_rw_account(const DevGraph &g, const grass_rw_params &p, const uint32
 
 void launch_rw_csr(const DevCsr &c, const grass_rw_params &p, const uint32_t *starts,
                    uint64_t W, uint32_t *paths, unsigned long long *edges, cudaStream_t s,
-                   const grass_tuning &tin, const L2Window &win) {
+                   const grass_tuning &tin, const L2Window &win, uint64_t w0) {
   if (!W) return;
   const grass_tuning t = resolve_tuning(tin, 2);
   const uint32_t L = p.length;
@@ -718,20 +729,20 @@ void launch_rw_csr(const DevCsr &c, const grass_rw_params &p, const uint32_t *st
   switch (t.rw_depth) {
     case 1: {
       const unsigned grid = resident_grid(rw_csr_kernel<1>, T, t.rw_blocks_per_sm, W, T);
-      launch_with_window(rw_csr_kernel<1>, grid, T, s, win, c, starts, W, L, p.seed, lay, paths,
-                         edges);
+      launch_with_window(rw_csr_kernel<1>, grid, T, s, win, c, starts, W, L, p.seed, w0, lay,
+                         paths, edges);
       break;
     }
     case 4: {
       const unsigned grid = resident_grid(rw_csr_kernel<4>, T, t.rw_blocks_per_sm, W, T * 4);
-      launch_with_window(rw_csr_kernel<4>, grid, T, s, win, c, starts, W, L, p.seed, lay, paths,
-                         edges);
+      launch_with_window(rw_csr_kernel<4>, grid, T, s, win, c, starts, W, L, p.seed, w0, lay,
+                         paths, edges);
       break;
     }
     default: {
       const unsigned grid = resident_grid(rw_csr_kernel<2>, T, t.rw_blocks_per_sm, W, T * 2);
-      launch_with_window(rw_csr_kernel<2>, grid, T, s, win, c, starts, W, L, p.seed, lay, paths,
-                         edges);
+      launch_with_window(rw_csr_kernel<2>, grid, T, s, win, c, starts, W, L, p.seed, w0, lay,
+                         paths, edges);
     }
   }
   count_launch();

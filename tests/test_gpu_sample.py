@@ -58,6 +58,28 @@ def test_rw_config1(oracle_mod, mode, tmp_path):
     assert e == re_ == 4096 * 80
 
 
+@pytest.mark.parametrize("mode", ["GT", "LE"])
+@pytest.mark.parametrize("layout", [G.LAYOUT_WALK_MAJOR, G.LAYOUT_STEP_MAJOR])
+def test_rw_host_chunked_pipeline(oracle_mod, mode, layout):
+    """grass_rw_host splits the walkers into 2^17-walker chunks on two streams;
+    the walks must equal one launch (here: the oracle) with a ragged tail."""
+    d, rowptr, cols, meta = golden_graph("hub")
+    g = G.Graph(os.path.join(d, mode), mode)
+    og = oracle_mod.OracleGraph(os.path.join(d, mode))
+    W, L = 300_001, 12
+    starts = oracle_mod.uniform_starts(g.n, W, 17)
+    paths, e = g.rw(starts, L, 9, layout=layout)
+    ref, re_ = og.rw(mode, starts, L, 9)
+    if layout == G.LAYOUT_STEP_MAJOR:
+        paths = paths.T
+    np.testing.assert_array_equal(paths, ref)
+    assert e == re_
+    # a second call reuses the workspace
+    paths2, e2 = g.rw(starts[:1000], L, 9, layout=layout)
+    ref2 = ref[:1000]
+    np.testing.assert_array_equal(paths2.T if layout == G.LAYOUT_STEP_MAJOR else paths2, ref2)
+
+
 def test_device_starts_match_oracle(oracle_mod, torch_cuda):
     torch = torch_cuda
     out = torch.empty(10001, dtype=torch.int32, device="cuda")
