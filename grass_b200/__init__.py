@@ -76,6 +76,27 @@ class MrwParams(C.Structure):
                 ("reserved", C.c_uint32), ("seed", C.c_uint64)]
 
 
+JOB_RW, JOB_KHOP, JOB_MRW = 0, 1, 2
+
+
+class Job(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("count", C.c_uint32), ("seed", C.c_uint64),
+                ("d_input", C.c_void_p), ("d_roots", C.c_void_p), ("d_out0", C.c_void_p),
+                ("d_out1", C.c_void_p), ("d_hops", C.c_void_p * MAX_HOPS),
+                ("d_edges", C.c_void_p), ("length", C.c_uint32), ("layout", C.c_uint32),
+                ("hops", C.c_uint32), ("fanouts", C.c_uint32 * MAX_HOPS),
+                ("walkers", C.c_uint32), ("steps", C.c_uint32), ("select", C.c_uint32)]
+
+
+class BatchConfig(C.Structure):
+    _fields_ = [("walker_tile", C.c_uint32), ("depth", C.c_uint32),
+                ("warps_per_block", C.c_uint32), ("khop_seeds", C.c_uint32),
+                ("use_graph", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -120,6 +141,16 @@ def _load():
         "grass_csr_info": ([P, P, P, P], i32),
         "grass_csr_rw": ([P, C.POINTER(RwParams), P, u64, P, P, P], i32),
         "grass_csr_khop": ([P, C.POINTER(KhopParams), P, u64, P, P, P], i32),
+        "grass_mrw_roots": ([u64, u64, u32, u64, P, P], i32),
+        "grass_batch_create": ([P, PP], i32),
+        "grass_batch_add": ([P, C.POINTER(Job)], i32),
+        "grass_batch_clear": ([P], i32),
+        "grass_batch_set_config": ([P, C.POINTER(BatchConfig)], i32),
+        "grass_batch_get_config": ([P, C.POINTER(BatchConfig)], i32),
+        "grass_batch_run": ([P, P, P], i32),
+        "grass_batch_autotune": ([P, P, C.POINTER(BatchConfig), C.POINTER(C.c_float)], i32),
+        "grass_batch_info": ([P, P, P], i32),
+        "grass_batch_destroy": ([P], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -390,6 +421,76 @@ class Graph:
         h = C.c_void_p()
         _check(lib.grass_csr_from_graph(self._h, C.byref(h)))
         return Csr(h)
+
+
+def mrw_roots_device(n: int, S: int, R: int, seed: int, out, stream=None):
+    _check(lib.grass_mrw_roots(n, S, R, seed, _ptr(out), _stream(stream)))
+
+
+class Batch:
+    """Many RW / k-hop / multi-RW jobs run by one persistent, graph-captured launch."""
+
+    def __init__(self, graph: "Graph"):
+        self._g = graph  # keep the graph alive
+        self._h = C.c_void_p()
+        self._keep = []
+        _check(lib.grass_batch_create(graph.handle, C.byref(self._h)))
+
+    def _add(self, job: Job):
+        _check(lib.grass_batch_add(self._h, C.byref(job)))
+
+    def add_rw(self, starts, count: int, length: int, seed: int, paths,
+               layout: int = LAYOUT_WALK_MAJOR, edges=None):
+        j = Job(type=JOB_RW, count=count, seed=seed, length=length, layout=layout)
+        j.d_input, j.d_out0, j.d_edges = _ptr(starts), _ptr(paths), _ptr(edges)
+        self._add(j)
+
+    def add_khop(self, seeds, count: int, fanouts, seed: int, hop_out, edges=None):
+        j = Job(type=JOB_KHOP, count=count, seed=seed, hops=len(fanouts))
+        j.d_input, j.d_edges = _ptr(seeds), _ptr(edges)
+        for h, f in enumerate(fanouts):
+            j.fanouts[h] = int(f)
+            j.d_hops[h] = _ptr(hop_out[h]).value
+        self._add(j)
+
+    def add_mrw(self, roots, count: int, walkers: int, steps: int, seed: int, src, dst,
+                select: int = SELECT_UNIFORM, edges=None):
+        j = Job(type=JOB_MRW, count=count, seed=seed, walkers=walkers, steps=steps, select=select)
+        j.d_roots, j.d_out0, j.d_out1, j.d_edges = _ptr(roots), _ptr(src), _ptr(dst), _ptr(edges)
+        self._add(j)
+
+    def set_config(self, **kw):
+        c = BatchConfig(**kw)
+        _check(lib.grass_batch_set_config(self._h, C.byref(c)))
+
+    def config(self) -> dict:
+        c = BatchConfig()
+        _check(lib.grass_batch_get_config(self._h, C.byref(c)))
+        return c.as_dict()
+
+    def run(self, stream=None, total=None):
+        _check(lib.grass_batch_run(self._h, _stream(stream), _ptr(total)))
+
+    def autotune(self, stream=None):
+        c, ms = BatchConfig(), C.c_float()
+        _check(lib.grass_batch_autotune(self._h, _stream(stream), C.byref(c), C.byref(ms)))
+        return c.as_dict(), float(ms.value)
+
+    def info(self):
+        j, w = C.c_uint64(), C.c_uint64()
+        _check(lib.grass_batch_info(self._h, C.byref(j), C.byref(w)))
+        return {"jobs": j.value, "work_items": w.value}
+
+    def close(self):
+        if self._h:
+            lib.grass_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def uniform_starts_device(n: int, count: int, seed: int, out, stream=None):

@@ -1,0 +1,452 @@
+// kernels_batch.cu -- many uneven sampling jobs in one persistent launch.
+//
+// The reference runs one app over all vertices per process, one kernel
+// pipeline per step (GT/src/grass.cu:1417-2037).  Here a batch holds any mix
+// of RW, k-hop and multi-RW jobs with their own sizes, parameters and seeds.
+// The host splits them into work items -- one multi-RW sample, a few k-hop
+// seeds, or a tile of walkers -- ordered longest first (multi-RW chains are
+// sequential by definition), and a persistent kernel's warps pull items from
+// a device counter until the queue is empty.  The queue reset, the restore of
+// the multi-RW start vertices and the kernel are captured once into a CUDA
+// graph and replayed by every run.
+#include <algorithm>
+#include <mutex>
+#include <vector>
+
+#include "graph.h"
+#include "sample_warp.cuh"
+
+namespace grass {
+namespace {
+
+struct BatchJob {
+  uint32_t type, count;
+  uint64_t seed;
+  const uint32_t *in;
+  uint32_t *roots, *deg, *out0, *out1;
+  unsigned long long *edges;
+  uint32_t length, layout, walkers, steps, select, pad;
+  KhopArgs khop;
+};
+
+struct BatchTask {
+  uint32_t job, pad;
+  uint64_t begin, end;
+};
+
+template <int MODE, int DEPTH>
+__global__ void __launch_bounds__(256) batch_kernel(DevGraph g, const BatchJob *__restrict__ jobs,
+                                                    const BatchTask *__restrict__ tasks,
+                                                    uint32_t ntasks, unsigned int *queue,
+                                                    unsigned long long *total,
+                                                    unsigned int *err) {
+  __shared__ SmemHdr sh[8];
+  SmemHdr &my = sh[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  uint64_t all = 0;
+  bool bad = false;
+  for (;;) {
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(queue, 1u);
+    t = __shfl_sync(kFull, t, 0);
+    if (t >= ntasks) break;
+    const BatchTask tk = tasks[t];
+    const BatchJob &jb = jobs[tk.job];
+    uint64_t cnt = 0;
+    if (jb.type == GRASS_JOB_RW) {
+      rw_warp<MODE, DEPTH>(g, jb.in, jb.count, jb.length, jb.seed, 0, (int)jb.layout, jb.out0,
+                           tk.begin, tk.end, cnt, bad);
+    } else if (jb.type == GRASS_JOB_KHOP) {
+      for (uint64_t s = tk.begin; s < tk.end; s++)
+        khop_seed_warp<MODE>(g, jb.in, jb.khop, s, my, cnt, bad);
+    } else {
+      for (uint64_t s = tk.begin; s < tk.end; s++)
+        mrw_warp<MODE>(g, jb.roots + s * jb.walkers, jb.deg + s * jb.walkers, jb.walkers,
+                       jb.steps, (int)jb.select, jb.seed, s, jb.out0, jb.out1, cnt, bad);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(kFull, cnt, o);
+    if (lane == 0 && cnt) {
+      if (jb.edges) atomicAdd(jb.edges, (unsigned long long)cnt);
+      all += cnt;
+    }
+  }
+  if (lane == 0 && total && all) atomicAdd(total, (unsigned long long)all);
+  if (bad && err) atomicOr(err, 1u);
+}
+
+using BatchKernel = void (*)(DevGraph, const BatchJob *, const BatchTask *, uint32_t,
+                             unsigned int *, unsigned long long *, unsigned int *);
+
+BatchKernel pick_kernel(int mode, uint32_t depth) {
+  if (mode == GRASS_MODE_GT)
+    return depth == 4 ? batch_kernel<0, 4> : depth == 2 ? batch_kernel<0, 2> : batch_kernel<0, 1>;
+  return depth == 4 ? batch_kernel<1, 4> : depth == 2 ? batch_kernel<1, 2> : batch_kernel<1, 1>;
+}
+
+grass_batch_config resolve(const grass_batch_config &c, int mode) {
+  grass_batch_config r = c;
+  if (!r.walker_tile) r.walker_tile = 128;
+  if (!r.depth) r.depth = mode == GRASS_MODE_GT ? 1 : 4;
+  if (!r.warps_per_block) r.warps_per_block = 8;
+  if (!r.khop_seeds) r.khop_seeds = 1;
+  if (!r.use_graph) r.use_graph = 1;
+  return r;
+}
+
+bool same_shape(const grass_batch_config &a, const grass_batch_config &b) {
+  return a.walker_tile == b.walker_tile && a.depth == b.depth &&
+         a.warps_per_block == b.warps_per_block && a.khop_seeds == b.khop_seeds;
+}
+
+}  // namespace
+}  // namespace grass
+
+using namespace grass;
+
+struct grass_batch {
+  const grass_graph *g = nullptr;
+  std::vector<grass_job> jobs;
+  grass_batch_config cfg{};
+  std::mutex mu;
+  // device state built from jobs + cfg
+  bool dirty = true;
+  grass_batch_config built_cfg{};
+  BatchJob *d_jobs = nullptr;
+  BatchTask *d_tasks = nullptr;
+  uint32_t ntasks = 0;
+  unsigned int *d_queue = nullptr;
+  std::vector<void *> owned;                      // MRW degree scratch (per build)
+  std::vector<uint32_t *> snap;                   // per job: MRW start vertices as added
+  std::vector<std::pair<uint32_t *, uint32_t *>> restore;  // (roots, snapshot)
+  std::vector<uint64_t> restore_n;
+  // captured graph
+  cudaStream_t cap = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long *exec_total = nullptr;
+
+  void free_device() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    cudaFree(d_jobs);
+    cudaFree(d_tasks);
+    cudaFree(d_queue);
+    d_jobs = nullptr;
+    d_tasks = nullptr;
+    d_queue = nullptr;
+    for (void *p : owned) cudaFree(p);
+    owned.clear();
+    restore.clear();
+    restore_n.clear();
+    ntasks = 0;
+  }
+  void free_snapshots() {
+    for (uint32_t *p : snap) cudaFree(p);
+    snap.clear();
+  }
+  ~grass_batch() {
+    free_device();
+    free_snapshots();
+    if (cap) cudaStreamDestroy(cap);
+  }
+};
+
+namespace {
+
+int build(grass_batch *b) {
+  const grass_batch_config c = resolve(b->cfg, b->g->mode);
+  b->free_device();
+  std::vector<BatchJob> hj;
+  std::vector<BatchTask> mrw, khop, rw;
+  for (size_t i = 0; i < b->jobs.size(); i++) {
+    const grass_job &j = b->jobs[i];
+    BatchJob bj{};
+    bj.type = j.type;
+    bj.count = j.count;
+    bj.seed = j.seed;
+    bj.in = j.d_input;
+    bj.roots = j.d_roots;
+    bj.out0 = j.d_out0;
+    bj.out1 = j.d_out1;
+    bj.edges = j.d_edges;
+    bj.length = j.length;
+    bj.layout = j.layout;
+    bj.walkers = j.walkers;
+    bj.steps = j.steps;
+    bj.select = j.select;
+    if (j.type == GRASS_JOB_KHOP) {
+      bj.khop.hops = j.hops;
+      uint64_t w = 1;
+      for (uint32_t h = 0; h < j.hops; h++) {
+        bj.khop.fan[h] = j.fanouts[h];
+        w *= j.fanouts[h];
+        bj.khop.width[h] = w;
+        bj.khop.out[h] = j.d_hops[h];
+      }
+      bj.khop.seed = j.seed;
+      for (uint64_t s = 0; s < j.count; s += c.khop_seeds)
+        khop.push_back({(uint32_t)i, 0, s, std::min<uint64_t>(j.count, s + c.khop_seeds)});
+    } else if (j.type == GRASS_JOB_MRW) {
+      const uint64_t nr = (uint64_t)j.count * j.walkers;
+      uint32_t *deg = nullptr;
+      GRASS_CUDA(cudaMalloc(&deg, std::max<uint64_t>(nr, 1) * 4));
+      b->owned.push_back(deg);
+      b->restore.push_back({j.d_roots, b->snap[i]});
+      b->restore_n.push_back(nr);
+      bj.deg = deg;
+      for (uint64_t s = 0; s < j.count; s++) mrw.push_back({(uint32_t)i, 0, s, s + 1});
+    } else {
+      for (uint64_t w = 0; w < j.count; w += c.walker_tile)
+        rw.push_back({(uint32_t)i, 0, w, std::min<uint64_t>(j.count, w + c.walker_tile)});
+    }
+    hj.push_back(bj);
+  }
+  std::vector<BatchTask> tasks;  // longest chains first
+  tasks.insert(tasks.end(), mrw.begin(), mrw.end());
+  tasks.insert(tasks.end(), khop.begin(), khop.end());
+  tasks.insert(tasks.end(), rw.begin(), rw.end());
+  if (tasks.size() > 0xFFFFFFF0ull) return set_error(GRASS_E_ARG, "batch: too many work items");
+  b->ntasks = (uint32_t)tasks.size();
+  GRASS_CUDA(cudaMalloc(&b->d_jobs, std::max<size_t>(hj.size(), 1) * sizeof(BatchJob)));
+  GRASS_CUDA(cudaMalloc(&b->d_tasks, std::max<size_t>(tasks.size(), 1) * sizeof(BatchTask)));
+  GRASS_CUDA(cudaMalloc(&b->d_queue, sizeof(unsigned int)));
+  if (!hj.empty())
+    GRASS_CUDA(cudaMemcpy(b->d_jobs, hj.data(), hj.size() * sizeof(BatchJob),
+                          cudaMemcpyHostToDevice));
+  if (!tasks.empty())
+    GRASS_CUDA(cudaMemcpy(b->d_tasks, tasks.data(), tasks.size() * sizeof(BatchTask),
+                          cudaMemcpyHostToDevice));
+  b->built_cfg = c;
+  b->dirty = false;
+  return GRASS_OK;
+}
+
+// Queue reset, multi-RW root restore and the persistent kernel, on stream s.
+int enqueue(grass_batch *b, cudaStream_t s, unsigned long long *total) {
+  const grass_batch_config &c = b->built_cfg;
+  for (size_t i = 0; i < b->restore.size(); i++)
+    GRASS_CUDA(cudaMemcpyAsync(b->restore[i].first, b->restore[i].second, b->restore_n[i] * 4,
+                               cudaMemcpyDeviceToDevice, s));
+  GRASS_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned int), s));
+  if (!b->ntasks) return GRASS_OK;
+  BatchKernel k = pick_kernel(b->g->mode, c.depth);
+  const int threads = 32 * (int)c.warps_per_block;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, 0);
+  if (per_sm < 1) per_sm = 1;
+  const uint64_t need = (b->ntasks + c.warps_per_block - 1) / c.warps_per_block;
+  const unsigned grid = (unsigned)std::max<uint64_t>(
+      1, std::min<uint64_t>(need, (uint64_t)sm_count(b->g->device) * per_sm));
+  k<<<grid, threads, 0, s>>>(b->g->view(), b->d_jobs, b->d_tasks, b->ntasks, b->d_queue, total,
+                             b->g->d_err);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "batch kernel launch");
+}
+
+int check_job(const grass_graph *g, const grass_job *j) {
+  if (!j) return set_error(GRASS_E_ARG, "null job");
+  switch (j->type) {
+    case GRASS_JOB_RW:
+      if (j->layout > 1 || (j->count && (!j->d_input || !j->d_out0)))
+        return set_error(GRASS_E_ARG, "RW job: bad arguments");
+      return GRASS_OK;
+    case GRASS_JOB_KHOP: {
+      if (j->hops == 0 || j->hops > GRASS_MAX_HOPS || (j->count && !j->d_input))
+        return set_error(GRASS_E_ARG, "k-hop job: bad arguments");
+      uint64_t w = 1;
+      for (uint32_t h = 0; h < j->hops; h++) {
+        if (!j->fanouts[h] || (j->count && !j->d_hops[h]))
+          return set_error(GRASS_E_ARG, "k-hop job: fanout or output %u missing", h);
+        w *= j->fanouts[h];
+        if (w > (1ull << 32)) return set_error(GRASS_E_ARG, "k-hop job: fanout product too large");
+      }
+      return GRASS_OK;
+    }
+    case GRASS_JOB_MRW:
+      if (!j->walkers || j->select > 1 || (j->count && (!j->d_roots || !j->d_out0 || !j->d_out1)))
+        return set_error(GRASS_E_ARG, "multi-RW job: bad arguments");
+      return GRASS_OK;
+  }
+  (void)g;
+  return set_error(GRASS_E_ARG, "unknown job type %u", j->type);
+}
+
+}  // namespace
+
+extern "C" {
+
+int grass_batch_create(const grass_graph *g, grass_batch **out) {
+  clear_error();
+  if (!g || !out) return set_error(GRASS_E_ARG, "null argument");
+  *out = nullptr;
+  auto *b = new (std::nothrow) grass_batch();
+  if (!b) return set_error(GRASS_E_OOM, "host allocation failed");
+  b->g = g;
+  *out = b;
+  return GRASS_OK;
+}
+
+int grass_batch_add(grass_batch *b, const grass_job *job) {
+  clear_error();
+  if (!b) return set_error(GRASS_E_ARG, "null batch");
+  if (int rc = check_job(b->g, job)) return rc;
+  std::lock_guard<std::mutex> lk(b->mu);
+  DeviceGuard dg(b->g->device);
+  // Multi-RW start vertices are copied now: every run starts from them, even
+  // though each run leaves the final positions in d_roots.
+  uint32_t *snap = nullptr;
+  if (job->type == GRASS_JOB_MRW) {
+    const uint64_t nr = (uint64_t)job->count * job->walkers;
+    GRASS_CUDA(cudaMalloc(&snap, std::max<uint64_t>(nr, 1) * 4));
+    const cudaError_t e = cudaMemcpy(snap, job->d_roots, nr * 4, cudaMemcpyDeviceToDevice);
+    if (e != cudaSuccess) {
+      cudaFree(snap);
+      return cuda_fail(e, "multi-RW root snapshot");
+    }
+  }
+  b->jobs.push_back(*job);
+  b->snap.push_back(snap);
+  b->dirty = true;
+  return GRASS_OK;
+}
+
+int grass_batch_clear(grass_batch *b) {
+  if (!b) return set_error(GRASS_E_ARG, "null batch");
+  std::lock_guard<std::mutex> lk(b->mu);
+  DeviceGuard dg(b->g->device);
+  b->jobs.clear();
+  b->free_device();
+  b->free_snapshots();
+  b->dirty = true;
+  return GRASS_OK;
+}
+
+int grass_batch_set_config(grass_batch *b, const grass_batch_config *cfg) {
+  if (!b || !cfg) return set_error(GRASS_E_ARG, "null argument");
+  const uint32_t t = cfg->walker_tile, d = cfg->depth, w = cfg->warps_per_block;
+  if ((t && (t % 32 || t > 4096)) || (d && d != 1 && d != 2 && d != 4) ||
+      (w && w != 1 && w != 2 && w != 4 && w != 8) || cfg->use_graph > 2)
+    return set_error(GRASS_E_ARG, "batch config: walker_tile multiple of 32 <= 4096, depth 1/2/4, "
+                                  "warps_per_block 1/2/4/8");
+  std::lock_guard<std::mutex> lk(b->mu);
+  b->cfg = *cfg;
+  if (!same_shape(resolve(b->cfg, b->g->mode), b->built_cfg)) b->dirty = true;
+  return GRASS_OK;
+}
+
+int grass_batch_get_config(const grass_batch *b, grass_batch_config *cfg) {
+  if (!b || !cfg) return set_error(GRASS_E_ARG, "null argument");
+  *cfg = resolve(b->cfg, b->g->mode);
+  return GRASS_OK;
+}
+
+int grass_batch_run(grass_batch *b, void *stream, unsigned long long *d_total_edges) {
+  clear_error();
+  if (!b) return set_error(GRASS_E_ARG, "null batch");
+  std::lock_guard<std::mutex> lk(b->mu);
+  DeviceGuard dg(b->g->device);
+  cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+  if (b->dirty) {
+    if (int rc = build(b)) return rc;
+  }
+  if (resolve(b->cfg, b->g->mode).use_graph == 2) {
+    const int rc = enqueue(b, st, d_total_edges);
+    if (!rc && b->ntasks) count_launch();
+    return rc;
+  }
+  if (!b->exec || b->exec_total != d_total_edges) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    b->exec = nullptr;
+    if (!b->cap) GRASS_CUDA(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+    GRASS_CUDA(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue(b, b->cap, d_total_edges);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(b->cap, &graph);
+    if (rc) {
+      if (graph) cudaGraphDestroy(graph);
+      return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    const cudaError_t e2 = cudaGraphInstantiate(&b->exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaGraphInstantiate");
+    b->exec_total = d_total_edges;
+  }
+  GRASS_CUDA(cudaGraphLaunch(b->exec, st));
+  count_launch();
+  return GRASS_OK;
+}
+
+int grass_batch_autotune(grass_batch *b, void *stream, grass_batch_config *best,
+                         float *best_ms) {
+  clear_error();
+  if (!b) return set_error(GRASS_E_ARG, "null batch");
+  const grass_batch_config keep = b->cfg;
+  grass_batch_config top{};
+  float top_ms = 1e30f;
+  cudaEvent_t e0, e1;
+  {
+    DeviceGuard dg(b->g->device);
+    GRASS_CUDA(cudaEventCreate(&e0));
+    GRASS_CUDA(cudaEventCreate(&e1));
+  }
+  const uint32_t tiles[] = {64, 128, 256}, depths[] = {1, 2, 4}, wpbs[] = {1, 2, 4, 8};
+  int rc = GRASS_OK;
+  for (uint32_t t : tiles) {
+    for (uint32_t d : depths) {
+      for (uint32_t w : wpbs) {
+        grass_batch_config c = keep;
+        c.walker_tile = t;
+        c.depth = d;
+        c.warps_per_block = w;
+        if ((rc = grass_batch_set_config(b, &c))) break;
+        if ((rc = grass_batch_run(b, stream, nullptr))) break;  // build + warm-up
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3 && !rc; rep++) {
+          DeviceGuard dg(b->g->device);
+          cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+          cudaEventRecord(e0, st);
+          rc = grass_batch_run(b, stream, nullptr);
+          cudaEventRecord(e1, st);
+          cudaEventSynchronize(e1);
+          float x = 0;
+          cudaEventElapsedTime(&x, e0, e1);
+          ms = std::min(ms, x);
+        }
+        if (rc) break;
+        if (ms < top_ms) {
+          top_ms = ms;
+          top = resolve(c, b->g->mode);
+        }
+      }
+      if (rc) break;
+    }
+    if (rc) break;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) {
+    grass_batch_set_config(b, &keep);
+    return rc;
+  }
+  grass_batch_set_config(b, &top);
+  if (best) *best = top;
+  if (best_ms) *best_ms = top_ms;
+  return GRASS_OK;
+}
+
+int grass_batch_info(const grass_batch *b, uint64_t *jobs, uint64_t *work_items) {
+  if (!b) return set_error(GRASS_E_ARG, "null batch");
+  if (jobs) *jobs = b->jobs.size();
+  if (work_items) *work_items = b->ntasks;
+  return GRASS_OK;
+}
+
+int grass_batch_destroy(grass_batch *b) {
+  if (!b) return GRASS_OK;
+  DeviceGuard dg(b->g->device);
+  delete b;
+  return GRASS_OK;
+}
+
+}  // extern "C"

@@ -9,6 +9,7 @@
 // each thread owns DEPTH walkers and interleaves them, which keeps DEPTH
 // independent decode chains in flight per thread.
 #include "graph.h"
+#include "sample_warp.cuh"
 
 namespace grass {
 
@@ -297,114 +298,17 @@ __global__ void __launch_bounds__(512) rw_csr_kernel(DevCsr c, const uint32_t *_
 // chunks of 32 transits: lane p decodes the header of transit p into shared
 // memory, then the chunk's f*32 draws are spread over the lanes.
 
-struct KhopArgs {
-  uint32_t hops;
-  uint32_t fan[GRASS_MAX_HOPS];
-  uint64_t width[GRASS_MAX_HOPS];  // prod_{j<=h} fan[j]
-  uint32_t *out[GRASS_MAX_HOPS];
-  uint64_t seed;
-};
-
-struct SmemHdr {
-  uint64_t P[32];
-  uint32_t v[32], d[32], bn[32], bl[32], om[32], fp[32];
-  int a[32], b[32];
-  __device__ __forceinline__ void put(int i, const VHdr &h) {
-    P[i] = h.P; v[i] = h.v; d[i] = h.d; bn[i] = h.bn; bl[i] = h.bl; om[i] = h.om; fp[i] = h.fp;
-    a[i] = h.a; b[i] = h.b;
-  }
-  __device__ __forceinline__ VHdr get(int i) const {
-    VHdr h;
-    h.P = P[i]; h.v = v[i]; h.d = d[i]; h.bn = bn[i]; h.bl = bl[i]; h.om = om[i]; h.fp = fp[i];
-    h.a = a[i]; h.b = b[i];
-    return h;
-  }
-};
-
 template <int MODE>
 __global__ void __launch_bounds__(256) khop_kernel(DevGraph g, const uint32_t *__restrict__ seeds,
                                                    uint64_t S, KhopArgs A,
                                                    unsigned long long *edges, unsigned int *err) {
   __shared__ SmemHdr sh[8];
-  __shared__ uint32_t gt_sh[8][32];
-  const int lane = threadIdx.x & 31;
   SmemHdr &my = sh[threadIdx.x >> 5];
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   uint64_t cnt = 0;
   bool bad = false;
-  for (uint64_t s = warp; s < S; s += nwarps) {
-    for (uint32_t hop = 0; hop < A.hops; hop++) {
-      const uint32_t f = A.fan[hop];
-      const uint64_t P = hop ? A.width[hop - 1] : 1;
-      uint32_t *out = A.out[hop] + s * A.width[hop];
-      const uint32_t *prev = hop ? A.out[hop - 1] + s * A.width[hop - 1] : nullptr;
-      for (uint64_t pc = 0; pc < P; pc += 32) {
-        const uint64_t p = pc + lane;
-        uint32_t t = INVALID_VERTEX;
-        if (p < P) t = hop ? prev[p] : seeds[s];
-        VHdr h;
-        if (t < g.n) {
-          h = header<MODE>(g, t);
-        } else {
-          h.d = 0;
-          h.P = 0;
-          h.v = t;
-          h.bn = h.bl = h.om = h.fp = 0;
-          h.a = h.b = 0;
-        }
-        my.put(lane, h);
-        __syncwarp();
-        const uint64_t nP = min((uint64_t)32, P - pc);
-        const uint64_t total = nP * f;
-        for (uint64_t j0 = 0; j0 < total; j0 += 32) {  // warp-uniform
-          const uint64_t j = j0 + lane;
-          const bool act = j < total;
-          uint64_t slot = 0;
-          bool draw = false;
-          uint32_t nv = INVALID_VERTEX, tv = 0;
-          GtRun run{0, 0, false};
-          int ra = 0, rb = 0;
-          if (act) {
-            const uint32_t pl = (uint32_t)(j / f);
-            slot = pc * f + j;
-            const VHdr hk = my.get(pl);
-            if (hk.d) {
-              draw = true;
-              const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(slot >> 2), (uint32_t)s,
-                                             (uint32_t)(s >> 32), TAG_KHOP | hop);
-              const uint32_t idx = mulhi_u32(pick(rr, (int)(slot & 3)), hk.d);
-              if (MODE == 0) {
-                run = gt_locate(hk, idx);
-                tv = hk.v;
-                ra = hk.a;
-                rb = hk.b;
-              } else {
-                nv = le_neighbor(g, hk, idx);
-              }
-            }
-          }
-          if (MODE == 0) {
-            const uint32_t x = gt_warp_neighbor(g.words, draw, tv, run, ra, rb,
-                                                gt_sh[threadIdx.x >> 5]);
-            if (draw) nv = x;
-          }
-          if (act) {
-            if (draw) {
-              if (nv >= g.n) {
-                bad = true;
-                nv = INVALID_VERTEX;
-              } else {
-                cnt++;
-              }
-            }
-            out[slot] = nv;
-          }
-        }
-        __syncwarp();
-      }
-    }
-  }
+  for (uint64_t s = warp; s < S; s += nwarps) khop_seed_warp<MODE>(g, seeds, A, s, my, cnt, bad);
   warp_add_u64(edges, cnt);
   if (bad && err) atomicOr(err, 1u);
 }
@@ -558,6 +462,26 @@ __global__ void __launch_bounds__(256) mrw_kernel(DevGraph g, uint32_t *__restri
     for (uint32_t i = lane; i < R; i += 32) rt[i] = rv[i];
     __syncwarp();
   }
+  warp_add_u64(edges, cnt);
+  if (bad && err) atomicOr(err, 1u);
+}
+
+// Multi random walk with the walkers' state in global memory (mrw_warp): any
+// number of walkers per sample; deg is S*R scratch.
+template <int MODE>
+__global__ void __launch_bounds__(256) mrw_global_kernel(DevGraph g, uint32_t *__restrict__ roots,
+                                                         uint32_t *__restrict__ deg, uint64_t S,
+                                                         uint32_t R, uint32_t T, int select,
+                                                         uint64_t seed, uint32_t *__restrict__ src,
+                                                         uint32_t *__restrict__ dst,
+                                                         unsigned long long *edges,
+                                                         unsigned int *err) {
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  uint64_t cnt = 0;
+  bool bad = false;
+  for (uint64_t s = warp; s < S; s += nwarps)
+    mrw_warp<MODE>(g, roots + s * R, deg + s * R, R, T, select, seed, s, src, dst, cnt, bad);
   warp_add_u64(edges, cnt);
   if (bad && err) atomicOr(err, 1u);
 }
@@ -790,10 +714,22 @@ int launch_mrw(const DevGraph &g, const grass_mrw_params &p, uint32_t *roots, ui
   if (!S || !p.steps) return GRASS_OK;
   const MrwLayout lay{p.walkers};
   const size_t per_warp = lay.bytes_per_warp();
+  if (per_warp > 48 * 1024) {
+    // Too many walkers for a shared-memory Fenwick tree per warp: keep the
+    // walkers' degrees in global scratch (mrw_warp).
+    uint32_t *deg = nullptr;
+    cudaError_t e = cudaMallocAsync(&deg, S * (uint64_t)p.walkers * sizeof(uint32_t), s);
+    if (e != cudaSuccess) return cuda_fail(e, "multi-RW scratch");
+    auto kern = g.mode == GRASS_MODE_GT ? mrw_global_kernel<0> : mrw_global_kernel<1>;
+    kern<<<grid_warps(S, 8, cur_dev(), 8), 256, 0, s>>>(g, roots, deg, S, p.walkers, p.steps,
+                                                        (int)p.select, p.seed, src, dst, edges,
+                                                        err);
+    count_launch();
+    cudaFreeAsync(deg, s);
+    return GRASS_OK;
+  }
   const size_t budget = 200 * 1024;
-  int warps = (int)std::min<size_t>(8, budget / per_warp);
-  if (warps < 1) return set_error(GRASS_E_ARG, "multi-RW: %u walkers exceed shared memory",
-                                  p.walkers);
+  const int warps = (int)std::min<size_t>(8, budget / per_warp);
   const size_t smem = per_warp * warps;
   auto kern = g.mode == GRASS_MODE_GT ? mrw_kernel<0> : mrw_kernel<1>;
   if (smem > 48 * 1024)

@@ -1,0 +1,300 @@
+// sample_warp.cuh -- warp-level sampling routines shared by the standalone
+// multi-RW kernel and the batched persistent kernel.  Each routine is run by
+// all 32 lanes of one warp and needs no shared memory, so a persistent warp
+// can pick up any job type from a work queue.
+#pragma once
+#include "device_common.cuh"
+
+namespace grass {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+__device__ __forceinline__ void path_store(uint32_t *paths, int layout, uint64_t W, uint32_t L,
+                                           uint64_t w, uint32_t s, uint32_t v) {
+  if (layout == GRASS_LAYOUT_WALK_MAJOR) store_out_u32(paths + w * (uint64_t)(L + 1) + s, v);
+  else store_out_u32(paths + (uint64_t)s * W + w, v);
+}
+
+// Random walk of walkers [b, e) of a job of W walkers (starts[0..W)), DEPTH
+// walkers per lane per pass.  Same draws as rw_kernel / rw_gt_kernel:
+// walker w uses Philox(seed; step>>2, w0+w, .., TAG_RW).
+template <int MODE, int DEPTH>
+__device__ __forceinline__ void rw_warp(const DevGraph &g, const uint32_t *starts, uint64_t W,
+                                        uint32_t L, uint64_t seed, uint64_t w0, int layout,
+                                        uint32_t *paths, uint64_t b, uint64_t e, uint64_t &cnt,
+                                        bool &bad) {
+  const int lane = threadIdx.x & 31;
+  for (uint64_t wb = b; wb < e; wb += 32 * DEPTH) {  // warp-uniform
+    uint32_t v[DEPTH];
+    u32x4 r[DEPTH];
+#pragma unroll
+    for (int k = 0; k < DEPTH; k++) {
+      const uint64_t w = wb + (uint64_t)k * 32 + lane;
+      v[k] = INVALID_VERTEX;
+      r[k] = u32x4{0, 0, 0, 0};
+      if (w < e) {
+        const uint32_t s0 = starts[w];
+        path_store(paths, layout, W, L, w, 0, s0);
+        v[k] = s0 < g.n ? s0 : INVALID_VERTEX;
+      }
+    }
+    for (uint32_t s = 0; s < L; s++) {
+#pragma unroll
+      for (int k = 0; k < DEPTH; k++) {
+        const uint64_t w = wb + (uint64_t)k * 32 + lane;
+        if ((s & 3) == 0) {
+          const uint64_t id = w0 + w;
+          r[k] = philox4x32_10(seed, s >> 2, (uint32_t)id, (uint32_t)(id >> 32), TAG_RW);
+        }
+        bool active = v[k] != INVALID_VERTEX;
+        uint32_t nv = INVALID_VERTEX;
+        if (MODE == 0) {
+          GtRun run{0, 0, false};
+          int ra = 0, rb = 0;
+          if (active) {
+            const VHdr h = header<0>(g, v[k]);
+            if (h.d == 0) {
+              active = false;
+              v[k] = INVALID_VERTEX;
+            } else {
+              run = gt_locate(h, mulhi_u32(pick(r[k], s & 3), h.d));
+              ra = h.a;
+              rb = h.b;
+            }
+          }
+          nv = gt_warp_neighbor(g.words, active, v[k], run, ra, rb, nullptr);
+        } else if (active) {
+          const VHdr h = header<1>(g, v[k]);
+          if (h.d == 0) {
+            active = false;
+            v[k] = INVALID_VERTEX;
+          } else {
+            nv = le_neighbor(g, h, mulhi_u32(pick(r[k], s & 3), h.d));
+          }
+        }
+        if (active) {
+          if (nv >= g.n) {
+            bad = true;
+            v[k] = INVALID_VERTEX;
+          } else {
+            v[k] = nv;
+            cnt++;
+          }
+        }
+        if (w < e) path_store(paths, layout, W, L, w, s + 1, v[k]);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// k-hop of one seed (KHopApp, GT/src/apps/khop/khop.cu:1-79, with runtime
+// fanouts).  For each hop the frontier is taken in chunks of 32 transits:
+// lane p decodes the header of transit p into the warp's shared-memory slot,
+// then the chunk's f*32 draws are spread over the lanes.
+
+struct KhopArgs {
+  uint32_t hops;
+  uint32_t fan[GRASS_MAX_HOPS];
+  uint64_t width[GRASS_MAX_HOPS];  // prod_{j<=h} fan[j]
+  uint32_t *out[GRASS_MAX_HOPS];
+  uint64_t seed;
+};
+
+struct SmemHdr {
+  uint64_t P[32];
+  uint32_t v[32], d[32], bn[32], bl[32], om[32], fp[32];
+  int a[32], b[32];
+  __device__ __forceinline__ void put(int i, const VHdr &h) {
+    P[i] = h.P; v[i] = h.v; d[i] = h.d; bn[i] = h.bn; bl[i] = h.bl; om[i] = h.om; fp[i] = h.fp;
+    a[i] = h.a; b[i] = h.b;
+  }
+  __device__ __forceinline__ VHdr get(int i) const {
+    VHdr h;
+    h.P = P[i]; h.v = v[i]; h.d = d[i]; h.bn = bn[i]; h.bl = bl[i]; h.om = om[i]; h.fp = fp[i];
+    h.a = a[i]; h.b = b[i];
+    return h;
+  }
+};
+
+template <int MODE>
+__device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t *seeds,
+                                               const KhopArgs &A, uint64_t s, SmemHdr &my,
+                                               uint64_t &cnt, bool &bad) {
+  const int lane = threadIdx.x & 31;
+  for (uint32_t hop = 0; hop < A.hops; hop++) {
+    const uint32_t f = A.fan[hop];
+    const uint64_t P = hop ? A.width[hop - 1] : 1;
+    uint32_t *out = A.out[hop] + s * A.width[hop];
+    const uint32_t *prev = hop ? A.out[hop - 1] + s * A.width[hop - 1] : nullptr;
+    for (uint64_t pc = 0; pc < P; pc += 32) {
+      const uint64_t p = pc + lane;
+      uint32_t t = INVALID_VERTEX;
+      if (p < P) t = hop ? prev[p] : seeds[s];
+      VHdr h;
+      if (t < g.n) {
+        h = header<MODE>(g, t);
+      } else {
+        h.d = 0;
+        h.P = 0;
+        h.v = t;
+        h.bn = h.bl = h.om = h.fp = 0;
+        h.a = h.b = 0;
+      }
+      my.put(lane, h);
+      __syncwarp();
+      const uint64_t nP = min((uint64_t)32, P - pc);
+      const uint64_t total = nP * f;
+      for (uint64_t j0 = 0; j0 < total; j0 += 32) {  // warp-uniform
+        const uint64_t j = j0 + lane;
+        const bool act = j < total;
+        uint64_t slot = 0;
+        bool draw = false;
+        uint32_t nv = INVALID_VERTEX, tv = 0;
+        GtRun run{0, 0, false};
+        int ra = 0, rb = 0;
+        if (act) {
+          const uint32_t pl = (uint32_t)(j / f);
+          slot = pc * f + j;
+          const VHdr hk = my.get(pl);
+          if (hk.d) {
+            draw = true;
+            const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(slot >> 2), (uint32_t)s,
+                                           (uint32_t)(s >> 32), TAG_KHOP | hop);
+            const uint32_t idx = mulhi_u32(pick(rr, (int)(slot & 3)), hk.d);
+            if (MODE == 0) {
+              run = gt_locate(hk, idx);
+              tv = hk.v;
+              ra = hk.a;
+              rb = hk.b;
+            } else {
+              nv = le_neighbor(g, hk, idx);
+            }
+          }
+        }
+        if (MODE == 0) {
+          const uint32_t x = gt_warp_neighbor(g.words, draw, tv, run, ra, rb, nullptr);
+          if (draw) nv = x;
+        }
+        if (act) {
+          if (draw) {
+            if (nv >= g.n) {
+              bad = true;
+              nv = INVALID_VERTEX;
+            } else {
+              cnt++;
+            }
+          }
+          out[slot] = nv;
+        }
+      }
+      __syncwarp();
+    }
+  }
+}
+
+// Multi random walk of one sample (MultiRWApp, GT/src/apps/multiRW/multiRW.cu:3-112):
+// R walkers whose vertices live in roots[0..R) (updated in place) and whose
+// degrees live in deg[0..R) (scratch).  Lane j keeps the total degree of
+// walkers [j*B, (j+1)*B), B = ceil(R/32); a degree-proportional pick scans
+// the 32 bucket sums with shuffles, then the chosen bucket with up to two
+// more 32-wide scans.  Step t draws from Philox(seed; t, sample, .., TAG_MRW):
+// word 0 (+ word 2 as high half) picks the walker, word 1 the neighbor.
+template <int MODE>
+__device__ __forceinline__ void mrw_warp(const DevGraph &g, uint32_t *roots, uint32_t *deg,
+                                         uint32_t R, uint32_t T, int select, uint64_t seed,
+                                         uint64_t sample, uint32_t *src, uint32_t *dst,
+                                         uint64_t &cnt, bool &bad) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t B = (R + 31) / 32;
+  uint64_t bsum = 0;  // this lane's bucket
+  for (uint32_t i = lane * B; i < min(R, (lane + 1) * B); i++) {
+    const uint32_t x = roots[i];
+    const uint32_t d = x < g.n ? record_degree(g, x) : 0u;
+    deg[i] = d;
+    bsum += d;
+  }
+  uint64_t wsum = bsum;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(kFull, wsum, o);
+  __syncwarp();
+  for (uint32_t t = 0; t < T; t++) {
+    const u32x4 rr = philox4x32_10(seed, t, (uint32_t)sample, (uint32_t)(sample >> 32), TAG_MRW);
+    const uint64_t io = sample * T + t;
+    uint32_t x;
+    if (select == GRASS_SELECT_DEGREE) {
+      if (wsum == 0) {
+        if (lane == 0) {
+          src[io] = INVALID_VERTEX;
+          dst[io] = INVALID_VERTEX;
+        }
+        continue;
+      }
+      const uint64_t u = mulhi_u64(((uint64_t)rr.z << 32) | rr.x, wsum);
+      // bucket: first lane whose inclusive prefix exceeds u
+      uint64_t incl = bsum;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint64_t y = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += y;
+      }
+      const int Lb = __ffs(__ballot_sync(kFull, incl > u)) - 1;
+      uint64_t acc = __shfl_sync(kFull, incl - bsum, Lb);  // prefix before the bucket
+      const uint32_t b0 = (uint32_t)Lb * B, b1 = min(R, b0 + B);
+      x = b1 - 1;
+      for (uint32_t c0 = b0; c0 < b1; c0 += 32) {  // at most two passes for R <= 2048
+        const uint32_t i = c0 + lane;
+        const uint64_t d = i < b1 ? deg[i] : 0u;
+        uint64_t ci = d;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint64_t y = __shfl_up_sync(kFull, ci, o);
+          if (lane >= o) ci += y;
+        }
+        const unsigned hit = __ballot_sync(kFull, i < b1 && acc + ci > u);
+        if (hit) {
+          x = c0 + (uint32_t)(__ffs(hit) - 1);
+          break;
+        }
+        acc += __shfl_sync(kFull, ci, 31);
+      }
+    } else {
+      x = mulhi_u32(rr.x, R);
+    }
+    // lane 0 moves walker x
+    uint32_t nd = 0, od = 0;
+    bool moved = false;
+    if (lane == 0) {
+      const uint32_t v = roots[x];
+      od = deg[x];
+      src[io] = v;
+      if (od == 0) {
+        dst[io] = INVALID_VERTEX;
+      } else {
+        const VHdr h = header<MODE>(g, v);
+        const uint32_t nv = neighbor<MODE>(g, h, mulhi_u32(rr.y, h.d));
+        if (nv >= g.n) {
+          bad = true;
+          dst[io] = INVALID_VERTEX;
+        } else {
+          dst[io] = nv;
+          cnt++;
+          roots[x] = nv;
+          nd = record_degree(g, nv);
+          deg[x] = nd;
+          moved = true;
+        }
+      }
+    }
+    moved = __shfl_sync(kFull, moved, 0);
+    if (moved) {
+      nd = __shfl_sync(kFull, nd, 0);
+      od = __shfl_sync(kFull, od, 0);
+      if (lane == (int)(x / B)) bsum = bsum - od + nd;
+      wsum = wsum - od + nd;
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace grass

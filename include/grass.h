@@ -251,6 +251,65 @@ int grass_mrw_roots(uint64_t n, uint64_t S, uint32_t R, uint64_t seed, uint32_t 
                     void *stream);
 
 /* =========================================================================
+ * Batched jobs: many RW / k-hop / multi-RW jobs of uneven size in ONE
+ * persistent launch, captured in a CUDA graph.  The reference runs one app
+ * per process through nextdoor() (GT/src/grass.cu:2066-2135); here warps of a
+ * persistent kernel pull work items (walker tiles, single seeds, single
+ * multi-RW samples -- the longest first) from a device queue.  Every job has
+ * its own Philox seed, so each job's output equals the standalone call with
+ * the same parameters (grass_rw / grass_khop / grass_mrw).
+ * ========================================================================= */
+#define GRASS_JOB_RW 0
+#define GRASS_JOB_KHOP 1
+#define GRASS_JOB_MRW 2
+
+typedef struct {
+  uint32_t type;                     /* GRASS_JOB_*                                    */
+  uint32_t count;                    /* walkers (RW), seeds (k-hop), samples (MRW)     */
+  uint64_t seed;                     /* Philox key of the job                          */
+  const uint32_t *d_input;           /* RW starts[count] / k-hop seeds[count]          */
+  uint32_t *d_roots;                 /* MRW [count][walkers]: initial walker vertices;
+                                        each run restores them, then leaves the final
+                                        positions                                      */
+  uint32_t *d_out0;                  /* RW paths / MRW src[count][steps]               */
+  uint32_t *d_out1;                  /* MRW dst[count][steps]                          */
+  uint32_t *d_hops[GRASS_MAX_HOPS];  /* k-hop outputs, [count][prod fanouts]           */
+  unsigned long long *d_edges;       /* optional: sampled edges of this job are added  */
+  uint32_t length, layout;           /* RW                                             */
+  uint32_t hops;                     /* k-hop                                          */
+  uint32_t fanouts[GRASS_MAX_HOPS];
+  uint32_t walkers, steps, select;   /* MRW                                            */
+} grass_job;
+
+/* Launch shape of the batched kernel; zero fields take defaults.  The
+ * autotuner sweeps walker_tile x depth x warps_per_block. */
+typedef struct {
+  uint32_t walker_tile;      /* RW walkers per work item: 64, 128, 256 (default 128)          */
+  uint32_t depth;            /* RW walkers in flight per lane: 1, 2, 4 (LE 4, GT 1)            */
+  uint32_t warps_per_block;  /* 1, 2, 4, 8 (default 8)                                        */
+  uint32_t khop_seeds;       /* k-hop seeds per work item (default 1)                         */
+  uint32_t use_graph;        /* 1 (default): replay a captured CUDA graph; 2: plain launches  */
+  uint32_t reserved[3];
+} grass_batch_config;
+
+typedef struct grass_batch grass_batch;
+int grass_batch_create(const grass_graph *g, grass_batch **out);
+int grass_batch_add(grass_batch *b, const grass_job *job);
+int grass_batch_clear(grass_batch *b);
+int grass_batch_set_config(grass_batch *b, const grass_batch_config *cfg);
+int grass_batch_get_config(const grass_batch *b, grass_batch_config *cfg);
+/* Runs every job once; d_total_edges (optional) receives the total number of
+ * sampled edges (added to).  Asynchronous on the stream. */
+int grass_batch_run(grass_batch *b, void *stream, unsigned long long *d_total_edges);
+/* Times every configuration of the sweep on this batch (each run repeats
+ * the whole batch), keeps the fastest and returns it with its time in ms. */
+int grass_batch_autotune(grass_batch *b, void *stream, grass_batch_config *best,
+                         float *best_ms);
+/* Number of work items the current jobs split into (for inspection). */
+int grass_batch_info(const grass_batch *b, uint64_t *jobs, uint64_t *work_items);
+int grass_batch_destroy(grass_batch *b);
+
+/* =========================================================================
  * Uncompressed-CSR baseline with the same RNG streams (no reference
  * counterpart: the reference's NextDoor CSR loaders, GT/src/graph.hpp, are
  * never called).  Produces the same walks as the compressed sampler.
