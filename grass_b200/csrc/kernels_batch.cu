@@ -13,26 +13,10 @@
 #include <mutex>
 #include <vector>
 
-#include "graph.h"
-#include "sample_warp.cuh"
+#include "batch.h"
 
 namespace grass {
 namespace {
-
-struct BatchJob {
-  uint32_t type, count;
-  uint64_t seed;
-  const uint32_t *in;
-  uint32_t *roots, *deg, *out0, *out1;
-  unsigned long long *edges;
-  uint32_t length, layout, walkers, steps, select, pad;
-  KhopArgs khop;
-};
-
-struct BatchTask {
-  uint32_t job, pad;
-  uint64_t begin, end;
-};
 
 template <int MODE, int DEPTH>
 __global__ void __launch_bounds__(256) batch_kernel(DevGraph g, const BatchJob *__restrict__ jobs,
@@ -85,6 +69,17 @@ BatchKernel pick_kernel(int mode, uint32_t depth) {
 }
 
 grass_batch_config resolve(const grass_batch_config &c, int mode) {
+  return resolve_batch_config(c, mode);
+}
+
+bool same_shape(const grass_batch_config &a, const grass_batch_config &b) {
+  return a.walker_tile == b.walker_tile && a.depth == b.depth &&
+         a.warps_per_block == b.warps_per_block && a.khop_seeds == b.khop_seeds;
+}
+
+}  // namespace
+
+grass_batch_config resolve_batch_config(const grass_batch_config &c, int mode) {
   grass_batch_config r = c;
   if (!r.walker_tile) r.walker_tile = 128;
   if (!r.depth) r.depth = mode == GRASS_MODE_GT ? 1 : 4;
@@ -94,12 +89,66 @@ grass_batch_config resolve(const grass_batch_config &c, int mode) {
   return r;
 }
 
-bool same_shape(const grass_batch_config &a, const grass_batch_config &b) {
-  return a.walker_tile == b.walker_tile && a.depth == b.depth &&
-         a.warps_per_block == b.warps_per_block && a.khop_seeds == b.khop_seeds;
+BatchJob make_batch_job(const grass_job &j, uint32_t *deg) {
+  BatchJob bj{};
+  bj.type = j.type;
+  bj.count = j.count;
+  bj.seed = j.seed;
+  bj.in = j.d_input;
+  bj.roots = j.d_roots;
+  bj.deg = deg;
+  bj.out0 = j.d_out0;
+  bj.out1 = j.d_out1;
+  bj.edges = j.d_edges;
+  bj.length = j.length;
+  bj.layout = j.layout;
+  bj.walkers = j.walkers;
+  bj.steps = j.steps;
+  bj.select = j.select;
+  if (j.type == GRASS_JOB_KHOP) {
+    bj.khop.hops = j.hops;
+    uint64_t w = 1;
+    for (uint32_t h = 0; h < j.hops; h++) {
+      bj.khop.fan[h] = j.fanouts[h];
+      w *= j.fanouts[h];
+      bj.khop.width[h] = w;
+      bj.khop.out[h] = j.d_hops[h];
+    }
+    bj.khop.seed = j.seed;
+  }
+  return bj;
 }
 
-}  // namespace
+void split_job(const grass_job &j, uint32_t ji, const grass_batch_config &c,
+               std::vector<BatchTask> &mrw, std::vector<BatchTask> &khop,
+               std::vector<BatchTask> &rw) {
+  if (j.type == GRASS_JOB_KHOP) {
+    for (uint64_t s = 0; s < j.count; s += c.khop_seeds)
+      khop.push_back({ji, 0, s, std::min<uint64_t>(j.count, s + c.khop_seeds)});
+  } else if (j.type == GRASS_JOB_MRW) {
+    for (uint64_t s = 0; s < j.count; s++) mrw.push_back({ji, 0, s, s + 1});
+  } else {
+    for (uint64_t w = 0; w < j.count; w += c.walker_tile)
+      rw.push_back({ji, 0, w, std::min<uint64_t>(j.count, w + c.walker_tile)});
+  }
+}
+
+int launch_batch(const grass_graph *g, const BatchJob *d_jobs, const BatchTask *d_tasks,
+                 uint32_t ntasks, unsigned int *d_queue, unsigned long long *d_total,
+                 cudaStream_t s, const grass_batch_config &c) {
+  BatchKernel k = pick_kernel(g->mode, c.depth);
+  const int threads = 32 * (int)c.warps_per_block;
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, 0);
+  if (per_sm < 1) per_sm = 1;
+  const uint64_t need = (ntasks + c.warps_per_block - 1) / c.warps_per_block;
+  const unsigned grid = (unsigned)std::max<uint64_t>(
+      1, std::min<uint64_t>(need, (uint64_t)sm_count(g->device) * per_sm));
+  k<<<grid, threads, 0, s>>>(g->view(), d_jobs, d_tasks, ntasks, d_queue, d_total, g->d_err);
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "batch kernel launch");
+}
+
 }  // namespace grass
 
 using namespace grass;
@@ -160,46 +209,16 @@ int build(grass_batch *b) {
   std::vector<BatchTask> mrw, khop, rw;
   for (size_t i = 0; i < b->jobs.size(); i++) {
     const grass_job &j = b->jobs[i];
-    BatchJob bj{};
-    bj.type = j.type;
-    bj.count = j.count;
-    bj.seed = j.seed;
-    bj.in = j.d_input;
-    bj.roots = j.d_roots;
-    bj.out0 = j.d_out0;
-    bj.out1 = j.d_out1;
-    bj.edges = j.d_edges;
-    bj.length = j.length;
-    bj.layout = j.layout;
-    bj.walkers = j.walkers;
-    bj.steps = j.steps;
-    bj.select = j.select;
-    if (j.type == GRASS_JOB_KHOP) {
-      bj.khop.hops = j.hops;
-      uint64_t w = 1;
-      for (uint32_t h = 0; h < j.hops; h++) {
-        bj.khop.fan[h] = j.fanouts[h];
-        w *= j.fanouts[h];
-        bj.khop.width[h] = w;
-        bj.khop.out[h] = j.d_hops[h];
-      }
-      bj.khop.seed = j.seed;
-      for (uint64_t s = 0; s < j.count; s += c.khop_seeds)
-        khop.push_back({(uint32_t)i, 0, s, std::min<uint64_t>(j.count, s + c.khop_seeds)});
-    } else if (j.type == GRASS_JOB_MRW) {
+    uint32_t *deg = nullptr;
+    if (j.type == GRASS_JOB_MRW) {
       const uint64_t nr = (uint64_t)j.count * j.walkers;
-      uint32_t *deg = nullptr;
       GRASS_CUDA(cudaMalloc(&deg, std::max<uint64_t>(nr, 1) * 4));
       b->owned.push_back(deg);
       b->restore.push_back({j.d_roots, b->snap[i]});
       b->restore_n.push_back(nr);
-      bj.deg = deg;
-      for (uint64_t s = 0; s < j.count; s++) mrw.push_back({(uint32_t)i, 0, s, s + 1});
-    } else {
-      for (uint64_t w = 0; w < j.count; w += c.walker_tile)
-        rw.push_back({(uint32_t)i, 0, w, std::min<uint64_t>(j.count, w + c.walker_tile)});
     }
-    hj.push_back(bj);
+    hj.push_back(make_batch_job(j, deg));
+    split_job(j, (uint32_t)i, c, mrw, khop, rw);
   }
   std::vector<BatchTask> tasks;  // longest chains first
   tasks.insert(tasks.end(), mrw.begin(), mrw.end());
@@ -229,18 +248,7 @@ int enqueue(grass_batch *b, cudaStream_t s, unsigned long long *total) {
                                cudaMemcpyDeviceToDevice, s));
   GRASS_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned int), s));
   if (!b->ntasks) return GRASS_OK;
-  BatchKernel k = pick_kernel(b->g->mode, c.depth);
-  const int threads = 32 * (int)c.warps_per_block;
-  int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, 0);
-  if (per_sm < 1) per_sm = 1;
-  const uint64_t need = (b->ntasks + c.warps_per_block - 1) / c.warps_per_block;
-  const unsigned grid = (unsigned)std::max<uint64_t>(
-      1, std::min<uint64_t>(need, (uint64_t)sm_count(b->g->device) * per_sm));
-  k<<<grid, threads, 0, s>>>(b->g->view(), b->d_jobs, b->d_tasks, b->ntasks, b->d_queue, total,
-                             b->g->d_err);
-  const cudaError_t e = cudaGetLastError();
-  return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "batch kernel launch");
+  return launch_batch(b->g, b->d_jobs, b->d_tasks, b->ntasks, b->d_queue, total, s, c);
 }
 
 int check_job(const grass_graph *g, const grass_job *j) {
