@@ -54,7 +54,8 @@ def parse():
     ap.add_argument("--length", type=int, default=80)
     ap.add_argument("--khop-seeds", type=int, default=65536)
     ap.add_argument("--mode", default="LE", choices=["LE", "GT"])
-    ap.add_argument("--only", default="", help="comma list: rw,khop,decode,csr,e2e,cpu")
+    ap.add_argument("--only", default="",
+                    help="comma list: rw,khop,decode,csr,e2e,cpu,batch,serve")
     ap.add_argument("--no-clocks", action="store_true")
     return ap.parse_args()
 
@@ -226,6 +227,143 @@ def timed(torch, fn, K, W, flush, dist=None, dev=None):
     return ms, max_over_ranks(dist, sum(ms), torch)
 
 
+# ---------------------------------------------------------------------------
+# batched uneven jobs (R-MAT s24 ef16) and the serving loop on the same graph
+
+MIX_FANOUTS = [(10, 5), (15, 10), (25, 10), (5, 5, 5)]
+
+
+def mix_jobs(n, k=256, seed=3):
+    """k jobs: 40% RW (L ~ U[10,100]), 40% k-hop (fanouts from MIX_FANOUTS),
+    20% multi-RW (one sample of 2000 walkers, 10,000 steps, degree-
+    proportional); RW walkers / k-hop seeds ~ lognormal(ln 1024, 1.5)
+    clipped to [1, 65536]."""
+    rng = np.random.default_rng(seed)
+    n_rw, n_kh = round(0.4 * k), round(0.4 * k)
+    types = [0] * n_rw + [1] * n_kh + [2] * (k - n_rw - n_kh)
+    rng.shuffle(types)
+    jobs = []
+    for i, t in enumerate(types):
+        size = int(np.clip(np.rint(rng.lognormal(np.log(1024), 1.5)), 1, 65536))
+        j = {"type": int(t), "seed": 1000 + i}
+        if t == 0:
+            j.update(count=size, length=int(rng.integers(10, 101)))
+        elif t == 1:
+            j.update(count=size, fanouts=MIX_FANOUTS[int(rng.integers(0, 4))])
+        else:
+            j.update(count=1, walkers=2000, steps=10000, select=1)
+        jobs.append(j)
+    return jobs
+
+
+def batch_bench(G, torch, graphs, n, stream, flush, K, W):
+    """One persistent captured launch over 256 uneven jobs, autotuned, against
+    the plain method (one standalone launch per job, same stream)."""
+    dev = torch.device("cuda", torch.cuda.current_device())
+    jobs = mix_jobs(n)
+    bufs = []
+    for j in jobs:
+        c = j["count"]
+        if j["type"] == 0:
+            inp = torch.empty(c, dtype=torch.int32, device=dev)
+            G.uniform_starts_device(n, c, j["seed"], inp, stream=stream)
+            outs = [torch.empty(c * (j["length"] + 1), dtype=torch.int32, device=dev)]
+        elif j["type"] == 1:
+            inp = torch.empty(c, dtype=torch.int32, device=dev)
+            G.uniform_starts_device(n, c, j["seed"], inp, stream=stream)
+            outs = [torch.empty(c * w, dtype=torch.int32, device=dev)
+                    for w in G.hop_widths(j["fanouts"])]
+        else:
+            inp = torch.empty(c * j["walkers"], dtype=torch.int32, device=dev)
+            G.mrw_roots_device(n, c, j["walkers"], j["seed"], inp, stream=stream)
+            outs = [torch.empty(c * j["steps"], dtype=torch.int32, device=dev)
+                    for _ in range(2)]
+        bufs.append((inp, outs, inp.clone()))
+    total = torch.zeros(1, dtype=torch.int64, device=dev)
+    draws = {0: 0, 1: 0, 2: 0}
+    res = {}
+    for m, g in graphs.items():
+        def make(types):
+            b = G.Batch(g)
+            for j, (inp, outs, _) in zip(jobs, bufs):
+                if j["type"] not in types:
+                    continue
+                if j["type"] == 0:
+                    b.add_rw(inp, j["count"], j["length"], j["seed"], outs[0])
+                elif j["type"] == 1:
+                    b.add_khop(inp, j["count"], j["fanouts"], j["seed"], outs)
+                else:
+                    b.add_mrw(inp, j["count"], j["walkers"], j["steps"], j["seed"], outs[0],
+                              outs[1], select=j["select"])
+            return b
+        b = make({0, 1, 2})
+        best, best_ms = b.autotune(stream=stream)
+        total.zero_()
+        b.run(stream=stream, total=total)
+        torch.cuda.synchronize()
+        edges = int(total.item())
+        lc0 = G.launch_count()
+        ms, tot = timed(torch, lambda: b.run(stream=stream), K, W, flush)
+        launches = (G.launch_count() - lc0) / (K + W)
+        short = make({0, 1})
+        short.set_config(**{k: v for k, v in best.items() if k != "use_graph"})
+        ms_s, tot_s = timed(torch, lambda: short.run(stream=stream), K, W, flush)
+
+        # plain method: each job its own launch, back to back on one stream
+        def plain():
+            for j, (inp, outs, snap) in zip(jobs, bufs):
+                if j["type"] == 0:
+                    g.rw_device(inp, j["count"], j["length"], j["seed"], outs[0], stream=stream)
+                elif j["type"] == 1:
+                    g.khop_device(inp, j["count"], j["fanouts"], j["seed"], outs, stream=stream)
+                else:
+                    inp.copy_(snap)
+                    g.mrw_device(inp, j["count"], j["walkers"], j["steps"], j["seed"], outs[0],
+                                 outs[1], select=j["select"], stream=stream)
+        pms, ptot = timed(torch, plain, 1, 1, flush)
+        res[m] = {"makespan_ms": tot / K, "ms_min": min(ms), "ms_max": max(ms),
+                  "edges_per_run": edges, "edges_per_s": edges / (tot / K / 1000.0),
+                  "launches_per_run": launches, "autotune_best": best,
+                  "autotune_best_ms": best_ms,
+                  "makespan_rw_khop_only_ms": tot_s / K,
+                  "plain_one_launch_per_job_ms": ptot,
+                  "speedup_vs_plain": ptot / (tot / K)}
+        b.close()
+        short.close()
+    for j in jobs:
+        t = j["type"]
+        if t == 0:
+            draws[0] += j["count"] * j["length"]
+        elif t == 1:
+            draws[1] += j["count"] * sum(G.hop_widths(j["fanouts"]))
+        else:
+            draws[2] += j["count"] * j["steps"]
+    res["jobs"] = {"rw": sum(j["type"] == 0 for j in jobs),
+                   "khop": sum(j["type"] == 1 for j in jobs),
+                   "mrw": sum(j["type"] == 2 for j in jobs),
+                   "max_draws_by_type": {"rw": draws[0], "khop": draws[1], "mrw": draws[2]}}
+    del bufs
+    return res
+
+
+def serve_bench(G, g, rates=(2000, 10000, 50000), seconds=0.2, plain_cap=1000):
+    """Open-loop Poisson arrivals of the same request mix through the serving
+    loop, and the first plain_cap requests of the same trace served one
+    standalone launch per request."""
+    out = {}
+    for rate in rates:
+        nreq = int(max(1000, rate * seconds))
+        a = G.loadgen(g, float(rate), nreq, mode=0, seed=5)
+        b = G.loadgen(g, float(rate), min(nreq, plain_cap), mode=1, seed=5)
+        keep = ("completed", "rejected", "failed", "batches", "p50_us", "p99_us", "p999_us",
+                "mean_us", "max_us", "p50_type_us", "p99_type_us", "wall_s", "edges",
+                "edges_per_s", "achieved_rate", "launches")
+        out[str(rate)] = {"requests": nreq, "batched": {k: a[k] for k in keep},
+                          "one_job_per_launch": {k: b[k] for k in keep},
+                          "plain_requests": min(nreq, plain_cap)}
+    return out
+
+
 def cpu_baseline(gdir, mode, n, length, seed, budget_s=12.0):
     import oracle
     oracle.lib()
@@ -321,7 +459,7 @@ def main():
     import grass_b200 as G
 
     only = set(args.only.split(",")) if args.only else {"rw", "khop", "decode", "csr", "e2e",
-                                                         "cpu"}
+                                                         "cpu", "batch", "serve"}
     gdir, meta = build_graph(args.scale, args.edge_factor)
     n, E = meta["n"], meta["num_edges"]
     W, L = args.walkers, args.length
@@ -408,6 +546,20 @@ def main():
         del rp_d, cl_d
 
     clk = clocks.stop()
+
+    # ---- batched uneven jobs and the serving loop (R-MAT s24 ef16), 1 GPU runs
+    if ws == 1 and ({"batch", "serve"} & only):
+        bdir, bmeta = build_graph(24, 16)
+        bgraphs = {m: G.Graph(os.path.join(bdir, m), m, device=local) for m in ("LE", "GT")}
+        bn = bmeta["n"]
+        extra = {"graph": f"R-MAT scale 24 edge factor 16 seed 42, graph_sort (undirected): "
+                          f"{bn} vertices, {bmeta['num_edges']} directed edges"}
+        if "batch" in only:
+            extra["batch"] = batch_bench(G, torch, bgraphs, bn, stream, flush, 5, 3)
+        if "serve" in only:
+            extra["serve"] = serve_bench(G, bgraphs[args.mode])
+        out["batched_jobs_and_serving"] = extra
+        del bgraphs
 
     # ---- accounting for the roofline of the headline kernel
     acct = torch.zeros(3, dtype=torch.int64, device=dev)

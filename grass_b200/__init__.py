@@ -14,6 +14,7 @@ Reference interface mirrored (calla212/GraSS):
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -97,6 +98,65 @@ class BatchConfig(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("scratch_budget", C.c_uint64), ("target_draws", C.c_uint64),
+                ("staging_bytes", C.c_uint64), ("window_min_us", C.c_uint32), ("window_max_us", C.c_uint32),
+                ("max_inflight", C.c_uint32), ("max_batch_jobs", C.c_uint32),
+                ("batch", BatchConfig), ("reserved", C.c_uint32 * 4)]
+
+
+class Request(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("count", C.c_uint32), ("seed", C.c_uint64),
+                ("input", C.c_void_p), ("length", C.c_uint32), ("layout", C.c_uint32),
+                ("hops", C.c_uint32), ("fanouts", C.c_uint32 * MAX_HOPS),
+                ("walkers", C.c_uint32), ("steps", C.c_uint32), ("select", C.c_uint32)]
+
+
+class Result(C.Structure):
+    _fields_ = [("status", C.c_int), ("n_outputs", C.c_uint32),
+                ("out", C.c_void_p * MAX_HOPS), ("out_words", C.c_uint64 * MAX_HOPS),
+                ("edges", C.c_uint64), ("submit_us", C.c_double), ("launch_us", C.c_double),
+                ("done_us", C.c_double), ("batch", C.c_uint64)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "rejected", "failed",
+                                          "batches", "edges", "waiting", "running",
+                                          "scratch_in_use", "scratch_peak")] + \
+               [("busy_us", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LoadgenConfig(C.Structure):
+    _fields_ = [("rate", C.c_double), ("requests", C.c_uint32), ("mode", C.c_uint32),
+                ("seed", C.c_uint64), ("pct_rw", C.c_uint32), ("pct_khop", C.c_uint32),
+                ("size_mu", C.c_double), ("size_sigma", C.c_double), ("size_max", C.c_uint32),
+                ("rw_len_min", C.c_uint32), ("rw_len_max", C.c_uint32),
+                ("n_fanouts", C.c_uint32), ("fanouts", (C.c_uint32 * 4) * 8),
+                ("mrw_samples", C.c_uint32), ("mrw_walkers", C.c_uint32),
+                ("mrw_steps", C.c_uint32), ("mrw_select", C.c_uint32),
+                ("timeout_ms", C.c_uint32), ("server", ServerConfig)]
+
+
+class LoadgenReport(C.Structure):
+    _fields_ = [("completed", C.c_uint64), ("rejected", C.c_uint64), ("failed", C.c_uint64),
+                ("batches", C.c_uint64), ("p50_us", C.c_double), ("p99_us", C.c_double),
+                ("p999_us", C.c_double), ("mean_us", C.c_double), ("max_us", C.c_double),
+                ("p50_type_us", C.c_double * 3), ("p99_type_us", C.c_double * 3),
+                ("wall_s", C.c_double), ("edges", C.c_double), ("edges_per_s", C.c_double),
+                ("offered_rate", C.c_double), ("achieved_rate", C.c_double),
+                ("launches", C.c_uint64)]
+
+    def as_dict(self):
+        d = {}
+        for k, _ in self._fields_:
+            v = getattr(self, k)
+            d[k] = list(v) if k.endswith("type_us") else v
+        return d
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -151,6 +211,14 @@ def _load():
         "grass_batch_autotune": ([P, P, C.POINTER(BatchConfig), C.POINTER(C.c_float)], i32),
         "grass_batch_info": ([P, P, P], i32),
         "grass_batch_destroy": ([P], i32),
+        "grass_server_create": ([P, C.POINTER(ServerConfig), PP], i32),
+        "grass_server_submit": ([P, C.POINTER(Request), C.POINTER(u64)], i32),
+        "grass_server_poll": ([P, u64, C.POINTER(i32)], i32),
+        "grass_server_wait": ([P, u64, u32, C.POINTER(Result)], i32),
+        "grass_server_release": ([P, u64], i32),
+        "grass_server_stats_get": ([P, C.POINTER(ServerStats)], i32),
+        "grass_server_destroy": ([P, u32], i32),
+        "grass_loadgen_run": ([P, C.POINTER(LoadgenConfig), C.POINTER(LoadgenReport)], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)
@@ -491,6 +559,131 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def _request(type_, count, seed, inp, **kw) -> tuple[Request, object]:
+    r = Request(type=type_, count=count, seed=seed)
+    keep = None
+    if inp is not None:
+        keep = np.ascontiguousarray(inp, dtype=np.uint32)
+        r.input = keep.ctypes.data
+    for k, v in kw.items():
+        if k == "fanouts":
+            r.hops = len(v)
+            for h, f in enumerate(v):
+                r.fanouts[h] = int(f)
+        else:
+            setattr(r, k, v)
+    return r, keep
+
+
+class Server:
+    """Serving loop over a resident graph: submit requests from any thread,
+    a dispatcher batches them into persistent launches."""
+
+    def __init__(self, graph: "Graph", **cfg):
+        self._g = graph
+        self._h = C.c_void_p()
+        c = ServerConfig()
+        for k, v in cfg.items():
+            if k == "batch":
+                c.batch = BatchConfig(**v)
+            else:
+                setattr(c, k, v)
+        _check(lib.grass_server_create(graph.handle, C.byref(c), C.byref(self._h)))
+
+    def submit(self, r: Request) -> int:
+        t = C.c_uint64()
+        _check(lib.grass_server_submit(self._h, C.byref(r), C.byref(t)))
+        return t.value
+
+    def submit_rw(self, starts, length: int, seed: int, layout: int = LAYOUT_WALK_MAJOR) -> int:
+        r, _ = _request(JOB_RW, len(starts), seed, starts, length=length, layout=layout)
+        return self.submit(r)
+
+    def submit_khop(self, seeds, fanouts, seed: int) -> int:
+        r, _ = _request(JOB_KHOP, len(seeds), seed, seeds, fanouts=fanouts)
+        return self.submit(r)
+
+    def submit_mrw(self, samples: int, walkers: int, steps: int, seed: int,
+                   select: int = SELECT_UNIFORM, roots=None) -> int:
+        r, _ = _request(JOB_MRW, samples, seed, roots, walkers=walkers, steps=steps,
+                        select=select)
+        return self.submit(r)
+
+    def poll(self, ticket: int) -> bool:
+        d = C.c_int()
+        _check(lib.grass_server_poll(self._h, ticket, C.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket: int, timeout_ms: int = 60000, release: bool = True) -> dict:
+        """Result as {'outputs': [np.uint32 arrays], 'edges', 'submit_us', ...}."""
+        res = Result()
+        rc = lib.grass_server_wait(self._h, ticket, timeout_ms, C.byref(res))
+        if rc == E_TIMEOUT:
+            raise GrassError(rc, last_error())
+        out = {"status": res.status, "edges": res.edges, "submit_us": res.submit_us,
+               "launch_us": res.launch_us, "done_us": res.done_us, "batch": res.batch,
+               "outputs": []}
+        for k in range(res.n_outputs):
+            n = res.out_words[k]
+            buf = (C.c_uint32 * n).from_address(res.out[k]) if n else None
+            out["outputs"].append(np.ctypeslib.as_array(buf).copy() if n
+                                  else np.zeros(0, np.uint32))
+        if release:
+            _check(lib.grass_server_release(self._h, ticket))
+        _check(rc)
+        return out
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(lib.grass_server_stats_get(self._h, C.byref(s)))
+        return s.as_dict()
+
+    def close(self, timeout_ms: int = 60000):
+        if self._h:
+            _check(lib.grass_server_destroy(self._h, timeout_ms))
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# Request mix of the batched-jobs workload: 40% RW with length U[10, 100],
+# 40% k-hop with fanouts from {(10,5), (15,10), (25,10), (5,5,5)}, 20%
+# multi-RW (one sample of 2000 walkers, 10,000 steps, degree-proportional);
+# RW walkers and k-hop seeds ~ lognormal(ln 1024, 1.5) clipped to [1, 65536].
+MIX_FANOUTS = [(10, 5), (15, 10), (25, 10), (5, 5, 5)]
+
+
+def loadgen(graph: "Graph", rate: float, requests: int, mode: int = 0, seed: int = 1,
+            pct_rw: int = 40, pct_khop: int = 40, size_mu: float = math.log(1024),
+            size_sigma: float = 1.5, size_max: int = 65536, rw_len=(10, 100),
+            fanouts=MIX_FANOUTS, mrw_samples: int = 1, mrw_walkers: int = 2000,
+            mrw_steps: int = 10000, mrw_select: int = SELECT_DEGREE, timeout_ms: int = 0,
+            **server) -> dict:
+    """Open-loop Poisson run of the request mix; mode 0 batched server,
+    mode 1 one standalone launch per request."""
+    c = LoadgenConfig(rate=rate, requests=requests, mode=mode, seed=seed, pct_rw=pct_rw,
+                      pct_khop=pct_khop, size_mu=size_mu, size_sigma=size_sigma,
+                      size_max=size_max, rw_len_min=rw_len[0], rw_len_max=rw_len[1],
+                      n_fanouts=len(fanouts), mrw_samples=mrw_samples,
+                      mrw_walkers=mrw_walkers, mrw_steps=mrw_steps, mrw_select=mrw_select,
+                      timeout_ms=timeout_ms)
+    for i, f in enumerate(fanouts):
+        for h, x in enumerate(f):
+            c.fanouts[i][h] = int(x)
+    for k, v in server.items():
+        if k == "batch":
+            c.server.batch = BatchConfig(**v)
+        else:
+            setattr(c.server, k, v)
+    r = LoadgenReport()
+    _check(lib.grass_loadgen_run(graph.handle, C.byref(c), C.byref(r)))
+    return r.as_dict()
 
 
 def uniform_starts_device(n: int, count: int, seed: int, out, stream=None):

@@ -38,8 +38,9 @@ void split_job(const grass_job &j, uint32_t ji, const grass_batch_config &c,
                std::vector<BatchTask> &rw);
 
 // Launches the persistent kernel over ntasks work items (queue must be zero).
+// Corrupt payloads set bit 0 of *d_err.
 int launch_batch(const grass_graph *g, const BatchJob *d_jobs, const BatchTask *d_tasks,
                  uint32_t ntasks, unsigned int *d_queue, unsigned long long *d_total,
-                 cudaStream_t s, const grass_batch_config &c);
+                 unsigned int *d_err, cudaStream_t s, const grass_batch_config &c);
 
 }  // namespace grass

@@ -135,7 +135,7 @@ void split_job(const grass_job &j, uint32_t ji, const grass_batch_config &c,
 
 int launch_batch(const grass_graph *g, const BatchJob *d_jobs, const BatchTask *d_tasks,
                  uint32_t ntasks, unsigned int *d_queue, unsigned long long *d_total,
-                 cudaStream_t s, const grass_batch_config &c) {
+                 unsigned int *d_err, cudaStream_t s, const grass_batch_config &c) {
   BatchKernel k = pick_kernel(g->mode, c.depth);
   const int threads = 32 * (int)c.warps_per_block;
   int per_sm = 0;
@@ -144,7 +144,7 @@ int launch_batch(const grass_graph *g, const BatchJob *d_jobs, const BatchTask *
   const uint64_t need = (ntasks + c.warps_per_block - 1) / c.warps_per_block;
   const unsigned grid = (unsigned)std::max<uint64_t>(
       1, std::min<uint64_t>(need, (uint64_t)sm_count(g->device) * per_sm));
-  k<<<grid, threads, 0, s>>>(g->view(), d_jobs, d_tasks, ntasks, d_queue, d_total, g->d_err);
+  k<<<grid, threads, 0, s>>>(g->view(), d_jobs, d_tasks, ntasks, d_queue, d_total, d_err);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "batch kernel launch");
 }
@@ -248,7 +248,8 @@ int enqueue(grass_batch *b, cudaStream_t s, unsigned long long *total) {
                                cudaMemcpyDeviceToDevice, s));
   GRASS_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned int), s));
   if (!b->ntasks) return GRASS_OK;
-  return launch_batch(b->g, b->d_jobs, b->d_tasks, b->ntasks, b->d_queue, total, s, c);
+  return launch_batch(b->g, b->d_jobs, b->d_tasks, b->ntasks, b->d_queue, total, b->g->d_err, s,
+                      c);
 }
 
 int check_job(const grass_graph *g, const grass_job *j) {

@@ -310,6 +310,128 @@ int grass_batch_info(const grass_batch *b, uint64_t *jobs, uint64_t *work_items)
 int grass_batch_destroy(grass_batch *b);
 
 /* =========================================================================
+ * Serving loop (no reference counterpart: the reference runs one app per
+ * process, GT/src/main.cu:28-50).  The graph stays resident; requests are
+ * submitted from any thread and a dispatcher thread groups them into batches
+ * of the persistent kernel above.
+ *
+ * Admission: a request's device scratch (input, outputs, multi-RW state) is
+ * reserved when its batch launches; launched batches never hold more than
+ * scratch_budget bytes together, and requests wait (FIFO) until it fits.  A
+ * request larger than the whole budget fails at submit with GRASS_E_BUDGET.
+ *
+ * Requests form two classes with their own queues and batches: RW and k-hop
+ * requests, and multi-RW requests (chains of dependent steps), so a short
+ * request never finishes with a long chain that shares its batch.
+ *
+ * Batching window: a batch of a class closes when a stream slot is free and
+ * either the class's oldest waiting request is window_min_us old while no
+ * batch of its class runs, window_max_us old while one does, the class's
+ * waiting work reaches target_draws sampled edges, or max_batch_jobs of its
+ * requests wait.
+ *
+ * Results are copied to pinned host memory owned by the server and stay
+ * valid until grass_server_release.  Each request's result equals the
+ * standalone call with the same parameters and seed.
+ * ========================================================================= */
+typedef struct {
+  uint64_t scratch_budget;   /* device bytes for launched requests (0: 8 GiB)         */
+  uint64_t target_draws;     /* close a batch at this much waiting work (0: 2^24)     */
+  uint64_t staging_bytes;    /* a batch holds at most this much request data unless
+                                one request is larger; 2 x max_inflight pinned host
+                                buffers of this size are made at create (0: 64 MiB) */
+  uint32_t window_min_us;    /* 0: 200                                                 */
+  uint32_t window_max_us;    /* 0: 2000                                                */
+  uint32_t max_inflight;     /* batches in flight, one stream each (0: 4, at most 8);
+                                multi-RW batches take at most half of them            */
+  uint32_t max_batch_jobs;   /* requests per batch (0: 4096)                           */
+  grass_batch_config batch;  /* kernel shape (zero fields: defaults)                   */
+  uint32_t reserved[4];
+} grass_server_config;
+
+typedef struct {
+  uint32_t type;                    /* GRASS_JOB_*                                     */
+  uint32_t count;                   /* walkers (RW), seeds (k-hop), samples (MRW)      */
+  uint64_t seed;                    /* Philox key                                      */
+  const uint32_t *input;            /* host: RW starts / k-hop seeds [count]; MRW roots
+                                       [count][walkers] or NULL to draw them from seed
+                                       as grass_mrw_roots does.  Copied at submit.     */
+  uint32_t length, layout;          /* RW                                              */
+  uint32_t hops;                    /* k-hop                                           */
+  uint32_t fanouts[GRASS_MAX_HOPS];
+  uint32_t walkers, steps, select;  /* MRW                                             */
+} grass_request;
+
+typedef struct {
+  int status;                               /* GRASS_OK or the request's error          */
+  uint32_t n_outputs;                       /* RW 1, k-hop hops, MRW 2 (src, dst)       */
+  const uint32_t *out[GRASS_MAX_HOPS];      /* host pointers, owned by the server       */
+  uint64_t out_words[GRASS_MAX_HOPS];
+  uint64_t edges;                           /* sampled edges                            */
+  double submit_us, launch_us, done_us;     /* since grass_server_create                */
+  uint64_t batch;                           /* batch sequence number                    */
+} grass_result;
+
+typedef struct {
+  uint64_t submitted, completed, rejected, failed, batches, edges;
+  uint64_t waiting, running, scratch_in_use, scratch_peak;
+  double busy_us;                           /* time with at least one batch in flight  */
+} grass_server_stats;
+
+typedef struct grass_server grass_server;
+int grass_server_create(const grass_graph *g, const grass_server_config *cfg,
+                        grass_server **out);
+/* Queues a request; *ticket identifies it.  Never blocks on the GPU. */
+int grass_server_submit(grass_server *s, const grass_request *r, uint64_t *ticket);
+/* *done = 1 once the request finished (successfully or not). */
+int grass_server_poll(grass_server *s, uint64_t ticket, int *done);
+/* Waits up to timeout_ms; GRASS_E_TIMEOUT if the request is still running.
+ * res (optional) receives the result; its status is the request's. */
+int grass_server_wait(grass_server *s, uint64_t ticket, uint32_t timeout_ms, grass_result *res);
+/* Frees a finished request's result memory. */
+int grass_server_release(grass_server *s, uint64_t ticket);
+int grass_server_stats_get(grass_server *s, grass_server_stats *st);
+/* Finishes the running batches (bounded by timeout_ms), fails waiting
+ * requests with GRASS_E_TIMEOUT and frees everything. */
+int grass_server_destroy(grass_server *s, uint32_t timeout_ms);
+
+/* Open-loop load generator for the serving loop: Poisson arrivals at `rate`
+ * requests/s; each request's type, size and parameters are drawn as below
+ * from the trace seed, and its Philox seed and start vertices from its own
+ * index.  mode 0 drives a grass_server; mode 1 serves the same trace with one
+ * standalone launch per request (grass_rw / grass_khop / grass_mrw, one
+ * stream, inputs and outputs copied per request), the plain method. */
+typedef struct {
+  double rate;                  /* requests per second                               */
+  uint32_t requests;            /* trace length                                       */
+  uint32_t mode;                /* 0 server, 1 one job per launch                     */
+  uint64_t seed;                /* trace seed                                         */
+  uint32_t pct_rw, pct_khop;    /* percent of RW and k-hop requests; the rest are MRW */
+  double size_mu, size_sigma;   /* RW walkers / k-hop seeds ~ lognormal(mu, sigma)    */
+  uint32_t size_max;            /* clipped to [1, size_max]                           */
+  uint32_t rw_len_min, rw_len_max;
+  uint32_t n_fanouts;           /* k-hop fanout sets to choose from (at most 8)       */
+  uint32_t fanouts[8][4];       /* zero-terminated                                    */
+  uint32_t mrw_samples, mrw_walkers, mrw_steps, mrw_select;
+  uint32_t timeout_ms;          /* bound on the wait for any one request              */
+  grass_server_config server;
+} grass_loadgen_config;
+
+typedef struct {
+  uint64_t completed, rejected, failed, batches;
+  double p50_us, p99_us, p999_us, mean_us, max_us;
+  double p50_type_us[3], p99_type_us[3];  /* per GRASS_JOB_* type                      */
+  double wall_s;                /* first arrival to last completion                   */
+  double edges;                 /* sampled edges of completed requests                */
+  double edges_per_s;           /* edges / wall_s                                     */
+  double offered_rate, achieved_rate;
+  uint64_t launches;            /* kernel launches of this run                        */
+} grass_loadgen_report;
+
+int grass_loadgen_run(const grass_graph *g, const grass_loadgen_config *c,
+                      grass_loadgen_report *r);
+
+/* =========================================================================
  * Uncompressed-CSR baseline with the same RNG streams (no reference
  * counterpart: the reference's NextDoor CSR loaders, GT/src/graph.hpp, are
  * never called).  Produces the same walks as the compressed sampler.
