@@ -321,11 +321,22 @@ def batch_bench(G, torch, graphs, n, stream, flush, K, W):
                     g.mrw_device(inp, j["count"], j["walkers"], j["steps"], j["seed"], outs[0],
                                  outs[1], select=j["select"], stream=stream)
         pms, ptot = timed(torch, plain, 1, 1, flush)
+        # one multi-RW chain alone (2000 walkers x 10,000 steps, degree-proportional)
+        mj = next(k for k, j in enumerate(jobs) if j["type"] == 2)
+        minp, mouts, msnap = bufs[mj]
+
+        def chain():
+            minp.copy_(msnap)
+            g.mrw_device(minp, 1, 2000, 10000, jobs[mj]["seed"], mouts[0], mouts[1], select=1,
+                         stream=stream)
+        cms, ctot = timed(torch, chain, 3, 1, flush)
         res[m] = {"makespan_ms": tot / K, "ms_min": min(ms), "ms_max": max(ms),
                   "edges_per_run": edges, "edges_per_s": edges / (tot / K / 1000.0),
                   "launches_per_run": launches, "autotune_best": best,
                   "autotune_best_ms": best_ms,
                   "makespan_rw_khop_only_ms": tot_s / K,
+                  "mrw_chain_alone_ms": ctot / 3,
+                  "mrw_step_us": ctot / 3 / 10000 * 1000,
                   "plain_one_launch_per_job_ms": ptot,
                   "speedup_vs_plain": ptot / (tot / K)}
         b.close()
@@ -356,8 +367,10 @@ def serve_bench(G, g, rates=(2000, 10000, 50000), seconds=0.2, plain_cap=1000):
         a = G.loadgen(g, float(rate), nreq, mode=0, seed=5)
         b = G.loadgen(g, float(rate), min(nreq, plain_cap), mode=1, seed=5)
         keep = ("completed", "rejected", "failed", "batches", "p50_us", "p99_us", "p999_us",
-                "mean_us", "max_us", "p50_type_us", "p99_type_us", "wall_s", "edges",
-                "edges_per_s", "achieved_rate", "launches")
+                "mean_us", "max_us", "p50_type_us", "p99_type_us", "queue_p50_us",
+                "queue_p99_us", "service_p50_us", "service_p99_us", "issue_us",
+                "staging_alloc_us", "wall_s", "edges", "edges_per_s", "achieved_rate",
+                "launches")
         out[str(rate)] = {"requests": nreq, "batched": {k: a[k] for k in keep},
                           "one_job_per_launch": {k: b[k] for k in keep},
                           "plain_requests": min(nreq, plain_cap)}

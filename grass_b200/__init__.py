@@ -123,7 +123,8 @@ class ServerStats(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("submitted", "completed", "rejected", "failed",
                                           "batches", "edges", "waiting", "running",
                                           "scratch_in_use", "scratch_peak")] + \
-               [("busy_us", C.c_double)]
+               [("busy_us", C.c_double), ("issue_us", C.c_double),
+                ("staging_alloc_us", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -145,6 +146,9 @@ class LoadgenReport(C.Structure):
                 ("batches", C.c_uint64), ("p50_us", C.c_double), ("p99_us", C.c_double),
                 ("p999_us", C.c_double), ("mean_us", C.c_double), ("max_us", C.c_double),
                 ("p50_type_us", C.c_double * 3), ("p99_type_us", C.c_double * 3),
+                ("queue_p50_us", C.c_double), ("queue_p99_us", C.c_double),
+                ("service_p50_us", C.c_double), ("service_p99_us", C.c_double),
+                ("issue_us", C.c_double), ("staging_alloc_us", C.c_double),
                 ("wall_s", C.c_double), ("edges", C.c_double), ("edges_per_s", C.c_double),
                 ("offered_rate", C.c_double), ("achieved_rate", C.c_double),
                 ("launches", C.c_uint64)]

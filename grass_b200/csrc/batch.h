@@ -12,7 +12,8 @@ struct BatchJob {
   uint32_t type, count;
   uint64_t seed;
   const uint32_t *in;
-  uint32_t *roots, *deg, *out0, *out1;
+  uint32_t *roots, *out0, *out1;
+  uint4 *wrec;  // multi-RW: count * walkers vertex records (scratch)
   unsigned long long *edges;
   uint32_t length, layout, walkers, steps, select, pad;
   KhopArgs khop;
@@ -27,9 +28,9 @@ struct BatchTask {
 // Zero fields of a config take the defaults for this decode mode.
 grass_batch_config resolve_batch_config(const grass_batch_config &c, int mode);
 
-// Fills a device job descriptor from a job (deg: multi-RW scratch, count *
-// walkers words, or null for other types).
-BatchJob make_batch_job(const grass_job &j, uint32_t *deg);
+// Fills a device job descriptor from a job (wrec: multi-RW scratch of count *
+// walkers records, or null for other types).
+BatchJob make_batch_job(const grass_job &j, uint4 *wrec);
 
 // Appends the work items of job index `ji`, split per config, to the three
 // queues (multi-RW samples, k-hop seed groups, walker tiles).

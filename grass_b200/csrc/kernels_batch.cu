@@ -45,7 +45,7 @@ __global__ void __launch_bounds__(256) batch_kernel(DevGraph g, const BatchJob *
         khop_seed_warp<MODE>(g, jb.in, jb.khop, s, my, cnt, bad);
     } else {
       for (uint64_t s = tk.begin; s < tk.end; s++)
-        mrw_warp<MODE>(g, jb.roots + s * jb.walkers, jb.deg + s * jb.walkers, jb.walkers,
+        mrw_warp<MODE>(g, jb.roots + s * jb.walkers, jb.wrec + s * jb.walkers, jb.walkers,
                        jb.steps, (int)jb.select, jb.seed, s, jb.out0, jb.out1, cnt, bad);
     }
 #pragma unroll
@@ -89,14 +89,14 @@ grass_batch_config resolve_batch_config(const grass_batch_config &c, int mode) {
   return r;
 }
 
-BatchJob make_batch_job(const grass_job &j, uint32_t *deg) {
+BatchJob make_batch_job(const grass_job &j, uint4 *wrec) {
   BatchJob bj{};
   bj.type = j.type;
   bj.count = j.count;
   bj.seed = j.seed;
   bj.in = j.d_input;
   bj.roots = j.d_roots;
-  bj.deg = deg;
+  bj.wrec = wrec;
   bj.out0 = j.d_out0;
   bj.out1 = j.d_out1;
   bj.edges = j.d_edges;
@@ -165,7 +165,7 @@ struct grass_batch {
   BatchTask *d_tasks = nullptr;
   uint32_t ntasks = 0;
   unsigned int *d_queue = nullptr;
-  std::vector<void *> owned;                      // MRW degree scratch (per build)
+  std::vector<void *> owned;                      // MRW record scratch (per build)
   std::vector<uint32_t *> snap;                   // per job: MRW start vertices as added
   std::vector<std::pair<uint32_t *, uint32_t *>> restore;  // (roots, snapshot)
   std::vector<uint64_t> restore_n;
@@ -209,15 +209,15 @@ int build(grass_batch *b) {
   std::vector<BatchTask> mrw, khop, rw;
   for (size_t i = 0; i < b->jobs.size(); i++) {
     const grass_job &j = b->jobs[i];
-    uint32_t *deg = nullptr;
+    uint4 *wrec = nullptr;
     if (j.type == GRASS_JOB_MRW) {
       const uint64_t nr = (uint64_t)j.count * j.walkers;
-      GRASS_CUDA(cudaMalloc(&deg, std::max<uint64_t>(nr, 1) * 4));
-      b->owned.push_back(deg);
+      GRASS_CUDA(cudaMalloc(&wrec, std::max<uint64_t>(nr, 1) * sizeof(uint4)));
+      b->owned.push_back(wrec);
       b->restore.push_back({j.d_roots, b->snap[i]});
       b->restore_n.push_back(nr);
     }
-    hj.push_back(make_batch_job(j, deg));
+    hj.push_back(make_batch_job(j, wrec));
     split_job(j, (uint32_t)i, c, mrw, khop, rw);
   }
   std::vector<BatchTask> tasks;  // longest chains first

@@ -355,31 +355,14 @@ __global__ void __launch_bounds__(256) khop_csr_kernel(DevCsr c, const uint32_t 
 // a Fenwick tree of degrees (degree-proportional selection) live in shared
 // memory; lane 0 runs the step chain, which is sequential by definition.
 
+// Shared-memory state of one sample: vertices (16-byte padded) + records.
 struct MrwLayout {
   uint32_t R;
-  __host__ __device__ size_t bytes_per_warp() const {
-    return ((size_t)R * 4 + 15) / 16 * 16 * 2 + ((size_t)R + 1) * 8;
-  }
+  __host__ __device__ size_t vtx_bytes() const { return ((size_t)R * 4 + 15) / 16 * 16; }
+  __host__ __device__ size_t bytes_per_warp() const { return vtx_bytes() + (size_t)R * 16; }
 };
 
-__device__ __forceinline__ void fen_add(uint64_t *fen, uint32_t R, uint32_t i, int64_t delta) {
-  for (uint32_t k = i + 1; k <= R; k += k & (0u - k)) fen[k] += (uint64_t)delta;
-}
-
-// largest k with prefix(k) <= u; the selected walker is k (0-based).
-__device__ __forceinline__ uint32_t fen_find(const uint64_t *fen, uint32_t R, uint32_t logR,
-                                             uint64_t u) {
-  uint32_t k = 0;
-  for (uint32_t step = 1u << logR; step; step >>= 1) {
-    const uint32_t nk = k + step;
-    if (nk <= R && fen[nk] <= u) {
-      k = nk;
-      u -= fen[nk];
-    }
-  }
-  return k;
-}
-
+// Multi random walk, one sample per warp, the sample's state in shared memory.
 template <int MODE>
 __global__ void __launch_bounds__(256) mrw_kernel(DevGraph g, uint32_t *__restrict__ roots,
                                                   uint64_t S, uint32_t R, uint32_t T, int select,
@@ -390,87 +373,30 @@ __global__ void __launch_bounds__(256) mrw_kernel(DevGraph g, uint32_t *__restri
   const MrwLayout lay{R};
   const int lane = threadIdx.x & 31;
   unsigned char *base = smem + (threadIdx.x >> 5) * lay.bytes_per_warp();
-  const size_t rbytes = ((size_t)R * 4 + 15) / 16 * 16;
-  uint32_t *rv = reinterpret_cast<uint32_t *>(base);
-  uint32_t *rd = reinterpret_cast<uint32_t *>(base + rbytes);
-  uint64_t *fen = reinterpret_cast<uint64_t *>(base + 2 * rbytes);
-  uint32_t logR = 0;
-  while ((1u << (logR + 1)) <= R) logR++;
+  uint32_t *vtx = reinterpret_cast<uint32_t *>(base);
+  uint4 *rec = reinterpret_cast<uint4 *>(base + lay.vtx_bytes());
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   uint64_t cnt = 0;
   bool bad = false;
   for (uint64_t s = warp; s < S; s += nwarps) {
     uint32_t *rt = roots + s * R;
-    for (uint32_t i = lane; i < R; i += 32) {
-      const uint32_t x = rt[i];
-      rv[i] = x;
-      uint32_t d = 0;
-      if (x < g.n) d = record_degree(g, x);
-      rd[i] = d;
-    }
+    for (uint32_t i = lane; i < R; i += 32) vtx[i] = rt[i];
     __syncwarp();
-    if (lane == 0) {
-      uint64_t wsum = 0;
-      if (select == GRASS_SELECT_DEGREE) {
-        for (uint32_t k = 0; k <= R; k++) fen[k] = 0;
-        for (uint32_t i = 0; i < R; i++) {
-          fen_add(fen, R, i, rd[i]);
-          wsum += rd[i];
-        }
-      }
-      for (uint32_t t = 0; t < T; t++) {
-        const u32x4 rr = philox4x32_10(seed, t, (uint32_t)s, (uint32_t)(s >> 32), TAG_MRW);
-        const uint64_t io = s * T + t;
-        uint32_t x;
-        if (select == GRASS_SELECT_DEGREE) {
-          if (wsum == 0) {
-            src[io] = INVALID_VERTEX;
-            dst[io] = INVALID_VERTEX;
-            continue;
-          }
-          const uint64_t r64 = ((uint64_t)rr.z << 32) | rr.x;
-          x = fen_find(fen, R, logR, mulhi_u64(r64, wsum));
-        } else {
-          x = mulhi_u32(rr.x, R);
-        }
-        const uint32_t v = rv[x];
-        src[io] = v;
-        if (rd[x] == 0) {
-          dst[io] = INVALID_VERTEX;
-          continue;
-        }
-        const VHdr h = header<MODE>(g, v);
-        uint32_t nv = neighbor<MODE>(g, h, mulhi_u32(rr.y, h.d));
-        if (nv >= g.n) {
-          bad = true;
-          dst[io] = INVALID_VERTEX;
-          continue;
-        }
-        dst[io] = nv;
-        cnt++;
-        rv[x] = nv;
-        const uint32_t nd = record_degree(g, nv);
-        if (select == GRASS_SELECT_DEGREE) {
-          fen_add(fen, R, x, (int64_t)nd - (int64_t)rd[x]);
-          wsum = wsum - rd[x] + nd;
-        }
-        rd[x] = nd;
-      }
-    }
+    mrw_warp<MODE>(g, vtx, rec, R, T, select, seed, s, src, dst, cnt, bad);
     __syncwarp();
-    for (uint32_t i = lane; i < R; i += 32) rt[i] = rv[i];
+    for (uint32_t i = lane; i < R; i += 32) rt[i] = vtx[i];
     __syncwarp();
   }
   warp_add_u64(edges, cnt);
   if (bad && err) atomicOr(err, 1u);
 }
 
-// Multi random walk with the walkers' state in global memory (mrw_warp): any
-// number of walkers per sample; deg is S*R scratch.
+// Same with the state in global memory (roots in place, rec = S*R records of
+// scratch): any number of walkers per sample.
 template <int MODE>
 __global__ void __launch_bounds__(256) mrw_global_kernel(DevGraph g, uint32_t *__restrict__ roots,
-                                                         uint32_t *__restrict__ deg, uint64_t S,
+                                                         uint4 *__restrict__ rec, uint64_t S,
                                                          uint32_t R, uint32_t T, int select,
                                                          uint64_t seed, uint32_t *__restrict__ src,
                                                          uint32_t *__restrict__ dst,
@@ -481,7 +407,7 @@ __global__ void __launch_bounds__(256) mrw_global_kernel(DevGraph g, uint32_t *_
   uint64_t cnt = 0;
   bool bad = false;
   for (uint64_t s = warp; s < S; s += nwarps)
-    mrw_warp<MODE>(g, roots + s * R, deg + s * R, R, T, select, seed, s, src, dst, cnt, bad);
+    mrw_warp<MODE>(g, roots + s * R, rec + s * R, R, T, select, seed, s, src, dst, cnt, bad);
   warp_add_u64(edges, cnt);
   if (bad && err) atomicOr(err, 1u);
 }
@@ -715,17 +641,16 @@ int launch_mrw(const DevGraph &g, const grass_mrw_params &p, uint32_t *roots, ui
   const MrwLayout lay{p.walkers};
   const size_t per_warp = lay.bytes_per_warp();
   if (per_warp > 48 * 1024) {
-    // Too many walkers for a shared-memory Fenwick tree per warp: keep the
-    // walkers' degrees in global scratch (mrw_warp).
-    uint32_t *deg = nullptr;
-    cudaError_t e = cudaMallocAsync(&deg, S * (uint64_t)p.walkers * sizeof(uint32_t), s);
+    // Too many walkers for shared memory: the state lives in global scratch.
+    uint4 *rec = nullptr;
+    cudaError_t e = cudaMallocAsync(&rec, S * (uint64_t)p.walkers * sizeof(uint4), s);
     if (e != cudaSuccess) return cuda_fail(e, "multi-RW scratch");
     auto kern = g.mode == GRASS_MODE_GT ? mrw_global_kernel<0> : mrw_global_kernel<1>;
-    kern<<<grid_warps(S, 8, cur_dev(), 8), 256, 0, s>>>(g, roots, deg, S, p.walkers, p.steps,
+    kern<<<grid_warps(S, 8, cur_dev(), 8), 256, 0, s>>>(g, roots, rec, S, p.walkers, p.steps,
                                                         (int)p.select, p.seed, src, dst, edges,
                                                         err);
     count_launch();
-    cudaFreeAsync(deg, s);
+    cudaFreeAsync(rec, s);
     return GRASS_OK;
   }
   const size_t budget = 200 * 1024;

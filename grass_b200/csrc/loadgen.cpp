@@ -94,7 +94,8 @@ double pct(std::vector<double> v, double p) {
 
 struct Outcome {
   std::vector<double> lat[3];
-  std::vector<double> all;
+  std::vector<double> all, queue, service;
+  double issue_us = 0, alloc_us = 0;
   double edges = 0, first = 1e300, last = 0;
   uint64_t completed = 0, rejected = 0, failed = 0;
 };
@@ -117,6 +118,12 @@ void finish_report(const grass_loadgen_config &c, const Outcome &o, grass_loadge
     r->p50_type_us[t] = pct(o.lat[t], 0.50);
     r->p99_type_us[t] = pct(o.lat[t], 0.99);
   }
+  r->queue_p50_us = pct(o.queue, 0.50);
+  r->queue_p99_us = pct(o.queue, 0.99);
+  r->service_p50_us = pct(o.service, 0.50);
+  r->service_p99_us = pct(o.service, 0.99);
+  r->issue_us = o.issue_us;
+  r->staging_alloc_us = o.alloc_us;
   r->wall_s = o.last > o.first ? (o.last - o.first) * 1e-6 : 0;
   r->edges = o.edges;
   r->edges_per_s = r->wall_s > 0 ? o.edges / r->wall_s : 0;
@@ -165,6 +172,8 @@ int run_server(const grass_graph *g, const grass_loadgen_config &c, std::vector<
         const double l = res.done_us - res.submit_us + lag[i];
         o.all.push_back(l);
         o.lat[std::min<uint32_t>(tr[i].rq.type, 2)].push_back(l);
+        o.queue.push_back(res.launch_us - res.submit_us + lag[i]);
+        o.service.push_back(res.done_us - res.launch_us);
         o.edges += (double)res.edges;
         o.completed++;
         o.last = std::max(o.last, submit_at[i] + (res.done_us - res.submit_us));
@@ -191,6 +200,8 @@ int run_server(const grass_graph *g, const grass_loadgen_config &c, std::vector<
   grass_server_stats st;
   grass_server_stats_get(srv, &st);
   batches = st.batches;
+  o.issue_us = st.issue_us;
+  o.alloc_us = st.staging_alloc_us;
   return grass_server_destroy(srv, c.timeout_ms);
 }
 

@@ -193,107 +193,128 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
   }
 }
 
-// Multi random walk of one sample (MultiRWApp, GT/src/apps/multiRW/multiRW.cu:3-112):
-// R walkers whose vertices live in roots[0..R) (updated in place) and whose
-// degrees live in deg[0..R) (scratch).  Lane j keeps the total degree of
-// walkers [j*B, (j+1)*B), B = ceil(R/32); a degree-proportional pick scans
-// the 32 bucket sums with shuffles, then the chosen bucket with up to two
-// more 32-wide scans.  Step t draws from Philox(seed; t, sample, .., TAG_MRW):
-// word 0 (+ word 2 as high half) picks the walker, word 1 the neighbor.
+// Multi random walk of one sample (MultiRWApp, GT/src/apps/multiRW/multiRW.cu:3-112).
+// The sample's state is vtx[0..R), the walkers' vertices (updated in place),
+// and rec[0..R), each walker's 16-byte vertex record (all zero for a vertex
+// out of range), in shared or global memory.  Keeping the record makes a
+// step cost two dependent DRAM reads (payload, then the new vertex's record)
+// instead of three.  Lane j keeps the total degree of walkers [j*B, (j+1)*B),
+// B = ceil(R/32); a degree-proportional pick scans the 32 bucket sums with
+// shuffles, then the chosen bucket 32 entries at a time.  Step t draws from
+// Philox(seed; t, sample, .., TAG_MRW): word 0 (+ word 2 as high half) picks
+// the walker, word 1 the neighbor.  Lane k computes the block of step
+// t0 + k, so one Philox evaluation per lane serves 32 steps.
 template <int MODE>
-__device__ __forceinline__ void mrw_warp(const DevGraph &g, uint32_t *roots, uint32_t *deg,
-                                         uint32_t R, uint32_t T, int select, uint64_t seed,
-                                         uint64_t sample, uint32_t *src, uint32_t *dst,
-                                         uint64_t &cnt, bool &bad) {
+__device__ __forceinline__ void mrw_warp(const DevGraph &g, uint32_t *vtx, uint4 *rec, uint32_t R,
+                                         uint32_t T, int select, uint64_t seed, uint64_t sample,
+                                         uint32_t *src, uint32_t *dst, uint64_t &cnt, bool &bad) {
   const int lane = threadIdx.x & 31;
   const uint32_t B = (R + 31) / 32;
-  uint64_t bsum = 0;  // this lane's bucket
-  for (uint32_t i = lane * B; i < min(R, (lane + 1) * B); i++) {
-    const uint32_t x = roots[i];
-    const uint32_t d = x < g.n ? record_degree(g, x) : 0u;
-    deg[i] = d;
-    bsum += d;
+  // Records of the start vertices: four independent loads in flight per lane.
+  for (uint32_t c0 = 0; c0 < R; c0 += 128) {
+    uint4 r[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint32_t i = c0 + k * 32 + lane;
+      const uint32_t x = i < R ? vtx[i] : INVALID_VERTEX;
+      r[k] = x < g.n ? load_record(g.recs + x) : make_uint4(0u, 0u, 0u, 0u);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      const uint32_t i = c0 + k * 32 + lane;
+      if (i < R) rec[i] = r[k];
+    }
   }
+  __syncwarp();
+  uint64_t bsum = 0;  // this lane's bucket
+  for (uint32_t i = lane * B; i < min(R, (lane + 1) * B); i++) bsum += rec[i].z;
   uint64_t wsum = bsum;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) wsum += __shfl_xor_sync(kFull, wsum, o);
-  __syncwarp();
-  for (uint32_t t = 0; t < T; t++) {
-    const u32x4 rr = philox4x32_10(seed, t, (uint32_t)sample, (uint32_t)(sample >> 32), TAG_MRW);
-    const uint64_t io = sample * T + t;
-    uint32_t x;
-    if (select == GRASS_SELECT_DEGREE) {
-      if (wsum == 0) {
-        if (lane == 0) {
-          src[io] = INVALID_VERTEX;
-          dst[io] = INVALID_VERTEX;
+  for (uint32_t t0 = 0; t0 < T; t0 += 32) {
+    const u32x4 mine =
+        philox4x32_10(seed, t0 + lane, (uint32_t)sample, (uint32_t)(sample >> 32), TAG_MRW);
+    const uint32_t tn = min(32u, T - t0);
+    for (uint32_t k = 0; k < tn; k++) {
+      const uint32_t rx = __shfl_sync(kFull, mine.x, k), ry = __shfl_sync(kFull, mine.y, k),
+                     rz = __shfl_sync(kFull, mine.z, k);
+      const uint64_t io = sample * T + t0 + k;
+      uint32_t x;
+      if (select == GRASS_SELECT_DEGREE) {
+        if (wsum == 0) {
+          if (lane == 0) {
+            src[io] = INVALID_VERTEX;
+            dst[io] = INVALID_VERTEX;
+          }
+          continue;
         }
-        continue;
-      }
-      const uint64_t u = mulhi_u64(((uint64_t)rr.z << 32) | rr.x, wsum);
-      // bucket: first lane whose inclusive prefix exceeds u
-      uint64_t incl = bsum;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint64_t y = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += y;
-      }
-      const int Lb = __ffs(__ballot_sync(kFull, incl > u)) - 1;
-      uint64_t acc = __shfl_sync(kFull, incl - bsum, Lb);  // prefix before the bucket
-      const uint32_t b0 = (uint32_t)Lb * B, b1 = min(R, b0 + B);
-      x = b1 - 1;
-      for (uint32_t c0 = b0; c0 < b1; c0 += 32) {  // at most two passes for R <= 2048
-        const uint32_t i = c0 + lane;
-        const uint64_t d = i < b1 ? deg[i] : 0u;
-        uint64_t ci = d;
+        const uint64_t u = mulhi_u64(((uint64_t)rz << 32) | rx, wsum);
+        // bucket: first lane whose inclusive prefix exceeds u
+        uint64_t incl = bsum;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-          const uint64_t y = __shfl_up_sync(kFull, ci, o);
-          if (lane >= o) ci += y;
+          const uint64_t y = __shfl_up_sync(kFull, incl, o);
+          if (lane >= o) incl += y;
         }
-        const unsigned hit = __ballot_sync(kFull, i < b1 && acc + ci > u);
-        if (hit) {
-          x = c0 + (uint32_t)(__ffs(hit) - 1);
-          break;
+        const int Lb = __ffs(__ballot_sync(kFull, incl > u)) - 1;
+        uint64_t acc = __shfl_sync(kFull, incl - bsum, Lb);  // prefix before the bucket
+        const uint32_t b0 = (uint32_t)Lb * B, b1 = min(R, b0 + B);
+        x = b1 - 1;
+        for (uint32_t c0 = b0; c0 < b1; c0 += 32) {  // two passes for R <= 2048
+          const uint32_t i = c0 + lane;
+          const uint64_t d = i < b1 ? rec[i].z : 0u;
+          uint64_t ci = d;
+#pragma unroll
+          for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t y = __shfl_up_sync(kFull, ci, o);
+            if (lane >= o) ci += y;
+          }
+          const unsigned hit = __ballot_sync(kFull, i < b1 && acc + ci > u);
+          if (hit) {
+            x = c0 + (uint32_t)(__ffs(hit) - 1);
+            break;
+          }
+          acc += __shfl_sync(kFull, ci, 31);
         }
-        acc += __shfl_sync(kFull, ci, 31);
-      }
-    } else {
-      x = mulhi_u32(rr.x, R);
-    }
-    // lane 0 moves walker x
-    uint32_t nd = 0, od = 0;
-    bool moved = false;
-    if (lane == 0) {
-      const uint32_t v = roots[x];
-      od = deg[x];
-      src[io] = v;
-      if (od == 0) {
-        dst[io] = INVALID_VERTEX;
       } else {
-        const VHdr h = header<MODE>(g, v);
-        const uint32_t nv = neighbor<MODE>(g, h, mulhi_u32(rr.y, h.d));
-        if (nv >= g.n) {
-          bad = true;
+        x = mulhi_u32(rx, R);
+      }
+      // lane 0 moves walker x
+      uint32_t nd = 0, od = 0;
+      bool moved = false;
+      if (lane == 0) {
+        const uint32_t v = vtx[x];
+        const uint4 r = rec[x];
+        od = r.z;
+        src[io] = v;
+        if (od == 0) {
           dst[io] = INVALID_VERTEX;
         } else {
-          dst[io] = nv;
-          cnt++;
-          roots[x] = nv;
-          nd = record_degree(g, nv);
-          deg[x] = nd;
-          moved = true;
+          const VHdr h = record_header<MODE>(r, v);
+          const uint32_t nv = neighbor<MODE>(g, h, mulhi_u32(ry, h.d));
+          if (nv >= g.n) {
+            bad = true;
+            dst[io] = INVALID_VERTEX;
+          } else {
+            dst[io] = nv;
+            cnt++;
+            const uint4 nr = load_record(g.recs + nv);
+            vtx[x] = nv;
+            rec[x] = nr;
+            nd = nr.z;
+            moved = true;
+          }
         }
       }
+      moved = __shfl_sync(kFull, moved, 0);
+      if (moved) {
+        nd = __shfl_sync(kFull, nd, 0);
+        od = __shfl_sync(kFull, od, 0);
+        if (lane == (int)(x / B)) bsum = bsum - od + nd;
+        wsum = wsum - od + nd;
+      }
+      __syncwarp();
     }
-    moved = __shfl_sync(kFull, moved, 0);
-    if (moved) {
-      nd = __shfl_sync(kFull, nd, 0);
-      od = __shfl_sync(kFull, od, 0);
-      if (lane == (int)(x / B)) bsum = bsum - od + nd;
-      wsum = wsum - od + nd;
-    }
-    __syncwarp();
   }
 }
 

@@ -20,7 +20,7 @@
 // 0-based walker / seed / sample ids, so its output is the standalone call's.
 //
 // Device block of one batch (every part 256-byte aligned):
-//   [multi-RW degree scratch] | H2D: [jobs][work items][queue][inputs]
+//   [multi-RW record scratch] | H2D: [jobs][work items][queue][inputs]
 //   | H2D+D2H: [edges u64 x jobs][error word] | D2H: [outputs]
 #include <algorithm>
 #include <chrono>
@@ -50,7 +50,8 @@ struct PinnedPool {
   std::multimap<uint64_t, void *> free_;
   std::vector<void *> all;
 
-  void *get(uint64_t bytes, uint64_t &cap) {
+  // alloc_us accumulates the time spent in cudaHostAlloc.
+  void *get(uint64_t bytes, uint64_t &cap, double &alloc_us) {
     // Capacities 2^k * {4, 5, 6, 7} / 4 (at most 25% slack), 1 MiB at least.
     uint64_t p2 = 1ull << 20;
     while (p2 * 2 <= bytes) p2 <<= 1;
@@ -67,7 +68,11 @@ struct PinnedPool {
       }
     }
     void *p = nullptr;
-    if (cudaHostAlloc(&p, cap, cudaHostAllocDefault) != cudaSuccess) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const cudaError_t e = cudaHostAlloc(&p, cap, cudaHostAllocDefault);
+    alloc_us +=
+        std::chrono::duration<double, std::micro>(std::chrono::steady_clock::now() - t0).count();
+    if (e != cudaSuccess) {
       cudaGetLastError();
       return nullptr;
     }
@@ -199,7 +204,7 @@ int size_request(const grass_request &r, Req &q) {
       if (!r.walkers || r.select > 1 || r.steps > (1u << 28))
         return set_error(GRASS_E_ARG, "multi-RW request: bad arguments");
       q.in_words = c * r.walkers;
-      q.deg_words = c * r.walkers;
+      q.deg_words = 4 * c * r.walkers;  // one 16-byte record per walker
       q.nout = 2;
       q.out_words[0] = q.out_words[1] = c * (uint64_t)r.steps;
       q.draws = c * (uint64_t)r.steps;
@@ -349,10 +354,12 @@ void grass_server::launch(Batch *b) {
 
   int rc = GRASS_OK;
   uint8_t *d = nullptr;
+  const double t_issue = now_us();
+  double t_alloc = 0;
   {
     DeviceGuard dg(g->device);
-    b->in_host = pinned.get(b->h2d_bytes, b->in_cap);
-    b->out_host = pinned.get(b->d2h_bytes, b->out_cap);
+    b->in_host = pinned.get(b->h2d_bytes, b->in_cap, t_alloc);
+    b->out_host = pinned.get(b->d2h_bytes, b->out_cap, t_alloc);
     if (!b->in_host || !b->out_host) rc = set_error(GRASS_E_OOM, "pinned staging allocation failed");
     cudaError_t e = cudaSuccess;
     if (!rc) e = cudaMallocFromPoolAsync((void **)&d, std::max<uint64_t>(total, kAlign), pool, s);
@@ -385,7 +392,7 @@ void grass_server::launch(Batch *b) {
           j.d_out0 = outs[0];
           j.d_out1 = outs[1];
         }
-        jobs[i] = make_batch_job(j, reinterpret_cast<uint32_t *>(d + deg_off[i]));
+        jobs[i] = make_batch_job(j, reinterpret_cast<uint4 *>(d + deg_off[i]));
         if (!q->draw_roots && q->in_words)
           memcpy(h + in_off[i], q->input.data(), q->in_words * 4);
       }
@@ -419,6 +426,11 @@ void grass_server::launch(Batch *b) {
       e = cudaLaunchHostFunc(s, on_batch_done, b);
       if (e != cudaSuccess) rc = cuda_fail(e, "server completion callback");
     }
+  }
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    st.issue_us += now_us() - t_issue;
+    st.staging_alloc_us += t_alloc;
   }
   if (rc) {
     // Nothing will call back: wait for what was queued, then fail the batch.
@@ -548,7 +560,8 @@ int grass_server_create(const grass_graph *g, const grass_server_config *cfg,
     std::vector<std::pair<void *, uint64_t>> pre;
     for (uint32_t i = 0; i < 2 * c.max_inflight; i++) {
       uint64_t cap = 0;
-      void *p = s->pinned.get(c.staging_bytes + (1ull << 20), cap);
+      double t = 0;
+      void *p = s->pinned.get(c.staging_bytes + (1ull << 20), cap, t);
       if (p) pre.emplace_back(p, cap);
     }
     for (auto &pc : pre) s->pinned.put(pc.first, pc.second);

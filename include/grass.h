@@ -376,6 +376,8 @@ typedef struct {
   uint64_t submitted, completed, rejected, failed, batches, edges;
   uint64_t waiting, running, scratch_in_use, scratch_peak;
   double busy_us;                           /* time with at least one batch in flight  */
+  double issue_us;                          /* dispatcher time issuing batches         */
+  double staging_alloc_us;                  /* of which pinned staging allocation      */
 } grass_server_stats;
 
 typedef struct grass_server grass_server;
@@ -421,6 +423,9 @@ typedef struct {
   uint64_t completed, rejected, failed, batches;
   double p50_us, p99_us, p999_us, mean_us, max_us;
   double p50_type_us[3], p99_type_us[3];  /* per GRASS_JOB_* type                      */
+  double queue_p50_us, queue_p99_us;      /* arrival to launch (server mode)             */
+  double service_p50_us, service_p99_us;  /* launch to done (server mode)                */
+  double issue_us, staging_alloc_us;      /* server: dispatcher time issuing batches     */
   double wall_s;                /* first arrival to last completion                   */
   double edges;                 /* sampled edges of completed requests                */
   double edges_per_s;           /* edges / wall_s                                     */
