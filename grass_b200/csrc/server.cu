@@ -43,8 +43,67 @@ constexpr uint32_t kMaxSlots = 8;
 
 inline uint64_t align_up(uint64_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 
-// Pinned host buffers, cached by power-of-two capacity.  cudaFreeHost
-// synchronises the device, so buffers are only freed when the server ends.
+// Pinned host staging: one arena made at create (cudaHostAlloc takes
+// milliseconds per 100 MB and must not sit in a request's latency), handed
+// out first-fit from address-ordered free ranges that coalesce on return.
+struct Staging {
+  std::mutex mu;
+  uint8_t *base = nullptr;
+  uint64_t size = 0;
+  std::map<uint64_t, uint64_t> free_;  // offset -> bytes
+
+  static uint64_t round(uint64_t b) { return (std::max<uint64_t>(b, 1) + 4095) & ~4095ull; }
+  cudaError_t init(uint64_t bytes) {
+    size = round(bytes);
+    const cudaError_t e = cudaHostAlloc(&base, size, cudaHostAllocDefault);
+    if (e != cudaSuccess) {
+      base = nullptr;
+      size = 0;
+      return e;
+    }
+    free_.emplace(0, size);
+    return e;
+  }
+  // A block of at least `bytes`, or nullptr while the arena has no room.
+  void *take(uint64_t bytes) {
+    bytes = round(bytes);
+    std::lock_guard<std::mutex> lk(mu);
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second < bytes) continue;
+      const uint64_t off = it->first, len = it->second;
+      free_.erase(it);
+      if (len > bytes) free_.emplace(off + bytes, len - bytes);
+      return base + off;
+    }
+    return nullptr;
+  }
+  void give(void *p, uint64_t bytes) {
+    if (!p) return;
+    bytes = round(bytes);
+    std::lock_guard<std::mutex> lk(mu);
+    uint64_t off = static_cast<uint8_t *>(p) - base;
+    auto next = free_.lower_bound(off);
+    if (next != free_.end() && off + bytes == next->first) {
+      bytes += next->second;
+      next = free_.erase(next);
+    }
+    if (next != free_.begin()) {
+      auto prev = std::prev(next);
+      if (prev->first + prev->second == off) {
+        prev->second += bytes;
+        return;
+      }
+    }
+    free_.emplace(off, bytes);
+  }
+  ~Staging() {
+    if (base) cudaFreeHost(base);
+  }
+};
+
+// Pinned buffers for batches larger than the whole arena, cached by size
+// class.  cudaFreeHost synchronises the device, so buffers are only freed
+// when the server ends.
 struct PinnedPool {
   std::mutex mu;
   std::multimap<uint64_t, void *> free_;
@@ -102,6 +161,7 @@ struct Req {
   uint64_t out_words[GRASS_MAX_HOPS] = {0};
   uint64_t in_words = 0, deg_words = 0;
   uint64_t bytes = 0;  // device scratch without the batch's tables
+  uint64_t in_bytes = 0, out_bytes = 0;  // staging (aligned inputs, aligned outputs)
   uint64_t draws = 0;  // sampled edges at most (batch sizing)
   double t_submit = 0, t_launch = 0, t_done = 0;
   int status = GRASS_OK;
@@ -120,7 +180,8 @@ struct Batch {
   uint64_t bytes = 0;  // device block (budget charge)
   uint64_t h2d_off = 0, h2d_bytes = 0, d2h_off = 0, d2h_bytes = 0;
   void *in_host = nullptr, *out_host = nullptr;
-  uint64_t in_cap = 0, out_cap = 0;
+  uint64_t in_cap = 0, out_cap = 0;  // reserved bytes
+  bool oversize = false;             // staging from the fallback pool, not the arena
   uint32_t refs = 0;  // requests not yet released
   grass_server *srv = nullptr;
 };
@@ -138,6 +199,7 @@ struct grass_server {
   cudaMemPool_t pool = nullptr;
   cudaStream_t streams[grass::kMaxSlots] = {nullptr};
   bool slot_busy[grass::kMaxSlots] = {false};
+  grass::Staging staging;
   grass::PinnedPool pinned;
 
   std::mutex mu;
@@ -165,6 +227,16 @@ struct grass_server {
   Batch *form(double now, int cls);
   void launch(Batch *b);
   void finish(Batch *b, int status);
+  void release_in(Batch *b) {
+    if (b->oversize) pinned.put(b->in_host, b->in_cap);
+    else staging.give(b->in_host, b->in_cap);
+    b->in_host = nullptr;
+  }
+  void release_out(Batch *b) {
+    if (b->oversize) pinned.put(b->out_host, b->out_cap);
+    else staging.give(b->out_host, b->out_cap);
+    b->out_host = nullptr;
+  }
 };
 
 namespace grass {
@@ -213,9 +285,10 @@ int size_request(const grass_request &r, Req &q) {
     default:
       return set_error(GRASS_E_ARG, "unknown request type %u", r.type);
   }
-  uint64_t b = align_up(q.in_words * 4) + align_up(q.deg_words * 4);
-  for (uint32_t k = 0; k < q.nout; k++) b += align_up(q.out_words[k] * 4);
-  q.bytes = b;
+  q.in_bytes = align_up(q.in_words * 4);
+  q.out_bytes = 0;
+  for (uint32_t k = 0; k < q.nout; k++) q.out_bytes += align_up(q.out_words[k] * 4);
+  q.bytes = q.in_bytes + align_up(q.deg_words * 4) + q.out_bytes;
   return GRASS_OK;
 }
 
@@ -259,8 +332,8 @@ double grass_server::window_left(int cls, double now) const {
   return wq.front()->t_submit + window - now;
 }
 
-// Takes waiting requests of one class (FIFO) while the budget allows.
-// Called with mu held.
+// Takes waiting requests of one class (FIFO) while the device budget and
+// the staging arena allow.  Called with mu held.
 Batch *grass_server::form(double now, int cls) {
   using namespace grass;
   auto &wq = waiting[cls];
@@ -268,15 +341,18 @@ Batch *grass_server::form(double now, int cls) {
   const uint32_t slot = free_slot(cls);
   if (slot == kMaxSlots || window_left(cls, now) > 0) return nullptr;
   Batch *b = new Batch();
-  uint64_t data = 0, ntasks = 0;
+  uint64_t data = 0, ntasks = 0, sin = 0, sout = 0;
+  const uint64_t cap = staging.size / 8;  // request data per batch (one request may exceed it)
   while (!wq.empty() && b->reqs.size() < cfg.max_batch_jobs) {
     Req *q = wq.front();
     const uint64_t nt = task_bound(*q, bcfg);
     const uint64_t need = data + q->bytes + table_bytes(b->reqs.size() + 1, ntasks + nt);
     if (in_use + need > cfg.scratch_budget) break;
-    if (!b->reqs.empty() && data + q->bytes > cfg.staging_bytes) break;
+    if (!b->reqs.empty() && data + q->bytes > cap) break;
     data += q->bytes;
     ntasks += nt;
+    sin += q->in_bytes;
+    sout += q->out_bytes;
     b->reqs.push_back(q);
     wq.pop_front();
     waiting_draws[cls] -= q->draws;
@@ -284,6 +360,24 @@ Batch *grass_server::form(double now, int cls) {
   if (b->reqs.empty()) {  // the oldest request waits for scratch to free up
     delete b;
     return nullptr;
+  }
+  // Staging: tables and inputs in, counters and outputs out.
+  b->in_cap = table_bytes(b->reqs.size(), ntasks) + sin;
+  b->out_cap = align_up(b->reqs.size() * 8 + 4) + sout;
+  if (Staging::round(b->in_cap) + Staging::round(b->out_cap) > staging.size) {
+    b->oversize = true;  // a single request larger than the arena
+  } else {
+    b->in_host = staging.take(b->in_cap);
+    b->out_host = b->in_host ? staging.take(b->out_cap) : nullptr;
+    if (!b->out_host) {  // wait for releases; requests go back in order
+      staging.give(b->in_host, b->in_cap);
+      for (auto it = b->reqs.rbegin(); it != b->reqs.rend(); ++it) {
+        wq.push_front(*it);
+        waiting_draws[cls] += (*it)->draws;
+      }
+      delete b;
+      return nullptr;
+    }
   }
   b->bytes = data + table_bytes(b->reqs.size(), ntasks);
   b->slot = slot;
@@ -358,9 +452,13 @@ void grass_server::launch(Batch *b) {
   double t_alloc = 0;
   {
     DeviceGuard dg(g->device);
-    b->in_host = pinned.get(b->h2d_bytes, b->in_cap, t_alloc);
-    b->out_host = pinned.get(b->d2h_bytes, b->out_cap, t_alloc);
+    if (b->oversize) {
+      b->in_host = pinned.get(b->h2d_bytes, b->in_cap, t_alloc);
+      b->out_host = pinned.get(b->d2h_bytes, b->out_cap, t_alloc);
+    }
     if (!b->in_host || !b->out_host) rc = set_error(GRASS_E_OOM, "pinned staging allocation failed");
+    if (!rc && (b->h2d_bytes > b->in_cap || b->d2h_bytes > b->out_cap))
+      rc = set_error(GRASS_E_ARG, "internal: staging layout exceeds its reservation");
     cudaError_t e = cudaSuccess;
     if (!rc) e = cudaMallocFromPoolAsync((void **)&d, std::max<uint64_t>(total, kAlign), pool, s);
     if (e != cudaSuccess) rc = cuda_fail(e, "server scratch allocation");
@@ -449,8 +547,7 @@ void grass_server::finish(Batch *b, int status) {
   const uint8_t *out = static_cast<const uint8_t *>(b->out_host);
   if (!status && out) memcpy(&err, out + b->reqs.size() * 8, 4);
   // Before any request is marked done: a release may free the batch.
-  pinned.put(b->in_host, b->in_cap);
-  b->in_host = nullptr;
+  release_in(b);
   {
     std::lock_guard<std::mutex> lk(mu);
     for (size_t i = 0; i < b->reqs.size(); i++) {
@@ -522,7 +619,7 @@ int grass_server_create(const grass_graph *g, const grass_server_config *cfg,
   grass_server_config &c = s->cfg;
   if (!c.scratch_budget) c.scratch_budget = 8ull << 30;
   if (!c.target_draws) c.target_draws = 1ull << 24;
-  if (!c.staging_bytes) c.staging_bytes = 64ull << 20;
+  if (!c.staging_bytes) c.staging_bytes = 1ull << 30;
   if (!c.window_min_us) c.window_min_us = 200;
   if (!c.window_max_us) c.window_max_us = 2000;
   if (c.window_max_us < c.window_min_us) c.window_max_us = c.window_min_us;
@@ -554,17 +651,14 @@ int grass_server_create(const grass_graph *g, const grass_server_config *cfg,
     delete s;
     return rc;
   }
-  // Staging buffers for the first batches (cudaHostAlloc takes milliseconds
-  // per 100 MB and must not sit in a request's latency).
-  {
-    std::vector<std::pair<void *, uint64_t>> pre;
-    for (uint32_t i = 0; i < 2 * c.max_inflight; i++) {
-      uint64_t cap = 0;
-      double t = 0;
-      void *p = s->pinned.get(c.staging_bytes + (1ull << 20), cap, t);
-      if (p) pre.emplace_back(p, cap);
-    }
-    for (auto &pc : pre) s->pinned.put(pc.first, pc.second);
+  e = s->staging.init(c.staging_bytes);
+  if (e != cudaSuccess) {
+    const int rc = cuda_fail(e, "server staging arena");
+    for (auto st : s->streams)
+      if (st) cudaStreamDestroy(st);
+    cudaMemPoolDestroy(s->pool);
+    delete s;
+    return rc;
   }
   s->t0 = Clock::now();
   try {
@@ -681,8 +775,9 @@ int grass_server_release(grass_server *s, uint64_t ticket) {
     delete q;
   }
   if (free_b) {
-    s->pinned.put(free_b->out_host, free_b->out_cap);
+    s->release_out(free_b);
     delete free_b;
+    s->cv_work.notify_all();  // staging freed: a waiting batch may fit now
   }
   return GRASS_OK;
 }
@@ -735,7 +830,7 @@ int grass_server_destroy(grass_server *s, uint32_t timeout_ms) {
   for (auto &kv : s->reqs) {
     Batch *b = kv.second->batch;
     if (b && --b->refs == 0) {
-      s->pinned.put(b->out_host, b->out_cap);
+      s->release_out(b);
       delete b;
     }
     delete kv.second;
