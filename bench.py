@@ -236,7 +236,8 @@ MIX_FANOUTS = [(10, 5), (15, 10), (25, 10), (5, 5, 5)]
 def mix_jobs(n, k=256, seed=3):
     """k jobs: 40% RW (L ~ U[10,100]), 40% k-hop (fanouts from MIX_FANOUTS),
     20% multi-RW (one sample of 2000 walkers, 10,000 steps, degree-
-    proportional); RW walkers / k-hop seeds ~ lognormal(ln 1024, 1.5)
+    proportional selection in its continuous-time construction, walkers
+    moving in parallel); RW walkers / k-hop seeds ~ lognormal(ln 1024, 1.5)
     clipped to [1, 65536]."""
     rng = np.random.default_rng(seed)
     n_rw, n_kh = round(0.4 * k), round(0.4 * k)
@@ -251,7 +252,7 @@ def mix_jobs(n, k=256, seed=3):
         elif t == 1:
             j.update(count=size, fanouts=MIX_FANOUTS[int(rng.integers(0, 4))])
         else:
-            j.update(count=1, walkers=2000, steps=10000, select=1)
+            j.update(count=1, walkers=2000, steps=10000, select=2)
         jobs.append(j)
     return jobs
 
@@ -321,22 +322,25 @@ def batch_bench(G, torch, graphs, n, stream, flush, K, W):
                     g.mrw_device(inp, j["count"], j["walkers"], j["steps"], j["seed"], outs[0],
                                  outs[1], select=j["select"], stream=stream)
         pms, ptot = timed(torch, plain, 1, 1, flush)
-        # one multi-RW chain alone (2000 walkers x 10,000 steps, degree-proportional)
+        # one multi-RW sample alone (2000 walkers x 10,000 steps, degree-proportional):
+        # continuous-time (walkers in parallel) and one Philox block per step (sequential)
         mj = next(k for k, j in enumerate(jobs) if j["type"] == 2)
         minp, mouts, msnap = bufs[mj]
-
-        def chain():
-            minp.copy_(msnap)
-            g.mrw_device(minp, 1, 2000, 10000, jobs[mj]["seed"], mouts[0], mouts[1], select=1,
-                         stream=stream)
-        cms, ctot = timed(torch, chain, 3, 1, flush)
+        chain_ms = {}
+        for sel in (2, 1):
+            def chain(sel=sel):
+                minp.copy_(msnap)
+                g.mrw_device(minp, 1, 2000, 10000, jobs[mj]["seed"], mouts[0], mouts[1],
+                             select=sel, stream=stream)
+            cms, ctot = timed(torch, chain, 3, 1, flush)
+            chain_ms[sel] = ctot / 3
         res[m] = {"makespan_ms": tot / K, "ms_min": min(ms), "ms_max": max(ms),
                   "edges_per_run": edges, "edges_per_s": edges / (tot / K / 1000.0),
                   "launches_per_run": launches, "autotune_best": best,
                   "autotune_best_ms": best_ms,
                   "makespan_rw_khop_only_ms": tot_s / K,
-                  "mrw_chain_alone_ms": ctot / 3,
-                  "mrw_step_us": ctot / 3 / 10000 * 1000,
+                  "mrw_sample_alone_ms": {"continuous_time": chain_ms[2],
+                                          "sequential_steps": chain_ms[1]},
                   "plain_one_launch_per_job_ms": ptot,
                   "speedup_vs_plain": ptot / (tot / K)}
         b.close()

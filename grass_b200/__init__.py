@@ -30,7 +30,7 @@ MODE_GT, MODE_LE = 0, 1
 MODES = {"GT": MODE_GT, "LE": MODE_LE, "gt": MODE_GT, "le": MODE_LE, 0: 0, 1: 1}
 INVALID = 0xFFFFFFFF
 LAYOUT_WALK_MAJOR, LAYOUT_STEP_MAJOR = 0, 1
-SELECT_UNIFORM, SELECT_DEGREE = 0, 1
+SELECT_UNIFORM, SELECT_DEGREE, SELECT_DEGREE_CT = 0, 1, 2
 MAX_HOPS = 8
 
 
@@ -658,7 +658,8 @@ class Server:
 
 # Request mix of the batched-jobs workload: 40% RW with length U[10, 100],
 # 40% k-hop with fanouts from {(10,5), (15,10), (25,10), (5,5,5)}, 20%
-# multi-RW (one sample of 2000 walkers, 10,000 steps, degree-proportional);
+# multi-RW (one sample of 2000 walkers, 10,000 steps, degree-proportional in
+# continuous time);
 # RW walkers and k-hop seeds ~ lognormal(ln 1024, 1.5) clipped to [1, 65536].
 MIX_FANOUTS = [(10, 5), (15, 10), (25, 10), (5, 5, 5)]
 
@@ -667,7 +668,7 @@ def loadgen(graph: "Graph", rate: float, requests: int, mode: int = 0, seed: int
             pct_rw: int = 40, pct_khop: int = 40, size_mu: float = math.log(1024),
             size_sigma: float = 1.5, size_max: int = 65536, rw_len=(10, 100),
             fanouts=MIX_FANOUTS, mrw_samples: int = 1, mrw_walkers: int = 2000,
-            mrw_steps: int = 10000, mrw_select: int = SELECT_DEGREE, timeout_ms: int = 0,
+            mrw_steps: int = 10000, mrw_select: int = SELECT_DEGREE_CT, timeout_ms: int = 0,
             **server) -> dict:
     """Open-loop Poisson run of the request mix; mode 0 batched server,
     mode 1 one standalone launch per request."""

@@ -580,7 +580,8 @@ int grass_mrw(const grass_graph *g, const grass_mrw_params *p, uint32_t *d_roots
               uint32_t *d_src, uint32_t *d_dst, unsigned long long *d_edge_count, void *stream) {
   clear_error();
   if (int rc = check_graph(g)) return rc;
-  if (!p || p->walkers == 0 || p->select > 1 || (S && (!d_roots || !d_src || !d_dst)))
+  if (!p || p->walkers == 0 || p->select > 2 || (S && (!d_roots || !d_src || !d_dst)) ||
+      (p->select == GRASS_SELECT_DEGREE_CT && S > 0xFFFFFFFFull))
     return set_error(GRASS_E_ARG, "multi-RW: bad arguments");
   DeviceGuard dg(g->device);
   if (int rc = launch_mrw(g->view(), *p, d_roots, S, d_src, d_dst, d_edge_count, g->d_err,
@@ -593,7 +594,8 @@ int grass_mrw_host(const grass_graph *g, const grass_mrw_params *p, uint32_t *h_
                    uint64_t S, uint32_t *h_src, uint32_t *h_dst, uint64_t *edges_out) {
   clear_error();
   if (int rc = check_graph(g)) return rc;
-  if (!p || p->walkers == 0 || p->select > 1 || (S && (!h_roots || !h_src || !h_dst)))
+  if (!p || p->walkers == 0 || p->select > 2 || (S && (!h_roots || !h_src || !h_dst)) ||
+      (p->select == GRASS_SELECT_DEGREE_CT && S > 0xFFFFFFFFull))
     return set_error(GRASS_E_ARG, "multi-RW: bad arguments");
   DeviceGuard dg(g->device);
   cudaStream_t st = 0;

@@ -3,6 +3,7 @@
 #include <vector>
 
 #include "graph.h"
+#include "mrw_cta.cuh"
 #include "sample_warp.cuh"
 
 namespace grass {
@@ -13,7 +14,8 @@ struct BatchJob {
   uint64_t seed;
   const uint32_t *in;
   uint32_t *roots, *out0, *out1;
-  uint4 *wrec;  // multi-RW: count * walkers vertex records (scratch)
+  unsigned char *mscr;  // multi-RW scratch: mstride bytes per sample
+  uint64_t mstride;
   unsigned long long *edges;
   uint32_t length, layout, walkers, steps, select, pad;
   KhopArgs khop;
@@ -28,20 +30,30 @@ struct BatchTask {
 // Zero fields of a config take the defaults for this decode mode.
 grass_batch_config resolve_batch_config(const grass_batch_config &c, int mode);
 
-// Fills a device job descriptor from a job (wrec: multi-RW scratch of count *
-// walkers records, or null for other types).
-BatchJob make_batch_job(const grass_job &j, uint4 *wrec);
+// Multi-RW scratch bytes of a job (count samples of mrw_sample_scratch).
+inline uint64_t mrw_job_scratch(const grass_job &j) {
+  return j.type == GRASS_JOB_MRW ? (uint64_t)j.count * mrw_sample_scratch(j.walkers, j.steps, j.select)
+                                 : 0;
+}
 
-// Appends the work items of job index `ji`, split per config, to the three
-// queues (multi-RW samples, k-hop seed groups, walker tiles).
+// Fills a device job descriptor from a job (mscr: mrw_job_scratch(j) bytes
+// for a multi-RW job, else null).
+BatchJob make_batch_job(const grass_job &j, unsigned char *mscr);
+
+// Appends the work items of job index `ji`, split per config, to the queues:
+// block-level items (multi-RW samples whose walkers move in parallel,
+// selections 0 and 2), then warp-level items (sequential multi-RW samples,
+// k-hop seed groups, walker tiles).
 void split_job(const grass_job &j, uint32_t ji, const grass_batch_config &c,
-               std::vector<BatchTask> &mrw, std::vector<BatchTask> &khop,
-               std::vector<BatchTask> &rw);
+               std::vector<BatchTask> &cta, std::vector<BatchTask> &mrw,
+               std::vector<BatchTask> &khop, std::vector<BatchTask> &rw);
 
-// Launches the persistent kernel over ntasks work items (queue must be zero).
-// Corrupt payloads set bit 0 of *d_err.
+// Launches the persistent kernel over ntasks work items, the first ncta of
+// them block-level.  d_queue: two zeroed counters.  Corrupt payloads set bit
+// 0 of *d_err.
 int launch_batch(const grass_graph *g, const BatchJob *d_jobs, const BatchTask *d_tasks,
-                 uint32_t ntasks, unsigned int *d_queue, unsigned long long *d_total,
-                 unsigned int *d_err, cudaStream_t s, const grass_batch_config &c);
+                 uint32_t ncta, uint32_t ntasks, unsigned int *d_queue,
+                 unsigned long long *d_total, unsigned int *d_err, cudaStream_t s,
+                 const grass_batch_config &c);
 
 }  // namespace grass

@@ -21,17 +21,40 @@ namespace {
 template <int MODE, int DEPTH>
 __global__ void __launch_bounds__(256) batch_kernel(DevGraph g, const BatchJob *__restrict__ jobs,
                                                     const BatchTask *__restrict__ tasks,
-                                                    uint32_t ntasks, unsigned int *queue,
+                                                    uint32_t ncta, uint32_t ntasks,
+                                                    unsigned int *queue,
                                                     unsigned long long *total,
                                                     unsigned int *err) {
   __shared__ SmemHdr sh[8];
+  __shared__ CtaSmem<8> csm;
   SmemHdr &my = sh[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   uint64_t all = 0;
   bool bad = false;
+  // Block-level items first: multi-RW samples whose walkers move in parallel.
+  while (ncta) {
+    if (threadIdx.x == 0) csm.task = atomicAdd(queue + 1, 1u);
+    __syncthreads();
+    const uint32_t c = csm.task;
+    __syncthreads();
+    if (c >= ncta) break;
+    const BatchTask tk = tasks[c];
+    const BatchJob &jb = jobs[tk.job];
+    const uint64_t s = tk.begin;
+    uint64_t cnt = 0;
+    mrw_cta_sample<MODE, 8>(g, jb.roots + s * jb.walkers, jb.out0 + s * jb.steps,
+                            jb.out1 + s * jb.steps, jb.walkers, jb.steps, jb.select, jb.seed, s,
+                            jb.mscr + s * jb.mstride, csm, cnt, bad);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(kFull, cnt, o);
+    if (lane == 0 && cnt) {
+      if (jb.edges) atomicAdd(jb.edges, (unsigned long long)cnt);
+      all += cnt;
+    }
+  }
   for (;;) {
     uint32_t t = 0;
-    if (lane == 0) t = atomicAdd(queue, 1u);
+    if (lane == 0) t = ncta + atomicAdd(queue, 1u);
     t = __shfl_sync(kFull, t, 0);
     if (t >= ntasks) break;
     const BatchTask tk = tasks[t];
@@ -45,7 +68,8 @@ __global__ void __launch_bounds__(256) batch_kernel(DevGraph g, const BatchJob *
         khop_seed_warp<MODE>(g, jb.in, jb.khop, s, my, cnt, bad);
     } else {
       for (uint64_t s = tk.begin; s < tk.end; s++)
-        mrw_warp<MODE>(g, jb.roots + s * jb.walkers, jb.wrec + s * jb.walkers, jb.walkers,
+        mrw_warp<MODE>(g, jb.roots + s * jb.walkers,
+                       reinterpret_cast<uint4 *>(jb.mscr + s * jb.mstride), jb.walkers,
                        jb.steps, (int)jb.select, jb.seed, s, jb.out0, jb.out1, cnt, bad);
     }
 #pragma unroll
@@ -59,7 +83,7 @@ __global__ void __launch_bounds__(256) batch_kernel(DevGraph g, const BatchJob *
   if (bad && err) atomicOr(err, 1u);
 }
 
-using BatchKernel = void (*)(DevGraph, const BatchJob *, const BatchTask *, uint32_t,
+using BatchKernel = void (*)(DevGraph, const BatchJob *, const BatchTask *, uint32_t, uint32_t,
                              unsigned int *, unsigned long long *, unsigned int *);
 
 BatchKernel pick_kernel(int mode, uint32_t depth) {
@@ -89,14 +113,15 @@ grass_batch_config resolve_batch_config(const grass_batch_config &c, int mode) {
   return r;
 }
 
-BatchJob make_batch_job(const grass_job &j, uint4 *wrec) {
+BatchJob make_batch_job(const grass_job &j, unsigned char *mscr) {
   BatchJob bj{};
   bj.type = j.type;
   bj.count = j.count;
   bj.seed = j.seed;
   bj.in = j.d_input;
   bj.roots = j.d_roots;
-  bj.wrec = wrec;
+  bj.mscr = mscr;
+  bj.mstride = j.type == GRASS_JOB_MRW ? mrw_sample_scratch(j.walkers, j.steps, j.select) : 0;
   bj.out0 = j.d_out0;
   bj.out1 = j.d_out1;
   bj.edges = j.d_edges;
@@ -120,13 +145,14 @@ BatchJob make_batch_job(const grass_job &j, uint4 *wrec) {
 }
 
 void split_job(const grass_job &j, uint32_t ji, const grass_batch_config &c,
-               std::vector<BatchTask> &mrw, std::vector<BatchTask> &khop,
-               std::vector<BatchTask> &rw) {
+               std::vector<BatchTask> &cta, std::vector<BatchTask> &mrw,
+               std::vector<BatchTask> &khop, std::vector<BatchTask> &rw) {
   if (j.type == GRASS_JOB_KHOP) {
     for (uint64_t s = 0; s < j.count; s += c.khop_seeds)
       khop.push_back({ji, 0, s, std::min<uint64_t>(j.count, s + c.khop_seeds)});
   } else if (j.type == GRASS_JOB_MRW) {
-    for (uint64_t s = 0; s < j.count; s++) mrw.push_back({ji, 0, s, s + 1});
+    auto &q = j.select == GRASS_SELECT_DEGREE ? mrw : cta;
+    for (uint64_t s = 0; s < j.count; s++) q.push_back({ji, 0, s, s + 1});
   } else {
     for (uint64_t w = 0; w < j.count; w += c.walker_tile)
       rw.push_back({ji, 0, w, std::min<uint64_t>(j.count, w + c.walker_tile)});
@@ -134,17 +160,19 @@ void split_job(const grass_job &j, uint32_t ji, const grass_batch_config &c,
 }
 
 int launch_batch(const grass_graph *g, const BatchJob *d_jobs, const BatchTask *d_tasks,
-                 uint32_t ntasks, unsigned int *d_queue, unsigned long long *d_total,
-                 unsigned int *d_err, cudaStream_t s, const grass_batch_config &c) {
+                 uint32_t ncta, uint32_t ntasks, unsigned int *d_queue,
+                 unsigned long long *d_total, unsigned int *d_err, cudaStream_t s,
+                 const grass_batch_config &c) {
   BatchKernel k = pick_kernel(g->mode, c.depth);
   const int threads = 32 * (int)c.warps_per_block;
   int per_sm = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, 0);
   if (per_sm < 1) per_sm = 1;
-  const uint64_t need = (ntasks + c.warps_per_block - 1) / c.warps_per_block;
+  const uint64_t need =
+      std::max<uint64_t>(ncta, (ntasks - ncta + c.warps_per_block - 1) / c.warps_per_block);
   const unsigned grid = (unsigned)std::max<uint64_t>(
       1, std::min<uint64_t>(need, (uint64_t)sm_count(g->device) * per_sm));
-  k<<<grid, threads, 0, s>>>(g->view(), d_jobs, d_tasks, ntasks, d_queue, d_total, d_err);
+  k<<<grid, threads, 0, s>>>(g->view(), d_jobs, d_tasks, ncta, ntasks, d_queue, d_total, d_err);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "batch kernel launch");
 }
@@ -163,7 +191,7 @@ struct grass_batch {
   grass_batch_config built_cfg{};
   BatchJob *d_jobs = nullptr;
   BatchTask *d_tasks = nullptr;
-  uint32_t ntasks = 0;
+  uint32_t ntasks = 0, ncta = 0;
   unsigned int *d_queue = nullptr;
   std::vector<void *> owned;                      // MRW record scratch (per build)
   std::vector<uint32_t *> snap;                   // per job: MRW start vertices as added
@@ -187,7 +215,7 @@ struct grass_batch {
     owned.clear();
     restore.clear();
     restore_n.clear();
-    ntasks = 0;
+    ntasks = ncta = 0;
   }
   void free_snapshots() {
     for (uint32_t *p : snap) cudaFree(p);
@@ -206,29 +234,31 @@ int build(grass_batch *b) {
   const grass_batch_config c = resolve(b->cfg, b->g->mode);
   b->free_device();
   std::vector<BatchJob> hj;
-  std::vector<BatchTask> mrw, khop, rw;
+  std::vector<BatchTask> cta, mrw, khop, rw;
   for (size_t i = 0; i < b->jobs.size(); i++) {
     const grass_job &j = b->jobs[i];
-    uint4 *wrec = nullptr;
+    unsigned char *mscr = nullptr;
     if (j.type == GRASS_JOB_MRW) {
       const uint64_t nr = (uint64_t)j.count * j.walkers;
-      GRASS_CUDA(cudaMalloc(&wrec, std::max<uint64_t>(nr, 1) * sizeof(uint4)));
-      b->owned.push_back(wrec);
+      GRASS_CUDA(cudaMalloc(&mscr, std::max<uint64_t>(mrw_job_scratch(j), 256)));
+      b->owned.push_back(mscr);
       b->restore.push_back({j.d_roots, b->snap[i]});
       b->restore_n.push_back(nr);
     }
-    hj.push_back(make_batch_job(j, wrec));
-    split_job(j, (uint32_t)i, c, mrw, khop, rw);
+    hj.push_back(make_batch_job(j, mscr));
+    split_job(j, (uint32_t)i, c, cta, mrw, khop, rw);
   }
-  std::vector<BatchTask> tasks;  // longest chains first
+  std::vector<BatchTask> tasks;  // block-level items, then the longest chains first
+  tasks.insert(tasks.end(), cta.begin(), cta.end());
   tasks.insert(tasks.end(), mrw.begin(), mrw.end());
   tasks.insert(tasks.end(), khop.begin(), khop.end());
   tasks.insert(tasks.end(), rw.begin(), rw.end());
   if (tasks.size() > 0xFFFFFFF0ull) return set_error(GRASS_E_ARG, "batch: too many work items");
   b->ntasks = (uint32_t)tasks.size();
+  b->ncta = (uint32_t)cta.size();
   GRASS_CUDA(cudaMalloc(&b->d_jobs, std::max<size_t>(hj.size(), 1) * sizeof(BatchJob)));
   GRASS_CUDA(cudaMalloc(&b->d_tasks, std::max<size_t>(tasks.size(), 1) * sizeof(BatchTask)));
-  GRASS_CUDA(cudaMalloc(&b->d_queue, sizeof(unsigned int)));
+  GRASS_CUDA(cudaMalloc(&b->d_queue, 2 * sizeof(unsigned int)));
   if (!hj.empty())
     GRASS_CUDA(cudaMemcpy(b->d_jobs, hj.data(), hj.size() * sizeof(BatchJob),
                           cudaMemcpyHostToDevice));
@@ -246,10 +276,10 @@ int enqueue(grass_batch *b, cudaStream_t s, unsigned long long *total) {
   for (size_t i = 0; i < b->restore.size(); i++)
     GRASS_CUDA(cudaMemcpyAsync(b->restore[i].first, b->restore[i].second, b->restore_n[i] * 4,
                                cudaMemcpyDeviceToDevice, s));
-  GRASS_CUDA(cudaMemsetAsync(b->d_queue, 0, sizeof(unsigned int), s));
+  GRASS_CUDA(cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(unsigned int), s));
   if (!b->ntasks) return GRASS_OK;
-  return launch_batch(b->g, b->d_jobs, b->d_tasks, b->ntasks, b->d_queue, total, b->g->d_err, s,
-                      c);
+  return launch_batch(b->g, b->d_jobs, b->d_tasks, b->ncta, b->ntasks, b->d_queue, total,
+                      b->g->d_err, s, c);
 }
 
 int check_job(const grass_graph *g, const grass_job *j) {
@@ -272,7 +302,7 @@ int check_job(const grass_graph *g, const grass_job *j) {
       return GRASS_OK;
     }
     case GRASS_JOB_MRW:
-      if (!j->walkers || j->select > 1 || (j->count && (!j->d_roots || !j->d_out0 || !j->d_out1)))
+      if (!j->walkers || j->select > 2 || (j->count && (!j->d_roots || !j->d_out0 || !j->d_out1)))
         return set_error(GRASS_E_ARG, "multi-RW job: bad arguments");
       return GRASS_OK;
   }

@@ -9,6 +9,7 @@
 // each thread owns DEPTH walkers and interleaves them, which keeps DEPTH
 // independent decode chains in flight per thread.
 #include "graph.h"
+#include "mrw_cta.cuh"
 #include "sample_warp.cuh"
 
 namespace grass {
@@ -412,6 +413,28 @@ __global__ void __launch_bounds__(256) mrw_global_kernel(DevGraph g, uint32_t *_
   if (bad && err) atomicOr(err, 1u);
 }
 
+// Multi random walk, one block per sample, walkers in parallel (mrw_cta.cuh);
+// scratch holds `stride` bytes per block, reused for its samples.
+template <int MODE>
+__global__ void __launch_bounds__(512) mrw_cta_kernel(DevGraph g, uint32_t *__restrict__ roots,
+                                                      uint64_t S, uint32_t R, uint32_t T,
+                                                      uint32_t select, uint64_t seed,
+                                                      uint32_t *__restrict__ src,
+                                                      uint32_t *__restrict__ dst,
+                                                      unsigned char *scratch, uint64_t stride,
+                                                      unsigned long long *edges,
+                                                      unsigned int *err) {
+  __shared__ CtaSmem<16> sm;
+  unsigned char *scr = scratch + blockIdx.x * stride;
+  uint64_t cnt = 0;
+  bool bad = false;
+  for (uint64_t s = blockIdx.x; s < S; s += gridDim.x)
+    mrw_cta_sample<MODE, 16>(g, roots + s * R, src + s * T, dst + s * T, R, T, select, seed, s,
+                             scr, sm, cnt, bad);
+  warp_add_u64(edges, cnt);
+  if (bad && err) atomicOr(err, 1u);
+}
+
 __global__ void starts_kernel(uint64_t n, uint64_t count, uint64_t seed, uint32_t tag,
                               uint32_t *out) {
   const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
@@ -638,6 +661,29 @@ int launch_mrw(const DevGraph &g, const grass_mrw_params &p, uint32_t *roots, ui
                uint32_t *src, uint32_t *dst, unsigned long long *edges, unsigned int *err,
                cudaStream_t s) {
   if (!S || !p.steps) return GRASS_OK;
+  // Block per sample (walkers in parallel) for continuous-time selection, and
+  // for uniform selection when there are few samples or long chains (same
+  // output as the warp kernels).
+  if (p.select == GRASS_SELECT_DEGREE_CT ||
+      (p.select == GRASS_SELECT_UNIFORM &&
+       (p.steps >= 1024 || S < (uint64_t)sm_count(cur_dev()) * 8))) {
+    const int threads = (int)std::min<uint64_t>(
+        512, std::max<uint64_t>(128, ((uint64_t)p.walkers / 2 + 31) / 32 * 32));
+    auto kern = g.mode == GRASS_MODE_GT ? mrw_cta_kernel<0> : mrw_cta_kernel<1>;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, 0);
+    const uint64_t grid =
+        std::min<uint64_t>(S, (uint64_t)sm_count(cur_dev()) * std::max(per_sm, 1));
+    const uint64_t stride = mrw_sample_scratch(p.walkers, p.steps, p.select);
+    unsigned char *scr = nullptr;
+    cudaError_t e = cudaMallocAsync(&scr, grid * stride, s);
+    if (e != cudaSuccess) return cuda_fail(e, "multi-RW scratch");
+    kern<<<(unsigned)grid, threads, 0, s>>>(g, roots, S, p.walkers, p.steps, p.select, p.seed, src,
+                                            dst, scr, stride, edges, err);
+    count_launch();
+    cudaFreeAsync(scr, s);
+    return GRASS_OK;
+  }
   const MrwLayout lay{p.walkers};
   const size_t per_warp = lay.bytes_per_warp();
   if (per_warp > 48 * 1024) {

@@ -20,7 +20,7 @@
 // 0-based walker / seed / sample ids, so its output is the standalone call's.
 //
 // Device block of one batch (every part 256-byte aligned):
-//   [multi-RW record scratch] | H2D: [jobs][work items][queue][inputs]
+//   [multi-RW scratch] | H2D: [jobs][work items][queue][inputs]
 //   | H2D+D2H: [edges u64 x jobs][error word] | D2H: [outputs]
 #include <algorithm>
 #include <chrono>
@@ -159,7 +159,7 @@ struct Req {
   int cls = 0;              // 0: RW / k-hop, 1: multi-RW
   uint32_t nout = 0;
   uint64_t out_words[GRASS_MAX_HOPS] = {0};
-  uint64_t in_words = 0, deg_words = 0;
+  uint64_t in_words = 0, mscr_bytes = 0;
   uint64_t bytes = 0;  // device scratch without the batch's tables
   uint64_t in_bytes = 0, out_bytes = 0;  // staging (aligned inputs, aligned outputs)
   uint64_t draws = 0;  // sampled edges at most (batch sizing)
@@ -273,10 +273,10 @@ int size_request(const grass_request &r, Req &q) {
       break;
     }
     case GRASS_JOB_MRW:
-      if (!r.walkers || r.select > 1 || r.steps > (1u << 28))
+      if (!r.walkers || r.select > 2 || r.steps > (1u << 28))
         return set_error(GRASS_E_ARG, "multi-RW request: bad arguments");
       q.in_words = c * r.walkers;
-      q.deg_words = 4 * c * r.walkers;  // one 16-byte record per walker
+      q.mscr_bytes = c * mrw_sample_scratch(r.walkers, r.steps, r.select);
       q.nout = 2;
       q.out_words[0] = q.out_words[1] = c * (uint64_t)r.steps;
       q.draws = c * (uint64_t)r.steps;
@@ -288,7 +288,7 @@ int size_request(const grass_request &r, Req &q) {
   q.in_bytes = align_up(q.in_words * 4);
   q.out_bytes = 0;
   for (uint32_t k = 0; k < q.nout; k++) q.out_bytes += align_up(q.out_words[k] * 4);
-  q.bytes = q.in_bytes + align_up(q.deg_words * 4) + q.out_bytes;
+  q.bytes = q.in_bytes + align_up(q.mscr_bytes) + q.out_bytes;
   return GRASS_OK;
 }
 
@@ -404,13 +404,13 @@ void grass_server::launch(Batch *b) {
   cudaStream_t s = streams[b->slot];
   const size_t nj = b->reqs.size();
   std::vector<BatchJob> jobs(nj);
-  std::vector<BatchTask> mrw, khop, rw;
+  std::vector<BatchTask> cta, mrw, khop, rw;
   // Offsets inside the device block.
   uint64_t off = 0;
-  std::vector<uint64_t> deg_off(nj), in_off(nj);
+  std::vector<uint64_t> mscr_off(nj), in_off(nj);
   for (size_t i = 0; i < nj; i++) {
-    deg_off[i] = off;
-    off += align_up(b->reqs[i]->deg_words * 4);
+    mscr_off[i] = off;
+    off += align_up(b->reqs[i]->mscr_bytes);
   }
   b->h2d_off = off;
   const uint64_t jobs_off = off;
@@ -421,9 +421,11 @@ void grass_server::launch(Batch *b) {
     gj.type = r.type;
     gj.count = r.count;
     gj.walkers = r.walkers;
-    split_job(gj, (uint32_t)i, bcfg, mrw, khop, rw);
+    gj.steps = r.steps;
+    gj.select = r.select;
+    split_job(gj, (uint32_t)i, bcfg, cta, mrw, khop, rw);
   }
-  const uint64_t ntasks = mrw.size() + khop.size() + rw.size();
+  const uint64_t ntasks = cta.size() + mrw.size() + khop.size() + rw.size();
   const uint64_t tasks_off = off;
   off += align_up(ntasks * sizeof(BatchTask));
   const uint64_t queue_off = off;
@@ -490,13 +492,13 @@ void grass_server::launch(Batch *b) {
           j.d_out0 = outs[0];
           j.d_out1 = outs[1];
         }
-        jobs[i] = make_batch_job(j, reinterpret_cast<uint4 *>(d + deg_off[i]));
+        jobs[i] = make_batch_job(j, d + mscr_off[i]);
         if (!q->draw_roots && q->in_words)
           memcpy(h + in_off[i], q->input.data(), q->in_words * 4);
       }
       memcpy(h + jobs_off, jobs.data(), nj * sizeof(BatchJob));
       BatchTask *ht = reinterpret_cast<BatchTask *>(h + tasks_off);
-      for (const auto *v : {&mrw, &khop, &rw})
+      for (const auto *v : {&cta, &mrw, &khop, &rw})
         for (const BatchTask &t : *v) *ht++ = t;
       memset(h + queue_off, 0, kAlign);
       memset(h + edges_off, 0, align_up(nj * 8 + 4));
@@ -511,7 +513,8 @@ void grass_server::launch(Batch *b) {
     }
     if (!rc && ntasks)
       rc = launch_batch(g, reinterpret_cast<const BatchJob *>(d + jobs_off),
-                        reinterpret_cast<const BatchTask *>(d + tasks_off), (uint32_t)ntasks,
+                        reinterpret_cast<const BatchTask *>(d + tasks_off), (uint32_t)cta.size(),
+                        (uint32_t)ntasks,
                         reinterpret_cast<unsigned int *>(d + queue_off), nullptr,
                         reinterpret_cast<unsigned int *>(d + err_off), s, bcfg);
     if (!rc && ntasks) count_launch();

@@ -47,6 +47,11 @@ extern "C" {
 /* Multi-RW walker selection. */
 #define GRASS_SELECT_UNIFORM 0 /* reference: MultiRWApp::stepTransits, GT/src/apps/multiRW/multiRW.cu:93-101 */
 #define GRASS_SELECT_DEGREE 1  /* frontier sampling: proportional to current degree */
+/* Degree-proportional as well, computed as the jump chain of independent
+ * continuous-time walks (a walker at degree d waits Exp(d), then moves): the
+ * same law as GRASS_SELECT_DEGREE with walkers moving in parallel, one
+ * Philox stream per walker (TAG_MRW_CT), so a different sample path. */
+#define GRASS_SELECT_DEGREE_CT 2
 
 /* Thread-local message for the last failing call on this thread. */
 const char *grass_last_error(void);

@@ -79,12 +79,19 @@ def lib():
         L.og_mrw.restype = u64
         L.og_mrw_roots.argtypes = [u32, u64, u32, u64, P]
         L.og_max_threads.restype = i32
+        L.og_det_log.argtypes = [C.c_double]
+        L.og_det_log.restype = C.c_double
         _lib = L
     return _lib
 
 
 def _p(a: np.ndarray):
     return a.ctypes.data_as(C.c_void_p)
+
+
+def det_log(u: float) -> float:
+    """ln u for u in (0, 1) with the exact operation sequence of the device."""
+    return float(lib().og_det_log(u))
 
 
 def max_threads() -> int:

@@ -520,6 +520,152 @@ uint64_t og_khop(const og_graph *g, int mode, const uint32_t *seeds, uint64_t S,
  * word 2 as the high half for degree-proportional selection) picks the
  * walker, word 1 the neighbor.  A walker on a vertex with no edges records
  * an invalid destination and stays. */
+/* ------------------------------------------------------------------------ */
+/* Continuous-time multi-RW (select 2).  Degree-proportional walker choice is
+ * the jump chain of R independent continuous-time walks in which a walker at
+ * a vertex of degree d waits Exp(d) and then moves to a uniform neighbor
+ * (competing exponentials: the next walker to move is x with probability
+ * d_x / sum d, independently of the past).  Each walker's events are then a
+ * stream of its own: event k of walker w draws Philox(seed; k, sample, w,
+ * TAG_MRW_CT), words 0-1 for the holding time before it, word 2 for the
+ * neighbor.  The sample's output is the first T events in (time, walker)
+ * order.  Here a binary heap pops them one by one.
+ *
+ * det_log: ln u for u in (0, 1) from correctly rounded +, *, / in a fixed
+ * order (compiled without FP contraction), bit-identical to the device:
+ * u = m 2^e, m in [sqrt(1/2), sqrt(2)), s = (m-1)/(m+1), z = s^2,
+ * ln u = e ln2 + 2 s (1 + z/3 + ... + z^10/21). */
+static double det_log(double u) {
+  uint64_t b;
+  memcpy(&b, &u, 8);
+  int e = (int)((b >> 52) & 0x7FF) - 1023;
+  uint64_t mb = (b & 0x000FFFFFFFFFFFFFull) | 0x3FF0000000000000ull;
+  double m;
+  memcpy(&m, &mb, 8);
+  if (m > 0x1.6a09e667f3bcdp+0) {
+    m = m * 0.5;
+    e += 1;
+  }
+  const double s = (m + -1.0) / (m + 1.0);
+  const double z = s * s;
+  static const double c[10] = {0x1.8618618618618p-5, 0x1.af286bca1af28p-5, 0x1.e1e1e1e1e1e1ep-5,
+                               0x1.1111111111111p-4, 0x1.3b13b13b13b14p-4, 0x1.745d1745d1746p-4,
+                               0x1.c71c71c71c71cp-4, 0x1.2492492492492p-3, 0x1.999999999999ap-3,
+                               0x1.5555555555555p-2}; /* 1/21 ... 1/3 */
+  double p = c[0];
+  for (int i = 1; i < 10; i++) p = c[i] + z * p;
+  const double t = s + s * (z * p);
+  return (double)e * 0x1.62e42fefa39efp-1 + 2.0 * t;
+}
+
+static double exp_variate(uint32_t w0, uint32_t w1) {
+  const uint64_t u52 = ((uint64_t)w0 << 20) | (w1 >> 12);
+  return -det_log(((double)u52 + 0.5) * 0x1p-52);
+}
+
+static double next_event_time(double t, double E, uint32_t d) {
+  double nt = t + E / (double)d;
+  if (nt > t) return nt;
+  uint64_t b;
+  memcpy(&b, &t, 8);
+  b += 1;
+  memcpy(&nt, &b, 8);
+  return nt;
+}
+
+double og_det_log(double u) { return det_log(u); }
+
+typedef struct {
+  uint32_t v, d, k, z;
+  double t;
+} ct_walker;
+
+static int ct_less(const ct_walker *W, uint32_t a, uint32_t b) {
+  return W[a].t < W[b].t || (W[a].t == W[b].t && a < b);
+}
+
+static void ct_push(uint32_t *heap, uint32_t *n, const ct_walker *W, uint32_t w) {
+  uint32_t i = (*n)++;
+  heap[i] = w;
+  while (i && ct_less(W, heap[i], heap[(i - 1) / 2])) {
+    uint32_t p = (i - 1) / 2, x = heap[p];
+    heap[p] = heap[i];
+    heap[i] = x;
+    i = p;
+  }
+}
+
+static uint32_t ct_pop(uint32_t *heap, uint32_t *n, const ct_walker *W) {
+  uint32_t top = heap[0];
+  heap[0] = heap[--(*n)];
+  uint32_t i = 0;
+  for (;;) {
+    uint32_t l = 2 * i + 1, r = l + 1, m = i;
+    if (l < *n && ct_less(W, heap[l], heap[m])) m = l;
+    if (r < *n && ct_less(W, heap[r], heap[m])) m = r;
+    if (m == i) break;
+    uint32_t x = heap[m];
+    heap[m] = heap[i];
+    heap[i] = x;
+    i = m;
+  }
+  return top;
+}
+
+static void ct_arm(const og_graph *g, int mode, ct_walker *w, uint32_t wid, uint64_t s,
+                   uint64_t seed, double t0) {
+  (void)g;
+  (void)mode;
+  uint32_t c[4] = {w->k, (uint32_t)s, wid, OG_TAG_MRW_CT}, o[4];
+  og_philox4x32_10((uint32_t)seed, (uint32_t)(seed >> 32), c, o);
+  w->z = o[2];
+  w->t = next_event_time(t0, exp_variate(o[0], o[1]), w->d);
+}
+
+static uint64_t mrw_ct_sample(const og_graph *g, int mode, uint32_t *rt, uint64_t s, uint32_t R,
+                              uint32_t T, uint64_t seed, uint32_t *src, uint32_t *dst) {
+  ct_walker *W = (ct_walker *)malloc((size_t)R * sizeof(ct_walker));
+  uint32_t *heap = (uint32_t *)malloc((size_t)R * sizeof(uint32_t));
+  uint32_t hn = 0;
+  uint64_t total = 0;
+  for (uint32_t w = 0; w < R; w++) {
+    W[w].v = rt[w];
+    W[w].d = rt[w] < g->n ? og_degree(g, mode, rt[w]) : 0;
+    if (W[w].d == OG_INVALID) W[w].d = 0;
+    W[w].k = 0;
+    if (W[w].d) {
+      ct_arm(g, mode, &W[w], w, s, seed, 0.0);
+      ct_push(heap, &hn, W, w);
+    }
+  }
+  for (uint32_t r = 0; r < T; r++) {
+    if (!hn) {
+      src[r] = OG_INVALID;
+      dst[r] = OG_INVALID;
+      continue;
+    }
+    const uint32_t w = ct_pop(heap, &hn, W);
+    ct_walker *x = &W[w];
+    hdr_t h = header(g, mode, x->v);
+    const uint32_t nv = getv(g, mode, &h, mulhi32(x->z, x->d));
+    src[r] = x->v;
+    dst[r] = nv;
+    total++;
+    x->v = nv;
+    x->d = og_degree(g, mode, nv);
+    if (x->d == OG_INVALID) x->d = 0;
+    x->k++;
+    if (x->d) {
+      ct_arm(g, mode, x, w, s, seed, x->t);
+      ct_push(heap, &hn, W, w);
+    }
+  }
+  for (uint32_t w = 0; w < R; w++) rt[w] = W[w].v;
+  free(W);
+  free(heap);
+  return total;
+}
+
 uint64_t og_mrw(const og_graph *g, int mode, uint32_t *roots, uint64_t S, uint32_t R,
                 uint32_t T, uint64_t seed, int select, uint32_t *src, uint32_t *dst,
                 int threads) {
@@ -528,6 +674,11 @@ uint64_t og_mrw(const og_graph *g, int mode, uint32_t *roots, uint64_t S, uint32
 #pragma omp parallel for schedule(dynamic, 1) reduction(+ : total)
   for (int64_t s = 0; s < (int64_t)S; s++) {
     uint32_t *rt = roots + (uint64_t)s * R;
+    if (select == 2) {
+      total += mrw_ct_sample(g, mode, rt, (uint64_t)s, R, T, seed, src + (uint64_t)s * T,
+                             dst + (uint64_t)s * T);
+      continue;
+    }
     uint32_t *deg = (uint32_t *)malloc((size_t)R * sizeof(uint32_t));
     uint64_t wsum = 0;
     for (uint32_t r = 0; r < R; r++) {

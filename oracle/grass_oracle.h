@@ -49,6 +49,7 @@ extern "C" {
 #define OG_TAG_MRW 0x4d520001u
 #define OG_TAG_START 0x53540001u
 #define OG_TAG_MRW_ROOT 0x4d520002u
+#define OG_TAG_MRW_CT 0x4d520003u
 
 typedef struct {
   uint32_t *words;    /* big-endian packed graph words + 2 zero guard words */
@@ -99,7 +100,9 @@ uint64_t og_khop(const og_graph *g, int mode, const uint32_t *seeds, uint64_t S,
                  uint32_t **hop_out, int threads);
 
 /* Multi random walk (frontier sampling).  roots is [S][R] (updated in place);
- * src/dst are [S][T].  select: 0 = uniform walker choice, 1 = degree-proportional. */
+ * src/dst are [S][T].  select: 0 = uniform walker choice, 1 = degree-
+ * proportional (one Philox block per step), 2 = degree-proportional as the
+ * jump chain of independent continuous-time walks (one stream per walker). */
 uint64_t og_mrw(const og_graph *g, int mode, uint32_t *roots, uint64_t S, uint32_t R,
                 uint32_t T, uint64_t seed, int select, uint32_t *src, uint32_t *dst,
                 int threads);
@@ -108,6 +111,9 @@ uint64_t og_mrw(const og_graph *g, int mode, uint32_t *roots, uint64_t S, uint32
 void og_mrw_roots(uint32_t n, uint64_t S, uint32_t R, uint64_t seed, uint32_t *roots);
 
 int og_max_threads(void);
+
+/* ln u for u in (0, 1), bit-identical to the device's det_log. */
+double og_det_log(double u);
 
 #ifdef __cplusplus
 }

@@ -30,7 +30,9 @@ class Mix:
             self._rw(rng, W, L, lay, seed=100 + k)
         for k, fan in enumerate([(25, 10), (5, 5, 5), (10,), (3, 7)]):
             self._khop(rng, int(rng.integers(1, 300)), fan, seed=200 + k)
-        for k, (S, R, T, sel) in enumerate([(3, 80, 100, 0), (1, 2000, 500, 1), (2, 7, 64, 1)]):
+        for k, (S, R, T, sel) in enumerate([(3, 80, 100, 0), (1, 2000, 500, 1), (2, 7, 64, 1),
+                                            (2, 300, 700, 2), (1, 2000, 3000, 2),
+                                            (4, 50, 20, 2)]):
             self._mrw(S, R, T, sel, seed=300 + k)
 
     def _ints(self, a):
@@ -93,7 +95,7 @@ def test_batch_matches_standalone_calls(mode):
     g = G.Graph(os.path.join(d, mode), mode)
     m = Mix(torch, g, g.n)
     info = m.batch.info()
-    assert info["jobs"] == 11
+    assert info["jobs"] == 14
     m.check(runs=2)  # graph capture, then replay (multi-RW roots restored)
     m.batch.set_config(use_graph=2)  # plain launches
     m.check()

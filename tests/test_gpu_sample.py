@@ -148,7 +148,7 @@ def test_csr_khop_equals_compressed(oracle_mod, torch_cuda):
 
 @pytest.mark.parametrize("name", ["edge_cases", "rmat_s10_e8"])
 @pytest.mark.parametrize("mode", ["GT", "LE"])
-@pytest.mark.parametrize("select", [G.SELECT_UNIFORM, G.SELECT_DEGREE])
+@pytest.mark.parametrize("select", [G.SELECT_UNIFORM, G.SELECT_DEGREE, G.SELECT_DEGREE_CT])
 def test_mrw_matches_oracle(oracle_mod, name, mode, select):
     d, rowptr, cols, meta = golden_graph(name)
     prefix = os.path.join(d, mode)
@@ -165,18 +165,30 @@ def test_mrw_matches_oracle(oracle_mod, name, mode, select):
 
 
 @pytest.mark.parametrize("mode", ["GT", "LE"])
-def test_mrw_large_frontier(oracle_mod, mode):
-    """2000 walkers x 2000 steps with degree-proportional selection."""
+@pytest.mark.parametrize("select,S,R,T", [
+    (G.SELECT_DEGREE, 3, 2000, 2000),     # warp per sample, sequential steps
+    (G.SELECT_DEGREE_CT, 3, 2000, 2000),  # block per sample, walkers in parallel
+    (G.SELECT_DEGREE_CT, 1, 2000, 10000), # the batched-jobs shape
+    (G.SELECT_DEGREE_CT, 2, 5000, 700),   # more walkers than threads x 2
+    (G.SELECT_DEGREE_CT, 5, 1, 300),      # a single walker
+    (G.SELECT_UNIFORM, 2, 2000, 10000),   # block per sample
+    (G.SELECT_UNIFORM, 1500, 8, 50),      # many samples: warp kernel
+])
+def test_mrw_large_frontier(oracle_mod, mode, select, S, R, T):
     d, rowptr, cols, meta = golden_graph("rmat_s10_e8")
     prefix = os.path.join(d, mode)
     g = G.Graph(prefix, mode)
     og = oracle_mod.OracleGraph(prefix)
-    roots = oracle_mod.mrw_roots(g.n, 3, 2000, 8)
-    src, dst, fin, e = g.mrw(roots, 2000, 23, G.SELECT_DEGREE)
-    rs, rd, rf, re_ = og.mrw(mode, roots, 2000, 23, G.SELECT_DEGREE)
+    roots = oracle_mod.mrw_roots(g.n, S, R, 8)
+    src, dst, fin, e = g.mrw(roots, T, 23, select)
+    rs, rd, rf, re_ = og.mrw(mode, roots, T, 23, select)
     np.testing.assert_array_equal(src, rs)
     np.testing.assert_array_equal(dst, rd)
+    np.testing.assert_array_equal(fin, rf)
     assert e == re_
+    ok = rd != G.INVALID  # every move is an edge
+    nb = [set(cols[rowptr[v]:rowptr[v + 1]].tolist()) for v in range(len(rowptr) - 1)]
+    assert all(int(b) in nb[int(a)] for a, b in zip(rs[ok][:2000], rd[ok][:2000]))
 
 
 def test_rw_paths_are_edges_at_scale(torch_cuda):

@@ -34,7 +34,7 @@ def _mix(n, rng, k):
         else:
             out.append(("mrw", dict(samples=int(rng.integers(1, 4)), walkers=int(rng.integers(1, 300)),
                                     steps=int(rng.integers(1, 120)), seed=seed,
-                                    select=i % 2, given=bool(i % 3 == 0))))
+                                    select=(i // 5) % 3, given=bool(i % 3 == 0))))
     return out
 
 

@@ -112,7 +112,7 @@ def test_oracle_khop_matches_python_restatement(oracle_mod, mode):
 
 
 @pytest.mark.parametrize("mode", ["GT", "LE"])
-@pytest.mark.parametrize("select", [0, 1])
+@pytest.mark.parametrize("select", [0, 1, 2])
 def test_oracle_mrw_matches_python_restatement(oracle_mod, mode, select):
     d, rowptr, cols, meta = golden_graph("edge_cases")
     g = oracle_mod.OracleGraph(os.path.join(d, mode))
@@ -122,6 +122,46 @@ def test_oracle_mrw_matches_python_restatement(oracle_mod, mode, select):
     np.testing.assert_array_equal(src, rs)
     np.testing.assert_array_equal(dst, rd)
     np.testing.assert_array_equal(fin, rf)
+
+
+def test_det_log(oracle_mod):
+    """The oracle's logarithm equals the Python restatement bit for bit and
+    math.log to within a few ulp, including the ends of (0, 1)."""
+    import math
+    rng = np.random.default_rng(3)
+    us = list(rng.random(20000)) + [2.0 ** -52 * 0.5, 1 - 2.0 ** -53, 0.5, 0.7071067811865476,
+                                    0.7071067811865475, 1e-300]
+    for u in us:
+        if not 0 < u < 1:
+            continue
+        a = oracle_mod.det_log(u)
+        assert a == pyref.det_log(u), u
+        assert abs(a - math.log(u)) <= 4e-16 * max(1.0, abs(math.log(u))), u
+
+
+def test_mrw_ct_has_the_law_of_sequential_degree_selection(oracle_mod):
+    """Continuous-time selection (2) and one-block-per-step selection (1) are
+    two constructions of the same process: the final walker positions and the
+    vertices visited at a fixed step have the same distribution (two-sample
+    chi-square over degree bins, 20,000 samples each)."""
+    from scipy import stats
+    d, rowptr, cols, meta = golden_graph("rmat_s10_e8")
+    g = oracle_mod.OracleGraph(os.path.join(d, "LE"))
+    deg = np.diff(rowptr)
+    S, R, T = 20000, 4, 24
+    roots = np.tile(oracle_mod.mrw_roots(g.n, 1, R, 77), (S, 1))
+    bins = np.unique(np.quantile(deg[deg > 0], np.linspace(0, 1, 13)))
+    out = []
+    for sel, seed in ((1, 5), (2, 6)):
+        src, dst, fin, _ = g.mrw("LE", roots, T, seed, sel)
+        out.append((np.digitize(deg[fin.ravel()], bins), np.digitize(deg[dst[:, T // 2]], bins),
+                    (src[:, :T // 2] == roots[:, :1]).sum(1)))
+    for a, b in zip(out[0], out[1]):
+        ks = np.union1d(a, b)
+        table = np.array([[np.sum(a == k) for k in ks], [np.sum(b == k) for k in ks]])
+        table = table[:, table.sum(0) >= 10]
+        pval = stats.chi2_contingency(table)[1]
+        assert pval > 0.001, (pval, table)
 
 
 def test_rw_visit_distribution_chi_square(oracle_mod):
