@@ -47,13 +47,26 @@ struct CtaSmem {
 
 __host__ __device__ inline uint64_t mrw_ct_cap(uint32_t T) { return 2ull * T + 4096; }
 
+// Byte offsets in the scratch of a continuous-time sample (from a 256-byte
+// aligned base): walkers (24 B), vertex records (16 B, 16-aligned), first
+// event past the T-th per walker (4 B), then two event buffers of cap each.
+struct CtLayout {
+  uint64_t rec, first, ev, total;
+  __host__ __device__ CtLayout(uint32_t R, uint32_t T) {
+    rec = ((uint64_t)R * sizeof(CtWalker) + 63) & ~63ull;
+    first = rec + (uint64_t)R * 16;
+    ev = (first + (uint64_t)R * 4 + 63) & ~63ull;
+    total = ev + 2 * mrw_ct_cap(T) * sizeof(CtEvent);
+  }
+};
+
 // Device scratch of one sample, by selection (256-byte multiple).
 __host__ __device__ inline uint64_t mrw_sample_scratch(uint32_t R, uint32_t T, uint32_t select) {
   uint64_t b;
   if (select == GRASS_SELECT_UNIFORM)
     b = ((uint64_t)R + 1 + T) * 4;  // step counts per walker + step lists
   else if (select == GRASS_SELECT_DEGREE_CT)
-    b = (uint64_t)R * (sizeof(CtWalker) + 16 + 4) + 2 * mrw_ct_cap(T) * sizeof(CtEvent) + 64;
+    b = CtLayout(R, T).total;
   else
     b = (uint64_t)R * 16;  // mrw_warp: one vertex record per walker
   return (b + 255) & ~255ull;
@@ -296,11 +309,11 @@ __device__ void mrw_ct_cta(const DevGraph &g, uint32_t *roots, uint32_t *src, ui
   const uint32_t tid = threadIdx.x, nt = blockDim.x;
   const uint32_t s_lo = (uint32_t)sample;
   const uint32_t cap = (uint32_t)mrw_ct_cap(T);
+  const CtLayout lay(R, T);
   CtWalker *W = reinterpret_cast<CtWalker *>(scr);
-  uint4 *rec = reinterpret_cast<uint4 *>(scr + (uint64_t)R * sizeof(CtWalker));
-  uint32_t *first = reinterpret_cast<uint32_t *>(scr + (uint64_t)R * (sizeof(CtWalker) + 16));
-  CtEvent *A = reinterpret_cast<CtEvent *>(
-      scr + (((uint64_t)R * (sizeof(CtWalker) + 16 + 4) + 63) & ~63ull));
+  uint4 *rec = reinterpret_cast<uint4 *>(scr + lay.rec);
+  uint32_t *first = reinterpret_cast<uint32_t *>(scr + lay.first);
+  CtEvent *A = reinterpret_cast<CtEvent *>(scr + lay.ev);
   CtEvent *B = A + cap;
   uint32_t N = 0;
   bool done = false;
