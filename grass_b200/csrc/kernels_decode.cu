@@ -43,6 +43,42 @@ __device__ __forceinline__ VHdr shfl_hdr(const VHdr &h, int src) {
   return o;
 }
 
+// 64 stream bits starting at bit `off`: three word loads, two funnel shifts
+// (the sweep reads the stream in order, so these hit L1).
+__device__ __forceinline__ uint64_t read_bits64(const uint32_t *w, uint64_t off) {
+  const uint32_t *q = w + (off >> 5);
+  const uint32_t s = (uint32_t)off & 31u;
+  const uint32_t x0 = ldw(q), x1 = ldw(q + 1), x2 = ldw(q + 2);
+  return ((uint64_t)__funnelshift_l(x1, x0, s) << 32) | __funnelshift_l(x2, x1, s);
+}
+
+// le_neighbor (device_common.cuh) with word reads instead of sector loads:
+// the same arithmetic, LE/src/bcg.cuh:195-261.
+__device__ __forceinline__ uint32_t le_neighbor_words(const uint32_t *words, const VHdr &h,
+                                                      uint32_t i) {
+  if (h.d == 1) return h.fp;
+  uint32_t tl = h.bl + 1;
+  const uint32_t split = h.om * tl;
+  const bool flag = i >= split;
+  const uint32_t j = flag ? i - split : i;
+  if (flag) tl -= 1;
+  uint32_t c = j / tl;
+  const uint32_t id = j - c * tl;
+  if (flag) c += h.om;
+  const uint64_t rwin = read_bits64(words, h.P + (uint64_t)c * (uint64_t)h.a);
+  const uint32_t r1m = (uint32_t)(rwin >> (64 - h.a));
+  const uint32_t r1 = (c < h.fp) ? h.v - r1m : h.v + r1m;
+  if (id == 0) return r1;
+  const uint32_t r2m = (uint32_t)((rwin << h.a) >> (64 - h.a));
+  const uint32_t r2 = (c + 1 < h.fp) ? h.v - r2m : h.v + r2m;
+  const uint64_t spos =
+      h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a +
+      ((uint64_t)(h.bl - 1) * c + min(h.om, c) + id - 1) * (uint64_t)(h.b + 1);
+  const uint32_t raw = (uint32_t)(read_bits64(words, spos) >> (63 - h.b));
+  const uint32_t mag = raw >> 1;
+  return ((r2 - r1) / tl) * id + r1 + ((raw & 1u) ? 0u - mag : mag);
+}
+
 // Largest v in [0, n) with rowptr[v] <= x, for x < rowptr[n].
 __device__ __forceinline__ uint32_t warp_row_of(const uint64_t *rowptr, uint32_t n, uint64_t x) {
   const int lane = threadIdx.x & 31;
@@ -97,45 +133,73 @@ __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint6
         carry = __shfl_sync(FULL, c, 0);
       }
     }
+    // Header of the vertex that holds the whole current round (fast path),
+    // kept across rounds of the same vertex.
+    uint32_t cv = 0xFFFFFFFFu;
+    uint64_t cstart = 0, cend = 0;
+    VHdr ch{};
+    bool ch_ok = false;
     for (uint64_t r = g0; r < g1; r += 32) {  // warp-uniform
       const uint64_t gl = r + lane;
       const bool act = gl < g1;
-      // window of vertices [vr, vr + 32): row ends and headers, one per lane
-      const uint32_t wv = vr + lane;
-      const uint64_t base = rowptr[vr];
-      const uint64_t e = wv < g.n ? rowptr[wv + 1] : ~0ull;
-      VHdr hw;
-      if (wv < g.n) {
-        hw = header<MODE>(g, wv);
-      } else {
-        hw.d = 0; hw.P = 0; hw.v = 0; hw.bn = hw.bl = hw.om = hw.fp = 0; hw.a = hw.b = 0;
+      const uint64_t rlast = min(g1, r + 32) - 1;
+      if (vr != cv) {
+        cv = vr;
+        cstart = rowptr[vr];
+        cend = rowptr[vr + 1];
+        ch_ok = false;
       }
-      // owner lane k: number of window rows that end at or before gl
-      // (binary lifting over 31 probes gives the exact count when it is
-      // below 32)
+      VHdr hk;
+      uint64_t startv;
+      bool far = false;
       int k = 0;
+      const bool single = cstart <= r && rlast < cend;  // warp-uniform
+      if (single) {
+        // Fast path: the round lies inside vertex vr (most rounds of a
+        // skewed graph): no window, no owner search.
+        if (!ch_ok) {
+          ch = header<MODE>(g, vr);
+          ch_ok = true;
+        }
+        hk = ch;
+        startv = cstart;
+      } else {
+        // window of vertices [vr, vr + 32): row ends and headers, one per lane
+        const uint32_t wv = vr + lane;
+        const uint64_t base = rowptr[vr];
+        const uint64_t e = wv < g.n ? rowptr[wv + 1] : ~0ull;
+        VHdr hw;
+        if (wv < g.n) {
+          hw = header<MODE>(g, wv);
+        } else {
+          hw.d = 0; hw.P = 0; hw.v = 0; hw.bn = hw.bl = hw.om = hw.fp = 0; hw.a = hw.b = 0;
+        }
+        // owner lane k: number of window rows that end at or before gl
+        // (binary lifting over 31 probes gives the exact count when it is
+        // below 32)
 #pragma unroll
-      for (int step = 16; step > 0; step >>= 1) {
-        const uint64_t ek = __shfl_sync(FULL, e, k + step - 1);
-        if (ek <= gl) k += step;
-      }
-      // a count of 32 means gl lies beyond the window (a run of >= 32 empty
-      // rows); those lanes resolve their vertex and header on their own.
-      const uint64_t e31 = __shfl_sync(FULL, e, 31);
-      const bool far = act && e31 <= gl;
-      const int src = far ? 0 : k;
-      const uint64_t prev_e = __shfl_sync(FULL, e, src > 0 ? src - 1 : 0);
-      VHdr hk = shfl_hdr(hw, src);
-      uint64_t startv = src == 0 ? base : prev_e;
-      if (far) {
-        const uint32_t v = row_of_serial(rowptr, vr + 32, g.n, gl);
-        hk = header<MODE>(g, v);
-        startv = rowptr[v];
+        for (int step = 16; step > 0; step >>= 1) {
+          const uint64_t ek = __shfl_sync(FULL, e, k + step - 1);
+          if (ek <= gl) k += step;
+        }
+        // a count of 32 means gl lies beyond the window (a run of >= 32 empty
+        // rows); those lanes resolve their vertex and header on their own.
+        const uint64_t e31 = __shfl_sync(FULL, e, 31);
+        far = act && e31 <= gl;
+        const int src = far ? 0 : k;
+        const uint64_t prev_e = __shfl_sync(FULL, e, src > 0 ? src - 1 : 0);
+        hk = shfl_hdr(hw, src);
+        startv = src == 0 ? base : prev_e;
+        if (far) {
+          const uint32_t v = row_of_serial(rowptr, vr + 32, g.n, gl);
+          hk = header<MODE>(g, v);
+          startv = rowptr[v];
+        }
       }
       const uint32_t i = (uint32_t)(gl - startv);
       uint32_t val = 0;
       if (MODE == 1) {
-        if (act) val = le_neighbor(g, hk, i);
+        if (act) val = le_neighbor_words(g.words, hk, i);
       } else {
         bool head = true;
         uint32_t x = 0;
@@ -172,12 +236,14 @@ __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint6
         cols[gl] = val;
       }
       // next window starts at the vertex of the round's last neighbor
-      const uint32_t vlast = __shfl_sync(FULL, far ? 0xFFFFFFFFu : vr + (uint32_t)k, 31);
-      if (vlast != 0xFFFFFFFFu) {
-        vr = vlast;
-      } else {
-        const uint64_t gl31 = r + 31;
-        vr = gl31 < g1 ? warp_row_of(rowptr, g.n, gl31) : vr;
+      if (!single) {
+        const uint32_t vlast = __shfl_sync(FULL, far ? 0xFFFFFFFFu : vr + (uint32_t)k, 31);
+        if (vlast != 0xFFFFFFFFu) {
+          vr = vlast;
+        } else {
+          const uint64_t gl31 = r + 31;
+          vr = gl31 < g1 ? warp_row_of(rowptr, g.n, gl31) : vr;
+        }
       }
     }
   }
