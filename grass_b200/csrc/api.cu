@@ -359,6 +359,8 @@ int grass_close(grass_graph *g) {
   cudaFree(g->d_offsets);
   cudaFree(g->d_recs);
   cudaFree(g->d_err);
+  cudaFree(g->d_plan_big);
+  cudaFree(g->d_plan_small);
   delete g;
   return GRASS_OK;
 }
@@ -419,9 +421,9 @@ int grass_decode_all(const grass_graph *g, uint64_t *d_rowptr, uint32_t *d_cols,
   GRASS_CUDA(cudaMallocAsync(&scan_tmp, (scan_tmp_words(n) + 1) * sizeof(uint64_t), st));
   launch_degrees64(g->view(), d_rowptr, st);
   launch_scan_u64_inplace(d_rowptr, n, scan_tmp, st);
-  launch_decode_all(g->view(), d_rowptr, d_cols, g->info.num_edges, g->d_err, st);
+  int rc = launch_decode_planned(g, d_rowptr, d_cols, g->d_err, st);
   cudaFreeAsync(scan_tmp, st);
-  return check_launch();
+  return rc ? rc : check_launch();
 }
 
 int grass_uniform_starts(uint64_t n, uint64_t count, uint64_t seed, uint32_t *d_out,

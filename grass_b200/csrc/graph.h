@@ -55,6 +55,15 @@ struct grass_graph {
   unsigned int *d_err = nullptr;   // device error word (GRASS_E_DATA on bad ids)
   grass_graph_info info{};
   grass_tuning tuning{};
+  // Decode plan, built by the first grass_decode_all and kept: the neighbor
+  // ranges (v, i0, i1, 0) of vertices with degree >= 32, at most 2048
+  // neighbors each, and the vertices of degree 1..31 grouped by
+  // floor(log2(degree)).
+  mutable std::mutex plan_mu;
+  mutable uint4 *d_plan_big = nullptr;
+  mutable uint32_t *d_plan_small = nullptr;
+  mutable uint64_t plan_nbig = 0, plan_nsmall = 0;
+  mutable bool plan_ok = false;
   grass::DevGraph view() const {
     grass::DevGraph g;
     g.words = d_words;
@@ -137,6 +146,11 @@ void launch_scan_u64_inplace(uint64_t *vals, uint64_t n, uint64_t *tmp, cudaStre
 
 // ---- decode (kernels_decode.cu) ----
 // E = rowptr[n] (the number of edges, known from load-time validation).
+// Decode sweep through the graph's decode plan (built on first use; the
+// build allocates and synchronises once).  rowptr must hold the scanned
+// degrees.
+int launch_decode_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
+                          unsigned int *err, cudaStream_t s);
 void launch_decode_all(const DevGraph &g, const uint64_t *rowptr, uint32_t *cols, uint64_t E,
                        unsigned int *err, cudaStream_t s);
 

@@ -20,6 +20,8 @@
 //     carried from round to round (and, at a task start inside a block,
 //     decoded once by lane 0);
 //  4. writes its 32 ids with one coalesced store.
+#include <type_traits>
+
 #include "graph.h"
 
 namespace grass {
@@ -250,7 +252,398 @@ __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint6
   if (bad && err) atomicOr(err, 1u);
 }
 
+// ---------------------------------------------------------------------------
+// Planned sweep.  The first sweep of a graph builds a plan once: vertices of
+// degree >= 32 become neighbor ranges of at most 2048 (hubs are split), the
+// others are grouped by floor(log2(degree)).  Then
+//  * a range is decoded by one warp in rounds of 32 consecutive neighbors
+//    (coalesced stores).  The round's chunk / block position is carried from
+//    round to round and each lane steps to its own with a few compares, so
+//    there is no per-neighbor division: LE divides once per chunk
+//    ((r2 - r1) / L_c, by the lane that starts the chunk, then shuffled), GT
+//    runs a segmented warp scan of gaps (LE/src/bcg.cuh:195-261,
+//    GT/src/bcg.cuh:153-168);
+//  * a small vertex is decoded by one lane, sequentially with bit cursors
+//    (seas, or heads and gaps, are contiguous in neighbor order); a warp
+//    takes 32 vertices of one degree class, so its lanes run for similar
+//    lengths.
+constexpr uint32_t kBigDegree = 32;
+constexpr uint32_t kRange = 2048;
+
+// Sequential decoders of one vertex (one lane each), from neighbor 0.
+struct LeSeq {
+  const uint32_t *w;
+  uint64_t P;
+  uint32_t v, fp, bl, om, bn, c, id, tl, r1, r2, step;
+  int a, sw;  // rock width, sea width (magnitude + sign)
+  bool one;   // degree 1: the neighbor is stored in the header
+  BitCur sea;
+
+  __device__ __forceinline__ uint32_t rock(uint32_t k) const {
+    const uint32_t m = read_field(w, P + (uint64_t)k * (uint64_t)a, a);
+    return k < fp ? v - m : v + m;
+  }
+  __device__ __forceinline__ void init(const uint32_t *words, const VHdr &h) {
+    w = words;
+    P = h.P;
+    v = h.v;
+    fp = h.fp;
+    one = h.d == 1;
+    if (one) return;
+    bl = h.bl;
+    om = h.om;
+    bn = h.bn;
+    a = h.a;
+    sw = h.b + 1;
+    c = 0;
+    id = 0;
+    tl = om ? bl + 1 : bl;
+    r1 = rock(0);
+    r2 = rock(1);
+    step = (r2 - r1) / tl;
+    sea.init(w, P + (uint64_t)(bn + 1) * (uint64_t)a);
+  }
+  __device__ __forceinline__ uint32_t next() {
+    if (one) return fp;
+    uint32_t val;
+    if (id == 0) {
+      val = r1;
+    } else {
+      uint32_t raw;
+      if (sw > 32) {  // 33-bit field: keep its low 32 bits, as the random-access decode does
+        sea.get(sw - 32);
+        raw = sea.get(32);
+      } else {
+        raw = sea.get(sw);
+      }
+      const uint32_t mag = raw >> 1;
+      val = step * id + r1 + ((raw & 1u) ? 0u - mag : mag);
+    }
+    if (++id == tl) {
+      c++;
+      id = 0;
+      tl = c < om ? bl + 1 : bl;
+      r1 = r2;
+      if (c < bn) {
+        r2 = rock(c + 1);
+        step = (r2 - r1) / tl;
+      }
+    }
+    return val;
+  }
+};
+
+struct GtSeq {
+  uint32_t v, fp, bl, om, blk, id, len, prev;
+  int a, b;
+  BitCur cur;
+
+  __device__ __forceinline__ void init(const uint32_t *words, const VHdr &h) {
+    v = h.v;
+    fp = h.fp;
+    bl = h.bl;
+    om = h.om;
+    a = h.a;
+    b = h.b;
+    blk = 0;
+    id = 0;
+    len = om ? bl + 1 : bl;
+    prev = 0;
+    cur.init(words, h.P);
+  }
+  __device__ __forceinline__ uint32_t next() {
+    uint32_t val;
+    if (id == 0) {
+      const uint32_t hv = (a ? cur.get(a) : 0u) + 1u;
+      val = blk >= fp ? v + hv : v - hv;
+    } else {
+      val = prev + (b ? cur.get(b) : 0u) + 1u;
+    }
+    prev = val;
+    if (++id == len) {
+      blk++;
+      id = 0;
+      len = blk < om ? bl + 1 : bl;
+    }
+    return val;
+  }
+};
+
+// Plan construction.  counts: [ranges, class 0..4]; cursors: output positions.
+__global__ void plan_count_kernel(const uint4 *__restrict__ recs, uint32_t n,
+                                  unsigned long long *counts) {
+  __shared__ unsigned long long sc[6];
+  if (threadIdx.x < 6) sc[threadIdx.x] = 0;
+  __syncthreads();
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t d = recs[v].z;
+    if (d >= kBigDegree) atomicAdd(&sc[0], (unsigned long long)((d + kRange - 1) / kRange));
+    else if (d) atomicAdd(&sc[1 + (31 - __clz(d))], 1ull);
+  }
+  __syncthreads();
+  if (threadIdx.x < 6 && sc[threadIdx.x]) atomicAdd(&counts[threadIdx.x], sc[threadIdx.x]);
+}
+
+__global__ void plan_fill_kernel(const uint4 *__restrict__ recs, uint32_t n,
+                                 unsigned long long *cursors, uint4 *big, uint32_t *small) {
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const uint32_t d = recs[v].z;
+    if (d >= kBigDegree) {
+      const uint32_t k = (d + kRange - 1) / kRange;
+      const unsigned long long p = atomicAdd(&cursors[0], (unsigned long long)k);
+      for (uint32_t j = 0; j < k; j++)
+        big[p + j] = make_uint4(v, j * kRange, min(d, (j + 1) * kRange), 0u);
+    } else if (d) {
+      small[atomicAdd(&cursors[1 + (31 - __clz(d))], 1ull)] = v;
+    }
+  }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uint64_t *rowptr,
+                                                             uint32_t *cols,
+                                                             const uint4 *__restrict__ items,
+                                                             uint64_t nitems, unsigned int *err) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  bool bad = false;
+  for (uint64_t t = warp; t < nitems; t += nwarps) {
+    const uint4 it = items[t];
+    const uint32_t i0 = it.y, i1 = it.z;
+    const VHdr h = header<MODE>(g, it.x);
+    uint32_t *out = cols + rowptr[it.x];
+    // position of neighbor i0: chunk (LE) / block (GT) c0, index id0, length tl0
+    uint32_t c0, id0, tl0;
+    if (MODE == 1) {
+      tl0 = h.bl + 1;
+      const uint32_t split = h.om * tl0;
+      const bool flag = i0 >= split;
+      const uint32_t j = flag ? i0 - split : i0;
+      if (flag) tl0 = h.bl;
+      c0 = j / tl0;
+      id0 = j - c0 * tl0;
+      if (flag) c0 += h.om;
+    } else {
+      const uint32_t split = (h.bl + 1) * h.om;
+      const bool flag = i0 < split;
+      const uint32_t j = flag ? i0 : i0 - split;
+      tl0 = h.bl + (flag ? 1u : 0u);
+      c0 = j / tl0;
+      id0 = j - c0 * tl0;
+      if (!flag) c0 += h.om;
+    }
+    uint32_t carry = 0;  // GT: value of neighbor i0 - 1 when i0 is inside a block
+    if (MODE == 0 && id0 > 0) {
+      uint32_t x = 0;
+      if (lane == 0) x = gt_neighbor(g, h, i0 - 1);
+      carry = __shfl_sync(FULL, x, 0);
+    }
+    const uint64_t sea0 = h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a;
+    const uint64_t blkbits = (uint64_t)h.a + (uint64_t)(h.bl - 1) * h.b;
+    const int sw = h.b + 1;
+    // LE: left rock and step of chunk c0, carried from round to round
+    uint32_t cr1 = 0, cstep = 0;
+    if (MODE == 1 && id0 > 0) {
+      const uint64_t rw = read_bits64(g.words, h.P + (uint64_t)c0 * (uint64_t)h.a);
+      const uint32_t r1m = (uint32_t)(rw >> (64 - h.a)), r2m = (uint32_t)((rw << h.a) >> (64 - h.a));
+      cr1 = c0 < h.fp ? h.v - r1m : h.v + r1m;
+      const uint32_t r2 = c0 + 1 < h.fp ? h.v - r2m : h.v + r2m;
+      cstep = (r2 - cr1) / tl0;
+    }
+    for (uint32_t r = i0; r < i1; r += 32) {
+      const uint32_t i = r + lane;
+      const bool act = i < i1;
+      uint32_t id = id0 + lane, c = c0, tl = tl0;
+      while (id >= tl) {  // at most a few steps: lanes are consecutive neighbors
+        id -= tl;
+        c++;
+        tl = c < h.om ? h.bl + 1 : h.bl;
+      }
+      uint32_t val = 0;
+      if (MODE == 1) {
+        // A lane that starts a chunk reads its rock pair and divides once;
+        // the chunk's other lanes take them by shuffle (or from the carry).
+        uint32_t lr1 = 0, lst = 0;
+        if (act && id == 0) {
+          const uint64_t rw = read_bits64(g.words, h.P + (uint64_t)c * (uint64_t)h.a);
+          const uint32_t r1m = (uint32_t)(rw >> (64 - h.a));
+          lr1 = c < h.fp ? h.v - r1m : h.v + r1m;
+          if (c < h.bn) {
+            const uint32_t r2m = (uint32_t)((rw << h.a) >> (64 - h.a));
+            lst = ((c + 1 < h.fp ? h.v - r2m : h.v + r2m) - lr1) / tl;
+          }
+        }
+        const int ld = lane - (int)min(id, (uint32_t)lane);  // the chunk's first lane, or 0
+        const uint32_t sr1 = __shfl_sync(FULL, lr1, ld), sst = __shfl_sync(FULL, lst, ld);
+        const bool in_round = id <= (uint32_t)lane;  // the chunk starts in this round
+        const uint32_t r1 = in_round ? sr1 : cr1, step = in_round ? sst : cstep;
+        if (act) {
+          if (id == 0) {
+            val = r1;
+          } else {
+            const uint64_t sp = sea0 + (uint64_t)(i - c - 1) * (uint64_t)sw;
+            const uint32_t raw = sw <= 32 ? read_field(g.words, sp, sw)
+                                          : (uint32_t)(read_bits64(g.words, sp) >> 31);
+            const uint32_t mag = raw >> 1;
+            val = step * id + r1 + ((raw & 1u) ? 0u - mag : mag);
+          }
+        }
+        cr1 = __shfl_sync(FULL, r1, 31);
+        cstep = __shfl_sync(FULL, step, 31);
+      } else {
+        bool head = true;
+        uint32_t x = 0;
+        if (act) {
+          const uint64_t hp = h.P + (uint64_t)c * blkbits + (uint64_t)min(c, h.om) * h.b;
+          if (id == 0) {
+            const uint32_t hv = read_field(g.words, hp, h.a) + 1u;
+            x = c >= h.fp ? h.v + hv : h.v - hv;
+          } else {
+            head = false;
+            x = read_field(g.words, hp + h.a + (uint64_t)(id - 1) * h.b, h.b) + 1u;
+          }
+        }
+        if (lane == 0 && !head) {
+          x += carry;
+          head = true;
+        }
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {  // segmented inclusive scan
+          const uint32_t y = __shfl_up_sync(FULL, x, o);
+          const int f = __shfl_up_sync(FULL, (int)head, o);
+          if (lane >= o && !head) {
+            x += y;
+            head = f;
+          }
+        }
+        carry = __shfl_sync(FULL, x, 31);
+        val = x;
+      }
+      if (act) {
+        bad |= val >= g.n;
+        out[i] = val;
+      }
+      // the next round starts one neighbor after lane 31
+      c0 = __shfl_sync(FULL, c, 31);
+      id0 = __shfl_sync(FULL, id, 31) + 1;
+      tl0 = __shfl_sync(FULL, tl, 31);
+      if (id0 == tl0) {
+        c0++;
+        id0 = 0;
+        tl0 = c0 < h.om ? h.bl + 1 : h.bl;
+      }
+    }
+  }
+  if (bad && err) atomicOr(err, 1u);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) decode_small_kernel(DevGraph g, const uint64_t *rowptr,
+                                                             uint32_t *cols,
+                                                             const uint32_t *__restrict__ verts,
+                                                             uint64_t nv, unsigned int *err) {
+  bool bad = false;
+  const uint64_t nt = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t q0 = (uint64_t)blockIdx.x * blockDim.x; q0 < nv; q0 += nt) {
+    const uint64_t q = q0 + threadIdx.x;
+    uint32_t d = 0;
+    uint32_t *out = nullptr;
+    std::conditional_t<MODE == 0, GtSeq, LeSeq> st;
+    if (q < nv) {
+      const uint32_t v = verts[q];
+      const VHdr h = header<MODE>(g, v);
+      d = h.d;
+      out = cols + rowptr[v];
+      st.init(g.words, h);
+    }
+    for (uint32_t k = 0; k < d; k++) {
+      const uint32_t val = st.next();
+      bad |= val >= g.n;
+      out[k] = val;
+    }
+  }
+  if (bad && err) atomicOr(err, 1u);
+}
+
 }  // namespace
+
+int launch_decode_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
+                          unsigned int *err, cudaStream_t s) {
+  const uint32_t n = (uint32_t)g->info.n;
+  if (!g->info.num_edges) return GRASS_OK;
+  const int dev = g->device;
+  {
+    std::lock_guard<std::mutex> lk(g->plan_mu);
+    if (!g->plan_ok) {
+      unsigned long long *cnt = nullptr;
+      GRASS_CUDA(cudaMalloc(&cnt, 12 * sizeof(unsigned long long)));
+      GRASS_CUDA(cudaMemset(cnt, 0, 12 * sizeof(unsigned long long)));
+      const unsigned grid = (unsigned)std::max<uint64_t>(
+          1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count(dev) * 8));
+      plan_count_kernel<<<grid, 256>>>(g->d_recs, n, cnt);
+      count_launch();
+      unsigned long long h[12] = {0};
+      cudaError_t e = cudaMemcpy(h, cnt, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+      if (e != cudaSuccess) {
+        cudaFree(cnt);
+        return cuda_fail(e, "decode plan counts");
+      }
+      h[6] = 0;  // cursors: ranges, then the classes back to back
+      uint64_t off = 0;
+      for (int k = 1; k < 6; k++) {
+        h[6 + k] = off;
+        off += h[k];
+      }
+      g->plan_nbig = h[0];
+      g->plan_nsmall = off;
+      e = cudaMalloc(&g->d_plan_big, std::max<uint64_t>(h[0], 1) * sizeof(uint4));
+      if (e == cudaSuccess)
+        e = cudaMalloc(&g->d_plan_small, std::max<uint64_t>(off, 1) * sizeof(uint32_t));
+      if (e == cudaSuccess)
+        e = cudaMemcpy(cnt + 6, h + 6, 6 * sizeof(unsigned long long), cudaMemcpyHostToDevice);
+      if (e != cudaSuccess) {
+        cudaFree(cnt);
+        cudaFree(g->d_plan_big);
+        cudaFree(g->d_plan_small);
+        g->d_plan_big = nullptr;
+        g->d_plan_small = nullptr;
+        return cuda_fail(e, "decode plan");
+      }
+      plan_fill_kernel<<<grid, 256>>>(g->d_recs, n, cnt + 6, g->d_plan_big, g->d_plan_small);
+      count_launch();
+      e = cudaDeviceSynchronize();
+      cudaFree(cnt);
+      if (e != cudaSuccess) return cuda_fail(e, "decode plan build");
+      g->plan_ok = true;
+    }
+  }
+  const DevGraph v = g->view();
+  const int per_sm = 8;
+  if (g->plan_nbig) {
+    const unsigned grid = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>((g->plan_nbig + 7) / 8, (uint64_t)sm_count(dev) * per_sm));
+    if (g->mode == GRASS_MODE_GT)
+      decode_range_kernel<0><<<grid, 256, 0, s>>>(v, rowptr, cols, g->d_plan_big, g->plan_nbig,
+                                                   err);
+    else
+      decode_range_kernel<1><<<grid, 256, 0, s>>>(v, rowptr, cols, g->d_plan_big, g->plan_nbig,
+                                                   err);
+    count_launch();
+  }
+  if (g->plan_nsmall) {
+    const unsigned grid = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>((g->plan_nsmall + 255) / 256, (uint64_t)sm_count(dev) * per_sm));
+    if (g->mode == GRASS_MODE_GT)
+      decode_small_kernel<0><<<grid, 256, 0, s>>>(v, rowptr, cols, g->d_plan_small,
+                                                  g->plan_nsmall, err);
+    else
+      decode_small_kernel<1><<<grid, 256, 0, s>>>(v, rowptr, cols, g->d_plan_small,
+                                                  g->plan_nsmall, err);
+    count_launch();
+  }
+  return GRASS_OK;
+}
 
 void launch_decode_all(const DevGraph &g, const uint64_t *rowptr, uint32_t *cols, uint64_t E,
                        unsigned int *err, cudaStream_t s) {
