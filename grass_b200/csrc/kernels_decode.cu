@@ -399,139 +399,195 @@ __global__ void plan_fill_kernel(const uint4 *__restrict__ recs, uint32_t n,
   }
 }
 
+// The warp asks L2 for every 128-byte line of stream bits [lo, hi): a range
+// reads its stream in order, so without this each new line is a full DRAM
+// round trip with nothing else in flight for the warp.
+__device__ __forceinline__ void prefetch_bits(const uint32_t *words, uint64_t lo, uint64_t hi) {
+  const int lane = threadIdx.x & 31;
+  if (hi <= lo) return;
+  const char *base = reinterpret_cast<const char *>(words);
+  const uint64_t l0 = (lo >> 3) >> 7, l1 = ((hi - 1) >> 3) >> 7;  // lines holding bits lo..hi-1
+  for (uint64_t l = l0 + lane; l <= l1; l += 32)
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(base + (l << 7)));
+}
+
+// A neighbor range is cut into runs of 8 consecutive CSR slots aligned to 8
+// (32 bytes); lane l of a warp takes run l of each group of 32 runs, decodes
+// it in order with a bit cursor and stores a full run with two 16-byte
+// writes, so the warp writes 1 KB contiguous per group.
+constexpr uint32_t kRun = 8;
+
 template <int MODE>
 __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uint64_t *rowptr,
                                                              uint32_t *cols,
                                                              const uint4 *__restrict__ items,
-                                                             uint64_t nitems, unsigned int *err) {
+                                                             uint64_t nitems, bool vec,
+                                                             unsigned int *err) {
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   bool bad = false;
   for (uint64_t t = warp; t < nitems; t += nwarps) {
     const uint4 it = items[t];
-    const uint32_t i0 = it.y, i1 = it.z;
     const VHdr h = header<MODE>(g, it.x);
-    uint32_t *out = cols + rowptr[it.x];
-    // position of neighbor i0: chunk (LE) / block (GT) c0, index id0, length tl0
-    uint32_t c0, id0, tl0;
-    if (MODE == 1) {
-      tl0 = h.bl + 1;
-      const uint32_t split = h.om * tl0;
-      const bool flag = i0 >= split;
-      const uint32_t j = flag ? i0 - split : i0;
-      if (flag) tl0 = h.bl;
-      c0 = j / tl0;
-      id0 = j - c0 * tl0;
-      if (flag) c0 += h.om;
-    } else {
-      const uint32_t split = (h.bl + 1) * h.om;
-      const bool flag = i0 < split;
-      const uint32_t j = flag ? i0 : i0 - split;
-      tl0 = h.bl + (flag ? 1u : 0u);
-      c0 = j / tl0;
-      id0 = j - c0 * tl0;
-      if (!flag) c0 += h.om;
-    }
-    uint32_t carry = 0;  // GT: value of neighbor i0 - 1 when i0 is inside a block
-    if (MODE == 0 && id0 > 0) {
-      uint32_t x = 0;
-      if (lane == 0) x = gt_neighbor(g, h, i0 - 1);
-      carry = __shfl_sync(FULL, x, 0);
-    }
+    const uint64_t base = rowptr[it.x];
+    const uint64_t G0 = base + it.y, G1 = base + it.z;  // CSR slots of the range
     const uint64_t sea0 = h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a;
     const uint64_t blkbits = (uint64_t)h.a + (uint64_t)(h.bl - 1) * h.b;
+    const uint32_t split = h.om * (h.bl + 1);
     const int sw = h.b + 1;
-    // LE: left rock and step of chunk c0, carried from round to round
-    uint32_t cr1 = 0, cstep = 0;
-    if (MODE == 1 && id0 > 0) {
-      const uint64_t rw = read_bits64(g.words, h.P + (uint64_t)c0 * (uint64_t)h.a);
-      const uint32_t r1m = (uint32_t)(rw >> (64 - h.a)), r2m = (uint32_t)((rw << h.a) >> (64 - h.a));
-      cr1 = c0 < h.fp ? h.v - r1m : h.v + r1m;
-      const uint32_t r2 = c0 + 1 < h.fp ? h.v - r2m : h.v + r2m;
-      cstep = (r2 - cr1) / tl0;
-    }
-    for (uint32_t r = i0; r < i1; r += 32) {
-      const uint32_t i = r + lane;
-      const bool act = i < i1;
-      uint32_t id = id0 + lane, c = c0, tl = tl0;
-      while (id >= tl) {  // at most a few steps: lanes are consecutive neighbors
-        id -= tl;
-        c++;
-        tl = c < h.om ? h.bl + 1 : h.bl;
-      }
-      uint32_t val = 0;
+    {  // ask L2 for the range's stream bits (read in order below), within the payload
+      const uint32_t i0 = it.y, i1 = it.z;
+      const uint64_t pend = payload_end<MODE>(g, h);
+      const uint32_t c0 = i0 < split ? i0 / (h.bl + 1) : h.om + (i0 - split) / max(h.bl, 1u);
+      const uint64_t cl = c0 + (i1 - i0) / max(h.bl, 1u) + 2;
       if (MODE == 1) {
-        // A lane that starts a chunk reads its rock pair and divides once;
-        // the chunk's other lanes take them by shuffle (or from the carry).
-        uint32_t lr1 = 0, lst = 0;
-        if (act && id == 0) {
+        prefetch_bits(g.words, h.P + (uint64_t)c0 * h.a,
+                      min(pend, h.P + min(cl, (uint64_t)h.bn + 1) * h.a));
+        prefetch_bits(g.words, sea0 + (uint64_t)(i0 > c0 ? i0 - c0 - 1 : 0) * sw,
+                      min(pend, sea0 + (uint64_t)i1 * sw));
+      } else {
+        prefetch_bits(g.words, h.P + (uint64_t)c0 * blkbits + (uint64_t)min(c0, h.om) * h.b,
+                      min(pend, h.P + cl * blkbits + min(cl, (uint64_t)h.om) * h.b));
+      }
+    }
+    uint32_t carry = 0;  // GT: value of the slot before the current group
+    bool carry_ok = false;
+    for (uint64_t gs = G0 & ~(uint64_t)(kRun - 1); gs < G1; gs += 32 * kRun) {
+      const uint64_t rs = gs + (uint64_t)lane * kRun;  // this lane's run [rs, rs + 8)
+      const uint64_t a0 = max(rs, G0), a1 = min(rs + kRun, G1);
+      const uint32_t cnt = a1 > a0 ? (uint32_t)(a1 - a0) : 0u;
+      const uint32_t s = cnt ? (uint32_t)(a0 - base) : it.y;  // first neighbor of the run
+      uint32_t vals[kRun];
+      // chunk / block c of neighbor s, index id within it, length tl
+      const bool hi = s < split;
+      uint32_t tl = hi ? h.bl + 1 : h.bl;
+      const uint32_t j = hi ? s : s - split;
+      uint32_t c = tl ? j / tl : 0u;
+      uint32_t id = j - c * tl;
+      if (!hi) c += h.om;
+      if (MODE == 1) {
+        uint32_t r1 = 0, r2 = 0, step = 0;
+        BitCur sea;
+        if (cnt) {
           const uint64_t rw = read_bits64(g.words, h.P + (uint64_t)c * (uint64_t)h.a);
           const uint32_t r1m = (uint32_t)(rw >> (64 - h.a));
-          lr1 = c < h.fp ? h.v - r1m : h.v + r1m;
+          r1 = c < h.fp ? h.v - r1m : h.v + r1m;
           if (c < h.bn) {
             const uint32_t r2m = (uint32_t)((rw << h.a) >> (64 - h.a));
-            lst = ((c + 1 < h.fp ? h.v - r2m : h.v + r2m) - lr1) / tl;
+            r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
+            step = (r2 - r1) / tl;
           }
+          // next sea in neighbor order: index s - c - 1 (id > 0) or s - c (id == 0)
+          sea.init(g.words, sea0 + (uint64_t)(s - c - (id ? 1u : 0u)) * (uint64_t)sw);
         }
-        const int ld = lane - (int)min(id, (uint32_t)lane);  // the chunk's first lane, or 0
-        const uint32_t sr1 = __shfl_sync(FULL, lr1, ld), sst = __shfl_sync(FULL, lst, ld);
-        const bool in_round = id <= (uint32_t)lane;  // the chunk starts in this round
-        const uint32_t r1 = in_round ? sr1 : cr1, step = in_round ? sst : cstep;
-        if (act) {
+#pragma unroll
+        for (uint32_t k = 0; k < kRun; k++) {
+          if (k >= cnt) break;
+          uint32_t val;
           if (id == 0) {
             val = r1;
           } else {
-            const uint64_t sp = sea0 + (uint64_t)(i - c - 1) * (uint64_t)sw;
-            const uint32_t raw = sw <= 32 ? read_field(g.words, sp, sw)
-                                          : (uint32_t)(read_bits64(g.words, sp) >> 31);
+            uint32_t raw;
+            if (sw > 32) {  // 33-bit field: keep its low 32 bits, as the random-access decode does
+              sea.get(sw - 32);
+              raw = sea.get(32);
+            } else {
+              raw = sea.get(sw);
+            }
             const uint32_t mag = raw >> 1;
             val = step * id + r1 + ((raw & 1u) ? 0u - mag : mag);
           }
-        }
-        cr1 = __shfl_sync(FULL, r1, 31);
-        cstep = __shfl_sync(FULL, step, 31);
-      } else {
-        bool head = true;
-        uint32_t x = 0;
-        if (act) {
-          const uint64_t hp = h.P + (uint64_t)c * blkbits + (uint64_t)min(c, h.om) * h.b;
-          if (id == 0) {
-            const uint32_t hv = read_field(g.words, hp, h.a) + 1u;
-            x = c >= h.fp ? h.v + hv : h.v - hv;
-          } else {
-            head = false;
-            x = read_field(g.words, hp + h.a + (uint64_t)(id - 1) * h.b, h.b) + 1u;
+          vals[k] = val;
+          if (++id == tl) {  // next chunk: its left rock is this chunk's right rock
+            c++;
+            id = 0;
+            tl = c < h.om ? h.bl + 1 : h.bl;
+            r1 = r2;
+            if (c < h.bn) {
+              const uint32_t r2m = read_field(g.words, h.P + (uint64_t)(c + 1) * h.a, h.a);
+              r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
+              step = (r2 - r1) / tl;
+            }
           }
         }
-        if (lane == 0 && !head) {
-          x += carry;
-          head = true;
+      } else {
+        // Fields in order: block c holds its head (a bits), then tl - 1 gaps.
+        // Slots before the run's first head are relative to the slot before
+        // the run, whose value a segmented warp scan over the runs supplies.
+        BitCur cur;
+        if (cnt) {
+          const uint64_t hp = h.P + (uint64_t)c * blkbits + (uint64_t)min(c, h.om) * h.b;
+          cur.init(g.words, id ? hp + h.a + (uint64_t)(id - 1) * h.b : hp);
+        }
+        uint32_t x = 0, rel = 0;  // rel: bit k set when slot k is relative
+        bool seen = false;         // a head has been read in this run
+#pragma unroll
+        for (uint32_t k = 0; k < kRun; k++) {
+          if (k >= cnt) break;
+          if (id == 0) {
+            const uint32_t hv = (h.a ? cur.get(h.a) : 0u) + 1u;
+            x = c >= h.fp ? h.v + hv : h.v - hv;
+            seen = true;
+          } else {
+            x += (h.b ? cur.get(h.b) : 0u) + 1u;
+            if (!seen) rel |= 1u << k;
+          }
+          vals[k] = x;
+          if (++id == tl) {
+            c++;
+            id = 0;
+            tl = c < h.om ? h.bl + 1 : h.bl;
+          }
+        }
+        // (absolute?, last value) of runs 0..lane; empty runs are the identity
+        uint32_t sx = cnt ? x : 0u;
+        bool sf = cnt && seen;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(FULL, sx, o);
+          const bool f = __shfl_up_sync(FULL, (int)sf, o);
+          if (lane >= o && !sf) {
+            sx += y;
+            sf = f;
+          }
+        }
+        uint32_t bx = __shfl_up_sync(FULL, sx, 1);
+        bool bf = __shfl_up_sync(FULL, (int)sf, 1);
+        if (lane == 0) {
+          bx = 0;
+          bf = false;
+        }
+        if (!carry_ok) {  // first group: the slot before G0 (used when G0 is inside a block)
+          uint32_t y = 0;
+          if (lane == 0 && it.y > 0) y = gt_neighbor(g, h, it.y - 1);
+          carry = __shfl_sync(FULL, y, 0);
+          carry_ok = true;
+        }
+        const uint32_t in = bf ? bx : carry + bx;  // value of the slot before the run
+#pragma unroll
+        for (uint32_t k = 0; k < kRun; k++)
+          if ((rel >> k) & 1u) vals[k] += in;
+        const unsigned has = __ballot_sync(FULL, cnt > 0);
+        uint32_t lastv = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < kRun; k++)
+          if (k + 1 == cnt) lastv = vals[k];
+        carry = __shfl_sync(FULL, lastv, 31 - __clz(has));
+      }
+      if (cnt) {
+        uint32_t *o = cols + a0;
+        if (cnt == kRun && vec) {  // aligned full run: two 16-byte stores
+          reinterpret_cast<uint4 *>(o)[0] = make_uint4(vals[0], vals[1], vals[2], vals[3]);
+          reinterpret_cast<uint4 *>(o)[1] = make_uint4(vals[4], vals[5], vals[6], vals[7]);
+        } else {
+#pragma unroll
+          for (uint32_t k = 0; k < kRun; k++)
+            if (k < cnt) o[k] = vals[k];
         }
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {  // segmented inclusive scan
-          const uint32_t y = __shfl_up_sync(FULL, x, o);
-          const int f = __shfl_up_sync(FULL, (int)head, o);
-          if (lane >= o && !head) {
-            x += y;
-            head = f;
-          }
-        }
-        carry = __shfl_sync(FULL, x, 31);
-        val = x;
-      }
-      if (act) {
-        bad |= val >= g.n;
-        out[i] = val;
-      }
-      // the next round starts one neighbor after lane 31
-      c0 = __shfl_sync(FULL, c, 31);
-      id0 = __shfl_sync(FULL, id, 31) + 1;
-      tl0 = __shfl_sync(FULL, tl, 31);
-      if (id0 == tl0) {
-        c0++;
-        id0 = 0;
-        tl0 = c0 < h.om ? h.bl + 1 : h.bl;
+        for (uint32_t k = 0; k < kRun; k++)
+          if (k < cnt) bad |= vals[k] >= g.n;
       }
     }
   }
@@ -623,12 +679,13 @@ int launch_decode_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t
   if (g->plan_nbig) {
     const unsigned grid = (unsigned)std::max<uint64_t>(
         1, std::min<uint64_t>((g->plan_nbig + 7) / 8, (uint64_t)sm_count(dev) * per_sm));
+    const bool vec = (reinterpret_cast<uintptr_t>(cols) & 15u) == 0;  // 16-byte stores allowed
     if (g->mode == GRASS_MODE_GT)
       decode_range_kernel<0><<<grid, 256, 0, s>>>(v, rowptr, cols, g->d_plan_big, g->plan_nbig,
-                                                   err);
+                                                   vec, err);
     else
       decode_range_kernel<1><<<grid, 256, 0, s>>>(v, rowptr, cols, g->d_plan_big, g->plan_nbig,
-                                                   err);
+                                                   vec, err);
     count_launch();
   }
   if (g->plan_nsmall) {
