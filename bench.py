@@ -363,32 +363,39 @@ def batch_bench(G, torch, graphs, n, stream, flush, K, W):
 
 SERVE_KEYS = ("completed", "rejected", "failed", "batches", "p50_us", "p99_us", "p999_us",
               "mean_us", "max_us", "p50_type_us", "p99_type_us", "queue_p50_us", "queue_p99_us",
-              "service_p50_us", "service_p99_us", "issue_us", "staging_alloc_us", "wall_s",
+              "service_p50_us", "service_p99_us", "issue_us", "staging_alloc_us", "phase_us",
+              "wall_s",
               "edges", "edges_per_s", "achieved_rate", "launches")
 
 
 def serve_bench(G, g, rates=(2000, 10000, 50000), seconds=0.25, plain_cap=1000):
     """Open-loop Poisson arrivals of the batched-jobs request mix through the
-    serving loop: (1) peak = the completion rate under 200k requests/s offered
-    (overload), (2) latency at 80% of that peak, (3) the listed rates.  At each
-    listed rate the first plain_cap requests of the same trace are also served
-    one standalone launch per request (the plain method)."""
-    def run(rate, nreq, mode=0):
-        r = G.loadgen(g, float(rate), nreq, mode=mode, seed=5)
+    serving loop, with results copied to host memory and with results kept
+    in device memory: (1) peak = the completion rate under 200k requests/s
+    offered (overload), (2) latency at 80% of that peak, (3) the listed
+    rates.  At each listed rate the first plain_cap requests of the same
+    trace are also served one standalone launch per request (the plain
+    method, results to the host)."""
+    def run(rate, nreq, mode=0, **kw):
+        r = G.loadgen(g, float(rate), nreq, mode=mode, seed=5, **kw)
         return {k: r[k] for k in SERVE_KEYS}
     out = {}
-    over = run(200000, 20000)
-    peak = over["achieved_rate"]
-    at80 = run(0.8 * peak, int(max(2000, 0.8 * peak * seconds)))
-    out["peak"] = {"offered_rate": 200000, "requests": 20000, "result": over,
-                   "peak_rate": peak, "peak_edges_per_s": over["edges_per_s"]}
-    out["at_80pct_of_peak"] = {"offered_rate": 0.8 * peak, "result": at80,
-                               "p99_under_5ms": at80["p99_us"] < 5000.0}
-    for rate in rates:
-        nreq = int(max(1000, rate * seconds))
-        out[str(rate)] = {"requests": nreq, "batched": run(rate, nreq),
-                          "one_job_per_launch": run(rate, min(nreq, plain_cap), mode=1),
-                          "plain_requests": min(nreq, plain_cap)}
+    for where, kw in (("host", {}), ("device", {"results_on_device": 1})):
+        o = {}
+        over = run(200000, 20000, **kw)
+        peak = over["achieved_rate"]
+        at80 = run(0.8 * peak, int(max(2000, 0.8 * peak * seconds)), **kw)
+        o["peak"] = {"offered_rate": 200000, "requests": 20000, "result": over,
+                     "peak_rate": peak, "peak_edges_per_s": over["edges_per_s"]}
+        o["at_80pct_of_peak"] = {"offered_rate": 0.8 * peak, "result": at80,
+                                 "p99_under_5ms": at80["p99_us"] < 5000.0}
+        for rate in rates:
+            nreq = int(max(1000, rate * seconds))
+            o[str(rate)] = {"requests": nreq, "batched": run(rate, nreq, **kw)}
+            if where == "host":
+                o[str(rate)]["one_job_per_launch"] = run(rate, min(nreq, plain_cap), mode=1)
+                o[str(rate)]["plain_requests"] = min(nreq, plain_cap)
+        out["results_" + where] = o
     return out
 
 

@@ -102,7 +102,8 @@ class ServerConfig(C.Structure):
     _fields_ = [("scratch_budget", C.c_uint64), ("target_draws", C.c_uint64),
                 ("staging_bytes", C.c_uint64), ("window_min_us", C.c_uint32), ("window_max_us", C.c_uint32),
                 ("max_inflight", C.c_uint32), ("max_batch_jobs", C.c_uint32),
-                ("batch", BatchConfig), ("reserved", C.c_uint32 * 4)]
+                ("batch", BatchConfig), ("results_on_device", C.c_uint32),
+                ("reserved", C.c_uint32 * 3)]
 
 
 class Request(C.Structure):
@@ -116,7 +117,8 @@ class Result(C.Structure):
     _fields_ = [("status", C.c_int), ("n_outputs", C.c_uint32),
                 ("out", C.c_void_p * MAX_HOPS), ("out_words", C.c_uint64 * MAX_HOPS),
                 ("edges", C.c_uint64), ("submit_us", C.c_double), ("launch_us", C.c_double),
-                ("done_us", C.c_double), ("batch", C.c_uint64)]
+                ("done_us", C.c_double), ("batch", C.c_uint64), ("on_device", C.c_uint32),
+                ("reserved", C.c_uint32)]
 
 
 class ServerStats(C.Structure):
@@ -124,10 +126,11 @@ class ServerStats(C.Structure):
                                           "batches", "edges", "waiting", "running",
                                           "scratch_in_use", "scratch_peak")] + \
                [("busy_us", C.c_double), ("issue_us", C.c_double),
-                ("staging_alloc_us", C.c_double)]
+                ("staging_alloc_us", C.c_double), ("phase_us", C.c_double * 6)]
 
     def as_dict(self):
-        return {k: getattr(self, k) for k, _ in self._fields_}
+        return {k: list(getattr(self, k)) if k == "phase_us" else getattr(self, k)
+                for k, _ in self._fields_}
 
 
 class LoadgenConfig(C.Structure):
@@ -149,6 +152,7 @@ class LoadgenReport(C.Structure):
                 ("queue_p50_us", C.c_double), ("queue_p99_us", C.c_double),
                 ("service_p50_us", C.c_double), ("service_p99_us", C.c_double),
                 ("issue_us", C.c_double), ("staging_alloc_us", C.c_double),
+                ("phase_us", C.c_double * 6),
                 ("wall_s", C.c_double), ("edges", C.c_double), ("edges_per_s", C.c_double),
                 ("offered_rate", C.c_double), ("achieved_rate", C.c_double),
                 ("launches", C.c_uint64)]
@@ -157,7 +161,7 @@ class LoadgenReport(C.Structure):
         d = {}
         for k, _ in self._fields_:
             v = getattr(self, k)
-            d[k] = list(v) if k.endswith("type_us") else v
+            d[k] = list(v) if k.endswith("type_us") or k == "phase_us" else v
         return d
 
 
@@ -565,6 +569,16 @@ class Batch:
             pass
 
 
+def _device_u32(ptr: int, n: int) -> np.ndarray:
+    """Host copy of n uint32 at a device address (a server result kept on the GPU)."""
+    import torch
+
+    class _View:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "<i4", "data": (ptr, False),
+                                    "version": 3}
+    return torch.as_tensor(_View(), device="cuda").cpu().numpy().view(np.uint32)
+
+
 def _request(type_, count, seed, inp, **kw) -> tuple[Request, object]:
     r = Request(type=type_, count=count, seed=seed)
     keep = None
@@ -629,11 +643,16 @@ class Server:
         out = {"status": res.status, "edges": res.edges, "submit_us": res.submit_us,
                "launch_us": res.launch_us, "done_us": res.done_us, "batch": res.batch,
                "outputs": []}
+        out["on_device"] = bool(res.on_device)
         for k in range(res.n_outputs):
             n = res.out_words[k]
-            buf = (C.c_uint32 * n).from_address(res.out[k]) if n else None
-            out["outputs"].append(np.ctypeslib.as_array(buf).copy() if n
-                                  else np.zeros(0, np.uint32))
+            if not n:
+                out["outputs"].append(np.zeros(0, np.uint32))
+            elif res.on_device:  # device memory: copy out through torch
+                out["outputs"].append(_device_u32(res.out[k], n))
+            else:
+                buf = (C.c_uint32 * n).from_address(res.out[k])
+                out["outputs"].append(np.ctypeslib.as_array(buf).copy())
         if release:
             _check(lib.grass_server_release(self._h, ticket))
         _check(rc)

@@ -95,7 +95,7 @@ double pct(std::vector<double> v, double p) {
 struct Outcome {
   std::vector<double> lat[3];
   std::vector<double> all, queue, service;
-  double issue_us = 0, alloc_us = 0;
+  double issue_us = 0, alloc_us = 0, phase_us[6] = {0, 0, 0, 0, 0, 0};
   double edges = 0, first = 1e300, last = 0;
   uint64_t completed = 0, rejected = 0, failed = 0;
 };
@@ -124,6 +124,7 @@ void finish_report(const grass_loadgen_config &c, const Outcome &o, grass_loadge
   r->service_p99_us = pct(o.service, 0.99);
   r->issue_us = o.issue_us;
   r->staging_alloc_us = o.alloc_us;
+  for (int k = 0; k < 6; k++) r->phase_us[k] = o.phase_us[k];
   r->wall_s = o.last > o.first ? (o.last - o.first) * 1e-6 : 0;
   r->edges = o.edges;
   r->edges_per_s = r->wall_s > 0 ? o.edges / r->wall_s : 0;
@@ -202,6 +203,7 @@ int run_server(const grass_graph *g, const grass_loadgen_config &c, std::vector<
   batches = st.batches;
   o.issue_us = st.issue_us;
   o.alloc_us = st.staging_alloc_us;
+  for (int k = 0; k < 6; k++) o.phase_us[k] = st.phase_us[k];
   return grass_server_destroy(srv, c.timeout_ms);
 }
 

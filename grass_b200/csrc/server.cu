@@ -6,9 +6,17 @@
 // groups waiting requests into a batch, reserves their device scratch against
 // the budget and issues, on one of up to eight streams:
 //
-//   pool alloc -> H2D (job table, work items, inputs, zeroed counters)
+//   H2D (job table, work items, inputs, zeroed counters)
 //     -> [multi-RW root draws] -> persistent batch kernel
-//     -> D2H (counters, outputs) -> pool free -> host callback
+//     -> D2H (counters, and the outputs unless they stay on the device)
+//     -> host callback
+//
+// Device scratch comes from one allocation of the whole budget made at
+// create and handed out first-fit when a batch is admitted (a stream-ordered
+// pool allocation per batch cost ~0.4 ms of dispatcher time as the pool grew
+// and fragmented); a batch's block returns when its callback runs, its
+// outputs' block (results on the device) when the last of its requests is
+// released.
 //
 // Requests come in two classes with separate queues and batches: RW / k-hop
 // (short, parallel over walkers and seeds) and multi-RW (sequential chains
@@ -19,9 +27,10 @@
 // dispatcher and the waiters.  Every request keeps its own Philox key and
 // 0-based walker / seed / sample ids, so its output is the standalone call's.
 //
-// Device block of one batch (every part 256-byte aligned):
-//   [multi-RW scratch] | H2D: [jobs][work items][queue][inputs]
-//   | H2D+D2H: [edges u64 x jobs][error word] | D2H: [outputs]
+// Device blocks of one batch (every part 256-byte aligned):
+//   work: [multi-RW scratch] | H2D: [jobs][work items][queue][inputs]
+//         | H2D+D2H: [edges u64 x jobs][error word] | D2H: [outputs]
+//   outputs on the device: the [outputs] part is a block of its own.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -43,26 +52,22 @@ constexpr uint32_t kMaxSlots = 8;
 
 inline uint64_t align_up(uint64_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 
-// Pinned host staging: one arena made at create (cudaHostAlloc takes
-// milliseconds per 100 MB and must not sit in a request's latency), handed
-// out first-fit from address-ordered free ranges that coalesce on return.
-struct Staging {
+// A region handed out first-fit from address-ordered free ranges that
+// coalesce on return: the pinned host staging arena (cudaHostAlloc takes
+// milliseconds per 100 MB and must not sit in a request's latency) and the
+// device scratch arena, both made once at create.
+struct Arena {
   std::mutex mu;
   uint8_t *base = nullptr;
   uint64_t size = 0;
   std::map<uint64_t, uint64_t> free_;  // offset -> bytes
 
   static uint64_t round(uint64_t b) { return (std::max<uint64_t>(b, 1) + 4095) & ~4095ull; }
-  cudaError_t init(uint64_t bytes) {
-    size = round(bytes);
-    const cudaError_t e = cudaHostAlloc(&base, size, cudaHostAllocDefault);
-    if (e != cudaSuccess) {
-      base = nullptr;
-      size = 0;
-      return e;
-    }
-    free_.emplace(0, size);
-    return e;
+  void reset(void *p, uint64_t bytes) {
+    base = static_cast<uint8_t *>(p);
+    size = bytes & ~4095ull;
+    free_.clear();
+    if (size) free_.emplace(0, size);
   }
   // A block of at least `bytes`, or nullptr while the arena has no room.
   void *take(uint64_t bytes) {
@@ -95,9 +100,6 @@ struct Staging {
       }
     }
     free_.emplace(off, bytes);
-  }
-  ~Staging() {
-    if (base) cudaFreeHost(base);
   }
 };
 
@@ -182,6 +184,8 @@ struct Batch {
   void *in_host = nullptr, *out_host = nullptr;
   uint64_t in_cap = 0, out_cap = 0;  // reserved bytes
   bool oversize = false;             // staging from the fallback pool, not the arena
+  uint8_t *d_work = nullptr, *d_out = nullptr;  // device blocks (d_out: results on device)
+  uint64_t work_bytes = 0, out_bytes = 0;       // their sizes (budget charges)
   uint32_t refs = 0;  // requests not yet released
   grass_server *srv = nullptr;
 };
@@ -196,11 +200,11 @@ struct grass_server {
   const grass_graph *g = nullptr;
   grass_server_config cfg{};
   grass_batch_config bcfg{};
-  cudaMemPool_t pool = nullptr;
   cudaStream_t streams[grass::kMaxSlots] = {nullptr};
   bool slot_busy[grass::kMaxSlots] = {false};
-  grass::Staging staging;
+  grass::Arena staging, scratch;  // pinned host, device
   grass::PinnedPool pinned;
+  bool dev_out = false;  // results stay on the device
 
   std::mutex mu;
   std::condition_variable cv_work;  // dispatcher: new request, finished batch, stop
@@ -236,6 +240,8 @@ struct grass_server {
     if (b->oversize) pinned.put(b->out_host, b->out_cap);
     else staging.give(b->out_host, b->out_cap);
     b->out_host = nullptr;
+    if (b->d_out) scratch.give(b->d_out, b->out_bytes);
+    b->d_out = nullptr;
   }
 };
 
@@ -361,25 +367,40 @@ Batch *grass_server::form(double now, int cls) {
     delete b;
     return nullptr;
   }
-  // Staging: tables and inputs in, counters and outputs out.
+  // Staging: tables and inputs in, counters (and outputs) out.  Device:
+  // the work block, and the outputs' own block when they stay on the device.
+  b->bytes = data + table_bytes(b->reqs.size(), ntasks);
+  b->out_bytes = dev_out ? sout : 0;
+  b->work_bytes = b->bytes - b->out_bytes;
   b->in_cap = table_bytes(b->reqs.size(), ntasks) + sin;
-  b->out_cap = align_up(b->reqs.size() * 8 + 4) + sout;
-  if (Staging::round(b->in_cap) + Staging::round(b->out_cap) > staging.size) {
+  b->out_cap = align_up(b->reqs.size() * 8 + 4) + (dev_out ? 0 : sout);
+  bool ok = true;
+  if (Arena::round(b->in_cap) + Arena::round(b->out_cap) > staging.size) {
     b->oversize = true;  // a single request larger than the arena
   } else {
     b->in_host = staging.take(b->in_cap);
     b->out_host = b->in_host ? staging.take(b->out_cap) : nullptr;
-    if (!b->out_host) {  // wait for releases; requests go back in order
-      staging.give(b->in_host, b->in_cap);
-      for (auto it = b->reqs.rbegin(); it != b->reqs.rend(); ++it) {
-        wq.push_front(*it);
-        waiting_draws[cls] += (*it)->draws;
-      }
-      delete b;
-      return nullptr;
-    }
+    ok = b->out_host != nullptr;
   }
-  b->bytes = data + table_bytes(b->reqs.size(), ntasks);
+  if (ok) {
+    b->d_work = static_cast<uint8_t *>(scratch.take(b->work_bytes));
+    b->d_out = !b->d_work || !b->out_bytes ? nullptr : static_cast<uint8_t *>(scratch.take(b->out_bytes));
+    ok = b->d_work && (b->d_out || !b->out_bytes);
+  }
+  if (!ok) {  // wait for releases (fragmented arenas); requests go back in order
+    if (!b->oversize) {
+      staging.give(b->in_host, b->in_cap);
+      staging.give(b->out_host, b->out_cap);
+    }
+    scratch.give(b->d_work, b->work_bytes);
+    scratch.give(b->d_out, b->out_bytes);
+    for (auto it = b->reqs.rbegin(); it != b->reqs.rend(); ++it) {
+      wq.push_front(*it);
+      waiting_draws[cls] += (*it)->draws;
+    }
+    delete b;
+    return nullptr;
+  }
   b->slot = slot;
   b->cls = cls;
   running_cls[cls]++;
@@ -436,22 +457,32 @@ void grass_server::launch(Batch *b) {
   }
   b->d2h_off = off;
   const uint64_t edges_off = off, err_off = off + nj * 8;
-  off += align_up(nj * 8 + 4);
+  const uint64_t hdr = align_up(nj * 8 + 4);
+  off += hdr;
   b->h2d_bytes = off - b->h2d_off;
+  // Outputs: after the header in the work block, or in their own block.
+  uint64_t oo = 0;
   for (size_t i = 0; i < nj; i++) {
     Req *q = b->reqs[i];
     for (uint32_t k = 0; k < q->nout; k++) {
-      q->out_off[k] = off - b->d2h_off;
-      off += align_up(q->out_words[k] * 4);
+      q->out_off[k] = oo;
+      oo += align_up(q->out_words[k] * 4);
     }
   }
-  b->d2h_bytes = off - b->d2h_off;
-  const uint64_t total = off;
+  b->d2h_bytes = hdr + (dev_out ? 0 : oo);
+  uint8_t *const d = b->d_work;
+  uint8_t *const dout = dev_out ? b->d_out : d + b->d2h_off + hdr;
 
   int rc = GRASS_OK;
-  uint8_t *d = nullptr;
   const double t_issue = now_us();
   double t_alloc = 0;
+  double ph[6] = {0, 0, 0, 0, 0, 0};
+  double tp = t_issue;
+  auto lap = [&](int k) {
+    const double x = now_us();
+    ph[k] += x - tp;
+    tp = x;
+  };
   {
     DeviceGuard dg(g->device);
     if (b->oversize) {
@@ -461,9 +492,10 @@ void grass_server::launch(Batch *b) {
     if (!b->in_host || !b->out_host) rc = set_error(GRASS_E_OOM, "pinned staging allocation failed");
     if (!rc && (b->h2d_bytes > b->in_cap || b->d2h_bytes > b->out_cap))
       rc = set_error(GRASS_E_ARG, "internal: staging layout exceeds its reservation");
+    if (!rc && (off > b->work_bytes || (dev_out && oo > b->out_bytes)))
+      rc = set_error(GRASS_E_ARG, "internal: device layout exceeds its reservation");
     cudaError_t e = cudaSuccess;
-    if (!rc) e = cudaMallocFromPoolAsync((void **)&d, std::max<uint64_t>(total, kAlign), pool, s);
-    if (e != cudaSuccess) rc = cuda_fail(e, "server scratch allocation");
+    lap(0);
     if (!rc) {
       uint8_t *h = static_cast<uint8_t *>(b->in_host) - b->h2d_off;  // h[x] mirrors d[x]
       for (size_t i = 0; i < nj; i++) {
@@ -485,7 +517,7 @@ void grass_server::launch(Batch *b) {
         j.select = r.select;
         uint32_t *outs[GRASS_MAX_HOPS] = {nullptr};
         for (uint32_t k = 0; k < q->nout; k++)
-          outs[k] = reinterpret_cast<uint32_t *>(d + b->d2h_off + q->out_off[k]);
+          outs[k] = reinterpret_cast<uint32_t *>(dout + q->out_off[k]);
         if (r.type == GRASS_JOB_KHOP)
           for (uint32_t k = 0; k < r.hops; k++) j.d_hops[k] = outs[k];
         else {
@@ -502,8 +534,10 @@ void grass_server::launch(Batch *b) {
         for (const BatchTask &t : *v) *ht++ = t;
       memset(h + queue_off, 0, kAlign);
       memset(h + edges_off, 0, align_up(nj * 8 + 4));
+      lap(1);
       e = cudaMemcpyAsync(d + b->h2d_off, b->in_host, b->h2d_bytes, cudaMemcpyHostToDevice, s);
       if (e != cudaSuccess) rc = cuda_fail(e, "server upload");
+      lap(2);
     }
     for (size_t i = 0; !rc && i < nj; i++) {
       const Req *q = b->reqs[i];
@@ -518,20 +552,23 @@ void grass_server::launch(Batch *b) {
                         reinterpret_cast<unsigned int *>(d + queue_off), nullptr,
                         reinterpret_cast<unsigned int *>(d + err_off), s, bcfg);
     if (!rc && ntasks) count_launch();
+    lap(3);
     if (!rc) {
       e = cudaMemcpyAsync(b->out_host, d + b->d2h_off, b->d2h_bytes, cudaMemcpyDeviceToHost, s);
       if (e != cudaSuccess) rc = cuda_fail(e, "server download");
     }
-    if (d) cudaFreeAsync(d, s);
+    lap(4);
     if (!rc) {
       e = cudaLaunchHostFunc(s, on_batch_done, b);
       if (e != cudaSuccess) rc = cuda_fail(e, "server completion callback");
     }
+    lap(5);
   }
   {
     std::lock_guard<std::mutex> lk(mu);
     st.issue_us += now_us() - t_issue;
     st.staging_alloc_us += t_alloc;
+    for (int k = 0; k < 6; k++) st.phase_us[k] += ph[k];
   }
   if (rc) {
     // Nothing will call back: wait for what was queued, then fail the batch.
@@ -549,8 +586,11 @@ void grass_server::finish(Batch *b, int status) {
   unsigned int err = 0;
   const uint8_t *out = static_cast<const uint8_t *>(b->out_host);
   if (!status && out) memcpy(&err, out + b->reqs.size() * 8, 4);
-  // Before any request is marked done: a release may free the batch.
+  // Before any request is marked done: a release may free the batch.  The
+  // batch's GPU work is over, so its work block can serve the next batch.
   release_in(b);
+  scratch.give(b->d_work, b->work_bytes);
+  b->d_work = nullptr;
   {
     std::lock_guard<std::mutex> lk(mu);
     for (size_t i = 0; i < b->reqs.size(); i++) {
@@ -566,7 +606,13 @@ void grass_server::finish(Batch *b, int status) {
       }
       q->done = true;
     }
-    in_use -= b->bytes;
+    in_use -= b->work_bytes;  // the outputs' block (if any) returns at release
+    if (status) {
+      scratch.give(b->d_out, b->out_bytes);
+      b->d_out = nullptr;
+      in_use -= b->out_bytes;
+      b->out_bytes = 0;
+    }
     slot_busy[b->slot] = false;
     running_cls[b->cls]--;
     if (--running == 0) st.busy_us += now - busy_since;
@@ -634,43 +680,35 @@ int grass_server_create(const grass_graph *g, const grass_server_config *cfg,
   }
   s->bcfg = resolve_batch_config(c.batch, g->mode);
   c.batch = s->bcfg;
+  s->dev_out = c.results_on_device != 0;
   DeviceGuard dg(g->device);
-  cudaMemPoolProps props{};
-  props.allocType = cudaMemAllocationTypePinned;
-  props.location.type = cudaMemLocationTypeDevice;
-  props.location.id = g->device;
-  cudaError_t e = cudaMemPoolCreate(&s->pool, &props);
-  if (e == cudaSuccess) {
-    uint64_t keep = UINT64_MAX;  // keep freed blocks for the next batches
-    e = cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
-  }
+  auto undo = [s]() {
+    for (auto st : s->streams)
+      if (st) cudaStreamDestroy(st);
+    if (s->scratch.base) cudaFree(s->scratch.base);
+    if (s->staging.base) cudaFreeHost(s->staging.base);
+    delete s;
+  };
+  cudaError_t e = cudaSuccess;
   for (uint32_t i = 0; e == cudaSuccess && i < c.max_inflight; i++)
     e = cudaStreamCreateWithFlags(&s->streams[i], cudaStreamNonBlocking);
+  void *dp = nullptr, *hp = nullptr;
+  // (slack for the 4 KiB rounding of a batch's blocks)
+  const uint64_t dbytes = ((c.scratch_budget + 4095) & ~4095ull) + (64u << 10);
+  if (e == cudaSuccess) e = cudaMalloc(&dp, dbytes);
+  if (e == cudaSuccess) s->scratch.reset(dp, dbytes);
+  if (e == cudaSuccess) e = cudaHostAlloc(&hp, Arena::round(c.staging_bytes), cudaHostAllocDefault);
+  if (e == cudaSuccess) s->staging.reset(hp, Arena::round(c.staging_bytes));
   if (e != cudaSuccess) {
-    const int rc = cuda_fail(e, "server setup");
-    for (auto st : s->streams)
-      if (st) cudaStreamDestroy(st);
-    if (s->pool) cudaMemPoolDestroy(s->pool);
-    delete s;
-    return rc;
-  }
-  e = s->staging.init(c.staging_bytes);
-  if (e != cudaSuccess) {
-    const int rc = cuda_fail(e, "server staging arena");
-    for (auto st : s->streams)
-      if (st) cudaStreamDestroy(st);
-    cudaMemPoolDestroy(s->pool);
-    delete s;
+    const int rc = cuda_fail(e, "server setup (streams, scratch, staging)");
+    undo();
     return rc;
   }
   s->t0 = Clock::now();
   try {
     s->th = std::thread([s] { s->loop(); });
   } catch (...) {
-    for (auto st : s->streams)
-      if (st) cudaStreamDestroy(st);
-    cudaMemPoolDestroy(s->pool);
-    delete s;
+    undo();
     return set_error(GRASS_E_OOM, "cannot start the dispatcher thread");
   }
   *out = s;
@@ -751,7 +789,11 @@ int grass_server_wait(grass_server *s, uint64_t ticket, uint32_t timeout_ms, gra
     if (!q->status) {
       res->n_outputs = q->nout;
       res->edges = q->edges;
-      const uint8_t *out = static_cast<const uint8_t *>(q->batch->out_host);
+      res->on_device = s->dev_out ? 1u : 0u;
+      const uint8_t *out =
+          s->dev_out ? q->batch->d_out
+                     : static_cast<const uint8_t *>(q->batch->out_host) +
+                           align_up(q->batch->reqs.size() * 8 + 4);
       for (uint32_t k = 0; k < q->nout; k++) {
         res->out[k] = reinterpret_cast<const uint32_t *>(out + q->out_off[k]);
         res->out_words[k] = q->out_words[k];
@@ -773,7 +815,10 @@ int grass_server_release(grass_server *s, uint64_t ticket) {
     if (it == s->reqs.end()) return set_error(GRASS_E_ARG, "unknown ticket %llu", (unsigned long long)ticket);
     Req *q = it->second;
     if (!q->done) return set_error(GRASS_E_ARG, "request %llu is still running", (unsigned long long)ticket);
-    if (q->batch && --q->batch->refs == 0) free_b = q->batch;
+    if (q->batch && --q->batch->refs == 0) {
+      free_b = q->batch;
+      s->in_use -= free_b->out_bytes;  // outputs kept on the device, if any
+    }
     s->reqs.erase(it);
     delete q;
   }
@@ -839,7 +884,8 @@ int grass_server_destroy(grass_server *s, uint32_t timeout_ms) {
     delete kv.second;
   }
   s->reqs.clear();
-  if (s->pool) cudaMemPoolDestroy(s->pool);
+  cudaFree(s->scratch.base);
+  cudaFreeHost(s->staging.base);
   delete s;
   return GRASS_OK;
 }

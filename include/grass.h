@@ -335,12 +335,14 @@ int grass_batch_destroy(grass_batch *b);
  * waiting work reaches target_draws sampled edges, or max_batch_jobs of its
  * requests wait.
  *
- * Results are copied to pinned host memory owned by the server and stay
- * valid until grass_server_release.  Each request's result equals the
- * standalone call with the same parameters and seed.
+ * Results are copied to pinned host memory owned by the server (or, with
+ * results_on_device, stay in device memory) and stay valid until
+ * grass_server_release.  Each request's result equals the standalone call
+ * with the same parameters and seed.
  * ========================================================================= */
 typedef struct {
-  uint64_t scratch_budget;   /* device bytes for launched requests (0: 8 GiB)         */
+  uint64_t scratch_budget;   /* device bytes for launched requests, allocated at create
+                                (0: 8 GiB)                                            */
   uint64_t target_draws;     /* close a batch at this much waiting work (0: 2^24)     */
   uint64_t staging_bytes;    /* pinned host arena for inputs and results, made at
                                 create (0: 1 GiB); a batch carries at most 1/8 of it
@@ -352,7 +354,11 @@ typedef struct {
                                 multi-RW batches take at most half of them            */
   uint32_t max_batch_jobs;   /* requests per batch (0: 4096)                           */
   grass_batch_config batch;  /* kernel shape (zero fields: defaults)                   */
-  uint32_t reserved[4];
+  uint32_t results_on_device;/* 1: results stay in device memory (grass_result.out are
+                                device pointers) until released; they count against
+                                scratch_budget meanwhile.  For callers that consume
+                                samples on the GPU: no device-to-host copy.         */
+  uint32_t reserved[3];
 } grass_server_config;
 
 typedef struct {
@@ -376,6 +382,8 @@ typedef struct {
   uint64_t edges;                           /* sampled edges                            */
   double submit_us, launch_us, done_us;     /* since grass_server_create                */
   uint64_t batch;                           /* batch sequence number                    */
+  uint32_t on_device;                       /* out[] are device pointers                */
+  uint32_t reserved;
 } grass_result;
 
 typedef struct {
@@ -384,6 +392,9 @@ typedef struct {
   double busy_us;                           /* time with at least one batch in flight  */
   double issue_us;                          /* dispatcher time issuing batches         */
   double staging_alloc_us;                  /* of which pinned staging allocation      */
+  double phase_us[6];                       /* issue time by step: pool allocation,
+                                               staging fill, H2D enqueue, kernel launch,
+                                               D2H enqueue, free + completion callback  */
 } grass_server_stats;
 
 typedef struct grass_server grass_server;
@@ -432,6 +443,7 @@ typedef struct {
   double queue_p50_us, queue_p99_us;      /* arrival to launch (server mode)             */
   double service_p50_us, service_p99_us;  /* launch to done (server mode)                */
   double issue_us, staging_alloc_us;      /* server: dispatcher time issuing batches     */
+  double phase_us[6];                     /* server: issue time by step (see stats)       */
   double wall_s;                /* first arrival to last completion                   */
   double edges;                 /* sampled edges of completed requests                */
   double edges_per_s;           /* edges / wall_s                                     */

@@ -75,6 +75,7 @@ def _submit(srv, kind, a):
     dict(window_min_us=5000, window_max_us=20000, max_inflight=4,
          batch=dict(walker_tile=64, depth=2, warps_per_block=2, khop_seeds=3)),
     dict(scratch_budget=1 << 20, max_inflight=3),             # admission waits for scratch
+    dict(results_on_device=1, window_min_us=50),              # outputs kept in HBM
 ])
 def test_server_results_equal_standalone(mode, cfg):
     import torch
@@ -102,6 +103,7 @@ def test_server_results_equal_standalone(mode, cfg):
     for (kind, a), tk, (outs, e) in zip(reqs, tickets, expect):
         res = srv.wait(tk, timeout_ms=60000)
         assert res["status"] == G.OK
+        assert res["on_device"] == bool(cfg.get("results_on_device"))
         assert res["edges"] == e, kind
         assert len(res["outputs"]) == len(outs)
         for o, r in zip(res["outputs"], outs):
@@ -114,6 +116,29 @@ def test_server_results_equal_standalone(mode, cfg):
     if "scratch_budget" in cfg:
         assert st["scratch_peak"] <= cfg["scratch_budget"]
         assert st["batches"] > 1
+    srv.close()
+
+
+def test_results_on_device_hold_budget_until_released():
+    """Results kept in device memory count against the scratch budget until
+    released: a request that does not fit waits, and runs after the release."""
+    import time
+    d, *_ = golden_graph("rmat_s10_e8")
+    g = G.Graph(os.path.join(d, "LE"), "LE")
+    starts = np.arange(4000, dtype=np.uint32) % g.n
+    # each request: 4000 starts + 4000 x 41 path words ~ 672 KB; budget fits one
+    srv = G.Server(g, results_on_device=1, scratch_budget=1 << 20, window_min_us=10)
+    ta = srv.submit_rw(starts, 40, 1)
+    ra = srv.wait(ta, release=False)
+    assert ra["on_device"]
+    tb = srv.submit_rw(starts, 40, 2)
+    time.sleep(0.3)
+    assert not srv.poll(tb)  # A's result still holds the budget
+    G.lib.grass_server_release(srv._h, ta)
+    rb = srv.wait(tb, timeout_ms=10000)
+    ref, e = g.rw(starts, 40, 2)
+    np.testing.assert_array_equal(rb["outputs"][0], ref.reshape(-1))
+    assert rb["edges"] == e
     srv.close()
 
 
