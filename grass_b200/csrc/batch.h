@@ -17,7 +17,8 @@ struct BatchJob {
   unsigned char *mscr;  // multi-RW scratch: mstride bytes per sample
   uint64_t mstride;
   unsigned long long *edges;
-  uint32_t length, layout, walkers, steps, select, pad;
+  uint32_t length, layout, walkers, steps, select;
+  uint32_t gen_roots;  // multi-RW: draw the start vertices first (as grass_mrw_roots)
   KhopArgs khop;
 };
 

@@ -10,6 +10,7 @@
 // the multi-RW start vertices and the kernel are captured once into a CUDA
 // graph and replayed by every run.
 #include <algorithm>
+#include <map>
 #include <mutex>
 #include <vector>
 
@@ -42,6 +43,11 @@ __global__ void __launch_bounds__(256) batch_kernel(DevGraph g, const BatchJob *
     const BatchJob &jb = jobs[tk.job];
     const uint64_t s = tk.begin;
     uint64_t cnt = 0;
+    if (jb.gen_roots) {
+      for (uint32_t w = threadIdx.x; w < jb.walkers; w += blockDim.x)
+        jb.roots[s * jb.walkers + w] = mrw_root(g.n, jb.seed, s * jb.walkers + w);
+      __syncthreads();
+    }
     mrw_cta_sample<MODE, 8>(g, jb.roots + s * jb.walkers, jb.out0 + s * jb.steps,
                             jb.out1 + s * jb.steps, jb.walkers, jb.steps, jb.select, jb.seed, s,
                             jb.mscr + s * jb.mstride, csm, cnt, bad);
@@ -67,10 +73,16 @@ __global__ void __launch_bounds__(256) batch_kernel(DevGraph g, const BatchJob *
       for (uint64_t s = tk.begin; s < tk.end; s++)
         khop_seed_warp<MODE>(g, jb.in, jb.khop, s, my, cnt, bad);
     } else {
-      for (uint64_t s = tk.begin; s < tk.end; s++)
+      for (uint64_t s = tk.begin; s < tk.end; s++) {
+        if (jb.gen_roots) {
+          for (uint32_t w = lane; w < jb.walkers; w += 32)
+            jb.roots[s * jb.walkers + w] = mrw_root(g.n, jb.seed, s * jb.walkers + w);
+          __syncwarp();
+        }
         mrw_warp<MODE>(g, jb.roots + s * jb.walkers,
                        reinterpret_cast<uint4 *>(jb.mscr + s * jb.mstride), jb.walkers,
                        jb.steps, (int)jb.select, jb.seed, s, jb.out0, jb.out1, cnt, bad);
+      }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(kFull, cnt, o);
@@ -165,8 +177,21 @@ int launch_batch(const grass_graph *g, const BatchJob *d_jobs, const BatchTask *
                  const grass_batch_config &c) {
   BatchKernel k = pick_kernel(g->mode, c.depth);
   const int threads = 32 * (int)c.warps_per_block;
+  // Resident blocks per SM, once per (kernel, block size): the query costs
+  // tens of microseconds and the serving loop launches thousands of batches.
+  static std::mutex occ_mu;
+  static std::map<std::pair<const void *, int>, int> occ;
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, 0);
+  {
+    std::lock_guard<std::mutex> lk(occ_mu);
+    auto it = occ.find({(const void *)k, threads});
+    if (it != occ.end()) {
+      per_sm = it->second;
+    } else {
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, 0);
+      occ[{(const void *)k, threads}] = per_sm;
+    }
+  }
   if (per_sm < 1) per_sm = 1;
   const uint64_t need =
       std::max<uint64_t>(ncta, (ntasks - ncta + c.warps_per_block - 1) / c.warps_per_block);

@@ -193,6 +193,14 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
   }
 }
 
+// Start vertex i of a multi-RW job whose roots are drawn from its seed: the
+// stream of grass_mrw_roots (word i & 3 of Philox(seed; i >> 2, 0, 0,
+// TAG_MRW_ROOT), mapped to [0, n)).
+__device__ __forceinline__ uint32_t mrw_root(uint32_t n, uint64_t seed, uint64_t i) {
+  const u32x4 r = philox4x32_10(seed, (uint32_t)(i >> 2), 0u, 0u, TAG_MRW_ROOT);
+  return mulhi_u32(pick(r, (int)(i & 3)), n);
+}
+
 // Multi random walk of one sample (MultiRWApp, GT/src/apps/multiRW/multiRW.cu:3-112).
 // The sample's state is vtx[0..R), the walkers' vertices (updated in place),
 // and rec[0..R), each walker's 16-byte vertex record (all zero for a vertex

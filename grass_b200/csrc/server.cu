@@ -7,7 +7,7 @@
 // the budget and issues, on one of up to eight streams:
 //
 //   H2D (job table, work items, inputs, zeroed counters)
-//     -> [multi-RW root draws] -> persistent batch kernel
+//     -> persistent batch kernel (which also draws multi-RW start vertices)
 //     -> D2H (counters, and the outputs unless they stay on the device)
 //     -> host callback
 //
@@ -157,6 +157,8 @@ struct Req {
   uint64_t ticket = 0;
   grass_request rq{};
   std::vector<uint32_t> input;
+  uint32_t *pin_in = nullptr;  // input copied at submit into pinned staging, read by the
+  uint64_t pin_bytes = 0;      // kernel in place (RW starts, k-hop seeds)
   bool draw_roots = false;  // MRW roots drawn on the device from the seed
   int cls = 0;              // 0: RW / k-hop, 1: multi-RW
   uint32_t nout = 0;
@@ -453,7 +455,7 @@ void grass_server::launch(Batch *b) {
   off += kAlign;
   for (size_t i = 0; i < nj; i++) {
     in_off[i] = off;
-    off += align_up(b->reqs[i]->in_words * 4);
+    if (!b->reqs[i]->pin_in) off += align_up(b->reqs[i]->in_words * 4);
   }
   b->d2h_off = off;
   const uint64_t edges_off = off, err_off = off + nj * 8;
@@ -505,7 +507,7 @@ void grass_server::launch(Batch *b) {
         j.type = r.type;
         j.count = r.count;
         j.seed = r.seed;
-        j.d_input = reinterpret_cast<const uint32_t *>(d + in_off[i]);
+        j.d_input = q->pin_in ? q->pin_in : reinterpret_cast<const uint32_t *>(d + in_off[i]);
         j.d_roots = reinterpret_cast<uint32_t *>(d + in_off[i]);
         j.d_edges = reinterpret_cast<unsigned long long *>(d + edges_off) + i;
         j.length = r.length;
@@ -525,7 +527,8 @@ void grass_server::launch(Batch *b) {
           j.d_out1 = outs[1];
         }
         jobs[i] = make_batch_job(j, d + mscr_off[i]);
-        if (!q->draw_roots && q->in_words)
+        jobs[i].gen_roots = q->draw_roots ? 1u : 0u;  // drawn by the batch kernel
+        if (!q->draw_roots && !q->pin_in && q->in_words)
           memcpy(h + in_off[i], q->input.data(), q->in_words * 4);
       }
       memcpy(h + jobs_off, jobs.data(), nj * sizeof(BatchJob));
@@ -538,12 +541,6 @@ void grass_server::launch(Batch *b) {
       e = cudaMemcpyAsync(d + b->h2d_off, b->in_host, b->h2d_bytes, cudaMemcpyHostToDevice, s);
       if (e != cudaSuccess) rc = cuda_fail(e, "server upload");
       lap(2);
-    }
-    for (size_t i = 0; !rc && i < nj; i++) {
-      const Req *q = b->reqs[i];
-      if (!q->draw_roots || !q->in_words) continue;
-      launch_uniform_starts(g->info.n, q->in_words, q->rq.seed,
-                            reinterpret_cast<uint32_t *>(d + in_off[i]), s, true);
     }
     if (!rc && ntasks)
       rc = launch_batch(g, reinterpret_cast<const BatchJob *>(d + jobs_off),
@@ -591,6 +588,10 @@ void grass_server::finish(Batch *b, int status) {
   release_in(b);
   scratch.give(b->d_work, b->work_bytes);
   b->d_work = nullptr;
+  for (Req *q : b->reqs) {
+    staging.give(q->pin_in, q->pin_bytes);
+    q->pin_in = nullptr;
+  }
   {
     std::lock_guard<std::mutex> lk(mu);
     for (size_t i = 0; i < b->reqs.size(); i++) {
@@ -667,12 +668,12 @@ int grass_server_create(const grass_graph *g, const grass_server_config *cfg,
   if (cfg) s->cfg = *cfg;
   grass_server_config &c = s->cfg;
   if (!c.scratch_budget) c.scratch_budget = 8ull << 30;
-  if (!c.target_draws) c.target_draws = 1ull << 24;
+  if (!c.target_draws) c.target_draws = 1ull << 23;
   if (!c.staging_bytes) c.staging_bytes = 1ull << 30;
   if (!c.window_min_us) c.window_min_us = 200;
-  if (!c.window_max_us) c.window_max_us = 2000;
+  if (!c.window_max_us) c.window_max_us = 1000;
   if (c.window_max_us < c.window_min_us) c.window_max_us = c.window_min_us;
-  if (!c.max_inflight) c.max_inflight = 4;
+  if (!c.max_inflight) c.max_inflight = 8;
   if (!c.max_batch_jobs) c.max_batch_jobs = 4096;
   if (c.max_inflight > kMaxSlots) {
     delete s;
@@ -736,11 +737,24 @@ int grass_server_submit(grass_server *s, const grass_request *r, uint64_t *ticke
     return set_error(GRASS_E_BUDGET, "request needs %llu scratch bytes, budget %llu",
                      (unsigned long long)need, (unsigned long long)s->cfg.scratch_budget);
   }
-  if (!q->draw_roots && q->in_words) q->input.assign(r->input, r->input + q->in_words);
+  if (r->type != GRASS_JOB_MRW && q->in_words) {
+    // Copied here, on the caller's thread, into pinned memory that the batch
+    // kernel reads in place; the dispatcher then has no input to copy.
+    q->pin_bytes = q->in_words * 4;
+    q->pin_in = static_cast<uint32_t *>(s->staging.take(q->pin_bytes));
+    if (q->pin_in) {
+      memcpy(q->pin_in, r->input, q->pin_bytes);
+      q->bytes -= q->in_bytes;  // no device copy of the input
+      q->in_bytes = 0;
+    }
+  }
+  if (!q->draw_roots && !q->pin_in && q->in_words)
+    q->input.assign(r->input, r->input + q->in_words);
   q->rq.input = nullptr;
   {
     std::lock_guard<std::mutex> lk(s->mu);
     if (s->stop) {
+      s->staging.give(q->pin_in, q->pin_bytes);
       delete q;
       return set_error(GRASS_E_ARG, "server is shutting down");
     }
@@ -856,6 +870,8 @@ int grass_server_destroy(grass_server *s, uint32_t timeout_ms) {
         q->status = GRASS_E_TIMEOUT;
         q->done = true;
         s->st.failed++;
+        s->staging.give(q->pin_in, q->pin_bytes);
+        q->pin_in = nullptr;
       }
       wq.clear();
     }
