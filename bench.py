@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--only", default="",
                     help="comma list: rw,khop,decode,csr,e2e,cpu,batch,serve")
     ap.add_argument("--no-clocks", action="store_true")
+    ap.add_argument("--batch-scale", type=int, default=24,
+                    help="R-MAT scale of the batched-jobs / serving graph (edge factor 16)")
     return ap.parse_args()
 
 
@@ -584,10 +586,11 @@ def main():
 
     # ---- batched uneven jobs and the serving loop (R-MAT s24 ef16), 1 GPU runs
     if ws == 1 and ({"batch", "serve"} & only):
-        bdir, bmeta = build_graph(24, 16)
+        bdir, bmeta = build_graph(args.batch_scale, 16)
         bgraphs = {m: G.Graph(os.path.join(bdir, m), m, device=local) for m in ("LE", "GT")}
         bn = bmeta["n"]
-        extra = {"graph": f"R-MAT scale 24 edge factor 16 seed 42, graph_sort (undirected): "
+        extra = {"graph": f"R-MAT scale {args.batch_scale} edge factor 16 seed 42, graph_sort "
+                          f"(undirected): "
                           f"{bn} vertices, {bmeta['num_edges']} directed edges"}
         if "batch" in only:
             extra["batch"] = batch_bench(G, torch, bgraphs, bn, stream, flush, 5, 3)
