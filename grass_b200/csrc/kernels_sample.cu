@@ -12,6 +12,20 @@
 #include "mrw_cta.cuh"
 #include "sample_warp.cuh"
 
+// Resident 512-thread blocks per SM each walk kernel is compiled for (its
+// register budget), as measured on the 1M x 80 walk: the LE walk keeps its
+// 120 registers (64 spill and run 5% slower), the GT walk is 23% faster at 64
+// registers, the CSR walk 2% faster.
+#ifndef GRASS_RW_LE_MIN_BLOCKS
+#define GRASS_RW_LE_MIN_BLOCKS 1
+#endif
+#ifndef GRASS_RW_GT_MIN_BLOCKS
+#define GRASS_RW_GT_MIN_BLOCKS 2
+#endif
+#ifndef GRASS_RW_CSR_MIN_BLOCKS
+#define GRASS_RW_CSR_MIN_BLOCKS 2
+#endif
+
 namespace grass {
 
 namespace {
@@ -25,7 +39,7 @@ __device__ __forceinline__ void store_path(uint32_t *paths, int layout, uint64_t
 // w0: walker id of starts[0] -- draws use walker id w0 + w, so a batch split
 // into chunks produces the same walks as one launch.
 template <int MODE, int DEPTH>
-__global__ void __launch_bounds__(512) rw_kernel(DevGraph g, const uint32_t *__restrict__ starts,
+__global__ void __launch_bounds__(512, GRASS_RW_LE_MIN_BLOCKS) rw_kernel(DevGraph g, const uint32_t *__restrict__ starts,
                                                  uint64_t W, uint32_t L, uint64_t seed,
                                                  uint64_t w0, int layout,
                                                  uint32_t *__restrict__ paths,
@@ -85,7 +99,7 @@ __global__ void __launch_bounds__(512) rw_kernel(DevGraph g, const uint32_t *__r
 // vertices whose blocks hold hundreds of gaps, which a per-lane loop would
 // serialise across the whole warp.
 template <int DEPTH>
-__global__ void __launch_bounds__(512) rw_gt_kernel(DevGraph g,
+__global__ void __launch_bounds__(512, GRASS_RW_GT_MIN_BLOCKS) rw_gt_kernel(DevGraph g,
                                                     const uint32_t *__restrict__ starts,
                                                     uint64_t W, uint32_t L, uint64_t seed,
                                                     uint64_t w0, int layout,
@@ -246,7 +260,7 @@ __global__ void __launch_bounds__(256) rw_account_kernel(DevGraph g,
 }
 
 template <int DEPTH>
-__global__ void __launch_bounds__(512) rw_csr_kernel(DevCsr c, const uint32_t *__restrict__ starts,
+__global__ void __launch_bounds__(512, GRASS_RW_CSR_MIN_BLOCKS) rw_csr_kernel(DevCsr c, const uint32_t *__restrict__ starts,
                                                      uint64_t W, uint32_t L, uint64_t seed,
                                                      uint64_t w0, int layout,
                                                      uint32_t *__restrict__ paths,
