@@ -55,7 +55,8 @@ def parse():
     ap.add_argument("--khop-seeds", type=int, default=65536)
     ap.add_argument("--mode", default="LE", choices=["LE", "GT"])
     ap.add_argument("--only", default="",
-                    help="comma list: rw,khop,decode,csr,e2e,cpu,batch,serve")
+                    help="comma list: rw,khop,decode,csr,e2e,cpu,batch,serve,cfg5 "
+                         "(cfg5, the 3B-edge Chung-Lu graph, runs only when named)")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--batch-scale", type=int, default=24,
                     help="R-MAT scale of the batched-jobs / serving graph (edge factor 16)")
@@ -128,6 +129,97 @@ def build_graph(scale, ef):
     np.save(os.path.join(d, "cols.npy"), cols)
     json.dump(meta, open(done, "w"))
     return d, meta
+
+
+def build_chung_lu(n, exponent, mean_degree, max_degree, seed=42):
+    """Chung-Lu graph (m = n * mean_degree / 2 generated edges), graph_sort
+    (undirected), written in both formats; cached per box like build_graph."""
+    import grass_b200 as G
+    key = f"chunglu_n{n}_x{exponent}_d{mean_degree}_max{max_degree}_seed{seed}"
+    d = os.path.join(CACHE, key)
+    done = os.path.join(d, "done.json")
+    if os.path.exists(done):
+        return d, json.load(open(done))
+    os.makedirs(d, exist_ok=True)
+    t0 = time.time()
+    src, dst = G.gen_chung_lu(n, exponent, mean_degree, max_degree, int(n * mean_degree // 2),
+                              seed=seed)
+    t1 = time.time()
+    rp, cols = G.graph_sort(src, dst, directed=False)
+    del src, dst
+    t2 = time.time()
+    meta = {"n": int(len(rp) - 1), "num_edges": int(len(cols)), "gen_s": t1 - t0,
+            "sort_s": t2 - t1, "max_degree": int(np.diff(rp).max())}
+    for mode in ("LE", "GT"):
+        t3 = time.time()
+        G.compress_to_files(rp, cols, mode, os.path.join(d, mode))
+        meta[f"compress_{mode}_s"] = time.time() - t3
+    np.save(os.path.join(d, "rowptr.npy"), rp)
+    json.dump(meta, open(done, "w"))
+    return d, meta
+
+
+def cfg5_bench(G, torch, stream, flush, K):
+    """Skewed large graph: Chung-Lu n = 100M, exponent 2.1, mean degree 30,
+    max degree 1M (~3B directed edges after symmetrising).  4M uniform walks
+    of length 40, k-hop (15, 10) for 262,144 seeds drawn among the vertices
+    of degree >= 1000, the decode sweep, and the footprints, in LE, GT and on
+    the CSR decoded from the LE graph."""
+    dev = torch.device("cuda", torch.cuda.current_device())
+    gdir, meta = build_chung_lu(100_000_000, 2.1, 30, 1_000_000)
+    n, E = meta["n"], meta["num_edges"]
+    out = {"graph": meta}
+    graphs = {m: G.Graph(os.path.join(gdir, m), m) for m in ("LE", "GT")}
+    infos = {m: graphs[m].info() for m in graphs}
+    csr = graphs["LE"].csr()
+    W, L = 4 << 20, 40
+    starts = torch.empty(W, dtype=torch.int32, device=dev)
+    G.uniform_starts_device(n, W, 7, starts, stream=stream)
+    paths = torch.empty(W * (L + 1), dtype=torch.int32, device=dev)
+    ecount = torch.zeros(1, dtype=torch.int64, device=dev)
+    for name, obj in [("LE", graphs["LE"]), ("GT", graphs["GT"]), ("CSR", csr)]:
+        ecount.zero_()
+        obj.rw_device(starts, W, L, 7, paths, ecount, layout=LAYOUT, stream=stream)
+        torch.cuda.synchronize()
+        e1 = int(ecount.item())
+        ms, tot = timed(torch, lambda o=obj: o.rw_device(starts, W, L, 7, paths, ecount,
+                                                         layout=LAYOUT, stream=stream),
+                        K, 2, flush)
+        out[f"rw_{name}"] = {"value": e1 * K / (tot / 1000.0), "ms_per_step": tot / K,
+                             "edges_per_step": e1}
+    del paths
+    rp = np.load(os.path.join(gdir, "rowptr.npy"))
+    hubs = np.nonzero(np.diff(rp) >= 1000)[0].astype(np.uint32)
+    del rp
+    S, fan = 262144, (15, 10)
+    pick = np.random.default_rng(11).integers(0, len(hubs), S)
+    seeds = torch.from_numpy(hubs[pick].view(np.int32)).to(dev)
+    hops = [torch.empty(S * w, dtype=torch.int32, device=dev) for w in G.hop_widths(fan)]
+    for name, obj in [("LE", graphs["LE"]), ("GT", graphs["GT"]), ("CSR", csr)]:
+        ecount.zero_()
+        obj.khop_device(seeds, S, fan, 13, hops, ecount, stream=stream)
+        torch.cuda.synchronize()
+        e1 = int(ecount.item())
+        ms, tot = timed(torch, lambda o=obj: o.khop_device(seeds, S, fan, 13, hops, ecount,
+                                                           stream=stream), K, 2, flush)
+        out[f"khop_{name}"] = {"value": e1 * K / (tot / 1000.0), "ms_per_step": tot / K,
+                               "seeds_with_degree_ge_1000": int(len(hubs))}
+    del hops
+    rp_d = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    cl_d = torch.empty(E, dtype=torch.int32, device=dev)
+    for m in ("LE", "GT"):
+        ms, tot = timed(torch, lambda g=graphs[m]: g.decode_all_device(rp_d, cl_d, stream=stream),
+                        K, 2, flush)
+        out[f"decode_{m}"] = {"value": E * K / (tot / 1000.0), "unit": "decoded edges/s",
+                              "ms_per_step": tot / K}
+    del rp_d, cl_d
+    csr_bytes = (n + 1) * 8 + 4 * E
+    out["footprint_bytes"] = {"CSR": csr_bytes, **{m: infos[m]["device_bytes"] for m in infos},
+                              **{f"ratio_{m}": csr_bytes / infos[m]["device_bytes"]
+                                 for m in infos}}
+    out["compressed_vs_csr"] = {m: out[f"rw_{m}"]["value"] / out["rw_CSR"]["value"]
+                                for m in ("LE", "GT")}
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -598,6 +690,10 @@ def main():
             extra["serve"] = serve_bench(G, bgraphs[args.mode])
         out["batched_jobs_and_serving"] = extra
         del bgraphs
+
+    # ---- skewed large graph (Chung-Lu, ~3B edges): only when asked for
+    if ws == 1 and "cfg5" in only:
+        out["chung_lu_100M"] = cfg5_bench(G, torch, stream, flush, 3)
 
     # ---- accounting for the roofline of the headline kernel
     acct = torch.zeros(3, dtype=torch.int64, device=dev)
