@@ -21,6 +21,7 @@
 //     decoded once by lane 0);
 //  4. writes its 32 ids with one coalesced store.
 #include <type_traits>
+#include <vector>
 
 #include "graph.h"
 
@@ -369,32 +370,86 @@ struct GtSeq {
   }
 };
 
-// Plan construction.  counts: [ranges, class 0..4]; cursors: output positions.
-__global__ void plan_count_kernel(const uint4 *__restrict__ recs, uint32_t n,
-                                  unsigned long long *counts) {
-  __shared__ unsigned long long sc[6];
-  if (threadIdx.x < 6) sc[threadIdx.x] = 0;
-  __syncthreads();
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-    const uint32_t d = recs[v].z;
-    if (d >= kBigDegree) atomicAdd(&sc[0], (unsigned long long)((d + kRange - 1) / kRange));
-    else if (d) atomicAdd(&sc[1 + (31 - __clz(d))], 1ull);
+// Plan construction, in vertex order so that a warp of the small-vertex
+// kernel takes 32 neighbouring vertices of one class (adjacent payloads).
+// One warp per chunk of kPlanChunk vertices: the count pass stores, per
+// chunk, the number of ranges and of vertices in each class; the host turns
+// them into per-chunk cursors; the fill pass writes in order (ballot ranks).
+constexpr int kCats = 6;  // ranges, then classes floor(log2(d)) = 0..4
+constexpr uint32_t kPlanChunk = 1024;
+
+__device__ __forceinline__ void plan_cat(uint32_t d, int &cat, uint32_t &w) {
+  if (d >= kBigDegree) {
+    cat = 0;
+    w = (d + kRange - 1) / kRange;
+  } else if (d) {
+    cat = 1 + (31 - __clz(d));
+    w = 1;
+  } else {
+    cat = -1;
+    w = 0;
   }
-  __syncthreads();
-  if (threadIdx.x < 6 && sc[threadIdx.x]) atomicAdd(&counts[threadIdx.x], sc[threadIdx.x]);
 }
 
-__global__ void plan_fill_kernel(const uint4 *__restrict__ recs, uint32_t n,
-                                 unsigned long long *cursors, uint4 *big, uint32_t *small) {
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
-    const uint32_t d = recs[v].z;
-    if (d >= kBigDegree) {
-      const uint32_t k = (d + kRange - 1) / kRange;
-      const unsigned long long p = atomicAdd(&cursors[0], (unsigned long long)k);
-      for (uint32_t j = 0; j < k; j++)
+__global__ void plan_count_kernel(const uint4 *__restrict__ recs, uint32_t n, uint32_t nchunks,
+                                  uint32_t *counts) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (warp >= nchunks) return;
+  uint32_t tot[kCats] = {0, 0, 0, 0, 0, 0};
+  const uint32_t v0 = warp * kPlanChunk, v1 = min(n, v0 + kPlanChunk);
+  for (uint32_t b = v0; b < v1; b += 32) {
+    const uint32_t v = b + lane;
+    int cat;
+    uint32_t w;
+    plan_cat(v < v1 ? recs[v].z : 0u, cat, w);
+#pragma unroll
+    for (int c = 0; c < kCats; c++) tot[c] += __reduce_add_sync(FULL, cat == c ? w : 0u);
+  }
+  if (lane < kCats) {
+    uint32_t x = 0;
+#pragma unroll
+    for (int c = 0; c < kCats; c++)
+      if (lane == c) x = tot[c];
+    counts[(uint64_t)warp * kCats + lane] = x;
+  }
+}
+
+__global__ void plan_fill_kernel(const uint4 *__restrict__ recs, uint32_t n, uint32_t nchunks,
+                                 const unsigned long long *cursors, uint4 *big,
+                                 uint32_t *small) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (warp >= nchunks) return;
+  unsigned long long cur[kCats];
+#pragma unroll
+  for (int c = 0; c < kCats; c++) cur[c] = cursors[(uint64_t)warp * kCats + c];
+  const uint32_t v0 = warp * kPlanChunk, v1 = min(n, v0 + kPlanChunk);
+  const unsigned below = (1u << lane) - 1u;
+  for (uint32_t b = v0; b < v1; b += 32) {
+    const uint32_t v = b + lane;
+    const uint32_t d = v < v1 ? recs[v].z : 0u;
+    int cat;
+    uint32_t w;
+    plan_cat(d, cat, w);
+    // ranges: exclusive scan of the range counts over the lanes
+    uint32_t incl = cat == 0 ? w : 0u;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (cat == 0) {
+      const unsigned long long p = cur[0] + incl - w;
+      for (uint32_t j = 0; j < w; j++)
         big[p + j] = make_uint4(v, j * kRange, min(d, (j + 1) * kRange), 0u);
-    } else if (d) {
-      small[atomicAdd(&cursors[1 + (31 - __clz(d))], 1ull)] = v;
+    }
+    cur[0] += __shfl_sync(FULL, incl, 31);
+#pragma unroll
+    for (int c = 1; c < kCats; c++) {
+      const unsigned m = __ballot_sync(FULL, cat == c);
+      if (cat == c) small[cur[c] + __popc(m & below)] = v;
+      cur[c] += __popc(m);
     }
   }
 }
@@ -632,45 +687,56 @@ int launch_decode_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t
   {
     std::lock_guard<std::mutex> lk(g->plan_mu);
     if (!g->plan_ok) {
-      unsigned long long *cnt = nullptr;
-      GRASS_CUDA(cudaMalloc(&cnt, 12 * sizeof(unsigned long long)));
-      GRASS_CUDA(cudaMemset(cnt, 0, 12 * sizeof(unsigned long long)));
-      const unsigned grid = (unsigned)std::max<uint64_t>(
-          1, std::min<uint64_t>((n + 255) / 256, (uint64_t)sm_count(dev) * 8));
-      plan_count_kernel<<<grid, 256>>>(g->d_recs, n, cnt);
+      const uint32_t nchunks = (n + kPlanChunk - 1) / kPlanChunk;
+      const unsigned pgrid = (nchunks + 7) / 8;  // 8 warps (chunks) per block
+      uint32_t *cnt = nullptr;
+      unsigned long long *cur = nullptr;
+      GRASS_CUDA(cudaMalloc(&cnt, (uint64_t)nchunks * kCats * sizeof(uint32_t)));
+      cudaError_t e = cudaMalloc(&cur, (uint64_t)nchunks * kCats * sizeof(unsigned long long));
+      if (e != cudaSuccess) {
+        cudaFree(cnt);
+        return cuda_fail(e, "decode plan scratch");
+      }
+      plan_count_kernel<<<pgrid, 256>>>(g->d_recs, n, nchunks, cnt);
       count_launch();
-      unsigned long long h[12] = {0};
-      cudaError_t e = cudaMemcpy(h, cnt, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
-      if (e != cudaSuccess) {
-        cudaFree(cnt);
-        return cuda_fail(e, "decode plan counts");
-      }
-      h[6] = 0;  // cursors: ranges, then the classes back to back
-      uint64_t off = 0;
-      for (int k = 1; k < 6; k++) {
-        h[6 + k] = off;
-        off += h[k];
-      }
-      g->plan_nbig = h[0];
-      g->plan_nsmall = off;
-      e = cudaMalloc(&g->d_plan_big, std::max<uint64_t>(h[0], 1) * sizeof(uint4));
+      std::vector<uint32_t> hc((uint64_t)nchunks * kCats);
+      std::vector<unsigned long long> hcur(hc.size());
+      e = cudaMemcpy(hc.data(), cnt, hc.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+      // cursors: ranges in chunk order; the classes back to back, each in chunk order
+      uint64_t tot[kCats] = {0, 0, 0, 0, 0, 0};
+      for (uint64_t k = 0; k < hc.size(); k++) tot[k % kCats] += hc[k];
+      uint64_t base[kCats] = {0, 0, 0, 0, 0, 0};
+      for (int c = 2; c < kCats; c++) base[c] = base[c - 1] + tot[c - 1];
+      for (uint32_t ch = 0; ch < nchunks; ch++)
+        for (int c = 0; c < kCats; c++) {
+          hcur[(uint64_t)ch * kCats + c] = base[c];
+          base[c] += hc[(uint64_t)ch * kCats + c];
+        }
+      g->plan_nbig = tot[0];
+      g->plan_nsmall = 0;
+      for (int c = 1; c < kCats; c++) g->plan_nsmall += tot[c];
       if (e == cudaSuccess)
-        e = cudaMalloc(&g->d_plan_small, std::max<uint64_t>(off, 1) * sizeof(uint32_t));
+        e = cudaMalloc(&g->d_plan_big, std::max<uint64_t>(g->plan_nbig, 1) * sizeof(uint4));
       if (e == cudaSuccess)
-        e = cudaMemcpy(cnt + 6, h + 6, 6 * sizeof(unsigned long long), cudaMemcpyHostToDevice);
+        e = cudaMalloc(&g->d_plan_small, std::max<uint64_t>(g->plan_nsmall, 1) * sizeof(uint32_t));
+      if (e == cudaSuccess)
+        e = cudaMemcpy(cur, hcur.data(), hcur.size() * sizeof(unsigned long long),
+                       cudaMemcpyHostToDevice);
+      if (e == cudaSuccess) {
+        plan_fill_kernel<<<pgrid, 256>>>(g->d_recs, n, nchunks, cur, g->d_plan_big,
+                                         g->d_plan_small);
+        count_launch();
+        e = cudaDeviceSynchronize();
+      }
+      cudaFree(cnt);
+      cudaFree(cur);
       if (e != cudaSuccess) {
-        cudaFree(cnt);
         cudaFree(g->d_plan_big);
         cudaFree(g->d_plan_small);
         g->d_plan_big = nullptr;
         g->d_plan_small = nullptr;
-        return cuda_fail(e, "decode plan");
+        return cuda_fail(e, "decode plan build");
       }
-      plan_fill_kernel<<<grid, 256>>>(g->d_recs, n, cnt + 6, g->d_plan_big, g->d_plan_small);
-      count_launch();
-      e = cudaDeviceSynchronize();
-      cudaFree(cnt);
-      if (e != cudaSuccess) return cuda_fail(e, "decode plan build");
       g->plan_ok = true;
     }
   }
