@@ -90,20 +90,28 @@ def barrier(dist, dev=None):
             dist.barrier()
 
 
-def max_over_ranks(dist, x: float, torch=None) -> float:
+def _reduce(dist, x: float, op, torch):
     if dist is None:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=op)
     return float(t.item())
+
+
+def max_over_ranks(dist, x: float, torch=None) -> float:
+    """Slowest rank's time: every multi-GPU number is timed as the max over ranks."""
+    return _reduce(dist, x, dist.ReduceOp.MAX if dist else None, torch)
 
 
 def sum_over_ranks(dist, x: float, torch=None) -> float:
-    if dist is None:
-        return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return float(t.item())
+    """Whole-job total (edges of all replicas)."""
+    return _reduce(dist, x, dist.ReduceOp.SUM if dist else None, torch)
+
+
+def replica_seed(base: int, rank: int) -> int:
+    """Philox seed of a replica's walks: each rank samples its own walkers."""
+    return base + rank
 
 
 # ---------------------------------------------------------------------------
@@ -605,14 +613,14 @@ def main():
 
     # per-rank walker ids offset so replicas sample different walks
     starts = torch.empty(W, dtype=torch.int32, device=dev)
-    G.uniform_starts_device(n, W, 7 + rank, starts, stream=stream)
+    G.uniform_starts_device(n, W, replica_seed(7, rank), starts, stream=stream)
     paths = torch.empty(W * (L + 1), dtype=torch.int32, device=dev)
     ecount = torch.zeros(1, dtype=torch.int64, device=dev)
     clocks = Clocks(local, enabled=not args.no_clocks)
     out = {}
 
     def rw_fn(obj):
-        return lambda: obj.rw_device(starts, W, L, 7 + rank, paths, ecount, layout=LAYOUT,
+        return lambda: obj.rw_device(starts, W, L, replica_seed(7, rank), paths, ecount, layout=LAYOUT,
                                      stream=stream)
 
     # ---- (a) random walk: headline mode first
@@ -620,7 +628,7 @@ def main():
     launches0 = G.launch_count()
     for m in order:
         ecount.zero_()
-        graphs[m].rw_device(starts, W, L, 7 + rank, paths, ecount, layout=LAYOUT, stream=stream)
+        graphs[m].rw_device(starts, W, L, replica_seed(7, rank), paths, ecount, layout=LAYOUT, stream=stream)
         torch.cuda.synchronize()
         edges_per_step = int(ecount.item())
         lc0 = G.launch_count()
@@ -632,7 +640,7 @@ def main():
                           "ms_min": min(ms), "ms_max": max(ms)}
     if "csr" in only and csr is not None:
         ecount.zero_()
-        csr.rw_device(starts, W, L, 7 + rank, paths, ecount, layout=LAYOUT, stream=stream)
+        csr.rw_device(starts, W, L, replica_seed(7, rank), paths, ecount, layout=LAYOUT, stream=stream)
         torch.cuda.synchronize()
         e1 = int(ecount.item())
         ms, tot = timed(torch, rw_fn(csr), args.steps, args.warmup, flush, dist, local)
@@ -697,7 +705,7 @@ def main():
 
     # ---- accounting for the roofline of the headline kernel
     acct = torch.zeros(3, dtype=torch.int64, device=dev)
-    graphs[args.mode].rw_account(starts, W, L, 7 + rank, acct, stream=stream)
+    graphs[args.mode].rw_account(starts, W, L, replica_seed(7, rank), acct, stream=stream)
     torch.cuda.synchronize()
     alg_bytes, sectors, draws = [int(x) for x in acct.cpu().tolist()]
     head = out[f"rw_{args.mode}"]
@@ -715,7 +723,7 @@ def main():
         hs = h_starts.numpy().view(np.uint32)
         hp = h_paths.numpy().view(np.uint32).reshape(W, L + 1)
         gm = graphs[args.mode]
-        p = G.RwParams(L, LAYOUT, 7 + rank)
+        p = G.RwParams(L, LAYOUT, replica_seed(7, rank))
         import ctypes as C
         ecnt = C.c_uint64()
 
