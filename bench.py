@@ -423,6 +423,14 @@ def batch_bench(G, torch, graphs, n, stream, flush, K, W):
                     inp.copy_(snap)
                     g.mrw_device(inp, j["count"], j["walkers"], j["steps"], j["seed"], outs[0],
                                  outs[1], select=j["select"], stream=stream)
+        if m == "CSR":  # the CSR side: the batched launch only (no standalone CSR multi-RW)
+            res[m] = {"makespan_ms": tot / K, "ms_min": min(ms), "ms_max": max(ms),
+                      "edges_per_run": edges, "edges_per_s": edges / (tot / K / 1000.0),
+                      "launches_per_run": launches, "autotune_best": best,
+                      "autotune_best_ms": best_ms, "makespan_rw_khop_only_ms": tot_s / K}
+            b.close()
+            short.close()
+            continue
         pms, ptot = timed(torch, plain, 1, 1, flush)
         # one multi-RW sample alone (2000 walkers x 10,000 steps, degree-proportional):
         # continuous-time (walkers in parallel) and one Philox block per step (sequential)
@@ -447,6 +455,9 @@ def batch_bench(G, torch, graphs, n, stream, flush, K, W):
                   "speedup_vs_plain": ptot / (tot / K)}
         b.close()
         short.close()
+    if "CSR" in res:
+        res["compressed_vs_csr"] = {m: res["CSR"]["makespan_ms"] / res[m]["makespan_ms"]
+                                    for m in ("LE", "GT") if m in res}
     for j in jobs:
         t = j["type"]
         if t == 0:
@@ -693,7 +704,11 @@ def main():
                           f"(undirected): "
                           f"{bn} vertices, {bmeta['num_edges']} directed edges"}
         if "batch" in only:
-            extra["batch"] = batch_bench(G, torch, bgraphs, bn, stream, flush, 5, 3)
+            bcsr = bgraphs["LE"].csr()  # uncompressed baseline of the same graph
+            extra["batch"] = batch_bench(G, torch, {**bgraphs, "CSR": bcsr}, bn, stream, flush,
+                                         5, 3)
+            bcsr.close()
+            del bcsr
         if "serve" in only:
             extra["serve"] = serve_bench(G, bgraphs[args.mode])
         out["batched_jobs_and_serving"] = extra

@@ -211,6 +211,7 @@ def _load():
         "grass_csr_khop": ([P, C.POINTER(KhopParams), P, u64, P, P, P], i32),
         "grass_mrw_roots": ([u64, u64, u32, u64, P, P], i32),
         "grass_batch_create": ([P, PP], i32),
+        "grass_batch_create_csr": ([P, PP], i32),
         "grass_batch_add": ([P, C.POINTER(Job)], i32),
         "grass_batch_clear": ([P], i32),
         "grass_batch_set_config": ([P, C.POINTER(BatchConfig)], i32),
@@ -506,11 +507,15 @@ def mrw_roots_device(n: int, S: int, R: int, seed: int, out, stream=None):
 class Batch:
     """Many RW / k-hop / multi-RW jobs run by one persistent, graph-captured launch."""
 
-    def __init__(self, graph: "Graph"):
+    def __init__(self, graph):
+        """graph: a Graph (compressed) or a Csr (uncompressed baseline)."""
         self._g = graph  # keep the graph alive
         self._h = C.c_void_p()
         self._keep = []
-        _check(lib.grass_batch_create(graph.handle, C.byref(self._h)))
+        if isinstance(graph, Csr):
+            _check(lib.grass_batch_create_csr(graph._h, C.byref(self._h)))
+        else:
+            _check(lib.grass_batch_create(graph.handle, C.byref(self._h)))
 
     def _add(self, job: Job):
         _check(lib.grass_batch_add(self._h, C.byref(job)))

@@ -49,10 +49,10 @@ void split_job(const grass_job &j, uint32_t ji, const grass_batch_config &c,
                std::vector<BatchTask> &cta, std::vector<BatchTask> &mrw,
                std::vector<BatchTask> &khop, std::vector<BatchTask> &rw);
 
-// Launches the persistent kernel over ntasks work items, the first ncta of
-// them block-level.  d_queue: two zeroed counters.  Corrupt payloads set bit
-// 0 of *d_err.
-int launch_batch(const grass_graph *g, const BatchJob *d_jobs, const BatchTask *d_tasks,
+// Launches the persistent kernel on graph `dg` (compressed or CSR) of device
+// `device` over ntasks work items, the first ncta of them block-level.
+// d_queue: two zeroed counters.  Corrupt payloads set bit 0 of *d_err.
+int launch_batch(const DevGraph &dg, int device, const BatchJob *d_jobs, const BatchTask *d_tasks,
                  uint32_t ncta, uint32_t ntasks, unsigned int *d_queue,
                  unsigned long long *d_total, unsigned int *d_err, cudaStream_t s,
                  const grass_batch_config &c);

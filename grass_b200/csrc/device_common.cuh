@@ -23,13 +23,19 @@ constexpr uint32_t INVALID_VERTEX = 0xFFFFFFFFu;
 //   y = P bits 32..47 | a << 16 (6 bits) | b << 22 (6 bits)
 //   z = degree d
 //   w = first_pos, or for LE degree 1 the single neighbor
+// A graph as the samplers see it: compressed (mode 0 GT, 1 LE: words and
+// records) or an uncompressed CSR (mode 2, GRASS_MODE_CSR_INTERNAL: rowptr and
+// cols), so that one sampler template serves both sides of a comparison.
 struct DevGraph {
   const uint32_t *__restrict__ words;
   const uint4 *__restrict__ recs;        // n vertex records (sampling, decode)
   const uint64_t *__restrict__ offsets;  // n + 1 bit offsets (load time only)
   uint32_t n;
   int32_t mode;
+  const uint64_t *__restrict__ rowptr;   // mode 2
+  const uint32_t *__restrict__ cols;     // mode 2
 };
+constexpr int GRASS_MODE_CSR_INTERNAL = 2;
 
 struct DevCsr {
   const uint64_t *__restrict__ rowptr;
@@ -495,6 +501,7 @@ __device__ __forceinline__ VHdr record_header(const uint4 r, uint32_t v) {
   h.b = (int)((r.y >> 22) & 63u);
   h.d = r.z;
   h.fp = r.w;
+  h.bn = h.bl = h.om = 0;  // (CSR, mode 2: no chunk geometry)
   if constexpr (MODE == 0) {
     const uint32_t s = isqrt_u32(h.d);
     if (s * s == h.d) {
@@ -505,7 +512,7 @@ __device__ __forceinline__ VHdr record_header(const uint4 r, uint32_t v) {
       h.bl = h.d / h.bn;
       h.om = h.d - h.bn * h.bl;
     }
-  } else {
+  } else if constexpr (MODE == 1) {
     h.bn = h.bl = h.om = 0;
     if (h.d > 1) {
       const uint32_t D = h.d - 1;
@@ -540,9 +547,22 @@ __device__ __forceinline__ void csr_row(const uint64_t *rowptr, uint32_t v, uint
   e = k == 0 ? a1 : k == 1 ? a2 : k == 2 ? a3 : __ldg(p + 4);
 }
 
+// The 16-byte record of vertex v; for a CSR (mode 2) one is made from its
+// row pointers: {start low 32 bits, start bits 32..47, degree, 0}.
+template <int MODE>
+__device__ __forceinline__ uint4 graph_record(const DevGraph &g, uint32_t v) {
+  if constexpr (MODE == 2) {
+    uint64_t b, e;
+    csr_row(g.rowptr, v, b, e);
+    return make_uint4((uint32_t)b, (uint32_t)(b >> 32) & 0xFFFFu, (uint32_t)(e - b), 0u);
+  } else {
+    return load_record(g.recs + v);
+  }
+}
+
 template <int MODE>
 __device__ __forceinline__ VHdr header(const DevGraph &g, uint32_t v) {
-  return record_header<MODE>(load_record(g.recs + v), v);
+  return record_header<MODE>(graph_record<MODE>(g, v), v);
 }
 
 __device__ __forceinline__ uint32_t record_degree(const DevGraph &g, uint32_t v) {
@@ -557,7 +577,8 @@ __device__ __forceinline__ uint32_t gamma_len(uint32_t x) {
 template <int MODE>
 __device__ __forceinline__ uint32_t neighbor(const DevGraph &g, const VHdr &h, uint32_t i) {
   if constexpr (MODE == 0) return gt_neighbor(g, h, i);
-  else return le_neighbor(g, h, i);
+  else if constexpr (MODE == 1) return le_neighbor(g, h, i);
+  else return load_cold_u32(g.cols + h.P + i);
 }
 
 // Number of bits a well-formed vertex occupies given its decoded header;

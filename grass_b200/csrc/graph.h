@@ -71,6 +71,8 @@ struct grass_graph {
     g.offsets = d_offsets;
     g.n = (uint32_t)info.n;
     g.mode = mode;
+    g.rowptr = nullptr;
+    g.cols = nullptr;
     return g;
   }
 };
@@ -88,6 +90,15 @@ struct grass_csr {
     c.cols = d_cols;
     c.n = (uint32_t)n;
     return c;
+  }
+  // The same CSR as a sampler graph (mode 2) for the batched kernel.
+  grass::DevGraph graph_view() const {
+    grass::DevGraph g{};
+    g.n = (uint32_t)n;
+    g.mode = grass::GRASS_MODE_CSR_INTERNAL;
+    g.rowptr = d_rowptr;
+    g.cols = d_cols;
+    return g;
   }
 };
 

@@ -108,6 +108,8 @@ using BatchKernel = void (*)(DevGraph, const BatchJob *, const BatchTask *, uint
 BatchKernel pick_kernel(int mode, uint32_t depth) {
   if (mode == GRASS_MODE_GT)
     return depth == 4 ? batch_kernel<0, 4> : depth == 2 ? batch_kernel<0, 2> : batch_kernel<0, 1>;
+  if (mode == GRASS_MODE_CSR_INTERNAL)
+    return depth == 4 ? batch_kernel<2, 4> : depth == 2 ? batch_kernel<2, 2> : batch_kernel<2, 1>;
   return depth == 4 ? batch_kernel<1, 4> : depth == 2 ? batch_kernel<1, 2> : batch_kernel<1, 1>;
 }
 
@@ -178,11 +180,11 @@ void split_job(const grass_job &j, uint32_t ji, const grass_batch_config &c,
   }
 }
 
-int launch_batch(const grass_graph *g, const BatchJob *d_jobs, const BatchTask *d_tasks,
+int launch_batch(const DevGraph &dg, int device, const BatchJob *d_jobs, const BatchTask *d_tasks,
                  uint32_t ncta, uint32_t ntasks, unsigned int *d_queue,
                  unsigned long long *d_total, unsigned int *d_err, cudaStream_t s,
                  const grass_batch_config &c) {
-  BatchKernel k = pick_kernel(g->mode, c.depth);
+  BatchKernel k = pick_kernel(dg.mode, c.depth);
   const int threads = 32 * (int)c.warps_per_block;
   // Resident blocks per SM, once per (kernel, block size): the query costs
   // tens of microseconds and the serving loop launches thousands of batches.
@@ -203,8 +205,8 @@ int launch_batch(const grass_graph *g, const BatchJob *d_jobs, const BatchTask *
   const uint64_t need =
       std::max<uint64_t>(ncta, (ntasks - ncta + c.warps_per_block - 1) / c.warps_per_block);
   const unsigned grid = (unsigned)std::max<uint64_t>(
-      1, std::min<uint64_t>(need, (uint64_t)sm_count(g->device) * per_sm));
-  k<<<grid, threads, 0, s>>>(g->view(), d_jobs, d_tasks, ncta, ntasks, d_queue, d_total, d_err);
+      1, std::min<uint64_t>(need, (uint64_t)sm_count(device) * per_sm));
+  k<<<grid, threads, 0, s>>>(dg, d_jobs, d_tasks, ncta, ntasks, d_queue, d_total, d_err);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "batch kernel launch");
 }
@@ -214,7 +216,12 @@ int launch_batch(const grass_graph *g, const BatchJob *d_jobs, const BatchTask *
 using namespace grass;
 
 struct grass_batch {
-  const grass_graph *g = nullptr;
+  // The graph sampled: a compressed graph or an uncompressed CSR (mode 2).
+  DevGraph dg{};
+  int device = 0;
+  unsigned int *d_err = nullptr;  // the graph's error word, or own_err (CSR)
+  unsigned int *own_err = nullptr;
+  int mode() const { return dg.mode; }
   std::vector<grass_job> jobs;
   grass_batch_config cfg{};
   std::mutex mu;
@@ -263,7 +270,7 @@ struct grass_batch {
 namespace {
 
 int build(grass_batch *b) {
-  const grass_batch_config c = resolve(b->cfg, b->g->mode);
+  const grass_batch_config c = resolve(b->cfg, b->mode());
   b->free_device();
   std::vector<BatchJob> hj;
   std::vector<BatchTask> cta, mrw, khop, rw;
@@ -310,11 +317,11 @@ int enqueue(grass_batch *b, cudaStream_t s, unsigned long long *total) {
                                cudaMemcpyDeviceToDevice, s));
   GRASS_CUDA(cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(unsigned int), s));
   if (!b->ntasks) return GRASS_OK;
-  return launch_batch(b->g, b->d_jobs, b->d_tasks, b->ncta, b->ntasks, b->d_queue, total,
-                      b->g->d_err, s, c);
+  return launch_batch(b->dg, b->device, b->d_jobs, b->d_tasks, b->ncta, b->ntasks, b->d_queue,
+                      total, b->d_err, s, c);
 }
 
-int check_job(const grass_graph *g, const grass_job *j) {
+int check_job(const grass_job *j) {
   if (!j) return set_error(GRASS_E_ARG, "null job");
   switch (j->type) {
     case GRASS_JOB_RW:
@@ -338,7 +345,6 @@ int check_job(const grass_graph *g, const grass_job *j) {
         return set_error(GRASS_E_ARG, "multi-RW job: bad arguments");
       return GRASS_OK;
   }
-  (void)g;
   return set_error(GRASS_E_ARG, "unknown job type %u", j->type);
 }
 
@@ -352,7 +358,30 @@ int grass_batch_create(const grass_graph *g, grass_batch **out) {
   *out = nullptr;
   auto *b = new (std::nothrow) grass_batch();
   if (!b) return set_error(GRASS_E_OOM, "host allocation failed");
-  b->g = g;
+  b->dg = g->view();
+  b->device = g->device;
+  b->d_err = g->d_err;
+  *out = b;
+  return GRASS_OK;
+}
+
+int grass_batch_create_csr(const grass_csr *c, grass_batch **out) {
+  clear_error();
+  if (!c || !out) return set_error(GRASS_E_ARG, "null argument");
+  *out = nullptr;
+  auto *b = new (std::nothrow) grass_batch();
+  if (!b) return set_error(GRASS_E_OOM, "host allocation failed");
+  b->dg = c->graph_view();
+  b->device = c->device;
+  DeviceGuard dg(c->device);
+  cudaError_t e = cudaMalloc(&b->own_err, sizeof(unsigned int));
+  if (e == cudaSuccess) e = cudaMemset(b->own_err, 0, sizeof(unsigned int));
+  if (e != cudaSuccess) {
+    cudaFree(b->own_err);
+    delete b;
+    return cuda_fail(e, "batch error word");
+  }
+  b->d_err = b->own_err;
   *out = b;
   return GRASS_OK;
 }
@@ -360,9 +389,9 @@ int grass_batch_create(const grass_graph *g, grass_batch **out) {
 int grass_batch_add(grass_batch *b, const grass_job *job) {
   clear_error();
   if (!b) return set_error(GRASS_E_ARG, "null batch");
-  if (int rc = check_job(b->g, job)) return rc;
+  if (int rc = check_job(job)) return rc;
   std::lock_guard<std::mutex> lk(b->mu);
-  DeviceGuard dg(b->g->device);
+  DeviceGuard dg(b->device);
   // Multi-RW start vertices are copied now: every run starts from them, even
   // though each run leaves the final positions in d_roots.
   uint32_t *snap = nullptr;
@@ -384,7 +413,7 @@ int grass_batch_add(grass_batch *b, const grass_job *job) {
 int grass_batch_clear(grass_batch *b) {
   if (!b) return set_error(GRASS_E_ARG, "null batch");
   std::lock_guard<std::mutex> lk(b->mu);
-  DeviceGuard dg(b->g->device);
+  DeviceGuard dg(b->device);
   b->jobs.clear();
   b->free_device();
   b->free_snapshots();
@@ -401,13 +430,13 @@ int grass_batch_set_config(grass_batch *b, const grass_batch_config *cfg) {
                                   "warps_per_block 1/2/4/8");
   std::lock_guard<std::mutex> lk(b->mu);
   b->cfg = *cfg;
-  if (!same_shape(resolve(b->cfg, b->g->mode), b->built_cfg)) b->dirty = true;
+  if (!same_shape(resolve(b->cfg, b->mode()), b->built_cfg)) b->dirty = true;
   return GRASS_OK;
 }
 
 int grass_batch_get_config(const grass_batch *b, grass_batch_config *cfg) {
   if (!b || !cfg) return set_error(GRASS_E_ARG, "null argument");
-  *cfg = resolve(b->cfg, b->g->mode);
+  *cfg = resolve(b->cfg, b->mode());
   return GRASS_OK;
 }
 
@@ -415,12 +444,12 @@ int grass_batch_run(grass_batch *b, void *stream, unsigned long long *d_total_ed
   clear_error();
   if (!b) return set_error(GRASS_E_ARG, "null batch");
   std::lock_guard<std::mutex> lk(b->mu);
-  DeviceGuard dg(b->g->device);
+  DeviceGuard dg(b->device);
   cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
   if (b->dirty) {
     if (int rc = build(b)) return rc;
   }
-  if (resolve(b->cfg, b->g->mode).use_graph == 2) {
+  if (resolve(b->cfg, b->mode()).use_graph == 2) {
     const int rc = enqueue(b, st, d_total_edges);
     if (!rc && b->ntasks) count_launch();
     return rc;
@@ -457,7 +486,7 @@ int grass_batch_autotune(grass_batch *b, void *stream, grass_batch_config *best,
   float top_ms = 1e30f;
   cudaEvent_t e0, e1;
   {
-    DeviceGuard dg(b->g->device);
+    DeviceGuard dg(b->device);
     GRASS_CUDA(cudaEventCreate(&e0));
     GRASS_CUDA(cudaEventCreate(&e1));
   }
@@ -474,7 +503,7 @@ int grass_batch_autotune(grass_batch *b, void *stream, grass_batch_config *best,
         if ((rc = grass_batch_run(b, stream, nullptr))) break;  // build + warm-up
         float ms = 1e30f;
         for (int rep = 0; rep < 3 && !rc; rep++) {
-          DeviceGuard dg(b->g->device);
+          DeviceGuard dg(b->device);
           cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
           cudaEventRecord(e0, st);
           rc = grass_batch_run(b, stream, nullptr);
@@ -487,7 +516,7 @@ int grass_batch_autotune(grass_batch *b, void *stream, grass_batch_config *best,
         if (rc) break;
         if (ms < top_ms) {
           top_ms = ms;
-          top = resolve(c, b->g->mode);
+          top = resolve(c, b->mode());
         }
       }
       if (rc) break;
@@ -515,7 +544,8 @@ int grass_batch_info(const grass_batch *b, uint64_t *jobs, uint64_t *work_items)
 
 int grass_batch_destroy(grass_batch *b) {
   if (!b) return GRASS_OK;
-  DeviceGuard dg(b->g->device);
+  DeviceGuard dg(b->device);
+  cudaFree(b->own_err);
   delete b;
   return GRASS_OK;
 }

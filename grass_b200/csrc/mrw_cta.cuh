@@ -249,7 +249,7 @@ __device__ void mrw_uniform_cta(const DevGraph &g, uint32_t *roots, uint32_t *sr
           list[j] = x;
         }
         v[q] = roots[w];
-        if (v[q] < g.n) rc[q] = load_record(g.recs + v[q]);
+        if (v[q] < g.n) rc[q] = graph_record<MODE>(g, v[q]);
       }
     }
     for (;;) {
@@ -275,7 +275,7 @@ __device__ void mrw_uniform_cta(const DevGraph &g, uint32_t *roots, uint32_t *sr
         dst[t] = nv;
         cnt++;
         v[q] = nv;
-        rc[q] = load_record(g.recs + nv);
+        rc[q] = graph_record<MODE>(g, nv);
       }
       if (!any) break;
     }
@@ -323,7 +323,7 @@ __device__ void mrw_ct_cta(const DevGraph &g, uint32_t *roots, uint32_t *src, ui
     for (uint32_t w = tid; w < R; w += nt) {
       CtWalker s{};
       s.v = roots[w];
-      const uint4 r = s.v < g.n ? load_record(g.recs + s.v) : make_uint4(0u, 0u, 0u, 0u);
+      const uint4 r = s.v < g.n ? graph_record<MODE>(g, s.v) : make_uint4(0u, 0u, 0u, 0u);
       ct_arm(s, r, seed, s_lo, w, 0.0);
       W[w] = s;
       rec[w] = r;
@@ -373,7 +373,7 @@ __device__ void mrw_ct_cta(const DevGraph &g, uint32_t *roots, uint32_t *src, ui
             }
             const uint32_t idx = atomicAdd(&sm.n_events, 1u);
             if (idx < cap) A[idx] = CtEvent{f64_bits(s[q].t), w, s[q].v, nv, 0u};
-            r[q] = load_record(g.recs + nv);
+            r[q] = graph_record<MODE>(g, nv);
             s[q].v = nv;
             s[q].k++;
             ct_arm(s[q], r[q], seed, s_lo, w, s[q].t);

@@ -64,12 +64,12 @@ __device__ __forceinline__ void rw_warp(const DevGraph &g, const uint32_t *start
           }
           nv = gt_warp_neighbor(g.words, active, v[k], run, ra, rb, nullptr);
         } else if (active) {
-          const VHdr h = header<1>(g, v[k]);
+          const VHdr h = header<MODE>(g, v[k]);
           if (h.d == 0) {
             active = false;
             v[k] = INVALID_VERTEX;
           } else {
-            nv = le_neighbor(g, h, mulhi_u32(pick(r[k], s & 3), h.d));
+            nv = neighbor<MODE>(g, h, mulhi_u32(pick(r[k], s & 3), h.d));
           }
         }
         if (active) {
@@ -168,7 +168,7 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
               ra = hk.a;
               rb = hk.b;
             } else {
-              nv = le_neighbor(g, hk, idx);
+              nv = neighbor<MODE>(g, hk, idx);
             }
           }
         }
@@ -225,7 +225,7 @@ __device__ __forceinline__ void mrw_warp(const DevGraph &g, uint32_t *vtx, uint4
     for (int k = 0; k < 4; k++) {
       const uint32_t i = c0 + k * 32 + lane;
       const uint32_t x = i < R ? vtx[i] : INVALID_VERTEX;
-      r[k] = x < g.n ? load_record(g.recs + x) : make_uint4(0u, 0u, 0u, 0u);
+      r[k] = x < g.n ? graph_record<MODE>(g, x) : make_uint4(0u, 0u, 0u, 0u);
     }
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -306,7 +306,7 @@ __device__ __forceinline__ void mrw_warp(const DevGraph &g, uint32_t *vtx, uint4
           } else {
             dst[io] = nv;
             cnt++;
-            const uint4 nr = load_record(g.recs + nv);
+            const uint4 nr = graph_record<MODE>(g, nv);
             vtx[x] = nv;
             rec[x] = nr;
             nd = nr.z;

@@ -543,7 +543,7 @@ void grass_server::launch(Batch *b) {
       lap(2);
     }
     if (!rc && ntasks)
-      rc = launch_batch(g, reinterpret_cast<const BatchJob *>(d + jobs_off),
+      rc = launch_batch(g->view(), g->device, reinterpret_cast<const BatchJob *>(d + jobs_off),
                         reinterpret_cast<const BatchTask *>(d + tasks_off), (uint32_t)cta.size(),
                         (uint32_t)ntasks,
                         reinterpret_cast<unsigned int *>(d + queue_off), nullptr,

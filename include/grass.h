@@ -110,6 +110,7 @@ int grass_compress_to_files(const uint64_t *rowptr, const uint32_t *cols, uint64
  * (GT/src/grass.cu:59), several graphs may be open at once.
  * ========================================================================= */
 typedef struct grass_graph grass_graph;
+typedef struct grass_csr grass_csr; /* uncompressed-CSR baseline, below */
 
 typedef struct {
   uint64_t n;                 /* vertices (byte-padding fields trimmed)   */
@@ -299,6 +300,10 @@ typedef struct {
 
 typedef struct grass_batch grass_batch;
 int grass_batch_create(const grass_graph *g, grass_batch **out);
+/* The same batched launch on an uncompressed CSR (grass_csr_*): the CSR side
+ * of the compressed-vs-CSR comparison for batched jobs.  Every job's output
+ * equals the compressed batch's on the graph the CSR was decoded from. */
+int grass_batch_create_csr(const grass_csr *c, grass_batch **out);
 int grass_batch_add(grass_batch *b, const grass_job *job);
 int grass_batch_clear(grass_batch *b);
 int grass_batch_set_config(grass_batch *b, const grass_batch_config *cfg);
@@ -459,7 +464,6 @@ int grass_loadgen_run(const grass_graph *g, const grass_loadgen_config *c,
  * counterpart: the reference's NextDoor CSR loaders, GT/src/graph.hpp, are
  * never called).  Produces the same walks as the compressed sampler.
  * ========================================================================= */
-typedef struct grass_csr grass_csr;
 int grass_csr_from_graph(const grass_graph *g, grass_csr **out);
 int grass_csr_from_host(const uint64_t *rowptr, const uint32_t *cols, uint64_t n, int device,
                         grass_csr **out);

@@ -20,10 +20,12 @@ def _u32(t):
 class Mix:
     """A batch of uneven jobs plus the standalone results to compare with."""
 
-    def __init__(self, torch, g, n):
+    def __init__(self, torch, g, n, on=None):
+        """on: what the batch samples (default the graph g itself; a Csr of
+        the same graph must give the same outputs)."""
         self.torch, self.g, self.n = torch, g, n
         self.dev = torch.device("cuda")
-        self.batch = G.Batch(g)
+        self.batch = G.Batch(g if on is None else on)
         self.jobs = []  # (kind, outputs, expected, edges tensor, expected edges)
         rng = np.random.default_rng(5)
         for k, (W, L, lay) in enumerate([(1000, 10, 0), (37, 80, 1), (4096, 3, 1), (1, 5, 0)]):
@@ -113,4 +115,18 @@ def test_batch_configs_and_autotune(mode):
     best, ms = m.batch.autotune()
     assert ms > 0 and best["walker_tile"] in (64, 128, 256)
     assert m.batch.config()["walker_tile"] == best["walker_tile"]
+    m.check()
+
+
+@pytest.mark.parametrize("mode", ["GT", "LE"])
+def test_batch_on_csr_equals_compressed(mode):
+    """The batched kernel on the uncompressed CSR decoded from a graph gives
+    every job the same output as the standalone compressed calls."""
+    import torch
+    d, rowptr, cols, meta = golden_graph("rmat_s10_e8")
+    g = G.Graph(os.path.join(d, mode), mode)
+    csr = g.csr()
+    m = Mix(torch, g, g.n, on=csr)
+    m.check(runs=2)
+    m.batch.set_config(walker_tile=64, depth=2, warps_per_block=4, khop_seeds=2)
     m.check()
