@@ -16,18 +16,23 @@
 
 #include "batch.h"
 
-// Resident blocks per SM the compiler must allow for: 3 caps registers at
-// 80 (a few spills to L1) and doubles the resident warps; measured 2x faster
-// on the batched-jobs workload, which waits on memory.
-#ifndef GRASS_BATCH_MIN_BLOCKS
-#define GRASS_BATCH_MIN_BLOCKS 3
+// Resident blocks per SM the compiler must allow for, per graph mode (the
+// register budget).  The batched-jobs workload waits on memory, so more
+// resident warps pay until spills cost more: measured on the 256-job mix,
+// LE is best at 3 (80 registers; 2x over 1), GT and CSR at 4 (64 registers).
+#ifndef GRASS_BATCH_MIN_BLOCKS_LE
+#define GRASS_BATCH_MIN_BLOCKS_LE 3
+#endif
+#ifndef GRASS_BATCH_MIN_BLOCKS_OTHER
+#define GRASS_BATCH_MIN_BLOCKS_OTHER 4
 #endif
 
 namespace grass {
 namespace {
 
 template <int MODE, int DEPTH>
-__global__ void __launch_bounds__(256, GRASS_BATCH_MIN_BLOCKS) batch_kernel(DevGraph g, const BatchJob *__restrict__ jobs,
+__global__ void __launch_bounds__(256, MODE == 1 ? GRASS_BATCH_MIN_BLOCKS_LE
+                                               : GRASS_BATCH_MIN_BLOCKS_OTHER) batch_kernel(DevGraph g, const BatchJob *__restrict__ jobs,
                                                     const BatchTask *__restrict__ tasks,
                                                     uint32_t ncta, uint32_t ntasks,
                                                     unsigned int *queue,
