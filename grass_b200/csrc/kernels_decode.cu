@@ -269,7 +269,10 @@ __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint6
 //    takes 32 vertices of one degree class, so its lanes run for similar
 //    lengths.
 constexpr uint32_t kBigDegree = 32;
-constexpr uint32_t kRange = 2048;
+#ifndef GRASS_DECODE_RANGE
+#define GRASS_DECODE_RANGE 2048
+#endif
+constexpr uint32_t kRange = GRASS_DECODE_RANGE;  // neighbors per range item
 
 // Sequential decoders of one vertex (one lane each), from neighbor 0.
 struct LeSeq {
@@ -470,7 +473,14 @@ __device__ __forceinline__ void prefetch_bits(const uint32_t *words, uint64_t lo
 // (32 bytes); lane l of a warp takes run l of each group of 32 runs, decodes
 // it in order with a bit cursor and stores a full run with two 16-byte
 // writes, so the warp writes 1 KB contiguous per group.
-constexpr uint32_t kRun = 8;
+#ifndef GRASS_DECODE_RUN
+#define GRASS_DECODE_RUN 8
+#endif
+// Slots per lane run (multiple of 4, <= 32).  Measured on R-MAT s22 ef32:
+// 8 -> LE 1.70 ms; 16 -> 2.52 ms; 4 -> 11.6 ms.  Range length (2048 or 4096)
+// made no difference.
+constexpr uint32_t kRun = GRASS_DECODE_RUN;
+static_assert(kRun % 4 == 0 && kRun <= 32, "run length");
 
 template <int MODE>
 __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uint64_t *rowptr,
@@ -632,9 +642,11 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
       }
       if (cnt) {
         uint32_t *o = cols + a0;
-        if (cnt == kRun && vec) {  // aligned full run: two 16-byte stores
-          reinterpret_cast<uint4 *>(o)[0] = make_uint4(vals[0], vals[1], vals[2], vals[3]);
-          reinterpret_cast<uint4 *>(o)[1] = make_uint4(vals[4], vals[5], vals[6], vals[7]);
+        if (cnt == kRun && vec) {  // aligned full run: 16-byte stores
+#pragma unroll
+          for (uint32_t q = 0; q < kRun / 4; q++)
+            reinterpret_cast<uint4 *>(o)[q] =
+                make_uint4(vals[4 * q], vals[4 * q + 1], vals[4 * q + 2], vals[4 * q + 3]);
         } else {
 #pragma unroll
           for (uint32_t k = 0; k < kRun; k++)
