@@ -675,7 +675,28 @@ def main():
                             args.steps, args.warmup, flush, dist, local)
             out[f"khop_{name}"] = {"value": sum_over_ranks(dist, e1 * args.steps, torch) /
                                    (tot / 1000.0), "ms_per_step": tot / args.steps}
-        del hops
+        # output compaction of the same frontiers to a (src, dst) edge list
+        slots = S * sum(G.hop_widths(fan))
+        csrc = torch.empty(slots, dtype=torch.int32, device=dev)
+        cdst = torch.empty(slots, dtype=torch.int32, device=dev)
+        ccount = torch.zeros(1, dtype=torch.int64, device=dev)
+
+        def compact():
+            G.khop_edges_device(seeds, S, fan, hops, csrc, cdst, slots, ccount, stream=stream)
+
+        compact()
+        torch.cuda.synchronize()
+        kept = int(ccount.item())
+        ms, tot = timed(torch, compact, args.steps, args.warmup, flush, dist, local)
+        # algorithmic bytes: every slot read once, every parent slot read once,
+        # every kept edge written as two words
+        alg = 4 * slots + 4 * (S + S * fan[0]) + 8 * kept
+        out["khop_compact"] = {
+            "value": sum_over_ranks(dist, slots * args.steps, torch) / (tot / 1000.0),
+            "unit": "frontier slots/s", "ms_per_step": tot / args.steps, "kept_edges": kept,
+            "algorithmic_bytes": alg,
+            "achieved_gbs": alg / (tot / args.steps / 1000.0) / 1e9}
+        del hops, csrc, cdst
 
     # ---- (c) decode-only sweep
     if "decode" in only:

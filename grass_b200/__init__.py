@@ -210,6 +210,9 @@ def _load():
         "grass_csr_rw": ([P, C.POINTER(RwParams), P, u64, P, P, P], i32),
         "grass_csr_khop": ([P, C.POINTER(KhopParams), P, u64, P, P, P], i32),
         "grass_mrw_roots": ([u64, u64, u32, u64, P, P], i32),
+        "grass_khop_edges": ([C.POINTER(KhopParams), P, u64, P, P, P, u64, P, P], i32),
+        "grass_rw_edges": ([C.POINTER(RwParams), P, u64, P, P, u64, P, P], i32),
+        "grass_mrw_edges": ([C.POINTER(MrwParams), u64, P, P, P, P, u64, P, P], i32),
         "grass_batch_create": ([P, PP], i32),
         "grass_batch_create_csr": ([P, PP], i32),
         "grass_batch_add": ([P, C.POINTER(Job)], i32),
@@ -502,6 +505,35 @@ class Graph:
 
 def mrw_roots_device(n: int, S: int, R: int, seed: int, out, stream=None):
     _check(lib.grass_mrw_roots(n, S, R, seed, _ptr(out), _stream(stream)))
+
+
+# -- output compaction: fixed-shape sampler outputs to dense edge lists --
+# Each call writes the valid edges (dst not INVALID_VERTEX) in output order to
+# src/dst[0, capacity) and their total to count[0] (a device u64).
+
+def khop_edges_device(seeds, S: int, fanouts, hop_out, src, dst, capacity: int, count,
+                      stream=None):
+    """k-hop edges in (hop, seed, slot) order."""
+    p = _khop_params(fanouts, 0)
+    arr = (C.c_void_p * len(hop_out))(*[None if o is None else _ptr(o).value for o in hop_out])
+    _check(lib.grass_khop_edges(C.byref(p), _ptr(seeds), S, C.cast(arr, C.c_void_p), _ptr(src),
+                                _ptr(dst), capacity, _ptr(count), _stream(stream)))
+
+
+def rw_edges_device(paths, W: int, length: int, src, dst, capacity: int, count,
+                    layout: int = LAYOUT_WALK_MAJOR, stream=None):
+    """Walk edges in (walk, step) order (walk-major) or (step, walk) order."""
+    p = RwParams(length, layout, 0)
+    _check(lib.grass_rw_edges(C.byref(p), _ptr(paths), W, _ptr(src), _ptr(dst), capacity,
+                              _ptr(count), _stream(stream)))
+
+
+def mrw_edges_device(step_src, step_dst, S: int, steps: int, src, dst, capacity: int, count,
+                     stream=None):
+    """Multi-RW step edges in (sample, step) order."""
+    p = MrwParams(0, steps, 0, 0, 0)
+    _check(lib.grass_mrw_edges(C.byref(p), S, _ptr(step_src), _ptr(step_dst), _ptr(src),
+                               _ptr(dst), capacity, _ptr(count), _stream(stream)))
 
 
 class Batch:

@@ -442,6 +442,61 @@ int grass_mrw_roots(uint64_t n, uint64_t S, uint32_t R, uint64_t seed, uint32_t 
   return check_launch();
 }
 
+namespace {
+int run_compact(const CompactSeg *segs, uint32_t nseg, uint32_t *d_src, uint32_t *d_dst,
+                uint64_t capacity, unsigned long long *d_count, void *stream) {
+  if (!d_count) return set_error(GRASS_E_ARG, "compaction: null count");
+  if (capacity && (!d_src || !d_dst)) return set_error(GRASS_E_ARG, "compaction: null output");
+  if (int rc = launch_compact(segs, nseg, d_src, d_dst, capacity, d_count, as_stream(stream)))
+    return rc;
+  return check_launch();
+}
+}  // namespace
+
+int grass_khop_edges(const grass_khop_params *p, const uint32_t *d_seeds, uint64_t S,
+                     const uint32_t *const *d_hop_out, uint32_t *d_src, uint32_t *d_dst,
+                     uint64_t capacity, unsigned long long *d_count, void *stream) {
+  clear_error();
+  uint64_t width[GRASS_MAX_HOPS];
+  if (int rc = check_khop(p, width)) return rc;
+  if (S > (1ull << 32)) return set_error(GRASS_E_ARG, "k-hop edges: more than 2^32 seeds");
+  if (S && (!d_seeds || !d_hop_out)) return set_error(GRASS_E_ARG, "k-hop edges: null buffers");
+  CompactSeg segs[GRASS_MAX_HOPS];
+  for (uint32_t h = 0; h < p->hops; h++) {
+    if (S && !d_hop_out[h]) return set_error(GRASS_E_ARG, "k-hop edges: null output for hop %u", h);
+    segs[h] = CompactSeg{h ? d_hop_out[h - 1] : d_seeds, S ? d_hop_out[h] : nullptr,
+                         S * width[h], 0, p->fanouts[h], kCompactFan};
+  }
+  return run_compact(segs, p->hops, d_src, d_dst, capacity, d_count, stream);
+}
+
+int grass_rw_edges(const grass_rw_params *p, const uint32_t *d_paths, uint64_t W,
+                   uint32_t *d_src, uint32_t *d_dst, uint64_t capacity,
+                   unsigned long long *d_count, void *stream) {
+  clear_error();
+  if (!p || p->layout > 1 || (W && !d_paths))
+    return set_error(GRASS_E_ARG, "walk edges: bad arguments");
+  if (W > (1ull << 40)) return set_error(GRASS_E_ARG, "walk edges: too many walks");
+  const uint64_t n = W * p->length;
+  CompactSeg sg;
+  if (p->layout == GRASS_LAYOUT_WALK_MAJOR)
+    sg = CompactSeg{d_paths, d_paths, n, 0, p->length, kCompactPath};
+  else  // step-major: column s + 1 starts W entries after column s
+    sg = CompactSeg{d_paths, n ? d_paths + W : nullptr, n, 0, 1, kCompactFan};
+  return run_compact(&sg, 1, d_src, d_dst, capacity, d_count, stream);
+}
+
+int grass_mrw_edges(const grass_mrw_params *p, uint64_t S, const uint32_t *d_step_src,
+                    const uint32_t *d_step_dst, uint32_t *d_src, uint32_t *d_dst,
+                    uint64_t capacity, unsigned long long *d_count, void *stream) {
+  clear_error();
+  if (!p || (S && p->steps && (!d_step_src || !d_step_dst)))
+    return set_error(GRASS_E_ARG, "multi-RW edges: bad arguments");
+  if (S > (1ull << 40)) return set_error(GRASS_E_ARG, "multi-RW edges: too many samples");
+  CompactSeg sg{d_step_src, d_step_dst, S * p->steps, 0, 1, kCompactFan};
+  return run_compact(&sg, 1, d_src, d_dst, capacity, d_count, stream);
+}
+
 int grass_rw(const grass_graph *g, const grass_rw_params *p, const uint32_t *d_starts,
              uint64_t W, uint32_t *d_paths, unsigned long long *d_edge_count, void *stream) {
   clear_error();

@@ -195,4 +195,23 @@ int launch_mrw(const DevGraph &g, const grass_mrw_params &p, uint32_t *roots, ui
                uint32_t *src, uint32_t *dst, unsigned long long *edges, unsigned int *err,
                cudaStream_t s);
 
+// ---- output compaction (kernels_compact.cu) ----
+constexpr uint32_t kCompactMaxSegs = GRASS_MAX_HOPS;
+constexpr uint32_t kCompactFan = 0;   // edge e: parent[e / div] -> child[e]
+constexpr uint32_t kCompactPath = 1;  // walk-major paths, div = L: edge (q, r) is
+                                      // child[q(L+1) + r] -> child[q(L+1) + r + 1]
+struct CompactSeg {
+  const uint32_t *parent;  // kCompactPath: the path array, as child
+  const uint32_t *child;
+  uint64_t n;              // edge slots
+  uint64_t tile0;          // set by launch_compact
+  uint32_t div;
+  uint32_t kind;
+};
+// Writes the valid edges of the segments, in segment then slot order, to
+// src/dst[0, cap) and their total number to *count (a device word).  An edge
+// is valid when its child is not GRASS_INVALID_VERTEX.
+int launch_compact(const CompactSeg *segs, uint32_t nseg, uint32_t *src, uint32_t *dst,
+                   uint64_t cap, unsigned long long *count, cudaStream_t s);
+
 }  // namespace grass

@@ -257,6 +257,39 @@ int grass_mrw_roots(uint64_t n, uint64_t S, uint32_t R, uint64_t seed, uint32_t 
                     void *stream);
 
 /* =========================================================================
+ * Output compaction: a sampler's fixed-shape output to a dense edge list.
+ * The reference cuts invalid walkers out of every step's frontier by a radix
+ * sort and a search for the first INVALID_VERTEX (invalidVertexStartPos,
+ * GT/src/grass.cu:1085-1117, launched :1641).  The samplers here write
+ * fixed-shape outputs with GRASS_INVALID_VERTEX in empty slots; these calls
+ * write the valid edges (src, dst) in output order -- an edge is valid when
+ * its dst is not GRASS_INVALID_VERTEX -- using per-warp ballot/popc ranks and
+ * one scan over 4096-entry tile counts.  Edges past `capacity` are not
+ * written; *d_count (a device word) receives the total number of valid
+ * edges, which equals the sampler's edge count.  The buffers must be on the
+ * current device; each call allocates its tile counts from the stream's
+ * memory pool.
+ * ========================================================================= */
+
+/* k-hop output (grass_khop / grass_csr_khop) in (hop, seed, slot) order:
+ * hop 0 edges are seeds[s] -> hop0[s][k]; hop h edges are
+ * hop_{h-1}[s][p] -> hop_h[s][p * fanouts[h] + k]. */
+int grass_khop_edges(const grass_khop_params *p, const uint32_t *d_seeds, uint64_t S,
+                     const uint32_t *const *d_hop_out, uint32_t *d_src, uint32_t *d_dst,
+                     uint64_t capacity, unsigned long long *d_count, void *stream);
+/* Walk paths (grass_rw / grass_csr_rw, W walks of p->length steps in
+ * p->layout): edge (w, s) is paths(w, s) -> paths(w, s + 1), in (walk, step)
+ * order for the walk-major layout and (step, walk) order for step-major. */
+int grass_rw_edges(const grass_rw_params *p, const uint32_t *d_paths, uint64_t W,
+                   uint32_t *d_src, uint32_t *d_dst, uint64_t capacity,
+                   unsigned long long *d_count, void *stream);
+/* Multi-RW step edges (grass_mrw, [S][p->steps] each) in (sample, step)
+ * order. */
+int grass_mrw_edges(const grass_mrw_params *p, uint64_t S, const uint32_t *d_step_src,
+                    const uint32_t *d_step_dst, uint32_t *d_src, uint32_t *d_dst,
+                    uint64_t capacity, unsigned long long *d_count, void *stream);
+
+/* =========================================================================
  * Batched jobs: many RW / k-hop / multi-RW jobs of uneven size in ONE
  * persistent launch, captured in a CUDA graph.  The reference runs one app
  * per process through nextdoor() (GT/src/grass.cu:2066-2135); here warps of a

@@ -225,6 +225,45 @@ def rw_csr(rowptr: np.ndarray, cols: np.ndarray, starts: np.ndarray, L: int, see
 
 
 # ---------------------------------------------------------------------------
+# Output compaction.  An entry is kept when it is not INVALID_VERTEX, the
+# test the reference's frontier cut applies to its sorted transits
+# (invalidVertexStartPos, GT/src/grass.cu:1085-1117); kept edges stay in
+# output order.
+
+def _kept(parent: np.ndarray, child: np.ndarray):
+    m = child != INVALID
+    return (np.ascontiguousarray(parent[m], dtype=np.uint32),
+            np.ascontiguousarray(child[m], dtype=np.uint32))
+
+
+def khop_edges(seeds: np.ndarray, hop_outs, fanouts):
+    """(src, dst) of the valid k-hop edges in (hop, seed, slot) order."""
+    src, dst = [], []
+    prev = np.asarray(seeds, dtype=np.uint32).reshape(-1, 1)
+    for h, f in enumerate(fanouts):
+        cur = np.asarray(hop_outs[h], dtype=np.uint32).reshape(len(prev), -1)
+        s, d = _kept(np.repeat(prev, f, axis=1), cur)
+        src.append(s)
+        dst.append(d)
+        prev = cur
+    return np.concatenate(src), np.concatenate(dst)
+
+
+def rw_edges(paths: np.ndarray, walk_major: bool = True):
+    """(src, dst) of the valid walk edges: (walk, step) order for [W][L+1]
+    paths, (step, walk) order for [L+1][W]."""
+    P = np.asarray(paths, dtype=np.uint32)
+    if walk_major:
+        return _kept(P[:, :-1], P[:, 1:])
+    return _kept(P[:-1], P[1:])
+
+
+def mrw_edges(step_src: np.ndarray, step_dst: np.ndarray):
+    """(src, dst) of the multi-RW steps that took an edge, in (sample, step) order."""
+    return _kept(np.asarray(step_src), np.asarray(step_dst))
+
+
+# ---------------------------------------------------------------------------
 # The reference's own CPU pieces, compiled from its sources into _ref/.
 
 def ref_available() -> bool:

@@ -189,3 +189,28 @@ def mrw_ct(philox, rowptr, cols, roots, T, seed):
             arm(w, t)
         roots[s] = v
     return src, dst, roots.astype(np.uint32)
+
+
+def khop_edges(seeds, outs, fanouts):
+    """Valid k-hop edges by explicit loops, (hop, seed, slot) order."""
+    src, dst = [], []
+    for h, f in enumerate(fanouts):
+        for s in range(len(seeds)):
+            for j in range(outs[h].shape[1]):
+                c = int(outs[h][s, j])
+                if c == INVALID:
+                    continue
+                src.append(int(seeds[s]) if h == 0 else int(outs[h - 1][s, j // f]))
+                dst.append(c)
+    return np.array(src, np.uint32), np.array(dst, np.uint32)
+
+
+def rw_edges(paths):
+    """Valid edges of walk-major [W][L+1] paths, (walk, step) order."""
+    src, dst = [], []
+    for row in paths:
+        for t in range(len(row) - 1):
+            if int(row[t + 1]) != INVALID:
+                src.append(int(row[t]))
+                dst.append(int(row[t + 1]))
+    return np.array(src, np.uint32), np.array(dst, np.uint32)

@@ -124,6 +124,35 @@ def test_oracle_mrw_matches_python_restatement(oracle_mod, mode, select):
     np.testing.assert_array_equal(fin, rf)
 
 
+
+@pytest.mark.parametrize("mode", ["GT", "LE"])
+def test_oracle_edge_compaction_matches_loops(oracle_mod, mode):
+    d, rowptr, cols, meta = golden_graph("edge_cases")
+    g = oracle_mod.OracleGraph(os.path.join(d, mode))
+    seeds = np.concatenate([oracle_mod.uniform_starts(g.n, 20, 5), np.array([g.n + 1], np.uint32)])
+    outs, tot = g.khop(mode, seeds, [3, 4, 2], 11)
+    s, t = oracle_mod.khop_edges(seeds, outs, [3, 4, 2])
+    rs, rt = pyref.khop_edges(seeds, outs, [3, 4, 2])
+    np.testing.assert_array_equal(s, rs)
+    np.testing.assert_array_equal(t, rt)
+    assert len(s) == tot
+    starts = np.concatenate([oracle_mod.uniform_starts(g.n, 60, 7),
+                             np.array([g.n + 5, 0, g.n - 1], np.uint32)])
+    paths, tot = g.rw(mode, starts, 12, 99)
+    s, t = oracle_mod.rw_edges(paths)
+    rs, rt = pyref.rw_edges(paths)
+    np.testing.assert_array_equal(s, rs)
+    np.testing.assert_array_equal(t, rt)
+    assert len(s) == tot
+    # the step-major layout lists the same edges in (step, walk) order
+    s2, t2 = oracle_mod.rw_edges(np.ascontiguousarray(paths.T), walk_major=False)
+    assert sorted(zip(s2.tolist(), t2.tolist())) == sorted(zip(s.tolist(), t.tolist()))
+    roots = oracle_mod.mrw_roots(g.n, 6, 9, 3)
+    src, dst, fin, tot = g.mrw(mode, roots, 40, 21, 1)
+    s, t = oracle_mod.mrw_edges(src, dst)
+    assert len(s) == tot
+    np.testing.assert_array_equal(t, dst[dst != pyref.INVALID])
+
 def test_det_log(oracle_mod):
     """The oracle's logarithm equals the Python restatement bit for bit and
     math.log to within a few ulp, including the ends of (0, 1)."""
