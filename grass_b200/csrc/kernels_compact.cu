@@ -10,9 +10,12 @@
 // callers that want only the sampled edges:
 //   1. count: one valid-entry count per tile of 4096 entries (ballot/popc);
 //   2. one exclusive scan over the tile counts;
-//   3. fill: each valid entry is ranked inside its warp with __ballot_sync and
-//      __popc, inside the block by a prefix over the eight warp counts, and
-//      written at tile offset + rank -- the output keeps the input order.
+//   3. fill: each warp owns 512 consecutive entries of a tile; a valid entry
+//      is ranked inside its warp with __ballot_sync and __popc, among the
+//      warps by a prefix over the eight warp counts, and written at tile
+//      offset + rank -- the output keeps the input order.
+// Parent indices advance incrementally (32 / div and 32 % div per step), so a
+// lane divides once per tile, not once per entry.
 #include "graph.h"
 
 namespace grass {
@@ -21,83 +24,87 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kPer = 16;
+constexpr int kPer = 16;                     // slots per lane per tile
+constexpr uint32_t kWarpSlots = 32 * kPer;   // a warp's contiguous chunk
 constexpr uint32_t kTileEntries = kThreads * kPer;
 
+// A segment as the kernels see it: adv_q / adv_r = 32 / div and 32 % div,
+// the step of the (parent, slot) pair between a lane's consecutive slots.
+struct KSeg {
+  const uint32_t *parent;
+  const uint32_t *child;
+  uint64_t n, tile0;
+  uint32_t div, adv_q, adv_r;
+};
+
 struct Plan {
-  CompactSeg seg[kCompactMaxSegs];
+  KSeg seg[kCompactMaxSegs];
   uint32_t nseg;
   uint64_t tiles;
 };
 
-// q0 + r / div, r % div for r = r0 + off, with r0 < div and off < kTileEntries:
-// the quotient step is 0 or 1 unless div is below the tile size, where r fits
-// 32 bits.
-__device__ __forceinline__ void step_div(uint64_t r, uint32_t div, uint64_t &qa, uint32_t &rem) {
-  if (r < div) {
-    qa = 0;
-    rem = (uint32_t)r;
-  } else if (div >= kTileEntries) {
-    qa = 1;
-    rem = (uint32_t)(r - div);
-  } else {
-    const uint32_t rr = (uint32_t)r;
-    qa = rr / div;
-    rem = rr - (uint32_t)qa * div;
-  }
-}
-
-struct TilePos {
-  const CompactSeg *sg;
-  uint64_t e0, q0;
-  uint32_t r0;
+// Slot cursor of one lane: slot e = q * div + r of its segment.
+struct Cursor {
+  uint64_t e, q, r;
 };
 
-__device__ __forceinline__ TilePos locate(const Plan &pl, uint64_t tile) {
+// Finds the tile's segment and starts the lane at slot
+// e0 + warp * kWarpSlots + lane.
+__device__ __forceinline__ Cursor start(const Plan &pl, uint64_t tile, const KSeg *&sg) {
   uint32_t k = 0;
   while (k + 1 < pl.nseg && tile >= pl.seg[k + 1].tile0) k++;
-  TilePos t;
-  t.sg = &pl.seg[k];
-  t.e0 = (tile - t.sg->tile0) * kTileEntries;
-  t.q0 = t.e0 / t.sg->div;
-  t.r0 = (uint32_t)(t.e0 - t.q0 * t.sg->div);
-  return t;
+  sg = &pl.seg[k];
+  const uint32_t div = sg->div;
+  const uint64_t e0 = (tile - sg->tile0) * kTileEntries;
+  const uint32_t off = (threadIdx.x >> 5) * kWarpSlots + (threadIdx.x & 31);
+  Cursor c;
+  c.e = e0 + off;
+  c.q = c.e / div;
+  c.r = c.e - c.q * div;
+  return c;
 }
 
-// Index of entry e0 + off's child; *pidx receives its parent's index.
-__device__ __forceinline__ uint64_t entry_index(const TilePos &t, uint32_t off, uint64_t *pidx) {
-  uint64_t qa;
-  uint32_t rem;
-  step_div((uint64_t)t.r0 + off, t.sg->div, qa, rem);
-  const uint64_t q = t.q0 + qa;
-  if (t.sg->kind == kCompactFan) {
-    *pidx = q;
-    return t.e0 + off;
+__device__ __forceinline__ void advance(Cursor &c, const KSeg &sg) {
+  c.e += 32;
+  c.q += sg.adv_q;
+  c.r += sg.adv_r;
+  if (c.r >= sg.div) {
+    c.r -= sg.div;
+    c.q++;
   }
-  // walk-major paths: edge (q, rem) joins path[q][rem] -> path[q][rem + 1]
-  const uint64_t i = q * ((uint64_t)t.sg->div + 1) + rem;
-  *pidx = i;
-  return i + 1;
 }
 
+// Child and parent indices of the slot under the cursor.
+template <int KIND>
+__device__ __forceinline__ uint64_t child_index(const Cursor &c, const KSeg &sg) {
+  if constexpr (KIND == kCompactFan) return c.e;
+  else return c.q * ((uint64_t)sg.div + 1) + c.r + 1;  // walk-major path
+}
+template <int KIND>
+__device__ __forceinline__ uint64_t parent_index(const Cursor &c, const KSeg &sg) {
+  if constexpr (KIND == kCompactFan) return c.q;
+  else return c.q * ((uint64_t)sg.div + 1) + c.r;
+}
+
+template <int KIND>
 __global__ void __launch_bounds__(kThreads) compact_count_kernel(Plan pl, uint32_t *counts) {
   __shared__ uint32_t wsum[kWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (uint64_t tile = blockIdx.x; tile < pl.tiles; tile += gridDim.x) {
-    const TilePos t = locate(pl, tile);
-    const uint64_t n = t.sg->n;
+    const KSeg *sg;
+    Cursor c = start(pl, tile, sg);
+    const uint64_t n = sg->n;
     uint32_t v[kPer];
 #pragma unroll
     for (int k = 0; k < kPer; k++) {
-      const uint32_t off = k * kThreads + threadIdx.x;
-      uint64_t pi;
-      const uint64_t ci = entry_index(t, off, &pi);
-      v[k] = t.e0 + off < n ? __ldg(t.sg->child + ci) : GRASS_INVALID_VERTEX;
+      v[k] = c.e < n ? __ldg(sg->child + child_index<KIND>(c, *sg)) : GRASS_INVALID_VERTEX;
+      advance(c, *sg);
     }
-    uint32_t c = 0;
+    uint32_t cnt = 0;
 #pragma unroll
-    for (int k = 0; k < kPer; k++) c += __popc(__ballot_sync(0xffffffffu, v[k] != GRASS_INVALID_VERTEX));
-    if (lane == 0) wsum[warp] = c;
+    for (int k = 0; k < kPer; k++)
+      cnt += __popc(__ballot_sync(0xffffffffu, v[k] != GRASS_INVALID_VERTEX));
+    if (lane == 0) wsum[warp] = cnt;
     __syncthreads();
     if (threadIdx.x == 0) {
       uint32_t s = 0;
@@ -109,49 +116,63 @@ __global__ void __launch_bounds__(kThreads) compact_count_kernel(Plan pl, uint32
   }
 }
 
+// Each warp owns kWarpSlots consecutive slots of the tile: it ranks its valid
+// slots with one ballot per 32, learns the counts of the warps before it
+// through shared memory (the tile's only barrier), and writes in slot order.
+template <int KIND>
 __global__ void __launch_bounds__(kThreads)
     compact_fill_kernel(Plan pl, const uint64_t *offs, uint32_t *src, uint32_t *dst, uint64_t cap) {
-  __shared__ uint32_t wcnt[2][kWarps];
+  __shared__ uint32_t wsum[kWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t below = (1u << lane) - 1;
   for (uint64_t tile = blockIdx.x; tile < pl.tiles; tile += gridDim.x) {
-    const TilePos t = locate(pl, tile);
-    const uint64_t n = t.sg->n;
+    const KSeg *sg;
+    Cursor c = start(pl, tile, sg);
+    const uint64_t n = sg->n;
     uint32_t cv[kPer], pv[kPer];
 #pragma unroll
     for (int k = 0; k < kPer; k++) {
-      const uint32_t off = k * kThreads + threadIdx.x;
-      uint64_t pi;
-      const uint64_t ci = entry_index(t, off, &pi);
-      const bool in = t.e0 + off < n;
-      cv[k] = in ? __ldg(t.sg->child + ci) : GRASS_INVALID_VERTEX;
-      pv[k] = in ? __ldg(t.sg->parent + pi) : GRASS_INVALID_VERTEX;
+      const bool in = c.e < n;
+      cv[k] = in ? __ldg(sg->child + child_index<KIND>(c, *sg)) : GRASS_INVALID_VERTEX;
+      pv[k] = in ? __ldg(sg->parent + parent_index<KIND>(c, *sg)) : GRASS_INVALID_VERTEX;
+      advance(c, *sg);
     }
-    uint64_t base = offs[tile];
+    uint32_t m[kPer], total = 0;
 #pragma unroll
     for (int k = 0; k < kPer; k++) {
-      const bool ok = cv[k] != GRASS_INVALID_VERTEX;
-      const uint32_t m = __ballot_sync(0xffffffffu, ok);
-      // wcnt[k & 1] is rewritten at round k + 2, after every thread passed the
-      // barrier of round k + 1, so one barrier per round suffices.
-      if (lane == 0) wcnt[k & 1][warp] = __popc(m);
-      __syncthreads();
-      uint32_t before = 0, total = 0;
+      m[k] = __ballot_sync(0xffffffffu, cv[k] != GRASS_INVALID_VERTEX);
+      total += __popc(m[k]);
+    }
+    if (lane == 0) wsum[warp] = total;
+    __syncthreads();
+    uint64_t pos = offs[tile];
 #pragma unroll
-      for (int w = 0; w < kWarps; w++) {
-        const uint32_t c = wcnt[k & 1][w];
-        before += w < warp ? c : 0;
-        total += c;
+    for (int w = 0; w < kWarps; w++) pos += w < warp ? wsum[w] : 0u;
+#pragma unroll
+    for (int k = 0; k < kPer; k++) {
+      const uint64_t at = pos + __popc(m[k] & below);
+      if (((m[k] >> lane) & 1u) && at < cap) {
+        store_out_u32(src + at, pv[k]);
+        store_out_u32(dst + at, cv[k]);
       }
-      const uint64_t pos = base + before + __popc(m & below);
-      if (ok && pos < cap) {
-        store_out_u32(src + pos, pv[k]);
-        store_out_u32(dst + pos, cv[k]);
-      }
-      base += total;
+      pos += __popc(m[k]);
     }
     __syncthreads();
   }
+}
+
+template <int KIND>
+void launch_kind(const Plan &pl, uint32_t *counts, uint64_t *offs, uint64_t *tmp, uint32_t *src,
+                 uint32_t *dst, uint64_t cap, cudaStream_t s) {
+  int dev = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, compact_fill_kernel<KIND>, kThreads, 0);
+  const uint64_t resident = (uint64_t)sm_count(dev) * (uint64_t)std::max(per_sm, 1) * 4;
+  const unsigned grid = (unsigned)std::min<uint64_t>(pl.tiles, resident);
+  compact_count_kernel<KIND><<<grid, kThreads, 0, s>>>(pl, counts);
+  launch_scan_u32(counts, pl.tiles, offs, tmp, s);
+  compact_fill_kernel<KIND><<<grid, kThreads, 0, s>>>(pl, offs, src, dst, cap);
+  count_launch(2);
 }
 
 }  // namespace
@@ -163,9 +184,15 @@ int launch_compact(const CompactSeg *segs, uint32_t nseg, uint32_t *src, uint32_
   pl.nseg = nseg;
   uint64_t tiles = 0;
   for (uint32_t k = 0; k < nseg; k++) {
-    pl.seg[k] = segs[k];
-    if (pl.seg[k].div == 0) pl.seg[k].div = 1;
-    pl.seg[k].tile0 = tiles;
+    if (segs[k].kind != segs[0].kind) return set_error(GRASS_E_ARG, "compaction: mixed segment kinds");
+    KSeg &q = pl.seg[k];
+    q.parent = segs[k].parent;
+    q.child = segs[k].child;
+    q.n = segs[k].n;
+    q.div = segs[k].div ? segs[k].div : 1u;
+    q.adv_q = 32u / q.div;
+    q.adv_r = 32u % q.div;
+    q.tile0 = tiles;
     tiles += (segs[k].n + kTileEntries - 1) / kTileEntries;
   }
   pl.tiles = tiles;
@@ -181,13 +208,8 @@ int launch_compact(const CompactSeg *segs, uint32_t nseg, uint32_t *src, uint32_
   uint32_t *counts = reinterpret_cast<uint32_t *>(scr);
   uint64_t *offs = scr + cnt_words;
   uint64_t *tmp = offs + tiles + 1;
-  int dev = 0;
-  cudaGetDevice(&dev);
-  const unsigned grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)sm_count(dev) * 8);
-  compact_count_kernel<<<grid, kThreads, 0, s>>>(pl, counts);
-  launch_scan_u32(counts, tiles, offs, tmp, s);
-  compact_fill_kernel<<<grid, kThreads, 0, s>>>(pl, offs, src, dst, cap);
-  count_launch(2);
+  if (segs[0].kind == kCompactFan) launch_kind<kCompactFan>(pl, counts, offs, tmp, src, dst, cap, s);
+  else launch_kind<kCompactPath>(pl, counts, offs, tmp, src, dst, cap, s);
   e = cudaMemcpyAsync(count, offs + tiles, sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
   cudaFreeAsync(scr, s);
   return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "compaction count");

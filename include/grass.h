@@ -150,7 +150,7 @@ int grass_device_view(const grass_graph *g, const uint32_t **words, uint64_t *n_
  * 1886).  Zero fields take the defaults; grass_autotune picks values. */
 typedef struct {
   uint32_t rw_depth;          /* walkers interleaved per thread: 1, 2, 4
-                                 (default 4 for LE and CSR, 1 for GT)                */
+                                 (default 1 for LE and GT, 4 for CSR)                */
   uint32_t rw_threads;        /* threads per block for walks (default 256)           */
   uint32_t rw_blocks_per_sm;  /* resident blocks per SM for walks (0 = all resident) */
   uint32_t l2_persist;        /* 1: launches mark the vertex records (or CSR row
