@@ -9,16 +9,13 @@
 // end leaves empty.  Compaction is a separate, order-preserving pass for
 // callers that want only the sampled edges:
 //   1. count: one valid-entry count per tile of 4096 entries (ballot/popc);
-//   2. an exclusive scan over the tile counts, by the count launch's last
-//      block to finish;
+//   2. one exclusive scan over the tile counts;
 //   3. fill: each warp owns 512 consecutive entries of a tile; a valid entry
 //      is ranked inside its warp with __ballot_sync and __popc, among the
 //      warps by a prefix over the eight warp counts, and written at tile
 //      offset + rank -- the output keeps the input order.
 // Parent indices advance incrementally (32 / div and 32 % div per step), so a
 // lane divides once per tile, not once per entry.
-#include <atomic>
-
 #include "graph.h"
 
 namespace grass {
@@ -89,60 +86,9 @@ __device__ __forceinline__ uint64_t parent_index(const Cursor &c, const KSeg &sg
   else return c.q * ((uint64_t)sg.div + 1) + c.r;
 }
 
-// Exclusive scan of counts[0, T) into offs[0, T], run by one block; *total
-// receives offs[T].  counts were written by other blocks of the same launch
-// and are read through L2.
-__device__ void block_scan_counts(const uint32_t *counts, uint64_t T, uint64_t *offs,
-                                  unsigned long long *total) {
-  __shared__ uint64_t wtot[kWarps];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  uint64_t carry = 0;
-  for (uint64_t base = 0; base < T; base += kTileEntries) {
-    const uint64_t i0 = base + (uint64_t)threadIdx.x * kPer;
-    uint32_t v[kPer];
-    uint64_t t = 0;
-#pragma unroll
-    for (int k = 0; k < kPer; k++) {
-      v[k] = i0 + k < T ? __ldcg(counts + i0 + k) : 0u;
-      t += v[k];
-    }
-    uint64_t inc = t;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-      const uint64_t y = __shfl_up_sync(0xffffffffu, inc, d);
-      if (lane >= d) inc += y;
-    }
-    if (lane == 31) wtot[warp] = inc;
-    __syncthreads();
-    uint64_t before = carry, all = carry;
-#pragma unroll
-    for (int w = 0; w < kWarps; w++) {
-      before += w < warp ? wtot[w] : 0u;
-      all += wtot[w];
-    }
-    uint64_t x = before + inc - t;
-#pragma unroll
-    for (int k = 0; k < kPer; k++) {
-      if (i0 + k < T) offs[i0 + k] = x;
-      x += v[k];
-    }
-    carry = all;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    offs[T] = carry;
-    *total = carry;
-  }
-}
-
-// Per-tile counts; the last block to finish (a ticket from *done, which
-// starts at zero) scans them, so no separate scan launch is needed.
 template <int KIND>
-__global__ void __launch_bounds__(kThreads)
-    compact_count_kernel(Plan pl, uint32_t *counts, uint64_t *offs, unsigned int *done,
-                         unsigned long long *total) {
+__global__ void __launch_bounds__(kThreads) compact_count_kernel(Plan pl, uint32_t *counts) {
   __shared__ uint32_t wsum[kWarps];
-  __shared__ bool last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (uint64_t tile = blockIdx.x; tile < pl.tiles; tile += gridDim.x) {
     const KSeg *sg;
@@ -167,15 +113,6 @@ __global__ void __launch_bounds__(kThreads)
       counts[tile] = s;
     }
     __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    __threadfence();
-    last = atomicAdd(done, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (last) {
-    __threadfence();
-    block_scan_counts(counts, pl.tiles, offs, total);
   }
 }
 
@@ -224,31 +161,16 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// Blocks of the compaction kernels resident per SM, from the occupancy
-// calculator (cached; every device this library runs on is the same part).
 template <int KIND>
-int resident_per_sm() {
-  static std::atomic<int> cached{0};
-  int v = cached.load(std::memory_order_relaxed);
-  if (!v) {
-    int a = 0, b = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a, compact_count_kernel<KIND>, kThreads, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, compact_fill_kernel<KIND>, kThreads, 0);
-    v = std::max(1, std::min(a, b));
-    cached.store(v, std::memory_order_relaxed);
-  }
-  return v;
-}
-
-template <int KIND>
-void launch_kind(const Plan &pl, uint32_t *counts, uint64_t *offs, unsigned int *done,
-                 unsigned long long *total, uint32_t *src, uint32_t *dst, uint64_t cap,
-                 cudaStream_t s) {
-  int dev = 0;
+void launch_kind(const Plan &pl, uint32_t *counts, uint64_t *offs, uint64_t *tmp, uint32_t *src,
+                 uint32_t *dst, uint64_t cap, cudaStream_t s) {
+  int dev = 0, per_sm = 0;
   cudaGetDevice(&dev);
-  const uint64_t resident = (uint64_t)sm_count(dev) * (uint64_t)resident_per_sm<KIND>() * 4;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, compact_fill_kernel<KIND>, kThreads, 0);
+  const uint64_t resident = (uint64_t)sm_count(dev) * (uint64_t)std::max(per_sm, 1) * 4;
   const unsigned grid = (unsigned)std::min<uint64_t>(pl.tiles, resident);
-  compact_count_kernel<KIND><<<grid, kThreads, 0, s>>>(pl, counts, offs, done, total);
+  compact_count_kernel<KIND><<<grid, kThreads, 0, s>>>(pl, counts);
+  launch_scan_u32(counts, pl.tiles, offs, tmp, s);
   compact_fill_kernel<KIND><<<grid, kThreads, 0, s>>>(pl, offs, src, dst, cap);
   count_launch(2);
 }
@@ -278,23 +200,19 @@ int launch_compact(const CompactSeg *segs, uint32_t nseg, uint32_t *src, uint32_
     cudaError_t e = cudaMemsetAsync(count, 0, sizeof(unsigned long long), s);
     return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "compaction count");
   }
-  // scratch: [done ticket (one u64 word)] [offs: tiles + 1 u64] [counts: tiles u32]
-  const uint64_t words = 1 + (tiles + 1) + (tiles + 1) / 2;
+  const uint64_t cnt_words = (tiles + 1) / 2;  // u32 counts in u64 words
+  const uint64_t words = cnt_words + (tiles + 1) + scan_tmp_words(tiles);
   uint64_t *scr = nullptr;
   cudaError_t e = cudaMallocAsync(&scr, words * sizeof(uint64_t), s);
   if (e != cudaSuccess) return cuda_fail(e, "compaction scratch");
-  unsigned int *done = reinterpret_cast<unsigned int *>(scr);
-  uint64_t *offs = scr + 1;
-  uint32_t *counts = reinterpret_cast<uint32_t *>(offs + tiles + 1);
-  e = cudaMemsetAsync(done, 0, sizeof(uint64_t), s);
-  if (e == cudaSuccess) {
-    if (segs[0].kind == kCompactFan)
-      launch_kind<kCompactFan>(pl, counts, offs, done, count, src, dst, cap, s);
-    else
-      launch_kind<kCompactPath>(pl, counts, offs, done, count, src, dst, cap, s);
-  }
+  uint32_t *counts = reinterpret_cast<uint32_t *>(scr);
+  uint64_t *offs = scr + cnt_words;
+  uint64_t *tmp = offs + tiles + 1;
+  if (segs[0].kind == kCompactFan) launch_kind<kCompactFan>(pl, counts, offs, tmp, src, dst, cap, s);
+  else launch_kind<kCompactPath>(pl, counts, offs, tmp, src, dst, cap, s);
+  e = cudaMemcpyAsync(count, offs + tiles, sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
   cudaFreeAsync(scr, s);
-  return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "compaction scratch");
+  return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "compaction count");
 }
 
 }  // namespace grass
