@@ -300,6 +300,8 @@ int read_err_flag(const grass_graph *g, cudaStream_t st) {
   if (e) {
     cudaMemsetAsync(g->d_err, 0, sizeof(unsigned int), st);
     cudaStreamSynchronize(st);
+    if (e & 2u)
+      return set_error(GRASS_E_TIMEOUT, "a decode warp's staged stream copy did not complete");
     return set_error(GRASS_E_DATA, "a decoded vertex id was out of range (corrupt payload)");
   }
   return GRASS_OK;
