@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -32,6 +33,41 @@ int cuda_fail(cudaError_t e, const char *what) {
   return set_error(e == cudaErrorMemoryAllocation ? GRASS_E_OOM : GRASS_E_CUDA, "%s: %s", what,
                    cudaGetErrorString(e));
 }
+
+// Stream-ordered scratch for this library's kernels, from a memory pool of
+// its own on each device.  The pool keeps up to 256 MiB of freed memory
+// mapped across synchronisations: the default pool returns freed memory at
+// every synchronisation, so the first allocation after one maps fresh memory,
+// which measured 0.2-1.2 ms on a 60 KB request against a 0.1 ms compaction.
+cudaError_t scratch_alloc(void **p, size_t bytes, cudaStream_t s) {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaMallocAsync(p, bytes, s);
+  cudaMemPool_t pool;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[dev]) {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      e = cudaMemPoolCreate(&pools[dev], &props);
+      if (e != cudaSuccess) {
+        pools[dev] = nullptr;
+        return e;
+      }
+      uint64_t keep = 256ull << 20;
+      cudaMemPoolSetAttribute(pools[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    pool = pools[dev];
+  }
+  return cudaMallocFromPoolAsync(p, bytes, pool, s);
+}
+
+void scratch_free(void *p, cudaStream_t s) { cudaFreeAsync(p, s); }
 
 int sm_count(int device) {
   static int cache[64] = {0};
@@ -420,11 +456,12 @@ int grass_decode_all(const grass_graph *g, uint64_t *d_rowptr, uint32_t *d_cols,
   // degrees as u64 straight into rowptr, scanned in place, then decode;
   // the only scratch is one u64 per 4096-vertex tile.
   uint64_t *scan_tmp = nullptr;
-  GRASS_CUDA(cudaMallocAsync(&scan_tmp, (scan_tmp_words(n) + 1) * sizeof(uint64_t), st));
+  GRASS_CUDA(scratch_alloc(reinterpret_cast<void **>(&scan_tmp),
+                           (scan_tmp_words(n) + 1) * sizeof(uint64_t), st));
   launch_degrees64(g->view(), d_rowptr, st);
   launch_scan_u64_inplace(d_rowptr, n, scan_tmp, st);
   int rc = launch_decode_planned(g, d_rowptr, d_cols, g->d_err, st);
-  cudaFreeAsync(scan_tmp, st);
+  scratch_free(scan_tmp, st);
   return rc ? rc : check_launch();
 }
 

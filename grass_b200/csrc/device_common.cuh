@@ -347,19 +347,93 @@ __device__ __forceinline__ uint32_t gap_sum(const uint32_t *words, uint64_t pos,
   return s;
 }
 
+// Gap runs up to this length are summed by their own lane; longer runs go to
+// a pool that the whole warp shares out evenly.  Measured on the 1M x 80 GT
+// walk (R-MAT s22 ef32): 4 -> 7.50 ms, 8 -> 7.01, 16 -> 6.52, 24 -> 6.41; the
+// previous scheme (each long run by the whole warp in turn) 8.0 ms.
+#ifndef GRASS_GT_SHORT_RUN
+#define GRASS_GT_SHORT_RUN 24
+#endif
+constexpr uint32_t kGtShortRun = GRASS_GT_SHORT_RUN;
+
+// Warp-cooperative GT draw: lane L may hold one draw (active) whose value is
+// v +/- (head + 1) + sum(gap + 1) over run.gaps gaps.  Short runs are summed
+// by their own lane.  The gap fields of all long runs, taken in lane order,
+// are cut into 32 equal contiguous shares, one per lane: a lane sums its
+// share with one sequential cursor per run it touches and adds each partial
+// sum to the run owner's word of acc (shared memory, 32 words per warp).  On
+// power-law graphs walks keep landing on hub vertices whose blocks hold
+// hundreds of gaps; this bounds every lane's work by the pool size / 32
+// instead of serialising the long runs one after another.  All 32 lanes must
+// call this together.
+__device__ __forceinline__ uint32_t gt_warp_neighbor(const uint32_t *words, bool active,
+                                                     uint32_t v, const GtRun &run, int a, int b,
+                                                     uint32_t *acc) {
+  const unsigned FULLM = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  const bool lng = active && run.gaps > kGtShortRun;
+  const uint32_t n = lng ? run.gaps : 0u;  // this lane's fields in the pool
+  uint32_t incl = n;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(FULLM, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t T = __shfl_sync(FULLM, incl, 31);
+  acc[lane] = 0u;
+  __syncwarp();
+  if (T) {  // warp-uniform
+    const unsigned owners = __ballot_sync(FULLM, n > 0);
+    const uint32_t per = (T + 31u) >> 5;
+    uint32_t k = min(T, (uint32_t)lane * per);
+    const uint32_t hi = min(T, k + per);
+    // the run holding pool field k: the first lane whose inclusive count exceeds k
+    int o = 0;
+#pragma unroll
+    for (int st = 16; st; st >>= 1) {
+      const uint32_t x = __shfl_sync(FULLM, incl, o + st - 1);
+      if (x <= k) o += st;
+    }
+    while (__any_sync(FULLM, k < hi)) {  // warp-uniform; o is valid wherever k < hi
+      const uint64_t po = __shfl_sync(FULLM, run.pos, o);
+      const int ao = __shfl_sync(FULLM, a, o), bo = __shfl_sync(FULLM, b, o);
+      const uint32_t io = __shfl_sync(FULLM, incl, o), no = __shfl_sync(FULLM, n, o);
+      if (k < hi) {
+        const uint32_t e = min(hi, io);
+        if (bo) {
+          BitCur c;
+          c.init(words, po + (uint64_t)ao + (uint64_t)(k - (io - no)) * (uint64_t)bo);
+          uint32_t s = 0;
+          for (uint32_t j = k; j < e; j++) s += c.get(bo);
+          atomicAdd(acc + o, s);
+        }
+        k = e;
+        if (k < hi) o = __ffs(owners & ~((2u << o) - 1u)) - 1;  // next run in the pool
+      }
+    }
+    __syncwarp();
+  }
+  if (!active) return v;
+  const uint32_t hv = read_field(words, run.pos, a) + 1u;
+  const uint32_t gs = lng ? run.gaps + acc[lane] : gap_sum(words, run.pos + (uint64_t)a, run.gaps, b);
+  return (run.up ? v + hv : v - hv) + gs;
+}
+
 // Gap runs longer than this are decoded by the whole warp.
 constexpr uint32_t kGtLongRun = 24;
 
-// Warp-cooperative GT draw: lane L may hold one draw (active) whose value is
+// Warp-cooperative GT draw, long runs one at a time (used by k-hop, whose
+// lanes mostly draw from the same few blocks of one transit): lane L may hold
+// one draw (active) whose value is
 // v +/- (head + 1) + sum(gap + 1) over run.gaps gaps.  Short runs are decoded
 // by their own lane.  Each long run (a hub vertex's block holds hundreds of
 // gaps) is split into 32 contiguous sub-ranges, one per lane, each summed by
 // its own cursor, and combined with __reduce_add_sync -- one memory round
 // trip and gaps/32 L1 reads per lane instead of one lane walking all gaps
 // while the rest of the warp waits.  All 32 lanes must call this together.
-__device__ __forceinline__ uint32_t gt_warp_neighbor(const uint32_t *words, bool active,
-                                                     uint32_t v, const GtRun &run, int a, int b,
-                                                     uint32_t * /* unused */) {
+__device__ __forceinline__ uint32_t gt_warp_neighbor_serial(const uint32_t *words, bool active,
+                                                            uint32_t v, const GtRun &run, int a,
+                                                            int b) {
   const unsigned FULLM = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const bool lng = active && run.gaps > kGtLongRun;

@@ -133,6 +133,10 @@ int cuda_fail(cudaError_t e, const char *what);
 
 // Streaming SM count of the current device (cached per device).
 int sm_count(int device);
+// Stream-ordered scratch on the current device from the library's own pool
+// (freed memory stays mapped for reuse).
+cudaError_t scratch_alloc(void **p, size_t bytes, cudaStream_t s);
+void scratch_free(void *p, cudaStream_t s);
 
 // ---- load path (kernels_load.cu) ----
 // In-place byte swap of n_words words.

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? GRASS_BATCH_MIN_BLOCKS_LE
     uint64_t cnt = 0;
     if (jb.type == GRASS_JOB_RW) {
       rw_warp<MODE, DEPTH>(g, jb.in, jb.count, jb.length, jb.seed, 0, (int)jb.layout, jb.out0,
-                           tk.begin, tk.end, cnt, bad);
+                           tk.begin, tk.end, cnt, bad, my.acc);
     } else if (jb.type == GRASS_JOB_KHOP) {
       for (uint64_t s = tk.begin; s < tk.end; s++)
         khop_seed_warp<MODE>(g, jb.in, jb.khop, s, my, cnt, bad);

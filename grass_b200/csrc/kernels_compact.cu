@@ -203,7 +203,7 @@ int launch_compact(const CompactSeg *segs, uint32_t nseg, uint32_t *src, uint32_
   const uint64_t cnt_words = (tiles + 1) / 2;  // u32 counts in u64 words
   const uint64_t words = cnt_words + (tiles + 1) + scan_tmp_words(tiles);
   uint64_t *scr = nullptr;
-  cudaError_t e = cudaMallocAsync(&scr, words * sizeof(uint64_t), s);
+  cudaError_t e = scratch_alloc(reinterpret_cast<void **>(&scr), words * sizeof(uint64_t), s);
   if (e != cudaSuccess) return cuda_fail(e, "compaction scratch");
   uint32_t *counts = reinterpret_cast<uint32_t *>(scr);
   uint64_t *offs = scr + cnt_words;
@@ -211,7 +211,7 @@ int launch_compact(const CompactSeg *segs, uint32_t nseg, uint32_t *src, uint32_
   if (segs[0].kind == kCompactFan) launch_kind<kCompactFan>(pl, counts, offs, tmp, src, dst, cap, s);
   else launch_kind<kCompactPath>(pl, counts, offs, tmp, src, dst, cap, s);
   e = cudaMemcpyAsync(count, offs + tiles, sizeof(uint64_t), cudaMemcpyDeviceToDevice, s);
-  cudaFreeAsync(scr, s);
+  scratch_free(scr, s);
   return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "compaction count");
 }
 

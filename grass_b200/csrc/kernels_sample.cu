@@ -95,9 +95,10 @@ __global__ void __launch_bounds__(512, GRASS_RW_LE_MIN_BLOCKS) rw_kernel(DevGrap
 
 // GT random walk.  A warp owns 32*DEPTH consecutive walkers and every step is
 // warp-synchronous, so the gap runs of all lanes are decoded cooperatively
-// (gt_warp_neighbor): on power-law graphs walks keep returning to hub
-// vertices whose blocks hold hundreds of gaps, which a per-lane loop would
-// serialise across the whole warp.
+// (gt_warp_neighbor, with the warp's 32 words of shared memory for the pooled
+// sums): on power-law graphs walks keep returning to hub vertices whose
+// blocks hold hundreds of gaps, which a per-lane loop would serialise across
+// the whole warp.
 template <int DEPTH>
 __global__ void __launch_bounds__(512, GRASS_RW_GT_MIN_BLOCKS) rw_gt_kernel(DevGraph g,
                                                     const uint32_t *__restrict__ starts,
@@ -691,12 +692,12 @@ int launch_mrw(const DevGraph &g, const grass_mrw_params &p, uint32_t *roots, ui
         std::min<uint64_t>(S, (uint64_t)sm_count(cur_dev()) * std::max(per_sm, 1));
     const uint64_t stride = mrw_sample_scratch(p.walkers, p.steps, p.select);
     unsigned char *scr = nullptr;
-    cudaError_t e = cudaMallocAsync(&scr, grid * stride, s);
+    cudaError_t e = scratch_alloc(reinterpret_cast<void **>(&scr), grid * stride, s);
     if (e != cudaSuccess) return cuda_fail(e, "multi-RW scratch");
     kern<<<(unsigned)grid, threads, 0, s>>>(g, roots, S, p.walkers, p.steps, p.select, p.seed, src,
                                             dst, scr, stride, edges, err);
     count_launch();
-    cudaFreeAsync(scr, s);
+    scratch_free(scr, s);
     return GRASS_OK;
   }
   const MrwLayout lay{p.walkers};
@@ -704,14 +705,15 @@ int launch_mrw(const DevGraph &g, const grass_mrw_params &p, uint32_t *roots, ui
   if (per_warp > 48 * 1024) {
     // Too many walkers for shared memory: the state lives in global scratch.
     uint4 *rec = nullptr;
-    cudaError_t e = cudaMallocAsync(&rec, S * (uint64_t)p.walkers * sizeof(uint4), s);
+    cudaError_t e =
+        scratch_alloc(reinterpret_cast<void **>(&rec), S * (uint64_t)p.walkers * sizeof(uint4), s);
     if (e != cudaSuccess) return cuda_fail(e, "multi-RW scratch");
     auto kern = g.mode == GRASS_MODE_GT ? mrw_global_kernel<0> : mrw_global_kernel<1>;
     kern<<<grid_warps(S, 8, cur_dev(), 8), 256, 0, s>>>(g, roots, rec, S, p.walkers, p.steps,
                                                         (int)p.select, p.seed, src, dst, edges,
                                                         err);
     count_launch();
-    cudaFreeAsync(rec, s);
+    scratch_free(rec, s);
     return GRASS_OK;
   }
   const size_t budget = 200 * 1024;

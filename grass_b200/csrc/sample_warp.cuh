@@ -1,7 +1,8 @@
 // sample_warp.cuh -- warp-level sampling routines shared by the standalone
 // multi-RW kernel and the batched persistent kernel.  Each routine is run by
-// all 32 lanes of one warp and needs no shared memory, so a persistent warp
-// can pick up any job type from a work queue.
+// all 32 lanes of one warp and needs at most the warp's own shared-memory
+// slot (SmemHdr), so a persistent warp can pick up any job type from a work
+// queue.
 #pragma once
 #include "device_common.cuh"
 
@@ -22,7 +23,7 @@ template <int MODE, int DEPTH>
 __device__ __forceinline__ void rw_warp(const DevGraph &g, const uint32_t *starts, uint64_t W,
                                         uint32_t L, uint64_t seed, uint64_t w0, int layout,
                                         uint32_t *paths, uint64_t b, uint64_t e, uint64_t &cnt,
-                                        bool &bad) {
+                                        bool &bad, uint32_t *acc) {
   const int lane = threadIdx.x & 31;
   for (uint64_t wb = b; wb < e; wb += 32 * DEPTH) {  // warp-uniform
     uint32_t v[DEPTH];
@@ -62,7 +63,7 @@ __device__ __forceinline__ void rw_warp(const DevGraph &g, const uint32_t *start
               rb = h.b;
             }
           }
-          nv = gt_warp_neighbor(g.words, active, v[k], run, ra, rb, nullptr);
+          nv = gt_warp_neighbor(g.words, active, v[k], run, ra, rb, acc);
         } else if (active) {
           const VHdr h = header<MODE>(g, v[k]);
           if (h.d == 0) {
@@ -105,6 +106,7 @@ struct SmemHdr {
   uint64_t P[32];
   uint32_t v[32], d[32], bn[32], bl[32], om[32], fp[32];
   int a[32], b[32];
+  uint32_t acc[32];  // GT: pooled gap sums (gt_warp_neighbor)
   __device__ __forceinline__ void put(int i, const VHdr &h) {
     P[i] = h.P; v[i] = h.v; d[i] = h.d; bn[i] = h.bn; bl[i] = h.bl; om[i] = h.om; fp[i] = h.fp;
     a[i] = h.a; b[i] = h.b;
@@ -173,7 +175,7 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
           }
         }
         if (MODE == 0) {
-          const uint32_t x = gt_warp_neighbor(g.words, draw, tv, run, ra, rb, nullptr);
+          const uint32_t x = gt_warp_neighbor_serial(g.words, draw, tv, run, ra, rb);
           if (draw) nv = x;
         }
         if (act) {
