@@ -48,7 +48,7 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 constexpr uint64_t kAlign = 256;
-constexpr uint32_t kMaxSlots = 8;
+constexpr uint32_t kMaxSlots = 16;
 
 inline uint64_t align_up(uint64_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 
@@ -668,12 +668,12 @@ int grass_server_create(const grass_graph *g, const grass_server_config *cfg,
   if (cfg) s->cfg = *cfg;
   grass_server_config &c = s->cfg;
   if (!c.scratch_budget) c.scratch_budget = 8ull << 30;
-  if (!c.target_draws) c.target_draws = 1ull << 23;
+  if (!c.target_draws) c.target_draws = 1ull << 22;
   if (!c.staging_bytes) c.staging_bytes = 1ull << 30;
   if (!c.window_min_us) c.window_min_us = 200;
   if (!c.window_max_us) c.window_max_us = 1000;
   if (c.window_max_us < c.window_min_us) c.window_max_us = c.window_min_us;
-  if (!c.max_inflight) c.max_inflight = 8;
+  if (!c.max_inflight) c.max_inflight = 16;
   if (!c.max_batch_jobs) c.max_batch_jobs = 4096;
   if (c.max_inflight > kMaxSlots) {
     delete s;

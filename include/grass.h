@@ -381,14 +381,14 @@ int grass_batch_destroy(grass_batch *b);
 typedef struct {
   uint64_t scratch_budget;   /* device bytes for launched requests, allocated at create
                                 (0: 8 GiB)                                            */
-  uint64_t target_draws;     /* close a batch at this much waiting work (0: 2^23)     */
+  uint64_t target_draws;     /* close a batch at this much waiting work (0: 2^22)     */
   uint64_t staging_bytes;    /* pinned host arena for inputs and results, made at
                                 create (0: 1 GiB); a batch carries at most 1/8 of it
                                 unless one request is larger.  Results hold their
                                 part until released, and batches wait for room.      */
   uint32_t window_min_us;    /* 0: 200                                                 */
   uint32_t window_max_us;    /* 0: 1000                                                */
-  uint32_t max_inflight;     /* batches in flight, one stream each (0: 8, at most 8);
+  uint32_t max_inflight;     /* batches in flight, one stream each (0: 16, at most 16);
                                 multi-RW batches take at most half of them            */
   uint32_t max_batch_jobs;   /* requests per batch (0: 4096)                           */
   grass_batch_config batch;  /* kernel shape (zero fields: defaults)                   */
