@@ -129,10 +129,15 @@ bool same_shape(const grass_batch_config &a, const grass_batch_config &b) {
 
 }  // namespace
 
+// Defaults: the autotuner's choice on the 256-job mix for LE, GT and CSR
+// alike, and in the serving loop (R-MAT s24 ef16, results in device memory)
+// 82 k req/s peak and p99 3.5 ms at 80 % of it, against 78 k and 3.8 ms with
+// 128-walker tiles of four interleaved walkers per lane.
 grass_batch_config resolve_batch_config(const grass_batch_config &c, int mode) {
+  (void)mode;
   grass_batch_config r = c;
-  if (!r.walker_tile) r.walker_tile = 128;
-  if (!r.depth) r.depth = mode == GRASS_MODE_GT ? 1 : 4;
+  if (!r.walker_tile) r.walker_tile = 64;
+  if (!r.depth) r.depth = 1;
   if (!r.warps_per_block) r.warps_per_block = 8;
   if (!r.khop_seeds) r.khop_seeds = 1;
   if (!r.use_graph) r.use_graph = 1;

@@ -323,8 +323,8 @@ typedef struct {
 /* Launch shape of the batched kernel; zero fields take defaults.  The
  * autotuner sweeps walker_tile x depth x warps_per_block. */
 typedef struct {
-  uint32_t walker_tile;      /* RW walkers per work item: 64, 128, 256 (default 128)          */
-  uint32_t depth;            /* RW walkers in flight per lane: 1, 2, 4 (LE 4, GT 1)            */
+  uint32_t walker_tile;      /* RW walkers per work item: 64, 128, 256 (default 64)           */
+  uint32_t depth;            /* RW walkers in flight per lane: 1, 2, 4 (default 1)            */
   uint32_t warps_per_block;  /* 1, 2, 4, 8 (default 8)                                        */
   uint32_t khop_seeds;       /* k-hop seeds per work item (default 1)                         */
   uint32_t use_graph;        /* 1 (default): replay a captured CUDA graph; 2: plain launches  */
