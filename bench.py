@@ -302,6 +302,24 @@ def ncu_traffic(workload_key: str):
     return d.get(workload_key)
 
 
+def random_sector_ceiling(G, torch, dev, flush, K=5, W=3):
+    """Uniform random 4-byte reads from a 2 GiB buffer (the library's
+    random-read probe: 8 loads in flight per thread, 2048 threads per SM).
+    Each read lands in its own 32-byte sector, so the rate is what HBM gives
+    random sector reads with no locality at all.  Reported beside the walks'
+    sector rates, which are higher: records and hub payloads are reused."""
+    n = 1 << 29
+    buf = torch.zeros(n, dtype=torch.int32, device=dev)
+    sink = torch.zeros(1, dtype=torch.int64, device=dev)
+    reads = 1 << 27
+    issued = G.random_read_probe(buf, n, reads, 3, sink)
+    ms, tot = timed(torch, lambda: G.random_read_probe(buf, n, reads, 3, sink), K, W, flush)
+    del buf
+    return {"reads_per_launch": issued, "ms_per_launch": tot / K,
+            "sectors_per_s": issued * K / (tot / 1000.0),
+            "method": "grass_random_read_probe: 2^27 uniform random 4-byte reads from a 2 GiB buffer"}
+
+
 # ---------------------------------------------------------------------------
 # timing
 
@@ -749,6 +767,19 @@ def main():
     peak, peak_kind = peaks()
     achieved = alg_bytes / avg_s / 1e9
     traffic = ncu_traffic(f"rw_{args.mode}_s{args.scale}_e{args.edge_factor}_W{W}_L{L}")
+    # random-access context: 32-byte sectors a walk reads per second, beside
+    # the rate of uniform random 4-byte reads over 2 GiB (no locality at all)
+    ceil = random_sector_ceiling(G, torch, dev, flush) if "rw" in only else None
+    rand = None
+    if ceil:
+        rand = {"uniform_random_reads_per_s": ceil["sectors_per_s"], "probe": ceil,
+                f"{args.mode}_sectors_per_draw": sectors / max(draws, 1),
+                f"{args.mode}_sectors_per_s": sectors / avg_s,
+                "note": "walk sectors include L2 hits (vertex records, hub payloads); "
+                        "uniform random reads have no locality, so they are not a ceiling"}
+        if "rw_CSR" in out:  # a CSR draw reads the row-pointer pair's sector and the column's
+            rand.update({"CSR_sectors_per_draw": 2.0,
+                         "CSR_sectors_per_s": 2 * draws / (out["rw_CSR"]["ms_per_step"] / 1000.0)})
 
     # ---- e2e through the host API, pinned buffers, copies inside the region
     e2e = None
@@ -801,6 +832,7 @@ def main():
                          "sector_bytes_per_launch": sectors * 32,
                          "sector_GBps": sectors * 32 / avg_s / 1e9,
                          "draws_per_launch": draws},
+            "random_access": rand,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": head["launches"],

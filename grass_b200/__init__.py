@@ -199,6 +199,7 @@ def _load():
         "grass_rw": ([P, C.POINTER(RwParams), P, u64, P, P, P], i32),
         "grass_rw_host": ([P, C.POINTER(RwParams), P, u64, P, P], i32),
         "grass_rw_account": ([P, C.POINTER(RwParams), P, u64, P, P], i32),
+        "grass_random_read_probe": ([P, u64, u64, u64, P, C.POINTER(u64), P], i32),
         "grass_khop": ([P, C.POINTER(KhopParams), P, u64, P, P, P], i32),
         "grass_khop_host": ([P, C.POINTER(KhopParams), P, u64, P, P], i32),
         "grass_mrw": ([P, C.POINTER(MrwParams), P, u64, P, P, P, P], i32),
@@ -501,6 +502,15 @@ class Graph:
         h = C.c_void_p()
         _check(lib.grass_csr_from_graph(self._h, C.byref(h)))
         return Csr(h)
+
+
+def random_read_probe(buf, n_words: int, reads: int, seed: int, sink, stream=None) -> int:
+    """About `reads` independent random 4-byte reads from buf[0, n_words); returns
+    the number issued (the device's random-read ceiling when timed)."""
+    k = C.c_uint64()
+    _check(lib.grass_random_read_probe(_ptr(buf), n_words, reads, seed, _ptr(sink), C.byref(k),
+                                       _stream(stream)))
+    return int(k.value)
 
 
 def mrw_roots_device(n: int, S: int, R: int, seed: int, out, stream=None):

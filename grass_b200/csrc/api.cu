@@ -558,6 +558,17 @@ int grass_rw_account(const grass_graph *g, const grass_rw_params *p, const uint3
   return check_launch();
 }
 
+int grass_random_read_probe(const uint32_t *d_buf, uint64_t n_words, uint64_t reads,
+                            uint64_t seed, unsigned long long *d_sink, uint64_t *issued,
+                            void *stream) {
+  clear_error();
+  if (!d_buf || !d_sink || !n_words || (n_words & (n_words - 1)))
+    return set_error(GRASS_E_ARG, "random-read probe: n_words must be a power of two");
+  const uint64_t k = launch_random_read(d_buf, n_words, reads, seed, d_sink, as_stream(stream));
+  if (issued) *issued = k;
+  return check_launch();
+}
+
 int grass_rw_host(const grass_graph *g, const grass_rw_params *p, const uint32_t *h_starts,
                   uint64_t W, uint32_t *h_paths, uint64_t *edges_out) {
   clear_error();

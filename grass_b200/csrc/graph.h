@@ -181,6 +181,10 @@ void launch_rw(const DevGraph &g, const grass_rw_params &p, const uint32_t *star
 // hot table of `bytes` at `base`.
 int apply_tuning(int device, const grass_tuning &t, const void *base, size_t bytes,
                  L2Window &win);
+// Random-read probe: about `reads` independent random 4-byte reads from
+// buf[0, n_words) (n_words a power of two); returns the exact count issued.
+uint64_t launch_random_read(const uint32_t *buf, uint64_t n_words, uint64_t reads, uint64_t seed,
+                            unsigned long long *sink, cudaStream_t s);
 void launch_rw_account(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts,
                        uint64_t W, unsigned long long *out, cudaStream_t s);
 void launch_rw_csr(const DevCsr &c, const grass_rw_params &p, const uint32_t *starts,

@@ -224,6 +224,32 @@ __device__ __forceinline__ void draw_footprint(const DevGraph &g, const VHdr &h,
 // (path entry) and the 32-byte sectors the reads span (+1 for the record).
 // out[0] = bytes, out[1] = sectors, out[2] = draws.  Start entries add 4
 // bytes each.
+// Independent random 4-byte reads: each thread draws xorshift64 indices into
+// buf[0, mask] and keeps 8 loads in flight; the sum goes to *sink so the loads
+// are not dropped.  Used to measure the device's random-read ceiling.
+__global__ void __launch_bounds__(256) random_read_kernel(const uint32_t *__restrict__ buf,
+                                                          uint64_t mask, uint64_t per_thread,
+                                                          uint64_t seed,
+                                                          unsigned long long *sink) {
+  const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  uint64_t x = (seed + 1) * 0x9E3779B97F4A7C15ull ^ (tid + 1) * 0xBF58476D1CE4E5B9ull;
+  uint32_t acc = 0;
+  for (uint64_t r = 0; r < per_thread; r += 8) {
+    uint32_t v[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      x ^= x << 13;
+      x ^= x >> 7;
+      x ^= x << 17;
+      v[k] = __ldg(buf + (x & mask));
+    }
+#pragma unroll
+    for (int k = 0; k < 8; k++) acc += v[k];
+  }
+  acc = __reduce_add_sync(0xFFFFFFFFu, acc);
+  if ((threadIdx.x & 31) == 0) atomicAdd(sink, (unsigned long long)acc);
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256) rw_account_kernel(DevGraph g,
                                                          const uint32_t *__restrict__ starts,
@@ -594,6 +620,16 @@ void launch_rw(const DevGraph &g, const grass_rw_params &p, const uint32_t *star
   if (g.mode == GRASS_MODE_GT) rw_dispatch<0>(g, p, starts, W, paths, edges, err, s, t, win, w0);
   else rw_dispatch<1>(g, p, starts, W, paths, edges, err, s, t, win, w0);
   count_launch();
+}
+
+uint64_t launch_random_read(const uint32_t *buf, uint64_t n_words, uint64_t reads, uint64_t seed,
+                            unsigned long long *sink, cudaStream_t s) {
+  const unsigned grid = (unsigned)sm_count(cur_dev()) * 8;
+  const uint64_t threads = (uint64_t)grid * 256;
+  const uint64_t per_thread = ((reads + threads - 1) / threads + 7) / 8 * 8;
+  random_read_kernel<<<grid, 256, 0, s>>>(buf, n_words - 1, per_thread, seed, sink);
+  count_launch();
+  return per_thread * threads;
 }
 
 void launch_rw_account(const DevGraph &g, const grass_rw_params &p, const uint32_t *starts,

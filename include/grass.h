@@ -217,6 +217,15 @@ int grass_rw_host(const grass_graph *g, const grass_rw_params *p, const uint32_t
  * for the offset) and to d_out[2] the number of draws. */
 int grass_rw_account(const grass_graph *g, const grass_rw_params *p, const uint32_t *d_starts,
                      uint64_t W, unsigned long long *d_out, void *stream);
+/* Random-read probe (no reference counterpart): about `reads` independent
+ * random 4-byte reads from d_buf[0, n_words) (n_words a power of two), eight
+ * in flight per thread, with the loaded values summed into *d_sink; *issued
+ * receives the exact number of reads.  Timed on a buffer far larger than L2,
+ * it gives the device's ceiling for random 32-byte sector reads, against
+ * which the samplers' dependent random reads are compared. */
+int grass_random_read_probe(const uint32_t *d_buf, uint64_t n_words, uint64_t reads,
+                            uint64_t seed, unsigned long long *d_sink, uint64_t *issued,
+                            void *stream);
 
 #define GRASS_MAX_HOPS 8
 typedef struct {

@@ -212,3 +212,17 @@ def test_rw_paths_are_edges_at_scale(torch_cuda):
     src = np.repeat(np.arange(len(rp) - 1, dtype=np.int64), np.diff(rp).astype(np.int64))
     edges = src * (1 << 32) + cols.astype(np.int64)
     assert np.isin(keys, edges, assume_unique=False).all()
+
+
+def test_random_read_probe_counts_every_read(torch_cuda):
+    """The random-read probe (the bench's random-access ceiling) reads what it
+    claims: over a buffer of ones the sink equals the number of reads."""
+    torch = torch_cuda
+    n = 1 << 20
+    buf = torch.ones(n, dtype=torch.int32, device="cuda")
+    sink = torch.zeros(1, dtype=torch.int64, device="cuda")
+    k = G.random_read_probe(buf, n, 1 << 22, 9, sink)
+    torch.cuda.synchronize()
+    assert k >= 1 << 22 and int(sink.item()) == k
+    with pytest.raises(G.GrassError):
+        G.random_read_probe(buf, n - 1, 1 << 10, 9, sink)
