@@ -419,8 +419,13 @@ __device__ __forceinline__ uint32_t gt_warp_neighbor(const uint32_t *words, bool
   return (run.up ? v + hv : v - hv) + gs;
 }
 
-// Gap runs longer than this are decoded by the whole warp.
-constexpr uint32_t kGtLongRun = 24;
+// Gap runs longer than this are decoded by the whole warp (k-hop).  Measured
+// on k-hop (25, 10) from 65,536 seeds, R-MAT s22 ef32: 12 -> 2.12 ms,
+// 24 -> 1.95 ms, 48 -> 1.81 ms.
+#ifndef GRASS_GT_LONG_RUN
+#define GRASS_GT_LONG_RUN 48
+#endif
+constexpr uint32_t kGtLongRun = GRASS_GT_LONG_RUN;
 
 // Warp-cooperative GT draw, long runs one at a time (used by k-hop, whose
 // lanes mostly draw from the same few blocks of one transit): lane L may hold
