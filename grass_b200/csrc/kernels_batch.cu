@@ -185,8 +185,9 @@ void split_job(const grass_job &j, uint32_t ji, const grass_batch_config &c,
     auto &q = j.select == GRASS_SELECT_DEGREE ? mrw : cta;
     for (uint64_t s = 0; s < j.count; s++) q.push_back({ji, 0, s, s + 1});
   } else {
-    for (uint64_t w = 0; w < j.count; w += c.walker_tile)
-      rw.push_back({ji, 0, w, std::min<uint64_t>(j.count, w + c.walker_tile)});
+    const uint64_t tile = rw_tile(j.count, c);
+    for (uint64_t w = 0; w < j.count; w += tile)
+      rw.push_back({ji, 0, w, std::min<uint64_t>(j.count, w + tile)});
   }
 }
 

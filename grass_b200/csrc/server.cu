@@ -308,7 +308,10 @@ uint64_t table_bytes(size_t njobs, size_t ntasks) {
 // Work items of a request (an upper bound is enough for the budget).
 uint64_t task_bound(const Req &q, const grass_batch_config &c) {
   const uint64_t n = q.rq.count;
-  if (q.rq.type == GRASS_JOB_RW) return (n + c.walker_tile - 1) / c.walker_tile;
+  if (q.rq.type == GRASS_JOB_RW) {
+    const uint64_t t = rw_tile(n, c);
+    return (n + t - 1) / t;
+  }
   if (q.rq.type == GRASS_JOB_KHOP) return (n + c.khop_seeds - 1) / c.khop_seeds;
   return n;
 }
