@@ -276,8 +276,8 @@ int grass_mrw_roots(uint64_t n, uint64_t S, uint32_t R, uint64_t seed, uint32_t 
  * one scan over 4096-entry tile counts.  Edges past `capacity` are not
  * written; *d_count (a device word) receives the total number of valid
  * edges, which equals the sampler's edge count.  The buffers must be on the
- * current device; each call allocates its tile counts from the stream's
- * memory pool.
+ * current device; each call takes its tile counts from a stream-ordered
+ * memory pool private to this library.
  * ========================================================================= */
 
 /* k-hop output (grass_khop / grass_csr_khop) in (hop, seed, slot) order:
