@@ -58,3 +58,25 @@ def test_header_has_citations():
     for ref in ("GT/src/grass.cu", "GT/src/bcg.cuh", "LE/src/bcg.cuh", "compressor.hpp",
                 "randomWalks.cu", "khop.cu", "multiRW.cu"):
         assert ref in txt
+
+
+def test_compaction_arguments_are_checked_before_any_device_work():
+    """The edge-list calls reject bad arguments on the host (no GPU needed)."""
+    with pytest.raises(G.GrassError) as e:  # no count word
+        G.khop_edges_device(None, 0, (25, 10), [None, None], None, None, 0, None)
+    assert e.value.code == G.E_ARG
+    with pytest.raises(G.GrassError) as e:  # capacity without outputs
+        G.rw_edges_device(16, 4, 8, None, None, 4, 16)
+    assert e.value.code == G.E_ARG
+    with pytest.raises(G.GrassError) as e:  # layout out of range
+        G.rw_edges_device(16, 4, 8, None, None, 0, 16, layout=5)
+    assert e.value.code == G.E_ARG
+    with pytest.raises(G.GrassError) as e:  # zero fanout
+        G.khop_edges_device(None, 0, (25, 0), [None, None], None, None, 0, 16)
+    assert e.value.code == G.E_ARG
+    with pytest.raises(G.GrassError) as e:  # multi-RW steps without step buffers
+        G.mrw_edges_device(None, None, 4, 10, None, None, 0, 16)
+    assert e.value.code == G.E_ARG
+    with pytest.raises(G.GrassError) as e:  # probe size not a power of two
+        G.random_read_probe(16, 1000, 10, 1, 16)
+    assert e.value.code == G.E_ARG
