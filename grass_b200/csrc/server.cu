@@ -4,7 +4,7 @@
 // nextdoor() in GT/src/grass.cu:2066-2135) and has no request path.  Here
 // client threads submit RW / k-hop / multi-RW requests; one dispatcher thread
 // groups waiting requests into a batch, reserves their device scratch against
-// the budget and issues, on one of up to eight streams:
+// the budget and issues, on one of up to sixteen streams:
 //
 //   H2D (job table, work items, inputs, zeroed counters)
 //     -> persistent batch kernel (which also draws multi-RW start vertices)
