@@ -58,3 +58,26 @@ def test_single_process_needs_no_group():
     assert bench.dist_init(1, "gloo") is None
     assert bench.max_over_ranks(None, 3.0) == 3.0
     assert bench.sum_over_ranks(None, 4.0) == 4.0
+
+
+def test_batched_jobs_mix_matches_its_specification():
+    """The 256-job mix of the batched-jobs workload: 40 % RW with L in
+    [10, 100], 40 % k-hop with fanouts from the fixed list, 20 % multi-RW of
+    one 2000-walker, 10,000-step continuous-time sample; sizes lognormal,
+    clipped to [1, 65536]; the same jobs for the same seed."""
+    import bench
+    jobs = bench.mix_jobs(1 << 20)
+    assert len(jobs) == 256 and jobs == bench.mix_jobs(1 << 20)
+    kinds = [j["type"] for j in jobs]
+    assert kinds.count(0) == 102 and kinds.count(1) == 102 and kinds.count(2) == 52
+    for j in jobs:
+        if j["type"] == 0:
+            assert 1 <= j["count"] <= 65536 and 10 <= j["length"] <= 100
+        elif j["type"] == 1:
+            assert 1 <= j["count"] <= 65536 and tuple(j["fanouts"]) in map(tuple, bench.MIX_FANOUTS)
+        else:
+            assert (j["count"], j["walkers"], j["steps"], j["select"]) == (1, 2000, 10000, 2)
+    import numpy as np
+    sizes = np.array([j["count"] for j in jobs if j["type"] != 2], dtype=np.float64)
+    assert 300 < np.median(sizes) < 3000  # lognormal(ln 1024, 1.5)
+    assert len({j["seed"] for j in jobs}) == 256
