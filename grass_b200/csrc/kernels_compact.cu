@@ -16,6 +16,8 @@
 //      offset + rank -- the output keeps the input order.
 // Parent indices advance incrementally (32 / div and 32 % div per step), so a
 // lane divides once per tile, not once per entry.
+#include <atomic>
+
 #include "graph.h"
 
 namespace grass {
@@ -164,10 +166,17 @@ __global__ void __launch_bounds__(kThreads)
 template <int KIND>
 void launch_kind(const Plan &pl, uint32_t *counts, uint64_t *offs, uint64_t *tmp, uint32_t *src,
                  uint32_t *dst, uint64_t cap, cudaStream_t s) {
-  int dev = 0, per_sm = 0;
+  // resident blocks per SM, queried once (every device here is the same part)
+  static std::atomic<int> cached{0};
+  int per_sm = cached.load(std::memory_order_relaxed);
+  if (!per_sm) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, compact_fill_kernel<KIND>, kThreads, 0);
+    per_sm = std::max(per_sm, 1);
+    cached.store(per_sm, std::memory_order_relaxed);
+  }
+  int dev = 0;
   cudaGetDevice(&dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, compact_fill_kernel<KIND>, kThreads, 0);
-  const uint64_t resident = (uint64_t)sm_count(dev) * (uint64_t)std::max(per_sm, 1) * 4;
+  const uint64_t resident = (uint64_t)sm_count(dev) * (uint64_t)per_sm * 4;
   const unsigned grid = (unsigned)std::min<uint64_t>(pl.tiles, resident);
   compact_count_kernel<KIND><<<grid, kThreads, 0, s>>>(pl, counts);
   launch_scan_u32(counts, pl.tiles, offs, tmp, s);
