@@ -16,6 +16,11 @@ on the launching stream, L2 flushed by a 256 MiB write between timed steps).
 `e2e` = the same metric through the public host API (grass_rw_host) from pinned
 host memory, copies of starts in and paths out inside the timed region.
 
+After each timed region rank 0 checks what the timed launches produced
+against the CPU oracle, bit for bit (`parity` key; the run exits non-zero on
+a mismatch): walkers 0..65535 of each walk, seeds 0..4095 of each k-hop, the
+whole decode sweep, 8 jobs of each batched run.
+
 `--impl reference` times the reference's CPU decode+sample path -- here the
 CPU oracle's restatement of the reference decoders and app logic (the
 reference has no CPU sampler) -- on all host cores.
@@ -55,7 +60,7 @@ def parse():
     ap.add_argument("--khop-seeds", type=int, default=65536)
     ap.add_argument("--mode", default="LE", choices=["LE", "GT"])
     ap.add_argument("--only", default="",
-                    help="comma list: rw,khop,decode,csr,e2e,cpu,batch,serve,cfg5 "
+                    help="comma list: rw,khop,decode,csr,e2e,cpu,batch,serve,parity,cfg5 "
                          "(cfg5, the 3B-edge Chung-Lu graph, runs only when named)")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--batch-scale", type=int, default=24,
@@ -167,7 +172,7 @@ def build_chung_lu(n, exponent, mean_degree, max_degree, seed=42):
     return d, meta
 
 
-def cfg5_bench(G, torch, stream, flush, K):
+def cfg5_bench(G, torch, stream, flush, K, parity=None):
     """Skewed large graph: Chung-Lu n = 100M, exponent 2.1, mean degree 30,
     max degree 1M (~3B directed edges after symmetrising).  4M uniform walks
     of length 40, k-hop (15, 10) for 262,144 seeds drawn among the vertices
@@ -199,6 +204,18 @@ def cfg5_bench(G, torch, stream, flush, K):
     rp = np.load(os.path.join(gdir, "rowptr.npy"))
     hubs = np.nonzero(np.diff(rp) >= 1000)[0].astype(np.uint32)
     del rp
+    if parity is not None and parity.enabled:
+        # walks that start on hubs (degree >= 1000): long LE chunks, long GT runs
+        Wh = 16384
+        hs = torch.from_numpy(hubs[np.random.default_rng(5).integers(0, len(hubs), Wh)]
+                              .view(np.int32)).to(dev)
+        hp = torch.empty(Wh * (L + 1), dtype=torch.int32, device=dev)
+        for m in ("LE", "GT"):
+            graphs[m].rw_device(hs, Wh, L, 9, hp, layout=LAYOUT, stream=stream)
+            torch.cuda.synchronize()
+            parity.rw(f"cfg5_rw_hub_starts_{m}", os.path.join(gdir, m), m, hs, Wh, L, 9, hp,
+                      LAYOUT)
+        del hp
     S, fan = 262144, (15, 10)
     pick = np.random.default_rng(11).integers(0, len(hubs), S)
     seeds = torch.from_numpy(hubs[pick].view(np.int32)).to(dev)
@@ -212,6 +229,9 @@ def cfg5_bench(G, torch, stream, flush, K):
                                                            stream=stream), K, 2, flush)
         out[f"khop_{name}"] = {"value": e1 * K / (tot / 1000.0), "ms_per_step": tot / K,
                                "seeds_with_degree_ge_1000": int(len(hubs))}
+        if parity is not None and name != "CSR":
+            parity.khop(f"cfg5_khop_{name}", os.path.join(gdir, name), name, seeds, S, fan, 13,
+                        hops, k=1024)
     del hops
     rp_d = torch.empty(n + 1, dtype=torch.int64, device=dev)
     cl_d = torch.empty(E, dtype=torch.int32, device=dev)
@@ -236,7 +256,8 @@ def cfg5_bench(G, torch, stream, flush, K):
 class Clocks:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,"
+              "utilization.gpu")
 
     def __init__(self, gpu_index: int, enabled: bool = True):
         self.p = None
@@ -262,17 +283,18 @@ class Clocks:
         except Exception:
             self.p.kill()
         self.f.close()
-        sm, mx, pw = [], [], []
+        sm, mx, pw, busy = [], [], [], []
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
                 sm.append(float(parts[1]))
                 mx.append(float(parts[2]))
                 pw.append(float(parts[3]))
+                busy.append(float(parts[9]) >= 50.0)
             except ValueError:
                 continue
             for nm, val in zip(names, parts[5:9]):
@@ -281,8 +303,12 @@ class Clocks:
         os.unlink(self.path)
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "samples": len(sm),
-                "power_w_max": max(pw), "reasons": sorted(reasons)}
+        # median under load: samples with the GPU busy (the sampler also runs
+        # while the host checks outputs between timed regions)
+        loaded = [c for c, b in zip(sm, busy) if b] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx), "samples": len(sm),
+                "samples_under_load": sum(busy), "power_w_max": max(pw),
+                "reasons": sorted(reasons)}
 
 
 def peaks():
@@ -291,6 +317,88 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+class Parity:
+    """Bit-exact checks of what the timed launches produced, against the CPU
+    oracle (the checker), run after each timed region and outside it.  Each
+    check compares a bounded slice of a benchmarked output -- walkers and
+    seeds 0..k-1 use the same Philox streams in the full launch and in the
+    oracle's run over those k inputs -- or, for the decode sweep, all of it."""
+
+    def __init__(self, enabled: bool):
+        self.enabled = enabled
+        self.res = {}
+        self._og = {}
+
+    def graph(self, prefix):
+        import oracle
+        if prefix not in self._og:
+            self._og[prefix] = oracle.OracleGraph(prefix)
+        return self._og[prefix]
+
+    def put(self, key, ok, **detail):
+        self.res[key] = {"ok": bool(ok), **detail}
+
+    def rw(self, key, prefix, mode, starts, W, L, seed, paths, layout, k=65536):
+        """paths: the launch's [L+1][W] (step-major) or [W][L+1] output."""
+        if not self.enabled:
+            return
+        k = min(k, W)
+        st = starts[:k].cpu().numpy().view(np.uint32)
+        ref, _ = self.graph(prefix).rw(mode, st, L, seed)
+        P = paths.view(L + 1, W)[:, :k].T if layout == 1 else paths.view(W, L + 1)[:k]
+        got = P.contiguous().cpu().numpy().view(np.uint32)
+        self.put(key, np.array_equal(got, ref), walkers=k, steps=L)
+
+    def khop(self, key, prefix, mode, seeds, S, fan, seed, hops, k=4096):
+        if not self.enabled:
+            return
+        k = min(k, S)
+        sd = seeds[:k].cpu().numpy().view(np.uint32)
+        refs, _ = self.graph(prefix).khop(mode, sd, fan, seed)
+        ok = True
+        for h, w in enumerate(np.cumprod(fan)):
+            got = hops[h].view(S, int(w))[:k].cpu().numpy().view(np.uint32)
+            ok = ok and np.array_equal(got, refs[h])
+        self.put(key, ok, seeds=k, fanouts=list(fan))
+
+    def batch(self, key, prefix, mode, jobs, bufs, per_type=(3, 3, 2)):
+        """The first per_type[t] jobs of each type of a batched run: RW paths
+        (walk-major), k-hop frontiers, multi-RW edges and final roots."""
+        if not self.enabled:
+            return
+        og = self.graph(prefix)
+        u32 = lambda t: t.cpu().numpy().view(np.uint32)  # noqa: E731
+        ok, picked = True, [0, 0, 0]
+        for j, (inp, outs, snap) in zip(jobs, bufs):
+            t = j["type"]
+            if picked[t] >= per_type[t]:
+                continue
+            picked[t] += 1
+            c = j["count"]
+            if t == 0:
+                ref, _ = og.rw(mode, u32(inp), j["length"], j["seed"])
+                ok = ok and np.array_equal(u32(outs[0]).reshape(c, -1), ref)
+            elif t == 1:
+                refs, _ = og.khop(mode, u32(inp), j["fanouts"], j["seed"])
+                ok = ok and all(np.array_equal(u32(o).reshape(c, -1), r)
+                                for o, r in zip(outs, refs))
+            else:
+                roots = u32(snap).reshape(c, j["walkers"])
+                src, dst, fin, _ = og.mrw(mode, roots, j["steps"], j["seed"], j["select"])
+                ok = (ok and np.array_equal(u32(outs[0]).reshape(c, -1), src) and
+                      np.array_equal(u32(outs[1]).reshape(c, -1), dst) and
+                      np.array_equal(u32(inp).reshape(c, -1), fin))
+        self.put(key, ok, jobs={"rw": picked[0], "khop": picked[1], "mrw": picked[2]})
+
+    def decode(self, key, prefix, mode, rowptr, cols):
+        if not self.enabled:
+            return
+        rp, cl = self.graph(prefix).decode_all(mode)
+        ok = (np.array_equal(rowptr.cpu().numpy().view(np.uint64), rp) and
+              np.array_equal(cols.cpu().numpy().view(np.uint32), cl))
+        self.put(key, ok, neighbors=int(len(cl)), vertices=int(len(rp) - 1))
 
 
 def ncu_traffic(workload_key: str):
@@ -377,9 +485,10 @@ def mix_jobs(n, k=256, seed=3):
     return jobs
 
 
-def batch_bench(G, torch, graphs, n, stream, flush, K, W):
+def batch_bench(G, torch, graphs, n, stream, flush, K, W, parity=None, gdir=None):
     """One persistent captured launch over 256 uneven jobs, autotuned, against
-    the plain method (one standalone launch per job, same stream)."""
+    the plain method (one standalone launch per job, same stream).  After the
+    timed runs of each compressed mode, parity checks 8 of the jobs."""
     dev = torch.device("cuda", torch.cuda.current_device())
     jobs = mix_jobs(n)
     bufs = []
@@ -426,6 +535,8 @@ def batch_bench(G, torch, graphs, n, stream, flush, K, W):
         lc0 = G.launch_count()
         ms, tot = timed(torch, lambda: b.run(stream=stream), K, W, flush)
         launches = (G.launch_count() - lc0) / (K + W)
+        if parity is not None and m in ("LE", "GT"):
+            parity.batch(f"batch_{m}", os.path.join(gdir, m), m, jobs, bufs)
         short = make({0, 1})
         short.set_config(**{k: v for k, v in best.items() if k != "use_graph"})
         ms_s, tot_s = timed(torch, lambda: short.run(stream=stream), K, W, flush)
@@ -625,7 +736,7 @@ def main():
     import grass_b200 as G
 
     only = set(args.only.split(",")) if args.only else {"rw", "khop", "decode", "csr", "e2e",
-                                                         "cpu", "batch", "serve"}
+                                                         "cpu", "batch", "serve", "parity"}
     gdir, meta = build_graph(args.scale, args.edge_factor)
     n, E = meta["n"], meta["num_edges"]
     W, L = args.walkers, args.length
@@ -647,6 +758,8 @@ def main():
     ecount = torch.zeros(1, dtype=torch.int64, device=dev)
     clocks = Clocks(local, enabled=not args.no_clocks)
     out = {}
+    # the oracle checks the benchmarked outputs on rank 0 (outside every timed region)
+    parity = Parity(rank == 0 and "parity" in only)
 
     def rw_fn(obj):
         return lambda: obj.rw_device(starts, W, L, replica_seed(7, rank), paths, ecount, layout=LAYOUT,
@@ -667,6 +780,8 @@ def main():
         out[f"rw_{m}"] = {"value": all_edges / (tot / 1000.0), "ms_per_step": tot / args.steps,
                           "edges_per_step": edges_per_step, "launches": lc,
                           "ms_min": min(ms), "ms_max": max(ms)}
+        parity.rw(f"rw_{m}", os.path.join(gdir, m), m, starts, W, L, replica_seed(7, rank),
+                  paths, LAYOUT)
     if "csr" in only and csr is not None:
         ecount.zero_()
         csr.rw_device(starts, W, L, replica_seed(7, rank), paths, ecount, layout=LAYOUT, stream=stream)
@@ -693,6 +808,9 @@ def main():
                             args.steps, args.warmup, flush, dist, local)
             out[f"khop_{name}"] = {"value": sum_over_ranks(dist, e1 * args.steps, torch) /
                                    (tot / 1000.0), "ms_per_step": tot / args.steps}
+            if name != "CSR":
+                parity.khop(f"khop_{name}", os.path.join(gdir, name), name, seeds, S, fan, 13,
+                            hops)
         # output compaction of the same frontiers to a (src, dst) edge list
         slots = S * sum(G.hop_widths(fan))
         csrc = torch.empty(slots, dtype=torch.int32, device=dev)
@@ -724,6 +842,7 @@ def main():
             ms, tot = timed(torch, lambda g=graphs[m]: g.decode_all_device(rp_d, cl_d,
                                                                            stream=stream),
                             args.steps, args.warmup, flush, dist, local)
+            parity.decode(f"decode_{m}", os.path.join(gdir, m), m, rp_d, cl_d)
             stream_bytes = infos[m]["graph_file_bytes"] + (n + 1) * 8
             out[f"decode_{m}"] = {
                 "value": sum_over_ranks(dist, E * args.steps, torch) / (tot / 1000.0),
@@ -745,7 +864,7 @@ def main():
         if "batch" in only:
             bcsr = bgraphs["LE"].csr()  # uncompressed baseline of the same graph
             extra["batch"] = batch_bench(G, torch, {**bgraphs, "CSR": bcsr}, bn, stream, flush,
-                                         5, 3)
+                                         5, 3, parity, bdir)
             bcsr.close()
             del bcsr
         if "serve" in only:
@@ -755,7 +874,7 @@ def main():
 
     # ---- skewed large graph (Chung-Lu, ~3B edges): only when asked for
     if ws == 1 and "cfg5" in only:
-        out["chung_lu_100M"] = cfg5_bench(G, torch, stream, flush, 3)
+        out["chung_lu_100M"] = cfg5_bench(G, torch, stream, flush, 3, parity)
 
     # ---- accounting for the roofline of the headline kernel
     acct = torch.zeros(3, dtype=torch.int64, device=dev)
@@ -845,10 +964,16 @@ def main():
                                 **{f"ratio_{m}": csr_bytes / infos[m]["device_bytes"]
                                    for m in infos}},
             "load_seconds": {m: infos[m]["upload_seconds"] for m in infos},
+            "parity": ({k: v["ok"] for k, v in parity.res.items()} if parity.enabled else None),
+            "parity_detail": parity.res if parity.enabled else None,
         }
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
+    bad = [k for k, v in parity.res.items() if not v["ok"]]
+    if bad:
+        print(f"parity mismatch against the oracle: {', '.join(bad)}", file=sys.stderr)
+        return 1
     return 0
 
 

@@ -264,6 +264,21 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
   cudaFree(g->d_offsets);
   g->d_offsets = nullptr;
 
+  // LE: payloads with short chunks are rewritten in neighbor order (one span
+  // per draw, le_chunked); the rewrite goes to a copy, which replaces the
+  // on-disk order stream.
+  if (mode == GRASS_MODE_LE) {
+    uint32_t *d_re = nullptr;
+    GRASS_CUDA(cudaMalloc(&d_re, alloc_words * 4));
+    tmp.dev.push_back(d_re);
+    GRASS_CUDA(cudaMemcpyAsync(d_re, g->d_words, alloc_words * 4, cudaMemcpyDeviceToDevice, st));
+    launch_le_reorder(g->d_words, d_re, g->d_recs, (uint32_t)n, st);
+    GRASS_CUDA(cudaStreamSynchronize(st));
+    GRASS_CUDA(cudaGetLastError());
+    tmp.dev.back() = g->d_words;  // the on-disk order copy is freed with tmp
+    g->d_words = d_re;
+  }
+
   g->info.n_file = n_file;
   g->info.num_edges = stats[0];
   g->info.max_degree = (uint32_t)stats[1];

@@ -499,25 +499,100 @@ __device__ __forceinline__ VHdr le_header(const DevGraph &g, uint32_t v) {
   return h;
 }
 
-// LE get_vertex, LE/src/bcg.cuh:195-261: two rocks and one signed sea.
-__device__ __forceinline__ uint32_t le_neighbor(const DevGraph &g, const VHdr &h, uint32_t i) {
-  if (h.d == 1) return h.fp;
-  uint32_t tl = h.bl + 1;
+// ---- LE payload layout in HBM ----
+// On disk an LE payload holds all chunk_num + 1 rocks, then all seas in chunk
+// order (LE/chunk_compress/compressor.hpp:352-359), so a draw reads its rock
+// pair from one place and its sea from another: two random sectors.  At load,
+// every vertex whose longest chunk spans at most kLeChunkSpan bits is rewritten
+// in neighbor order, chunk by chunk:
+//   [rock 0][seas of chunk 0][rock 1][seas of chunk 1] ... [rock chunk_num]
+// The same fields with the same widths, permuted inside the vertex's own bit
+// range (P and the payload length do not change, nor does the footprint), so a
+// draw finds its left rock, its sea and its right rock in one contiguous span
+// of at most kLeChunkSpan bits: one sector, or two when the span crosses a
+// sector end.  Vertices with longer chunks (hubs) keep the on-disk order,
+// where the rock pair is adjacent and the sea is one more sector.  Whether a
+// vertex is rewritten follows from its header alone (le_chunked).
+#ifndef GRASS_LE_CHUNK_SPAN
+#define GRASS_LE_CHUNK_SPAN 256
+#endif
+constexpr uint32_t kLeChunkSpan = GRASS_LE_CHUNK_SPAN;
+
+__device__ __forceinline__ bool le_chunked(const VHdr &h) {
+  if (h.d < 2) return false;
+  const uint32_t seas = h.bl - (h.om ? 0u : 1u);  // seas of the longest chunk
+  return 2u * (uint32_t)h.a + seas * (uint32_t)(h.b + 1) <= kLeChunkSpan;
+}
+
+// Chunk c and index id of neighbor i, and the chunk's length tl
+// (LE/src/bcg.cuh:198-205).
+__device__ __forceinline__ void le_locate(const VHdr &h, uint32_t i, uint32_t &c, uint32_t &id,
+                                          uint32_t &tl) {
+  tl = h.bl + 1;
   const uint32_t split = h.om * tl;
   const bool flag = i >= split;
   const uint32_t j = flag ? i - split : i;
   if (flag) tl -= 1;
-  uint32_t c = j / tl;
-  const uint32_t id = j - c * tl;
+  c = j / tl;
+  id = j - c * tl;
   if (flag) c += h.om;
-  // Rocks c and c+1 (2a <= 64 bits) and the sea (b+1 <= 32 bits) are read
-  // with one 32-byte sector load each, plus the next sector only when a
-  // field crosses a sector end; the sea's position depends only on the
-  // header, so both loads are in flight together.
+}
+
+// Bit offset of chunk c's left rock in the neighbor-order layout: c rocks and
+// c (chunk_len - 1) + min(c, om) seas precede it.
+__device__ __forceinline__ uint64_t le_chunk_pos(const VHdr &h, uint32_t c) {
+  return h.P + (uint64_t)c * (uint64_t)h.a +
+         ((uint64_t)(h.bl - 1) * c + min(h.om, c)) * (uint64_t)(h.b + 1);
+}
+
+// Word k (0..7) of the 512 stream bits held by sectors A and B; 0 beyond.
+__device__ __forceinline__ uint64_t sec2_word(const Sec &A, const Sec &B, uint32_t k) {
+  const uint32_t q = k & 3u;
+  const uint64_t x = k < 4 ? sec_word(A, q) : sec_word(B, q);
+  return k < 8 ? x : 0ull;
+}
+
+// The w (1..33) stream bits at bit `off` (< 512) of sectors A:B, right-aligned.
+__device__ __forceinline__ uint64_t sec2_field(const Sec &A, const Sec &B, uint32_t off, int w) {
+  const uint32_t k = off >> 6, s = off & 63u;
+  const uint64_t x = sec2_word(A, B, k);
+  const uint64_t win = s ? (x << s) | (sec2_word(A, B, k + 1) >> (64 - s)) : x;
+  return win >> (64 - w);
+}
+
+// LE get_vertex, LE/src/bcg.cuh:195-261: two rocks and one signed sea, from
+// either layout.  A sea field is sea_bit magnitude bits and a sign bit; with
+// sea_bit = 32 (33-bit fields, vertex ids of 2^31 and more) the magnitude is
+// the field's top 32 bits, as LE/src/bcg.cuh:245-252 reads it.
+__device__ __forceinline__ uint32_t le_neighbor(const DevGraph &g, const VHdr &h, uint32_t i) {
+  if (h.d == 1) return h.fp;
+  uint32_t c, id, tl;
+  le_locate(h, i, c, id, tl);
+  const Sec zero{0, 0, 0, 0};
+  if (le_chunked(h)) {
+    // [rock c][seas of chunk c][rock c+1]: one sector, two when it crosses
+    const uint32_t sw = (uint32_t)h.b + 1u;
+    const uint64_t X = le_chunk_pos(h, c);
+    const uint32_t off = (uint32_t)X & 255u;
+    const uint32_t need = id ? 2u * (uint32_t)h.a + (tl - 1u) * sw : (uint32_t)h.a;
+    const Sec A = load_sector(g.words, X >> 8);
+    const Sec B = off + need > 256u ? load_sector(g.words, (X >> 8) + 1) : zero;
+    const uint32_t r1m = (uint32_t)sec2_field(A, B, off, h.a);
+    const uint32_t r1 = (c < h.fp) ? h.v - r1m : h.v + r1m;
+    if (id == 0) return r1;
+    const uint64_t raw = sec2_field(A, B, off + (uint32_t)h.a + (id - 1u) * sw, (int)sw);
+    const uint32_t r2m = (uint32_t)sec2_field(A, B, off + (uint32_t)h.a + (tl - 1u) * sw, h.a);
+    const uint32_t r2 = (c + 1 < h.fp) ? h.v - r2m : h.v + r2m;
+    const uint32_t mag = (uint32_t)(raw >> 1);
+    return ((r2 - r1) / tl) * id + r1 + ((raw & 1u) ? 0u - mag : mag);
+  }
+  // On-disk order.  Rocks c and c+1 (2a <= 64 bits) and the sea (b+1 <= 33
+  // bits) are read with one 32-byte sector load each, plus the next sector
+  // only when a field crosses a sector end; the sea's position depends only
+  // on the header, so both loads are in flight together.
   const uint64_t rpos = h.P + (uint64_t)c * (uint64_t)h.a;
   const uint64_t rsec = rpos >> 8;
   const uint32_t roff = (uint32_t)rpos & 255u;
-  const Sec zero{0, 0, 0, 0};
   if (id == 0) {  // the chunk's left rock itself
     const bool cross = roff + (uint32_t)h.a > 256u;
     const Sec A = load_sector(g.words, rsec);
@@ -546,8 +621,8 @@ __device__ __forceinline__ uint32_t le_neighbor(const DevGraph &g, const VHdr &h
   const uint32_t r1 = (c < h.fp) ? h.v - r1m : h.v + r1m;
   const uint32_t r2m = (uint32_t)((rwin << h.a) >> (64 - h.a));
   const uint32_t r2 = (c + 1 < h.fp) ? h.v - r2m : h.v + r2m;
-  const uint32_t raw = (uint32_t)(sec_window(B, B2, soff) >> (63 - h.b));
-  const uint32_t mag = raw >> 1;
+  const uint64_t raw = sec_window(B, B2, soff) >> (63 - h.b);
+  const uint32_t mag = (uint32_t)(raw >> 1);
   // (r2 - r1) >= 0 for sorted rows: unsigned division is the compressor's.
   return ((r2 - r1) / tl) * id + r1 + ((raw & 1u) ? 0u - mag : mag);
 }

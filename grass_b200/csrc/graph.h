@@ -154,6 +154,10 @@ void launch_scan_u32(const uint32_t *counts, uint64_t n, uint64_t *out, uint64_t
 void launch_validate(const DevGraph &g, uint32_t *deg, unsigned long long *stats,
                      cudaStream_t s);
 void launch_build_records(const DevGraph &g, uint4 *recs, cudaStream_t s);
+// LE: dst (a copy of the stream src) gets the payload of every vertex that
+// le_chunked selects rewritten in neighbor order.
+void launch_le_reorder(const uint32_t *src, uint32_t *dst, const uint4 *recs, uint32_t n,
+                       cudaStream_t s);
 void launch_degrees(const DevGraph &g, uint32_t *deg, cudaStream_t s);
 void launch_degrees64(const DevGraph &g, uint64_t *deg, cudaStream_t s);
 // In-place exclusive scan of vals[0..n) into vals[0..n]; tmp as above.

@@ -56,30 +56,51 @@ __device__ __forceinline__ uint64_t read_bits64(const uint32_t *w, uint64_t off)
 }
 
 // le_neighbor (device_common.cuh) with word reads instead of sector loads:
-// the same arithmetic, LE/src/bcg.cuh:195-261.
+// the same arithmetic, LE/src/bcg.cuh:195-261, in either payload layout.
 __device__ __forceinline__ uint32_t le_neighbor_words(const uint32_t *words, const VHdr &h,
                                                       uint32_t i) {
   if (h.d == 1) return h.fp;
-  uint32_t tl = h.bl + 1;
-  const uint32_t split = h.om * tl;
-  const bool flag = i >= split;
-  const uint32_t j = flag ? i - split : i;
-  if (flag) tl -= 1;
-  uint32_t c = j / tl;
-  const uint32_t id = j - c * tl;
-  if (flag) c += h.om;
-  const uint64_t rwin = read_bits64(words, h.P + (uint64_t)c * (uint64_t)h.a);
-  const uint32_t r1m = (uint32_t)(rwin >> (64 - h.a));
+  uint32_t c, id, tl;
+  le_locate(h, i, c, id, tl);
+  const uint64_t sw = (uint64_t)h.b + 1;
+  uint64_t r1pos, r2pos, spos;
+  if (le_chunked(h)) {  // [rock c][seas of chunk c][rock c+1]
+    r1pos = le_chunk_pos(h, c);
+    spos = r1pos + h.a + (uint64_t)(id ? id - 1 : 0) * sw;
+    r2pos = r1pos + h.a + (uint64_t)(tl - 1) * sw;
+  } else {  // all rocks, then all seas
+    r1pos = h.P + (uint64_t)c * (uint64_t)h.a;
+    r2pos = r1pos + h.a;
+    spos = h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a +
+           ((uint64_t)(h.bl - 1) * c + min(h.om, c) + (id ? id - 1 : 0)) * sw;
+  }
+  const uint32_t r1m = (uint32_t)(read_bits64(words, r1pos) >> (64 - h.a));
   const uint32_t r1 = (c < h.fp) ? h.v - r1m : h.v + r1m;
   if (id == 0) return r1;
-  const uint32_t r2m = (uint32_t)((rwin << h.a) >> (64 - h.a));
+  const uint32_t r2m = (uint32_t)(read_bits64(words, r2pos) >> (64 - h.a));
   const uint32_t r2 = (c + 1 < h.fp) ? h.v - r2m : h.v + r2m;
-  const uint64_t spos =
-      h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a +
-      ((uint64_t)(h.bl - 1) * c + min(h.om, c) + id - 1) * (uint64_t)(h.b + 1);
-  const uint32_t raw = (uint32_t)(read_bits64(words, spos) >> (63 - h.b));
-  const uint32_t mag = raw >> 1;
+  const uint64_t raw = read_bits64(words, spos) >> (64 - sw);
+  const uint32_t mag = (uint32_t)(raw >> 1);
   return ((r2 - r1) / tl) * id + r1 + ((raw & 1u) ? 0u - mag : mag);
+}
+
+// The next sea of a cursor (sw = sea_bit + 1 bits: magnitude, then sign;
+// sw = 33 keeps the whole 32-bit magnitude, LE/src/bcg.cuh:245-252) added to
+// its interpolated position base.
+template <class Cur>
+__device__ __forceinline__ uint32_t le_sea(Cur &cur, int sw, uint32_t base) {
+  uint32_t mag, neg;
+  if (sw > 32) {
+    const uint32_t top = cur.get(1);
+    const uint32_t rest = cur.get(32);
+    mag = (top << 31) | (rest >> 1);
+    neg = rest & 1u;
+  } else {
+    const uint32_t raw = cur.get(sw);
+    mag = raw >> 1;
+    neg = raw & 1u;
+  }
+  return base + (neg ? 0u - mag : mag);
 }
 
 // Largest v in [0, n) with rowptr[v] <= x, for x < rowptr[n].
@@ -279,12 +300,12 @@ struct LeSeq {
   const uint32_t *w;
   uint64_t P;
   uint32_t v, fp, bl, om, bn, c, id, tl, r1, r2, step;
-  int a, sw;  // rock width, sea width (magnitude + sign)
-  bool one;   // degree 1: the neighbor is stored in the header
-  BitCur sea;
+  int a, sw;     // rock width, sea width (magnitude + sign)
+  bool one;      // degree 1: the neighbor is stored in the header
+  bool chunked;  // neighbor-order payload (le_chunked): cur reads every field
+  BitCur cur;    // on-disk order: the seas
 
-  __device__ __forceinline__ uint32_t rock(uint32_t k) const {
-    const uint32_t m = read_field(w, P + (uint64_t)k * (uint64_t)a, a);
+  __device__ __forceinline__ uint32_t signed_rock(uint32_t m, uint32_t k) const {
     return k < fp ? v - m : v + m;
   }
   __device__ __forceinline__ void init(const uint32_t *words, const VHdr &h) {
@@ -302,35 +323,42 @@ struct LeSeq {
     c = 0;
     id = 0;
     tl = om ? bl + 1 : bl;
-    r1 = rock(0);
-    r2 = rock(1);
-    step = (r2 - r1) / tl;
-    sea.init(w, P + (uint64_t)(bn + 1) * (uint64_t)a);
+    chunked = le_chunked(h);
+    if (chunked) {
+      cur.init(w, P);
+    } else {
+      r1 = signed_rock(read_field(w, P, a), 0);
+      r2 = signed_rock(read_field(w, P + (uint64_t)a, a), 1);
+      step = (r2 - r1) / tl;
+      cur.init(w, P + (uint64_t)(bn + 1) * (uint64_t)a);
+    }
   }
   __device__ __forceinline__ uint32_t next() {
     if (one) return fp;
     uint32_t val;
     if (id == 0) {
+      if (chunked) {  // this chunk's rock, then a look-ahead to the next one
+        r1 = signed_rock(cur.get(a), c);
+        if (c < bn) {
+          const uint64_t at = cur.pos(w) + (uint64_t)(tl - 1) * (uint64_t)sw;
+          r2 = signed_rock(read_field(w, at, a), c + 1);
+          step = (r2 - r1) / tl;
+        }
+      }
       val = r1;
     } else {
-      uint32_t raw;
-      if (sw > 32) {  // 33-bit field: keep its low 32 bits, as the random-access decode does
-        sea.get(sw - 32);
-        raw = sea.get(32);
-      } else {
-        raw = sea.get(sw);
-      }
-      const uint32_t mag = raw >> 1;
-      val = step * id + r1 + ((raw & 1u) ? 0u - mag : mag);
+      val = le_sea(cur, sw, step * id + r1);
     }
     if (++id == tl) {
       c++;
       id = 0;
       tl = c < om ? bl + 1 : bl;
-      r1 = r2;
-      if (c < bn) {
-        r2 = rock(c + 1);
-        step = (r2 - r1) / tl;
+      if (!chunked) {
+        r1 = r2;
+        if (c < bn) {
+          r2 = signed_rock(read_field(w, P + (uint64_t)(c + 1) * (uint64_t)a, a), c + 1);
+          step = (r2 - r1) / tl;
+        }
       }
     }
     return val;
@@ -604,6 +632,7 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
     const uint64_t blkbits = (uint64_t)h.a + (uint64_t)(h.bl - 1) * h.b;
     const uint32_t split = h.om * (h.bl + 1);
     const int sw = h.b + 1;
+    const bool chunked = MODE == 1 && le_chunked(h);  // neighbor-order LE payload
     bool staged = false;  // the range's seas are in the warp's shared buffer
 #if GRASS_DECODE_STAGE
     const uint32_t *sbuf = g.words;  // sea cursor words, and the stream bit of sbuf[0]
@@ -614,7 +643,10 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
       const uint64_t pend = payload_end<MODE>(g, h);
       const uint32_t c0 = i0 < split ? i0 / (h.bl + 1) : h.om + (i0 - split) / max(h.bl, 1u);
       const uint64_t cl = c0 + (i1 - i0) / max(h.bl, 1u) + 2;
-      if (MODE == 1) {
+      if (chunked) {  // the range's fields are contiguous
+        prefetch_bits(g.words, le_chunk_pos(h, c0),
+                      min(pend, le_chunk_pos(h, (uint32_t)min(cl, (uint64_t)h.bn)) + h.a));
+      } else if (MODE == 1) {
         prefetch_bits(g.words, h.P + (uint64_t)c0 * h.a,
                       min(pend, h.P + min(cl, (uint64_t)h.bn + 1) * h.a));
         const uint64_t lo = sea0 + (uint64_t)(i0 > c0 ? i0 - c0 - 1 : 0) * sw;
@@ -662,7 +694,50 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
       uint32_t c = tl ? j / tl : 0u;
       uint32_t id = j - c * tl;
       if (!hi) c += h.om;
-      if (MODE == 1) {
+      if (chunked) {
+        // neighbor order: the cursor reads every field (rock c, its seas,
+        // rock c+1, ...); each chunk's right rock is a look-ahead read
+        uint32_t r1 = 0, r2 = 0, step = 0;
+        BitCur cur;
+        if (cnt) {
+          const uint64_t X = le_chunk_pos(h, c);
+          if (id) {
+            const uint32_t r1m = read_field(g.words, X, h.a);
+            r1 = c < h.fp ? h.v - r1m : h.v + r1m;
+            const uint32_t r2m =
+                read_field(g.words, X + h.a + (uint64_t)(tl - 1) * (uint64_t)sw, h.a);
+            r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
+            step = (r2 - r1) / tl;
+            cur.init(g.words, X + h.a + (uint64_t)(id - 1) * (uint64_t)sw);
+          } else {
+            cur.init(g.words, X);
+          }
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kRun; k++) {
+          if (k >= cnt) break;
+          uint32_t val;
+          if (id == 0) {
+            const uint32_t r1m = cur.get(h.a);
+            r1 = c < h.fp ? h.v - r1m : h.v + r1m;
+            if (c < h.bn) {
+              const uint64_t at = cur.pos(g.words) + (uint64_t)(tl - 1) * (uint64_t)sw;
+              const uint32_t r2m = read_field(g.words, at, h.a);
+              r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
+              step = (r2 - r1) / tl;
+            }
+            val = r1;
+          } else {
+            val = le_sea(cur, sw, step * id + r1);
+          }
+          vals[k] = val;
+          if (++id == tl) {
+            c++;
+            id = 0;
+            tl = c < h.om ? h.bl + 1 : h.bl;
+          }
+        }
+      } else if (MODE == 1) {
         uint32_t r1 = 0, r2 = 0, step = 0;
 #if GRASS_DECODE_STAGE
         GenCur sea;
@@ -688,20 +763,7 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
 #pragma unroll
         for (uint32_t k = 0; k < kRun; k++) {
           if (k >= cnt) break;
-          uint32_t val;
-          if (id == 0) {
-            val = r1;
-          } else {
-            uint32_t raw;
-            if (sw > 32) {  // 33-bit field: keep its low 32 bits, as the random-access decode does
-              sea.get(sw - 32);
-              raw = sea.get(32);
-            } else {
-              raw = sea.get(sw);
-            }
-            const uint32_t mag = raw >> 1;
-            val = step * id + r1 + ((raw & 1u) ? 0u - mag : mag);
-          }
+          const uint32_t val = id == 0 ? r1 : le_sea(sea, sw, step * id + r1);
           vals[k] = val;
           if (++id == tl) {  // next chunk: its left rock is this chunk's right rock
             c++;

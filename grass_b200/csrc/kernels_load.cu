@@ -164,7 +164,7 @@ __global__ void validate_kernel(DevGraph g, uint32_t *deg, unsigned long long *s
       } else {
         uint32_t rb = c.gamma(), sb = c.gamma(), fp = c.gamma();
         VHdr h = le_header(g, (uint32_t)v);
-        ok = rb >= 1 && rb <= 32 && sb <= 31 && fp <= h.bn + 2 && d < 0x7FFFFFFFu;
+        ok = rb >= 1 && rb <= 32 && sb <= 32 && fp <= h.bn + 2 && d < 0x7FFFFFFFu;
         end = ok ? payload_end<1>(g, h) : 0;
       }
     }
@@ -201,6 +201,70 @@ __global__ void build_records_kernel(DevGraph g, uint4 *recs) {
   for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < g.n;
        v += (uint64_t)gridDim.x * blockDim.x)
     recs[v] = pack_record(stream_header<MODE>(g, (uint32_t)v));
+}
+
+// The w (1..33) stream bits at bit `off`, right-aligned (reads two words past
+// the field at most: inside the zero guard).
+__device__ __forceinline__ uint64_t bits_at(const uint32_t *w, uint64_t off, int width) {
+  const uint32_t *q = w + (off >> 5);
+  const uint32_t s = (uint32_t)off & 31u;
+  const uint32_t x0 = ldw(q), x1 = ldw(q + 1), x2 = ldw(q + 2);
+  const uint64_t win = ((uint64_t)__funnelshift_l(x1, x0, s) << 32) | __funnelshift_l(x2, x1, s);
+  return win >> (64 - width);
+}
+
+// ORs the w (1..33) bits of `val` into the stream at bit `off` (two words at
+// most; the caller has cleared them).
+__device__ __forceinline__ void or_bits(uint32_t *w, uint64_t off, uint64_t val, int width) {
+  const uint32_t s = (uint32_t)off & 31u;  // s + width <= 64
+  const uint64_t x = val << (64 - s - width);
+  const uint32_t hi = (uint32_t)(x >> 32), lo = (uint32_t)x;
+  if (hi) atomicOr(w + (off >> 5), hi);
+  if (lo) atomicOr(w + (off >> 5) + 1, lo);
+}
+
+// LE payloads in neighbor order (le_chunked, device_common.cuh): one warp per
+// vertex.  dst starts as a copy of src; the lanes clear the vertex's payload
+// bits [P, end) in dst, then move every field from its on-disk position
+// (rock c at P + c a; sea k at P + (chunk_num + 1) a + k (sea_bit + 1),
+// LE/src/bcg.cuh:211, 237) to its neighbor-order position.  Words shared with
+// another vertex's header or payload are changed with atomicAnd / atomicOr on
+// this vertex's bits only; the warp's clears are ordered before its writes by
+// __syncwarp.
+__global__ void __launch_bounds__(256) le_reorder_kernel(const uint32_t *__restrict__ src,
+                                                         uint32_t *dst,
+                                                         const uint4 *__restrict__ recs,
+                                                         uint32_t n) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
+    const VHdr h = record_header<1>(recs[v], (uint32_t)v);
+    if (!le_chunked(h)) continue;  // warp-uniform
+    const uint32_t sw = (uint32_t)h.b + 1u;
+    const uint64_t end = payload_end<1>(DevGraph{}, h);
+    const uint64_t w0 = h.P >> 5, w1 = (end - 1) >> 5;
+    for (uint64_t k = w0 + lane; k <= w1; k += 32) {
+      uint32_t m = 0xFFFFFFFFu;  // bits of word k inside [P, end), MSB first
+      if (k == w0) m &= 0xFFFFFFFFu >> ((uint32_t)h.P & 31u);
+      if (k == w1) m &= 0xFFFFFFFFu << (31u - ((uint32_t)(end - 1) & 31u));
+      if (m == 0xFFFFFFFFu) dst[k] = 0u;
+      else atomicAnd(dst + k, ~m);
+    }
+    __syncwarp();
+    const uint64_t sea0 = h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a;
+    for (uint32_t i = lane; i < h.d; i += 32) {
+      uint32_t c, id, tl;
+      le_locate(h, i, c, id, tl);
+      const uint64_t X = le_chunk_pos(h, c);
+      if (id == 0) {
+        or_bits(dst, X, bits_at(src, h.P + (uint64_t)c * h.a, h.a), h.a);
+      } else {
+        const uint64_t k = (uint64_t)(h.bl - 1) * c + min(h.om, c) + id - 1;
+        or_bits(dst, X + h.a + (uint64_t)(id - 1) * sw, bits_at(src, sea0 + k * sw, (int)sw),
+                (int)sw);
+      }
+    }
+  }
 }
 
 unsigned grid_for(uint64_t items, int threads, int device) {
@@ -247,6 +311,14 @@ void launch_build_records(const DevGraph &g, uint4 *recs, cudaStream_t s) {
   unsigned grid = grid_for(g.n, 256, dev);
   if (g.mode == GRASS_MODE_GT) build_records_kernel<0><<<grid, 256, 0, s>>>(g, recs);
   else build_records_kernel<1><<<grid, 256, 0, s>>>(g, recs);
+  count_launch();
+}
+
+void launch_le_reorder(const uint32_t *src, uint32_t *dst, const uint4 *recs, uint32_t n,
+                       cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  le_reorder_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(src, dst, recs, n);
   count_launch();
 }
 

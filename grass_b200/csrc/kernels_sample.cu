@@ -188,15 +188,19 @@ __device__ __forceinline__ void draw_footprint(const DevGraph &g, const VHdr &h,
                          (uint64_t)min(blk, h.om) * (uint64_t)h.b;
     r0[nr] = pos;
     r1[nr++] = pos + h.a + (uint64_t)id * h.b;
+  } else if (h.d > 1 && le_chunked(h)) {
+    // neighbor order: rock c, the sea, rock c+1 lie in one span (le_neighbor
+    // loads the sectors of the span)
+    uint32_t c, id, tl;
+    le_locate(h, i, c, id, tl);
+    const uint64_t X = le_chunk_pos(h, c);
+    const uint64_t span = id ? 2ull * h.a + (uint64_t)(tl - 1) * (h.b + 1) : (uint64_t)h.a;
+    bits = id ? 2ull * h.a + h.b + 1 : (uint64_t)h.a;
+    sectors = ((X + span - 1) >> 8) - (X >> 8) + 1;
+    return;
   } else if (h.d > 1) {
-    uint32_t tl = h.bl + 1;
-    const uint32_t split = h.om * tl;
-    const bool flag = i >= split;
-    const uint32_t j = flag ? i - split : i;
-    if (flag) tl -= 1;
-    uint32_t c = j / tl;
-    const uint32_t id = j - c * tl;
-    if (flag) c += h.om;
+    uint32_t c, id, tl;
+    le_locate(h, i, c, id, tl);
     const uint64_t rp = h.P + (uint64_t)c * h.a;
     r0[nr] = rp;
     r1[nr++] = rp + (id ? 2u : 1u) * (uint64_t)h.a;
