@@ -25,11 +25,11 @@ MODES = {"GT": MODE_GT, "LE": MODE_LE, "gt": MODE_GT, "le": MODE_LE}
 INVALID = 0xFFFFFFFF
 
 
-def build(ref: bool | None = None) -> None:
-    """Compile the oracle (and the reference's CPU pieces when present)."""
+def build(ref: bool = True) -> None:
+    """Compile the oracle and, with ref, the reference's CPU pieces (the
+    Makefile's `ref` target builds them where the reference sources are
+    found, GRASS_REFERENCE, and does nothing otherwise)."""
     subprocess.check_call(["make", "-s", "-C", HERE, "all"])
-    if ref is None:
-        ref = os.path.isdir("/root/reference")
     if ref:
         subprocess.check_call(["make", "-s", "-C", HERE, "ref"])
 

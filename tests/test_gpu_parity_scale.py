@@ -91,9 +91,12 @@ def test_batched_jobs_bit_exact_at_scale(s20, oracle_mod, mode):
     rng = np.random.default_rng(3)
     b = G.Batch(g)
     checks = []
+    alive = []  # the batch holds raw device pointers: keep every input alive
 
     def ints(a):
-        return torch.from_numpy(np.ascontiguousarray(a, np.uint32).view(np.int32)).cuda()
+        t = torch.from_numpy(np.ascontiguousarray(a, np.uint32).view(np.int32)).cuda()
+        alive.append(t)
+        return t
 
     for k, (W, L) in enumerate([(3000, 60), (40000, 12), (1, 100)]):
         st = rng.integers(0, n, W).astype(np.uint32)
