@@ -268,6 +268,7 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
   // per draw, le_chunked); the rewrite goes to a copy, which replaces the
   // on-disk order stream.
   if (mode == GRASS_MODE_LE) {
+    Nvtx nv("LE payloads to neighbor order");
     uint32_t *d_re = nullptr;
     GRASS_CUDA(cudaMalloc(&d_re, alloc_words * 4));
     tmp.dev.push_back(d_re);
@@ -278,6 +279,37 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
     tmp.dev.back() = g->d_words;  // the on-disk order copy is freed with tmp
     g->d_words = d_re;
   }
+  // GT: the stream is rebuilt with a skip field every kGtSkip gaps of a block
+  // (payloads only, new offsets in the records).
+  uint64_t words_alloc = alloc_words;
+  if (mode == GRASS_MODE_GT) {
+    Nvtx nv("GT stream with skip fields");
+    unsigned char *d_cx = nullptr;
+    uint64_t *d_len = nullptr, *d_stmp = nullptr;
+    GRASS_CUDA(cudaMalloc(&d_cx, n));
+    tmp.dev.push_back(d_cx);
+    GRASS_CUDA(cudaMalloc(&d_len, (n + 1) * sizeof(uint64_t)));
+    tmp.dev.push_back(d_len);
+    GRASS_CUDA(cudaMalloc(&d_stmp, (scan_tmp_words(n) + 1) * sizeof(uint64_t)));
+    tmp.dev.push_back(d_stmp);
+    launch_gt_skip_measure(g->d_words, g->d_recs, (uint32_t)n, d_cx, d_len, st);
+    launch_scan_u64_inplace(d_len, n, d_stmp, st);  // new payload offsets, total in d_len[n]
+    uint64_t bits = 0;
+    GRASS_CUDA(cudaMemcpyAsync(&bits, d_len + n, sizeof bits, cudaMemcpyDeviceToHost, st));
+    GRASS_CUDA(cudaStreamSynchronize(st));
+    const uint64_t nw = (bits + 31) / 32;
+    words_alloc = (nw + kGuardWords + 7) / 8 * 8;
+    uint32_t *d_sk = nullptr;
+    GRASS_CUDA(cudaMalloc(&d_sk, words_alloc * 4));
+    tmp.dev.push_back(d_sk);
+    GRASS_CUDA(cudaMemsetAsync(d_sk, 0, words_alloc * 4, st));
+    launch_gt_skip_write(g->d_words, d_sk, g->d_recs, (uint32_t)n, d_cx, d_len, st);
+    GRASS_CUDA(cudaStreamSynchronize(st));
+    GRASS_CUDA(cudaGetLastError());
+    tmp.dev.back() = g->d_words;  // the on-disk stream is freed with tmp
+    g->d_words = d_sk;
+    g->n_words = nw;
+  }
 
   g->info.n_file = n_file;
   g->info.num_edges = stats[0];
@@ -287,7 +319,7 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
   g->info.device = device;
   g->info.graph_file_bytes = gsize;
   g->info.offset_file_bytes = osize;
-  g->info.device_bytes = alloc_words * 4 + n * sizeof(uint4);
+  g->info.device_bytes = words_alloc * 4 + n * sizeof(uint4);
   g->info.read_seconds = src.read_s;
   g->info.upload_seconds = now_s() - t0;
   *out = g;
@@ -370,6 +402,7 @@ uint64_t grass_launch_count(void) { return grass::g_launches.load(); }
 const char *grass_version(void) { return "grass_b200 0.1 (sm_100a)"; }
 
 int grass_open(const char *prefix, int mode, int device, grass_graph **out) {
+  grass::Nvtx nvtx_("grass_open");
   clear_error();
   if (!prefix || !out) return set_error(GRASS_E_ARG, "null argument");
   *out = nullptr;
@@ -393,6 +426,7 @@ int grass_open(const char *prefix, int mode, int device, grass_graph **out) {
 
 int grass_open_mem(const void *graph_bytes, uint64_t graph_size, const void *offset_bytes,
                    uint64_t offset_size, int mode, int device, grass_graph **out) {
+  grass::Nvtx nvtx_("grass_open_mem");
   clear_error();
   if (!out || (!graph_bytes && graph_size) || !offset_bytes)
     return set_error(GRASS_E_ARG, "null argument");
@@ -453,6 +487,7 @@ int grass_get_tuning(const grass_graph *g, grass_tuning *t) {
 }
 
 int grass_degrees(const grass_graph *g, uint32_t *d_deg, void *stream) {
+  grass::Nvtx nvtx_("grass_degrees");
   clear_error();
   if (int rc = check_graph(g)) return rc;
   if (!d_deg) return set_error(GRASS_E_ARG, "null output");
@@ -462,6 +497,7 @@ int grass_degrees(const grass_graph *g, uint32_t *d_deg, void *stream) {
 }
 
 int grass_decode_all(const grass_graph *g, uint64_t *d_rowptr, uint32_t *d_cols, void *stream) {
+  grass::Nvtx nvtx_("grass_decode_all");
   clear_error();
   if (int rc = check_graph(g)) return rc;
   if (!d_rowptr || (!d_cols && g->info.num_edges)) return set_error(GRASS_E_ARG, "null output");
@@ -510,6 +546,7 @@ int run_compact(const CompactSeg *segs, uint32_t nseg, uint32_t *d_src, uint32_t
 int grass_khop_edges(const grass_khop_params *p, const uint32_t *d_seeds, uint64_t S,
                      const uint32_t *const *d_hop_out, uint32_t *d_src, uint32_t *d_dst,
                      uint64_t capacity, unsigned long long *d_count, void *stream) {
+  grass::Nvtx nvtx_("grass_khop_edges");
   clear_error();
   uint64_t width[GRASS_MAX_HOPS];
   if (int rc = check_khop(p, width)) return rc;
@@ -527,6 +564,7 @@ int grass_khop_edges(const grass_khop_params *p, const uint32_t *d_seeds, uint64
 int grass_rw_edges(const grass_rw_params *p, const uint32_t *d_paths, uint64_t W,
                    uint32_t *d_src, uint32_t *d_dst, uint64_t capacity,
                    unsigned long long *d_count, void *stream) {
+  grass::Nvtx nvtx_("grass_rw_edges");
   clear_error();
   if (!p || p->layout > 1 || (W && !d_paths))
     return set_error(GRASS_E_ARG, "walk edges: bad arguments");
@@ -543,6 +581,7 @@ int grass_rw_edges(const grass_rw_params *p, const uint32_t *d_paths, uint64_t W
 int grass_mrw_edges(const grass_mrw_params *p, uint64_t S, const uint32_t *d_step_src,
                     const uint32_t *d_step_dst, uint32_t *d_src, uint32_t *d_dst,
                     uint64_t capacity, unsigned long long *d_count, void *stream) {
+  grass::Nvtx nvtx_("grass_mrw_edges");
   clear_error();
   if (!p || (S && p->steps && (!d_step_src || !d_step_dst)))
     return set_error(GRASS_E_ARG, "multi-RW edges: bad arguments");
@@ -553,6 +592,7 @@ int grass_mrw_edges(const grass_mrw_params *p, uint64_t S, const uint32_t *d_ste
 
 int grass_rw(const grass_graph *g, const grass_rw_params *p, const uint32_t *d_starts,
              uint64_t W, uint32_t *d_paths, unsigned long long *d_edge_count, void *stream) {
+  grass::Nvtx nvtx_("grass_rw");
   clear_error();
   if (int rc = check_graph(g)) return rc;
   if (!p || p->layout > 1 || (W && (!d_starts || !d_paths)))
@@ -586,6 +626,7 @@ int grass_random_read_probe(const uint32_t *d_buf, uint64_t n_words, uint64_t re
 
 int grass_rw_host(const grass_graph *g, const grass_rw_params *p, const uint32_t *h_starts,
                   uint64_t W, uint32_t *h_paths, uint64_t *edges_out) {
+  grass::Nvtx nvtx_("grass_rw_host");
   clear_error();
   if (int rc = check_graph(g)) return rc;
   if (!p || p->layout > 1 || (W && (!h_starts || !h_paths)))
@@ -656,6 +697,7 @@ int grass_rw_host(const grass_graph *g, const grass_rw_params *p, const uint32_t
 int grass_khop(const grass_graph *g, const grass_khop_params *p, const uint32_t *d_seeds,
                uint64_t S, uint32_t *const *d_hop_out, unsigned long long *d_edge_count,
                void *stream) {
+  grass::Nvtx nvtx_("grass_khop");
   clear_error();
   if (int rc = check_graph(g)) return rc;
   uint64_t width[GRASS_MAX_HOPS];
@@ -670,6 +712,7 @@ int grass_khop(const grass_graph *g, const grass_khop_params *p, const uint32_t 
 
 int grass_khop_host(const grass_graph *g, const grass_khop_params *p, const uint32_t *h_seeds,
                     uint64_t S, uint32_t *const *h_hop_out, uint64_t *edges_out) {
+  grass::Nvtx nvtx_("grass_khop_host");
   clear_error();
   if (int rc = check_graph(g)) return rc;
   uint64_t width[GRASS_MAX_HOPS];
@@ -700,6 +743,7 @@ int grass_khop_host(const grass_graph *g, const grass_khop_params *p, const uint
 
 int grass_mrw(const grass_graph *g, const grass_mrw_params *p, uint32_t *d_roots, uint64_t S,
               uint32_t *d_src, uint32_t *d_dst, unsigned long long *d_edge_count, void *stream) {
+  grass::Nvtx nvtx_("grass_mrw");
   clear_error();
   if (int rc = check_graph(g)) return rc;
   if (!p || p->walkers == 0 || p->select > 2 || (S && (!d_roots || !d_src || !d_dst)) ||
@@ -714,6 +758,7 @@ int grass_mrw(const grass_graph *g, const grass_mrw_params *p, uint32_t *d_roots
 
 int grass_mrw_host(const grass_graph *g, const grass_mrw_params *p, uint32_t *h_roots,
                    uint64_t S, uint32_t *h_src, uint32_t *h_dst, uint64_t *edges_out) {
+  grass::Nvtx nvtx_("grass_mrw_host");
   clear_error();
   if (int rc = check_graph(g)) return rc;
   if (!p || p->walkers == 0 || p->select > 2 || (S && (!h_roots || !h_src || !h_dst)) ||
@@ -746,6 +791,7 @@ int grass_mrw_host(const grass_graph *g, const grass_mrw_params *p, uint32_t *h_
 // ---- CSR baseline ----
 
 int grass_csr_from_graph(const grass_graph *g, grass_csr **out) {
+  grass::Nvtx nvtx_("grass_csr_from_graph");
   clear_error();
   if (int rc = check_graph(g)) return rc;
   if (!out) return set_error(GRASS_E_ARG, "null output");
@@ -832,6 +878,7 @@ int grass_csr_set_tuning(grass_csr *c, const grass_tuning *t) {
 
 int grass_csr_rw(const grass_csr *c, const grass_rw_params *p, const uint32_t *d_starts,
                  uint64_t W, uint32_t *d_paths, unsigned long long *d_edge_count, void *stream) {
+  grass::Nvtx nvtx_("grass_csr_rw");
   clear_error();
   if (!c || !p || p->layout > 1 || (W && (!d_starts || !d_paths)))
     return set_error(GRASS_E_ARG, "CSR random walk: bad arguments");
@@ -844,6 +891,7 @@ int grass_csr_rw(const grass_csr *c, const grass_rw_params *p, const uint32_t *d
 int grass_csr_khop(const grass_csr *c, const grass_khop_params *p, const uint32_t *d_seeds,
                    uint64_t S, uint32_t *const *d_hop_out, unsigned long long *d_edge_count,
                    void *stream) {
+  grass::Nvtx nvtx_("grass_csr_khop");
   clear_error();
   if (!c) return set_error(GRASS_E_ARG, "null csr");
   uint64_t width[GRASS_MAX_HOPS];

@@ -204,6 +204,21 @@ __device__ __forceinline__ uint64_t sec_window(const Sec &a, const Sec &b, uint3
   return s ? (x << s) | (y >> (64 - s)) : x;
 }
 
+// Word k (0..7) of the 512 stream bits held by sectors A and B; 0 beyond.
+__device__ __forceinline__ uint64_t sec2_word(const Sec &A, const Sec &B, uint32_t k) {
+  const uint32_t q = k & 3u;
+  const uint64_t x = k < 4 ? sec_word(A, q) : sec_word(B, q);
+  return k < 8 ? x : 0ull;
+}
+
+// The w (1..33) stream bits at bit `off` (< 512) of sectors A:B, right-aligned.
+__device__ __forceinline__ uint64_t sec2_field(const Sec &A, const Sec &B, uint32_t off, int w) {
+  const uint32_t k = off >> 6, s = off & 63u;
+  const uint64_t x = sec2_word(A, B, k);
+  const uint64_t win = s ? (x << s) | (sec2_word(A, B, k + 1) >> (64 - s)) : x;
+  return win >> (64 - w);
+}
+
 __device__ __forceinline__ uint32_t isqrt_u32(uint32_t x) {
   uint32_t r = (uint32_t)__fsqrt_rn((float)x);
   if ((uint64_t)r * r > x) r--;
@@ -219,6 +234,7 @@ struct VHdr {
   uint64_t P;  // bit offset of the payload
   uint32_t v, d, bn, bl, om, fp;
   int a, b;
+  int cx;      // GT: extra width of a skip field over a gap field (device layout)
 };
 
 // GT header: BCGVertex ctor, GT/src/bcg.cuh:109-136 (isqrt instead of
@@ -233,6 +249,7 @@ __device__ __forceinline__ VHdr gt_header(const DevGraph &g, uint32_t v) {
   h.b = (int)c.gamma();
   h.fp = c.gamma();
   h.P = c.pos(g.words);
+  h.cx = 0;
   uint32_t s = isqrt_u32(h.d);
   if (s * s == h.d) {
     h.bn = h.bl = s;
@@ -245,226 +262,164 @@ __device__ __forceinline__ VHdr gt_header(const DevGraph &g, uint32_t v) {
   return h;
 }
 
-// GT get_vertex, GT/src/bcg.cuh:153-168: locate (block, id), read the head,
-// then add id gaps.
-__device__ __forceinline__ uint32_t gt_neighbor(const DevGraph &g, const VHdr &h, uint32_t i) {
+// ---- GT payload layout in HBM ----
+// On disk a GT block is its head and then len - 1 gaps, so neighbor id of a
+// block costs id sequential gap reads (GT/src/bcg.cuh:153-168), O(sqrt d) for
+// hubs.  At load the stream is rebuilt with a skip field in every block at
+// each position t = g * kGtSkip (g >= 1): in place of gap t it holds the sum
+// of the block's raw gaps 1..t, in b + cx bits (cx per vertex, in its record).
+// Neighbor id of a block is then
+//   head value + id + (id >= kGtSkip ? skip field g = id / kGtSkip : 0)
+//              + the raw gaps after that skip field (fewer than kGtSkip),
+// the sum being the reference's head + sum of (gap + 1) regrouped.  Blocks of
+// at most kGtSkip neighbors are unchanged.  The rebuilt stream holds the
+// payloads only, back to back in vertex order (the headers live in the
+// records).  Footprint: cx bits per kGtSkip gaps of long blocks.
+#ifndef GRASS_GT_SKIP
+#define GRASS_GT_SKIP 16
+#endif
+constexpr uint32_t kGtSkip = GRASS_GT_SKIP;
+
+// Bits of a block of L >= 1 neighbors.
+__device__ __host__ __forceinline__ uint64_t gt_block_bits(const VHdr &h, uint32_t L) {
+  return (uint64_t)h.a + (uint64_t)(L - 1) * (uint64_t)h.b +
+         (uint64_t)((L - 1) / kGtSkip) * (uint64_t)h.cx;
+}
+
+// Bit offset of block blk (blocks before om hold bl + 1 neighbors, the rest bl).
+__device__ __forceinline__ uint64_t gt_block_pos(const VHdr &h, uint32_t blk) {
+  const uint32_t lo = min(blk, h.om);
+  return h.P + (uint64_t)lo * gt_block_bits(h, h.bl + 1) +
+         (uint64_t)(blk - lo) * gt_block_bits(h, h.bl);
+}
+
+// Bit offset of field t >= 1 (a gap, or a skip field when t % kGtSkip == 0)
+// of the block at bit offset bpos.
+__device__ __forceinline__ uint64_t gt_field_pos(const VHdr &h, uint64_t bpos, uint32_t t) {
+  return bpos + (uint64_t)h.a + (uint64_t)(t - 1) * (uint64_t)h.b +
+         (uint64_t)((t - 1) / kGtSkip) * (uint64_t)h.cx;
+}
+
+// Block blk and index id of neighbor i (GT/src/bcg.cuh:153-160).
+__device__ __forceinline__ void gt_block_of(const VHdr &h, uint32_t i, uint32_t &blk,
+                                            uint32_t &id) {
   const uint32_t split = (h.bl + 1) * h.om;
   const bool flag = i < split;
   const uint32_t j = flag ? i : i - split;
   const uint32_t len = h.bl + (flag ? 1u : 0u);
-  uint32_t blk = j / len;
-  uint32_t id = j - blk * len;
+  blk = j / len;
+  id = j - blk * len;
   if (!flag) blk += h.om;
-  const uint64_t pos = h.P + (uint64_t)blk * (uint64_t)(h.a + (h.bl - 1) * h.b) +
-                       (uint64_t)min(blk, h.om) * (uint64_t)h.b;
-  const uint32_t off = (uint32_t)pos & 255u;
-  const uint64_t span = (uint64_t)h.a + (uint64_t)id * (uint64_t)h.b;
-  if (off + span <= 512u) {
-    // Head and gaps lie in at most two sectors: two vector loads, then the
-    // fields are pulled from registers through a 128-bit shift window
-    // (buf holds nb valid bits at the top, nxt the next 64 stream bits).
-    const Sec zero{0, 0, 0, 0};
-    const uint64_t s0 = pos >> 8;
-    const Sec A = load_sector(g.words, s0);
-    const Sec B = off + span > 256u ? load_sector(g.words, s0 + 1) : zero;
-    uint32_t k = off >> 6;
-    auto word = [&](uint32_t i) -> uint64_t {
-      return i < 4 ? sec_word(A, i) : i < 8 ? sec_word(B, i - 4) : 0ull;
-    };
-    const uint32_t sh = off & 63u;
-    uint64_t buf = word(k) << sh;
-    int nb = 64 - (int)sh;
-    uint64_t nxt = word(++k);
-    auto get = [&](int w) -> uint32_t {  // w in [1, 32]
-      uint32_t v;
-      if (nb >= w) {
-        v = (uint32_t)(buf >> (64 - w));
-        buf = w == 64 ? 0 : buf << w;
-        nb -= w;
-      } else {
-        const int r = w - nb;  // bits taken from nxt, 1..32
-        v = (uint32_t)(((nb ? buf >> (64 - nb) : 0ull) << r) | (nxt >> (64 - r)));
-        buf = nxt << r;
-        nb = 64 - r;
-        nxt = word(++k);
-      }
-      return v;
-    };
-    const uint32_t head = get(h.a);
-    uint32_t cur = (blk >= h.fp) ? h.v + head + 1u : h.v - head - 1u;
-    for (uint32_t j = 0; j < id; j++) cur += get(h.b) + 1u;
-    return cur;
-  }
-  // Long runs (hub vertices): prefetch every sector of the run into L1 so
-  // the sequential cursor below waits on one memory round trip, not one per
-  // word.
-  const uint64_t l_first = pos >> 10, l_last = (pos + span - 1) >> 10;  // 128-byte lines
-  for (uint64_t l = l_first; l <= l_last; l++)
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(g.words + l * 32));
-  BitCur c;
-  c.init(g.words, pos);
-  uint32_t head = c.get(h.a);
-  uint32_t cur = (blk >= h.fp) ? h.v + head + 1u : h.v - head - 1u;
-  for (uint32_t k = 0; k < id; k++) cur += c.get(h.b) + 1u;
-  return cur;
 }
 
-// GT draw of neighbor i, located but not decoded: the bit offset of the
-// block's head, how many gaps follow it to reach neighbor i, and the head's
-// sign (GT/src/bcg.cuh:153-163).
+// A GT draw of neighbor i, located: the head field, the skip field (when id
+// >= kGtSkip), and the run of raw gaps to add after it.
 struct GtRun {
   uint64_t pos;   // bit offset of the head field
-  uint32_t gaps;  // gaps to add after the head (neighbor_id)
+  uint64_t spos;  // bit offset of the skip field (skip) or of the first gap
+  uint32_t id;    // index within the block
+  uint32_t gaps;  // raw gaps after the skip field (or after the head)
   bool up;        // head counts upward from v (block >= first_pos)
+  bool skip;
 };
 
 __device__ __forceinline__ GtRun gt_locate(const VHdr &h, uint32_t i) {
-  const uint32_t split = (h.bl + 1) * h.om;
-  const bool flag = i < split;
-  const uint32_t j = flag ? i : i - split;
-  const uint32_t len = h.bl + (flag ? 1u : 0u);
-  uint32_t blk = j / len;
-  const uint32_t id = j - blk * len;
-  if (!flag) blk += h.om;
+  uint32_t blk, id;
+  gt_block_of(h, i, blk, id);
   GtRun r;
-  r.pos = h.P + (uint64_t)blk * (uint64_t)(h.a + (h.bl - 1) * h.b) +
-          (uint64_t)min(blk, h.om) * (uint64_t)h.b;
-  r.gaps = id;
+  r.pos = gt_block_pos(h, blk);
+  r.id = id;
   r.up = blk >= h.fp;
+  const uint32_t q = id / kGtSkip;
+  r.skip = q != 0;
+  r.gaps = id - q * kGtSkip;
+  r.spos = q ? gt_field_pos(h, r.pos, q * kGtSkip) : r.pos + (uint64_t)h.a;
   return r;
 }
 
-// Sum of (field + 1) over `n` consecutive b-bit fields starting at bit pos,
-// through a sequential cursor (the first load is one memory round trip, the
-// rest hit L1).
-__device__ __forceinline__ uint32_t gap_sum(const uint32_t *words, uint64_t pos, uint32_t n,
-                                            int b) {
-  if (!n) return 0;
-  BitCur c;
-  c.init(words, pos);
-  uint32_t s = n;
-  for (uint32_t k = 0; k < n; k++) s += c.get(b);
+// Sum of n w-bit fields starting at bit off (< 512) of the 512-bit window
+// A:B, all inside it; a 128-bit shift window pulls the next word when needed.
+__device__ __forceinline__ uint32_t sec2_sum(const Sec &A, const Sec &B, uint32_t off, uint32_t n,
+                                             int w) {
+  if (!n || !w) return 0;
+  uint32_t k = off >> 6;
+  const uint32_t sh = off & 63u;
+  uint64_t buf = sec2_word(A, B, k) << sh;
+  int nb = 64 - (int)sh;
+  uint64_t nxt = sec2_word(A, B, ++k);
+  uint32_t s = 0;
+  for (uint32_t j = 0; j < n; j++) {
+    uint32_t v;
+    if (nb >= w) {
+      v = (uint32_t)(buf >> (64 - w));
+      buf <<= w;
+      nb -= w;
+    } else {
+      const int r = w - nb;  // bits taken from nxt, 1..32
+      v = (uint32_t)(((nb ? buf >> (64 - nb) : 0ull) << r) | (nxt >> (64 - r)));
+      buf = nxt << r;
+      nb = 64 - r;
+      nxt = sec2_word(A, B, ++k);
+    }
+    s += v;
+  }
   return s;
 }
 
-// Gap runs up to this length are summed by their own lane; longer runs go to
-// a pool that the whole warp shares out evenly.  Measured on the 1M x 80 GT
-// walk (R-MAT s22 ef32): 4 -> 7.50 ms, 8 -> 7.01, 16 -> 6.52, 24 -> 6.41; the
-// previous scheme (each long run by the whole warp in turn) 8.0 ms.
-#ifndef GRASS_GT_SHORT_RUN
-#define GRASS_GT_SHORT_RUN 24
-#endif
-constexpr uint32_t kGtShortRun = GRASS_GT_SHORT_RUN;
-
-// Warp-cooperative GT draw: lane L may hold one draw (active) whose value is
-// v +/- (head + 1) + sum(gap + 1) over run.gaps gaps.  Short runs are summed
-// by their own lane.  The gap fields of all long runs, taken in lane order,
-// are cut into 32 equal contiguous shares, one per lane: a lane sums its
-// share with one sequential cursor per run it touches and adds each partial
-// sum to the run owner's word of acc (shared memory, 32 words per warp).  On
-// power-law graphs walks keep landing on hub vertices whose blocks hold
-// hundreds of gaps; this bounds every lane's work by the pool size / 32
-// instead of serialising the long runs one after another.  All 32 lanes must
-// call this together.
-__device__ __forceinline__ uint32_t gt_warp_neighbor(const uint32_t *words, bool active,
-                                                     uint32_t v, const GtRun &run, int a, int b,
-                                                     uint32_t *acc) {
-  const unsigned FULLM = 0xFFFFFFFFu;
-  const int lane = threadIdx.x & 31;
-  const bool lng = active && run.gaps > kGtShortRun;
-  const uint32_t n = lng ? run.gaps : 0u;  // this lane's fields in the pool
-  uint32_t incl = n;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(FULLM, incl, o);
-    if (lane >= o) incl += y;
-  }
-  const uint32_t T = __shfl_sync(FULLM, incl, 31);
-  acc[lane] = 0u;
-  __syncwarp();
-  if (T) {  // warp-uniform
-    const unsigned owners = __ballot_sync(FULLM, n > 0);
-    const uint32_t per = (T + 31u) >> 5;
-    uint32_t k = min(T, (uint32_t)lane * per);
-    const uint32_t hi = min(T, k + per);
-    // the run holding pool field k: the first lane whose inclusive count exceeds k
-    int o = 0;
-#pragma unroll
-    for (int st = 16; st; st >>= 1) {
-      const uint32_t x = __shfl_sync(FULLM, incl, o + st - 1);
-      if (x <= k) o += st;
-    }
-    while (__any_sync(FULLM, k < hi)) {  // warp-uniform; o is valid wherever k < hi
-      const uint64_t po = __shfl_sync(FULLM, run.pos, o);
-      const int ao = __shfl_sync(FULLM, a, o), bo = __shfl_sync(FULLM, b, o);
-      const uint32_t io = __shfl_sync(FULLM, incl, o), no = __shfl_sync(FULLM, n, o);
-      if (k < hi) {
-        const uint32_t e = min(hi, io);
-        if (bo) {
-          BitCur c;
-          c.init(words, po + (uint64_t)ao + (uint64_t)(k - (io - no)) * (uint64_t)bo);
-          uint32_t s = 0;
-          for (uint32_t j = k; j < e; j++) s += c.get(bo);
-          atomicAdd(acc + o, s);
-        }
-        k = e;
-        if (k < hi) o = __ffs(owners & ~((2u << o) - 1u)) - 1;  // next run in the pool
-      }
-    }
-    __syncwarp();
-  }
-  if (!active) return v;
-  const uint32_t hv = read_field(words, run.pos, a) + 1u;
-  const uint32_t gs = lng ? run.gaps + acc[lane] : gap_sum(words, run.pos + (uint64_t)a, run.gaps, b);
-  return (run.up ? v + hv : v - hv) + gs;
+// Sum of n >= 0 consecutive w-bit fields at bit pos through a sequential
+// cursor (the first load is one memory round trip, the rest hit L1).
+__device__ __forceinline__ uint32_t field_sum(const uint32_t *words, uint64_t pos, uint32_t n,
+                                              int w) {
+  if (!n || !w) return 0;
+  BitCur c;
+  c.init(words, pos);
+  uint32_t s = 0;
+  for (uint32_t k = 0; k < n; k++) s += c.get(w);
+  return s;
 }
 
-// Gap runs longer than this are decoded by the whole warp (k-hop).  Measured
-// on k-hop (25, 10) from 65,536 seeds, R-MAT s22 ef32: 12 -> 2.12 ms,
-// 24 -> 1.95 ms, 48 -> 1.81 ms.
-#ifndef GRASS_GT_LONG_RUN
-#define GRASS_GT_LONG_RUN 48
-#endif
-constexpr uint32_t kGtLongRun = GRASS_GT_LONG_RUN;
-
-// Warp-cooperative GT draw, long runs one at a time (used by k-hop, whose
-// lanes mostly draw from the same few blocks of one transit): lane L may hold
-// one draw (active) whose value is
-// v +/- (head + 1) + sum(gap + 1) over run.gaps gaps.  Short runs are decoded
-// by their own lane.  Each long run (a hub vertex's block holds hundreds of
-// gaps) is split into 32 contiguous sub-ranges, one per lane, each summed by
-// its own cursor, and combined with __reduce_add_sync -- one memory round
-// trip and gaps/32 L1 reads per lane instead of one lane walking all gaps
-// while the rest of the warp waits.  All 32 lanes must call this together.
-__device__ __forceinline__ uint32_t gt_warp_neighbor_serial(const uint32_t *words, bool active,
-                                                            uint32_t v, const GtRun &run, int a,
-                                                            int b) {
-  const unsigned FULLM = 0xFFFFFFFFu;
-  const int lane = threadIdx.x & 31;
-  const bool lng = active && run.gaps > kGtLongRun;
-  uint32_t cur = 0;
-  if (active && !lng) {
-    const uint32_t hv = read_field(words, run.pos, a) + 1u;
-    cur = (run.up ? v + hv : v - hv) + gap_sum(words, run.pos + (uint64_t)a, run.gaps, b);
-  }
-  unsigned mask = __ballot_sync(FULLM, lng);
-  while (mask) {
-    const int L = __ffs(mask) - 1;
-    mask &= mask - 1;
-    const uint64_t pos = __shfl_sync(FULLM, run.pos, L);
-    const uint32_t gaps = __shfl_sync(FULLM, run.gaps, L);
-    const int aL = __shfl_sync(FULLM, a, L);
-    const int bL = __shfl_sync(FULLM, b, L);
-    const uint32_t m = (gaps + 31) / 32;
-    const uint32_t g0 = min(gaps, (uint32_t)lane * m), g1 = min(gaps, g0 + m);
-    uint32_t s = gap_sum(words, pos + (uint64_t)aL + (uint64_t)g0 * (uint64_t)bL, g1 - g0, bL);
-    s = __reduce_add_sync(FULLM, s);
-    if (lane == L) {
-      const uint32_t hv = read_field(words, run.pos, a) + 1u;
-      cur = (run.up ? v + hv : v - hv) + s;
+// GT get_vertex, GT/src/bcg.cuh:153-168, on the skip-field layout: the head
+// from its sector(s); the skip field and the gaps after it from theirs (the
+// same two sectors when they lie within 512 bits of the head's sector).
+__device__ __forceinline__ uint32_t gt_neighbor(const DevGraph &g, const VHdr &h, uint32_t i) {
+  const GtRun r = gt_locate(h, i);
+  const int sw = h.b + h.cx;  // skip field width
+  const uint64_t end = r.spos + (r.skip ? (uint64_t)sw : 0ull) + (uint64_t)r.gaps * h.b;
+  const uint64_t s0 = r.pos >> 8;
+  const uint32_t off = (uint32_t)r.pos & 255u;
+  const Sec zero{0, 0, 0, 0};
+  const bool near = end - (s0 << 8) <= 512u;  // head, skip field and gaps in s0, s0 + 1
+  const bool two = near ? end - (s0 << 8) > 256u : off + (uint32_t)h.a > 256u;
+  const Sec A = load_sector(g.words, s0);
+  const Sec A2 = two ? load_sector(g.words, s0 + 1) : zero;
+  const uint32_t hv = (uint32_t)sec2_field(A, A2, off, h.a) + 1u;
+  uint32_t acc = (r.up ? h.v + hv : h.v - hv) + r.id;
+  if (near) {
+    uint32_t o = (uint32_t)(r.spos - (s0 << 8));
+    if (r.skip) {
+      acc += (uint32_t)sec2_field(A, A2, o, sw);
+      o += (uint32_t)sw;
     }
+    return acc + sec2_sum(A, A2, o, r.gaps, h.b);
   }
-  return active ? cur : v;
+  const uint64_t t0 = r.spos >> 8;
+  const uint32_t toff = (uint32_t)r.spos & 255u;
+  if (end - (t0 << 8) <= 512u) {  // the skip field and its gaps in two sectors
+    const Sec B = load_sector(g.words, t0);
+    const Sec B2 = end - (t0 << 8) > 256u ? load_sector(g.words, t0 + 1) : zero;
+    uint32_t o = toff;
+    if (r.skip) {
+      acc += (uint32_t)sec2_field(B, B2, o, sw);
+      o += (uint32_t)sw;
+    }
+    return acc + sec2_sum(B, B2, o, r.gaps, h.b);
+  }
+  uint64_t p = r.spos;  // wide fields: a sequential cursor
+  if (r.skip) {
+    acc += read_field(g.words, p, sw);
+    p += (uint64_t)sw;
+  }
+  return acc + field_sum(g.words, p, r.gaps, h.b);
 }
 
 // LE header: BCGVertex ctor, LE/src/bcg.cuh:130-152.
@@ -474,7 +429,7 @@ __device__ __forceinline__ VHdr le_header(const DevGraph &g, uint32_t v) {
   c.init(g.words, g.offsets[v]);
   h.v = v;
   h.d = c.gamma();
-  h.a = h.b = 0;
+  h.a = h.b = h.cx = 0;
   h.bn = h.bl = h.om = h.fp = 0;
   if (h.d == 0) {
     h.P = 0;
@@ -543,21 +498,6 @@ __device__ __forceinline__ void le_locate(const VHdr &h, uint32_t i, uint32_t &c
 __device__ __forceinline__ uint64_t le_chunk_pos(const VHdr &h, uint32_t c) {
   return h.P + (uint64_t)c * (uint64_t)h.a +
          ((uint64_t)(h.bl - 1) * c + min(h.om, c)) * (uint64_t)(h.b + 1);
-}
-
-// Word k (0..7) of the 512 stream bits held by sectors A and B; 0 beyond.
-__device__ __forceinline__ uint64_t sec2_word(const Sec &A, const Sec &B, uint32_t k) {
-  const uint32_t q = k & 3u;
-  const uint64_t x = k < 4 ? sec_word(A, q) : sec_word(B, q);
-  return k < 8 ? x : 0ull;
-}
-
-// The w (1..33) stream bits at bit `off` (< 512) of sectors A:B, right-aligned.
-__device__ __forceinline__ uint64_t sec2_field(const Sec &A, const Sec &B, uint32_t off, int w) {
-  const uint32_t k = off >> 6, s = off & 63u;
-  const uint64_t x = sec2_word(A, B, k);
-  const uint64_t win = s ? (x << s) | (sec2_word(A, B, k + 1) >> (64 - s)) : x;
-  return win >> (64 - w);
 }
 
 // LE get_vertex, LE/src/bcg.cuh:195-261: two rocks and one signed sea, from
@@ -640,7 +580,7 @@ __device__ __forceinline__ uint4 pack_record(const VHdr &h) {
   r.y = ((uint32_t)(h.P >> 32) & 0xFFFFu) | ((uint32_t)h.a & 63u) << 16 |
         ((uint32_t)h.b & 63u) << 22;
   r.z = h.d;
-  r.w = h.fp;
+  r.w = h.fp | ((uint32_t)h.cx & 63u) << 16;  // cx: GT only (0 elsewhere)
   return r;
 }
 
@@ -655,8 +595,11 @@ __device__ __forceinline__ VHdr record_header(const uint4 r, uint32_t v) {
   h.b = (int)((r.y >> 22) & 63u);
   h.d = r.z;
   h.fp = r.w;
+  h.cx = 0;
   h.bn = h.bl = h.om = 0;  // (CSR, mode 2: no chunk geometry)
   if constexpr (MODE == 0) {
+    h.fp = r.w & 0xFFFFu;  // GT: first_pos <= 46342, skip-field extra width above it
+    h.cx = (int)((r.w >> 16) & 63u);
     const uint32_t s = isqrt_u32(h.d);
     if (s * s == h.d) {
       h.bn = h.bl = s;
@@ -742,7 +685,7 @@ __device__ __forceinline__ uint32_t neighbor(const DevGraph &g, const VHdr &h, u
 template <int MODE>
 __device__ __forceinline__ uint64_t payload_end(const DevGraph &g, const VHdr &h) {
   if constexpr (MODE == 0) {
-    return h.P + (uint64_t)h.bn * h.a + (uint64_t)(h.d - h.bn) * h.b;
+    return gt_block_pos(h, h.bn);
   } else {
     if (h.d <= 1) return 0;  // caller checks via the header cursor instead
     return h.P + (uint64_t)(h.bn + 1) * h.a + (uint64_t)(h.d - h.bn - 1) * (h.b + 1);

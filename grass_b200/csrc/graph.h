@@ -158,6 +158,13 @@ void launch_build_records(const DevGraph &g, uint4 *recs, cudaStream_t s);
 // le_chunked selects rewritten in neighbor order.
 void launch_le_reorder(const uint32_t *src, uint32_t *dst, const uint4 *recs, uint32_t n,
                        cudaStream_t s);
+// GT stream with skip fields: pass 1 measures every vertex's skip-field
+// extra width cx[v] and rebuilt payload length len[v] (bits); pass 2 writes
+// the payloads at newP[v] into dst (zeroed) and updates the records in place.
+void launch_gt_skip_measure(const uint32_t *src, const uint4 *recs, uint32_t n,
+                            unsigned char *cx, uint64_t *len, cudaStream_t s);
+void launch_gt_skip_write(const uint32_t *src, uint32_t *dst, uint4 *recs, uint32_t n,
+                          const unsigned char *cx, const uint64_t *newP, cudaStream_t s);
 void launch_degrees(const DevGraph &g, uint32_t *deg, cudaStream_t s);
 void launch_degrees64(const DevGraph &g, uint64_t *deg, cudaStream_t s);
 // In-place exclusive scan of vals[0..n) into vals[0..n]; tmp as above.
@@ -170,6 +177,12 @@ void launch_scan_u64_inplace(uint64_t *vals, uint64_t n, uint64_t *tmp, cudaStre
 // degrees.
 int launch_decode_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
                           unsigned int *err, cudaStream_t s);
+// The planned sweep if the graph's plan is already built (it then allocates
+// nothing); false, with nothing launched, if it is not.
+bool launch_decode_if_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
+                              unsigned int *err, cudaStream_t s);
+// Decode sweep without a plan: warps over fixed 2048-neighbor tasks of the
+// CSR being written (no allocation, no set-up; about 2.4x slower).
 void launch_decode_all(const DevGraph &g, const uint64_t *rowptr, uint32_t *cols, uint64_t E,
                        unsigned int *err, cudaStream_t s);
 

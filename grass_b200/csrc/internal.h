@@ -4,12 +4,25 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include <atomic>
 #include <string>
 
 #include "../../include/grass.h"
 
 namespace grass {
+
+// NVTX range over a scope (header-only NVTX3: a no-op unless a profiler such
+// as Nsight Systems is attached), so a timeline shows each entry point and
+// the phases of a graph load; the reference times its phases with host
+// timers instead (GT/src/grass.cu:1564-1569, 2002-2003).
+struct Nvtx {
+  explicit Nvtx(const char *name) { nvtxRangePushA(name); }
+  ~Nvtx() { nvtxRangePop(); }
+  Nvtx(const Nvtx &) = delete;
+  Nvtx &operator=(const Nvtx &) = delete;
+};
 
 // Records a message for grass_last_error() on this thread and returns code.
 int set_error(int code, const char *fmt, ...) __attribute__((format(printf, 2, 3)));

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? GRASS_BATCH_MIN_BLOCKS_LE
     uint64_t cnt = 0;
     if (jb.type == GRASS_JOB_RW) {
       rw_warp<MODE, DEPTH>(g, jb.in, jb.count, jb.length, jb.seed, 0, (int)jb.layout, jb.out0,
-                           tk.begin, tk.end, cnt, bad, my.acc);
+                           tk.begin, tk.end, cnt, bad);
     } else if (jb.type == GRASS_JOB_KHOP) {
       for (uint64_t s = tk.begin; s < tk.end; s++)
         khop_seed_warp<MODE>(g, jb.in, jb.khop, s, my, cnt, bad);
@@ -452,6 +452,7 @@ int grass_batch_get_config(const grass_batch *b, grass_batch_config *cfg) {
 }
 
 int grass_batch_run(grass_batch *b, void *stream, unsigned long long *d_total_edges) {
+  grass::Nvtx nvtx_("grass_batch_run");
   clear_error();
   if (!b) return set_error(GRASS_E_ARG, "null batch");
   std::lock_guard<std::mutex> lk(b->mu);
@@ -490,6 +491,7 @@ int grass_batch_run(grass_batch *b, void *stream, unsigned long long *d_total_ed
 
 int grass_batch_autotune(grass_batch *b, void *stream, grass_batch_config *best,
                          float *best_ms) {
+  grass::Nvtx nvtx_("grass_batch_autotune");
   clear_error();
   if (!b) return set_error(GRASS_E_ARG, "null batch");
   const grass_batch_config keep = b->cfg;

@@ -41,6 +41,7 @@ __device__ __forceinline__ VHdr shfl_hdr(const VHdr &h, int src) {
   o.bl = __shfl_sync(FULL, h.bl, src);
   o.om = __shfl_sync(FULL, h.om, src);
   o.fp = __shfl_sync(FULL, h.fp, src);
+  o.cx = __shfl_sync(FULL, h.cx, src);
   o.a = __shfl_sync(FULL, h.a, src);
   o.b = __shfl_sync(FULL, h.b, src);
   return o;
@@ -196,7 +197,7 @@ __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint6
         if (wv < g.n) {
           hw = header<MODE>(g, wv);
         } else {
-          hw.d = 0; hw.P = 0; hw.v = 0; hw.bn = hw.bl = hw.om = hw.fp = 0; hw.a = hw.b = 0;
+          hw.d = 0; hw.P = 0; hw.v = 0; hw.bn = hw.bl = hw.om = hw.fp = 0; hw.a = hw.b = hw.cx = 0;
         }
         // owner lane k: number of window rows that end at or before gl
         // (binary lifting over 31 probes gives the exact count when it is
@@ -231,12 +232,15 @@ __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint6
           const GtRun run = gt_locate(hk, i);
           if (far) {
             x = gt_neighbor(g, hk, i);  // complete value; starts its own segment
-          } else if (run.gaps == 0) {
+          } else if (run.gaps == 0) {  // a head or a skip field: an absolute value
             const uint32_t hv = read_field(g.words, run.pos, hk.a) + 1u;
             x = run.up ? hk.v + hv : hk.v - hv;
+            if (run.skip) x += run.id + read_field(g.words, run.spos, hk.b + hk.cx);
           } else {
             head = false;
-            x = read_field(g.words, run.pos + hk.a + (uint64_t)(run.gaps - 1) * hk.b, hk.b) + 1u;
+            const uint64_t at = run.spos + (run.skip ? (uint64_t)(hk.b + hk.cx) : 0ull) +
+                                (uint64_t)(run.gaps - 1) * hk.b;
+            x = (hk.b ? read_field(g.words, at, hk.b) : 0u) + 1u;
           }
         }
         if (lane == 0 && !head) {
@@ -366,8 +370,8 @@ struct LeSeq {
 };
 
 struct GtSeq {
-  uint32_t v, fp, bl, om, blk, id, len, prev;
-  int a, b;
+  uint32_t v, fp, bl, om, blk, id, len, prev, head;
+  int a, b, sw;  // head, gap and skip-field widths
   BitCur cur;
 
   __device__ __forceinline__ void init(const uint32_t *words, const VHdr &h) {
@@ -377,17 +381,20 @@ struct GtSeq {
     om = h.om;
     a = h.a;
     b = h.b;
+    sw = h.b + h.cx;
     blk = 0;
     id = 0;
     len = om ? bl + 1 : bl;
-    prev = 0;
+    prev = head = 0;
     cur.init(words, h.P);
   }
   __device__ __forceinline__ uint32_t next() {
     uint32_t val;
     if (id == 0) {
       const uint32_t hv = (a ? cur.get(a) : 0u) + 1u;
-      val = blk >= fp ? v + hv : v - hv;
+      val = head = blk >= fp ? v + hv : v - hv;
+    } else if (id % kGtSkip == 0) {  // skip field: the block's raw gaps 1..id summed
+      val = head + id + (sw ? cur.get(sw) : 0u);
     } else {
       val = prev + (b ? cur.get(b) : 0u) + 1u;
     }
@@ -629,7 +636,6 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
     const uint64_t base = rowptr[it.x];
     const uint64_t G0 = base + it.y, G1 = base + it.z;  // CSR slots of the range
     const uint64_t sea0 = h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a;
-    const uint64_t blkbits = (uint64_t)h.a + (uint64_t)(h.bl - 1) * h.b;
     const uint32_t split = h.om * (h.bl + 1);
     const int sw = h.b + 1;
     const bool chunked = MODE == 1 && le_chunked(h);  // neighbor-order LE payload
@@ -675,8 +681,8 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
 #endif
         if (!staged) prefetch_bits(g.words, lo, hi);
       } else {
-        prefetch_bits(g.words, h.P + (uint64_t)c0 * blkbits + (uint64_t)min(c0, h.om) * h.b,
-                      min(pend, h.P + cl * blkbits + min(cl, (uint64_t)h.om) * h.b));
+        prefetch_bits(g.words, gt_block_pos(h, c0),
+                      min(pend, gt_block_pos(h, (uint32_t)min(cl, (uint64_t)h.bn))));
       }
     }
     uint32_t carry = 0;  // GT: value of the slot before the current group
@@ -778,22 +784,36 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
           }
         }
       } else {
-        // Fields in order: block c holds its head (a bits), then tl - 1 gaps.
-        // Slots before the run's first head are relative to the slot before
-        // the run, whose value a segmented warp scan over the runs supplies.
+        // Fields in order: block c holds its head (a bits), then tl - 1 gaps,
+        // with a skip field (an absolute value relative to the head) at every
+        // kGtSkip-th position.  Slots before the run's first head or skip field
+        // are relative to the slot before the run, whose value a segmented
+        // warp scan over the runs supplies.
         BitCur cur;
+        const int sk = h.b + h.cx;  // skip-field width
+        uint64_t hp = 0;            // bit offset of block c
         if (cnt) {
-          const uint64_t hp = h.P + (uint64_t)c * blkbits + (uint64_t)min(c, h.om) * h.b;
-          cur.init(g.words, id ? hp + h.a + (uint64_t)(id - 1) * h.b : hp);
+          hp = gt_block_pos(h, c);
+          cur.init(g.words, id ? gt_field_pos(h, hp, id) : hp);
         }
         uint32_t x = 0, rel = 0;  // rel: bit k set when slot k is relative
-        bool seen = false;         // a head has been read in this run
+        bool seen = false;         // an absolute value has been read in this run
+        uint32_t hv0 = 0;          // head value of block c, once known
+        bool hk = false;
 #pragma unroll
         for (uint32_t k = 0; k < kRun; k++) {
           if (k >= cnt) break;
           if (id == 0) {
             const uint32_t hv = (h.a ? cur.get(h.a) : 0u) + 1u;
-            x = c >= h.fp ? h.v + hv : h.v - hv;
+            x = hv0 = c >= h.fp ? h.v + hv : h.v - hv;
+            hk = seen = true;
+          } else if (id % kGtSkip == 0) {
+            if (!hk) {  // the run started inside the block: read its head
+              const uint32_t hv = read_field(g.words, hp, h.a) + 1u;
+              hv0 = c >= h.fp ? h.v + hv : h.v - hv;
+              hk = true;
+            }
+            x = hv0 + id + (sk ? cur.get(sk) : 0u);
             seen = true;
           } else {
             x += (h.b ? cur.get(h.b) : 0u) + 1u;
@@ -892,6 +912,9 @@ __global__ void __launch_bounds__(256) decode_small_kernel(DevGraph g, const uin
 
 }  // namespace
 
+static void launch_plan_kernels(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
+                                unsigned int *err, cudaStream_t s);
+
 int launch_decode_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
                           unsigned int *err, cudaStream_t s) {
   const uint32_t n = (uint32_t)g->info.n;
@@ -953,6 +976,24 @@ int launch_decode_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t
       g->plan_ok = true;
     }
   }
+  launch_plan_kernels(g, rowptr, cols, err, s);
+  return GRASS_OK;
+}
+
+bool launch_decode_if_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
+                              unsigned int *err, cudaStream_t s) {
+  {
+    std::lock_guard<std::mutex> lk(g->plan_mu);
+    if (!g->plan_ok) return false;
+  }
+  if (g->info.num_edges) launch_plan_kernels(g, rowptr, cols, err, s);
+  return true;
+}
+
+// The range and small-vertex sweeps of a built plan (launches only).
+static void launch_plan_kernels(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
+                                unsigned int *err, cudaStream_t s) {
+  const int dev = g->device;
   const DevGraph v = g->view();
   const int per_sm = 8;
   if (g->plan_nbig) {
@@ -990,7 +1031,6 @@ int launch_decode_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t
                                                   g->plan_nsmall, err);
     count_launch();
   }
-  return GRASS_OK;
 }
 
 void launch_decode_all(const DevGraph &g, const uint64_t *rowptr, uint32_t *cols, uint64_t E,

@@ -267,6 +267,94 @@ __global__ void __launch_bounds__(256) le_reorder_kernel(const uint32_t *__restr
   }
 }
 
+// ---- GT stream with skip fields (gt_block_pos, device_common.cuh) ----
+// Both kernels take one warp per vertex and one lane per block, reading the
+// on-disk stream through each block's cursor: head (a bits), then len - 1
+// raw gaps (b bits), GT/chunk_compress/compressor.hpp:297-349.
+
+__device__ __forceinline__ uint32_t bit_len(uint32_t x) { return x ? 32u - __clz(x) : 1u; }
+
+// Pass 1: per vertex the skip-field extra width cx (bits of the largest
+// running gap sum at a skip position, beyond b) and the rebuilt payload's
+// length in bits.
+__global__ void __launch_bounds__(256) gt_skip_measure_kernel(const uint32_t *__restrict__ src,
+                                                              const uint4 *__restrict__ recs,
+                                                              uint32_t n,
+                                                              unsigned char *__restrict__ cx,
+                                                              uint64_t *__restrict__ len) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
+    const VHdr h = record_header<0>(recs[v], (uint32_t)v);  // on-disk layout (cx = 0)
+    if (h.d == 0) {
+      if (lane == 0) cx[v] = 0, len[v] = 0;
+      continue;
+    }
+    const uint32_t longest = h.bl + (h.om ? 1u : 0u);
+    uint32_t mx = 0;  // bits of the largest gap sum at a skip position
+    if (longest - 1 >= kGtSkip) {
+      for (uint32_t blk = lane; blk < h.bn; blk += 32) {
+        const uint32_t L = blk < h.om ? h.bl + 1 : h.bl;
+        BitCur c;
+        c.init(src, gt_block_pos(h, blk) + h.a);
+        uint32_t sum = 0;
+        for (uint32_t t = 1; t < L; t++) {
+          sum += h.b ? c.get(h.b) : 0u;
+          if (t % kGtSkip == 0) mx = max(mx, bit_len(sum));
+        }
+      }
+      mx = __reduce_max_sync(0xFFFFFFFFu, mx);
+    }
+    if (lane == 0) {
+      const uint32_t x = mx > (uint32_t)h.b ? mx - (uint32_t)h.b : 0u;
+      VHdr hn = h;
+      hn.cx = (int)x;
+      cx[v] = (unsigned char)x;
+      len[v] = payload_end<0>(DevGraph{}, hn) - h.P;
+    }
+  }
+}
+
+// Pass 2: the rebuilt payload of every vertex at its new offset newP[v] in
+// dst (zeroed), and its record updated in place (P, and cx above first_pos).
+__global__ void __launch_bounds__(256) gt_skip_write_kernel(const uint32_t *__restrict__ src,
+                                                            uint32_t *dst, uint4 *recs,
+                                                            uint32_t n,
+                                                            const unsigned char *__restrict__ cx,
+                                                            const uint64_t *__restrict__ newP) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
+    const VHdr h = record_header<0>(recs[v], (uint32_t)v);
+    VHdr hn = h;
+    hn.P = newP[v];
+    hn.cx = cx[v];
+    const int sk = hn.b + hn.cx;
+    for (uint32_t blk = lane; blk < h.bn; blk += 32) {
+      const uint32_t L = blk < h.om ? h.bl + 1 : h.bl;
+      BitCur c;
+      c.init(src, gt_block_pos(h, blk));
+      uint64_t at = gt_block_pos(hn, blk);
+      or_bits(dst, at, c.get(h.a), h.a);
+      at += h.a;
+      uint32_t sum = 0;
+      for (uint32_t t = 1; t < L; t++) {
+        const uint32_t gap = h.b ? c.get(h.b) : 0u;
+        sum += gap;
+        if (t % kGtSkip == 0) {
+          if (sk) or_bits(dst, at, sum, sk);
+          at += sk;
+        } else {
+          if (h.b) or_bits(dst, at, gap, h.b);
+          at += h.b;
+        }
+      }
+    }
+    __syncwarp();  // every lane has read the old record
+    if (lane == 0) recs[v] = pack_record(hn);
+  }
+}
+
 unsigned grid_for(uint64_t items, int threads, int device) {
   uint64_t blocks = (items + threads - 1) / threads;
   uint64_t cap = (uint64_t)sm_count(device) * 16;
@@ -319,6 +407,22 @@ void launch_le_reorder(const uint32_t *src, uint32_t *dst, const uint4 *recs, ui
   int dev = 0;
   cudaGetDevice(&dev);
   le_reorder_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(src, dst, recs, n);
+  count_launch();
+}
+
+void launch_gt_skip_measure(const uint32_t *src, const uint4 *recs, uint32_t n,
+                            unsigned char *cx, uint64_t *len, cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  gt_skip_measure_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(src, recs, n, cx, len);
+  count_launch();
+}
+
+void launch_gt_skip_write(const uint32_t *src, uint32_t *dst, uint4 *recs, uint32_t n,
+                          const unsigned char *cx, const uint64_t *newP, cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  gt_skip_write_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(src, dst, recs, n, cx, newP);
   count_launch();
 }
 

@@ -40,7 +40,7 @@ __device__ __forceinline__ void store_path(uint32_t *paths, int layout, uint64_t
 // w0: walker id of starts[0] -- draws use walker id w0 + w, so a batch split
 // into chunks produces the same walks as one launch.
 template <int MODE, int DEPTH>
-__global__ void __launch_bounds__(512, GRASS_RW_LE_MIN_BLOCKS) rw_kernel(DevGraph g, const uint32_t *__restrict__ starts,
+__global__ void __launch_bounds__(512, MODE == 0 ? GRASS_RW_GT_MIN_BLOCKS : GRASS_RW_LE_MIN_BLOCKS) rw_kernel(DevGraph g, const uint32_t *__restrict__ starts,
                                                  uint64_t W, uint32_t L, uint64_t seed,
                                                  uint64_t w0, int layout,
                                                  uint32_t *__restrict__ paths,
@@ -94,81 +94,6 @@ __global__ void __launch_bounds__(512, GRASS_RW_LE_MIN_BLOCKS) rw_kernel(DevGrap
   if (bad && err) atomicOr(err, 1u);
 }
 
-// GT random walk.  A warp owns 32*DEPTH consecutive walkers and every step is
-// warp-synchronous, so the gap runs of all lanes are decoded cooperatively
-// (gt_warp_neighbor, with the warp's 32 words of shared memory for the pooled
-// sums): on power-law graphs walks keep returning to hub vertices whose
-// blocks hold hundreds of gaps, which a per-lane loop would serialise across
-// the whole warp.
-template <int DEPTH>
-__global__ void __launch_bounds__(512, GRASS_RW_GT_MIN_BLOCKS) rw_gt_kernel(DevGraph g,
-                                                    const uint32_t *__restrict__ starts,
-                                                    uint64_t W, uint32_t L, uint64_t seed,
-                                                    uint64_t w0, int layout,
-                                                    uint32_t *__restrict__ paths,
-                                                    unsigned long long *edges,
-                                                    unsigned int *err) {
-  __shared__ uint32_t sh_all[16][32];
-  uint32_t *sh = sh_all[threadIdx.x >> 5];
-  const int lane = threadIdx.x & 31;
-  const uint64_t gwarp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  uint64_t cnt = 0;
-  bool bad = false;
-  for (uint64_t wb = gwarp * 32 * DEPTH; wb < W; wb += nwarps * 32 * DEPTH) {
-    uint32_t v[DEPTH];
-    u32x4 r[DEPTH];
-#pragma unroll
-    for (int k = 0; k < DEPTH; k++) {
-      const uint64_t w = wb + (uint64_t)k * 32 + lane;
-      v[k] = INVALID_VERTEX;
-      r[k] = u32x4{0, 0, 0, 0};
-      if (w < W) {
-        const uint32_t s0 = starts[w];
-        store_path(paths, layout, W, L, w, 0, s0);
-        v[k] = s0 < g.n ? s0 : INVALID_VERTEX;
-      }
-    }
-    for (uint32_t s = 0; s < L; s++) {
-#pragma unroll
-      for (int k = 0; k < DEPTH; k++) {
-        const uint64_t w = wb + (uint64_t)k * 32 + lane;
-        if ((s & 3) == 0) {
-          const uint64_t id = w0 + w;
-          r[k] = philox4x32_10(seed, s >> 2, (uint32_t)id, (uint32_t)(id >> 32), TAG_RW);
-        }
-        bool active = v[k] != INVALID_VERTEX;
-        GtRun run{0, 0, false};
-        int a = 0, b = 0;
-        if (active) {
-          const VHdr h = header<0>(g, v[k]);
-          if (h.d == 0) {
-            active = false;
-            v[k] = INVALID_VERTEX;
-          } else {
-            run = gt_locate(h, mulhi_u32(pick(r[k], s & 3), h.d));
-            a = h.a;
-            b = h.b;
-          }
-        }
-        const uint32_t nv = gt_warp_neighbor(g.words, active, v[k], run, a, b, sh);
-        if (active) {
-          if (nv >= g.n) {
-            bad = true;
-            v[k] = INVALID_VERTEX;
-          } else {
-            v[k] = nv;
-            cnt++;
-          }
-        }
-        if (w < W) store_path(paths, layout, W, L, w, s + 1, v[k]);
-      }
-    }
-  }
-  warp_add_u64(edges, cnt);
-  if (bad && err) atomicOr(err, 1u);
-}
-
 // Stream bits a draw of neighbor i reads (the payload fields; the header is
 // in the vertex record), and the 32-byte sectors those reads span.
 template <int MODE>
@@ -176,18 +101,15 @@ __device__ __forceinline__ void draw_footprint(const DevGraph &g, const VHdr &h,
                                                uint64_t &bits, uint64_t &sectors) {
   uint64_t r0[3], r1[3];  // half-open bit ranges, in stream order
   int nr = 0;
-  if (MODE == 0) {
-    const uint32_t split = (h.bl + 1) * h.om;
-    const bool flag = i < split;
-    const uint32_t j = flag ? i : i - split;
-    const uint32_t len = h.bl + (flag ? 1u : 0u);
-    uint32_t blk = j / len;
-    const uint32_t id = j - blk * len;
-    if (!flag) blk += h.om;
-    const uint64_t pos = h.P + (uint64_t)blk * (uint64_t)(h.a + (h.bl - 1) * h.b) +
-                         (uint64_t)min(blk, h.om) * (uint64_t)h.b;
-    r0[nr] = pos;
-    r1[nr++] = pos + h.a + (uint64_t)id * h.b;
+  if (MODE == 0) {  // the head; the skip field and the gaps after it
+    const GtRun r = gt_locate(h, i);
+    r0[nr] = r.pos;
+    r1[nr++] = r.pos + h.a;
+    const uint64_t e = r.spos + (r.skip ? (uint64_t)(h.b + h.cx) : 0ull) + (uint64_t)r.gaps * h.b;
+    if (e > r.spos) {
+      r0[nr] = r.spos;
+      r1[nr++] = e;
+    }
   } else if (h.d > 1 && le_chunked(h)) {
     // neighbor order: rock c, the sea, rock c+1 lie in one span (le_neighbor
     // loads the sectors of the span)
@@ -596,9 +518,7 @@ static void rw_launch_depth(const DevGraph &g, const grass_rw_params &p, const u
                             uint64_t W, uint32_t *paths, unsigned long long *edges,
                             unsigned int *err, cudaStream_t s, const grass_tuning &t,
                             const L2Window &win, uint64_t w0) {
-  // GT: warp-synchronous kernel with cooperative gap decoding; LE: one
-  // independent O(1) decode per lane.
-  auto kern = MODE == 0 ? rw_gt_kernel<DEPTH> : rw_kernel<MODE, DEPTH>;
+  auto kern = rw_kernel<MODE, DEPTH>;
   const unsigned grid =
       resident_grid(kern, (int)t.rw_threads, t.rw_blocks_per_sm, W, (uint64_t)t.rw_threads * DEPTH);
   launch_with_window(kern, grid, t.rw_threads, s, win, g, starts, W, p.length, p.seed, w0,

@@ -45,6 +45,7 @@ int scratch_for_device(int device, uint64_t **out) {
 
 extern "C" int grass_decode_all_noalloc(const grass_graph *g, uint64_t *d_rowptr,
                                         uint32_t *d_cols, void *stream) {
+  grass::Nvtx nvtx_("grass_decode_all_noalloc");
   using namespace grass;
   clear_error();
   if (!g) return set_error(GRASS_E_ARG, "null graph");
@@ -64,7 +65,11 @@ extern "C" int grass_decode_all_noalloc(const grass_graph *g, uint64_t *d_rowptr
   // the GPU (other streams, other threads) race on it.
   launch_degrees64(g->view(), d_rowptr, st);
   launch_scan_u64_inplace(d_rowptr, n, scratch, st);
-  launch_decode_all(g->view(), d_rowptr, d_cols, g->info.num_edges, g->d_err, st);
+  // The planned sweep once an earlier grass_decode_all has built the graph's
+  // plan (launching it allocates nothing); until then the unplanned sweep,
+  // which needs no plan and is about 2.4x slower.
+  if (!launch_decode_if_planned(g, d_rowptr, d_cols, g->d_err, st))
+    launch_decode_all(g->view(), d_rowptr, d_cols, g->info.num_edges, g->d_err, st);
   const cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GRASS_OK : cuda_fail(e, "kernel launch");
 }

@@ -23,7 +23,7 @@ template <int MODE, int DEPTH>
 __device__ __forceinline__ void rw_warp(const DevGraph &g, const uint32_t *starts, uint64_t W,
                                         uint32_t L, uint64_t seed, uint64_t w0, int layout,
                                         uint32_t *paths, uint64_t b, uint64_t e, uint64_t &cnt,
-                                        bool &bad, uint32_t *acc) {
+                                        bool &bad) {
   const int lane = threadIdx.x & 31;
   for (uint64_t wb = b; wb < e; wb += 32 * DEPTH) {  // warp-uniform
     uint32_t v[DEPTH];
@@ -49,22 +49,7 @@ __device__ __forceinline__ void rw_warp(const DevGraph &g, const uint32_t *start
         }
         bool active = v[k] != INVALID_VERTEX;
         uint32_t nv = INVALID_VERTEX;
-        if (MODE == 0) {
-          GtRun run{0, 0, false};
-          int ra = 0, rb = 0;
-          if (active) {
-            const VHdr h = header<0>(g, v[k]);
-            if (h.d == 0) {
-              active = false;
-              v[k] = INVALID_VERTEX;
-            } else {
-              run = gt_locate(h, mulhi_u32(pick(r[k], s & 3), h.d));
-              ra = h.a;
-              rb = h.b;
-            }
-          }
-          nv = gt_warp_neighbor(g.words, active, v[k], run, ra, rb, acc);
-        } else if (active) {
+        if (active) {
           const VHdr h = header<MODE>(g, v[k]);
           if (h.d == 0) {
             active = false;
@@ -105,16 +90,15 @@ struct KhopArgs {
 struct SmemHdr {
   uint64_t P[32];
   uint32_t v[32], d[32], bn[32], bl[32], om[32], fp[32];
-  int a[32], b[32];
-  uint32_t acc[32];  // GT: pooled gap sums (gt_warp_neighbor)
+  int a[32], b[32], cx[32];
   __device__ __forceinline__ void put(int i, const VHdr &h) {
     P[i] = h.P; v[i] = h.v; d[i] = h.d; bn[i] = h.bn; bl[i] = h.bl; om[i] = h.om; fp[i] = h.fp;
-    a[i] = h.a; b[i] = h.b;
+    a[i] = h.a; b[i] = h.b; cx[i] = h.cx;
   }
   __device__ __forceinline__ VHdr get(int i) const {
     VHdr h;
     h.P = P[i]; h.v = v[i]; h.d = d[i]; h.bn = bn[i]; h.bl = bl[i]; h.om = om[i]; h.fp = fp[i];
-    h.a = a[i]; h.b = b[i];
+    h.a = a[i]; h.b = b[i]; h.cx = cx[i];
     return h;
   }
 };
@@ -141,6 +125,7 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
         h.P = 0;
         h.v = t;
         h.bn = h.bl = h.om = h.fp = 0;
+        h.cx = 0;
         h.a = h.b = 0;
       }
       my.put(lane, h);
@@ -152,9 +137,7 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
         const bool act = j < total;
         uint64_t slot = 0;
         bool draw = false;
-        uint32_t nv = INVALID_VERTEX, tv = 0;
-        GtRun run{0, 0, false};
-        int ra = 0, rb = 0;
+        uint32_t nv = INVALID_VERTEX;
         if (act) {
           const uint32_t pl = (uint32_t)(j / f);
           slot = pc * f + j;
@@ -163,20 +146,8 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
             draw = true;
             const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(slot >> 2), (uint32_t)s,
                                            (uint32_t)(s >> 32), TAG_KHOP | hop);
-            const uint32_t idx = mulhi_u32(pick(rr, (int)(slot & 3)), hk.d);
-            if (MODE == 0) {
-              run = gt_locate(hk, idx);
-              tv = hk.v;
-              ra = hk.a;
-              rb = hk.b;
-            } else {
-              nv = neighbor<MODE>(g, hk, idx);
-            }
+            nv = neighbor<MODE>(g, hk, mulhi_u32(pick(rr, (int)(slot & 3)), hk.d));
           }
-        }
-        if (MODE == 0) {
-          const uint32_t x = gt_warp_neighbor_serial(g.words, draw, tv, run, ra, rb);
-          if (draw) nv = x;
         }
         if (act) {
           if (draw) {

@@ -661,6 +661,7 @@ extern "C" {
 
 int grass_server_create(const grass_graph *g, const grass_server_config *cfg,
                         grass_server **out) {
+  grass::Nvtx nvtx_("grass_server_create");
   using namespace grass;
   clear_error();
   if (!g || !out) return set_error(GRASS_E_ARG, "null argument");
@@ -720,6 +721,7 @@ int grass_server_create(const grass_graph *g, const grass_server_config *cfg,
 }
 
 int grass_server_submit(grass_server *s, const grass_request *r, uint64_t *ticket) {
+  grass::Nvtx nvtx_("grass_server_submit");
   using namespace grass;
   clear_error();
   if (!s || !r || !ticket) return set_error(GRASS_E_ARG, "null argument");
@@ -861,6 +863,7 @@ int grass_server_stats_get(grass_server *s, grass_server_stats *out) {
 }
 
 int grass_server_destroy(grass_server *s, uint32_t timeout_ms) {
+  grass::Nvtx nvtx_("grass_server_destroy");
   using namespace grass;
   clear_error();
   if (!s) return GRASS_OK;

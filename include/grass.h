@@ -135,13 +135,22 @@ int grass_open_mem(const void *graph_bytes, uint64_t graph_size, const void *off
 int grass_close(grass_graph *g);
 int grass_get_info(const grass_graph *g, grass_graph_info *info);
 /* Device view of the resident graph (for callers that launch their own
- * kernels): the stream words (n_words + 16 zero guard words, each word the
- * next 32 stream bits MSB-first) and the n vertex records, 16 bytes each:
- * {P low 32 bits, P bits 32..47 | a << 16 | b << 22, degree, first_pos},
- * where P is the bit offset of the vertex's payload after its gamma header,
- * a/b are the GT head/body or LE rock/sea widths and, for an LE vertex of
- * degree 1, first_pos holds its neighbor.  The records replace the
- * reference's uint64 bit-offset table (GT/src/utils.hpp:363). */
+ * kernels): the stream words (n_words + at least 16 zero guard words, each
+ * word the next 32 stream bits MSB-first) and the n vertex records, 16 bytes
+ * each: {P low 32 bits, P bits 32..47 | a << 16 | b << 22, degree, w}, where
+ * P is the bit offset of the vertex's payload, a/b are the GT head/body or LE
+ * rock/sea widths, and w is first_pos (LE degree 1: the single neighbor; GT:
+ * first_pos in bits 0..15 and the skip-field extra width cx in bits 16..21).
+ * The records replace the reference's uint64 bit-offset table
+ * (GT/src/utils.hpp:363).  The stream is the .graph stream re-laid for random
+ * access, the field values unchanged:
+ *   LE: the file's stream; the payload of every vertex whose longest chunk
+ *       spans at most 256 bits (2 rock_bit + its seas x (sea_bit + 1)) is in
+ *       neighbor order, [rock 0][seas of chunk 0][rock 1]...[last rock],
+ *       instead of all rocks then all seas (same bits, same P);
+ *   GT: the payloads only, back to back in vertex order; in every block the
+ *       field at each position t = 16, 32, ... holds the sum of the block's
+ *       raw gaps 1..t in b + cx bits instead of gap t. */
 int grass_device_view(const grass_graph *g, const uint32_t **words, uint64_t *n_words,
                       const void **records);
 
@@ -181,7 +190,11 @@ int grass_decode_all(const grass_graph *g, uint64_t *d_rowptr, uint32_t *d_cols,
  * limits graphs to 268,435,456 vertices (larger ones return GRASS_E_ARG).
  * The first call on a device looks up the array's device address, so make it
  * before any stream capture.  All calls share the array: calls that overlap
- * on the GPU race. */
+ * on the GPU (other streams, other threads) race, so the caller serialises
+ * them.  Speed: once a grass_decode_all on the same graph has built its
+ * decode plan (that call allocates, once), this call runs the same planned
+ * sweep; before that it runs an unplanned sweep that needs no set-up, about
+ * 2.4x slower (4.1 ms against 1.7 ms for 250 M neighbors on one B200). */
 int grass_decode_all_noalloc(const grass_graph *g, uint64_t *d_rowptr, uint32_t *d_cols,
                              void *stream);
 

@@ -187,3 +187,41 @@ def test_loadgen_batched_equals_one_job_per_launch(mode):
         assert r["launches"] > 0
     assert a["edges"] == b["edges"]  # same trace, same Philox streams
     assert a["batches"] < 300        # requests were batched
+
+
+@pytest.mark.parametrize("mode", ["GT", "LE"])
+def test_requests_overlap_a_running_batch(mode):
+    """Continuous batching: a walk request that arrives while a long multi-RW
+    chain is on the GPU is admitted on another stream and completes inside the
+    chain's [launch, done] interval, so its work overlapped the chain's on the
+    device (one at a time, it would finish after the chain).  Both results
+    equal their standalone calls."""
+    import time
+    d, *_ = golden_graph("rmat_s10_e8")
+    g = G.Graph(os.path.join(d, mode), mode)
+    srv = G.Server(g, window_min_us=50, window_max_us=200)
+    # one sequential degree-proportional chain: ~2 us per step, tens of ms
+    chain = dict(samples=1, walkers=2000, steps=20000, seed=77, select=1)
+    t_chain = srv.submit_mrw(chain["samples"], chain["walkers"], chain["steps"], chain["seed"],
+                             select=chain["select"])
+    time.sleep(0.003)  # the chain's batch is on the GPU
+    starts = np.random.default_rng(2).integers(0, g.n, 500).astype(np.uint32)
+    t_walk = srv.submit_rw(starts, 30, 78)
+    walk = srv.wait(t_walk, timeout_ms=60000)
+    res = srv.wait(t_chain, timeout_ms=60000)
+    assert walk["status"] == G.OK and res["status"] == G.OK
+    assert walk["batch"] != res["batch"]
+    assert res["launch_us"] < walk["launch_us"] and walk["done_us"] < res["done_us"], (
+        res["launch_us"], res["done_us"], walk["launch_us"], walk["done_us"])
+    p, e = g.rw(starts, 30, 78)
+    np.testing.assert_array_equal(walk["outputs"][0], p.reshape(-1))
+    assert walk["edges"] == e
+    import torch  # the chain's roots were drawn on the device from its seed
+    rt = torch.empty(chain["walkers"], dtype=torch.int32, device="cuda")
+    G.mrw_roots_device(g.n, 1, chain["walkers"], chain["seed"], rt)
+    roots = rt.cpu().numpy().view(np.uint32).reshape(1, -1)
+    src, dst, _, e2 = g.mrw(roots, chain["steps"], chain["seed"], select=chain["select"])
+    np.testing.assert_array_equal(res["outputs"][0], src.reshape(-1))
+    np.testing.assert_array_equal(res["outputs"][1], dst.reshape(-1))
+    assert res["edges"] == e2
+    srv.close()

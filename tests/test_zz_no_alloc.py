@@ -33,9 +33,12 @@ def _decode(fn, g):
 
 
 def _check(g, cols=None):
-    ref = _decode(G.lib.grass_decode_all, g)
-    for _ in range(2):  # two calls in a row on the shared scratch
-        got = _decode(G.lib.grass_decode_all_noalloc, g)
+    # before any grass_decode_all the graph has no decode plan: the unplanned sweep
+    before = [_decode(G.lib.grass_decode_all_noalloc, g) for _ in range(2)]
+    ref = _decode(G.lib.grass_decode_all, g)  # builds the plan
+    # two calls in a row on the shared scratch, now through the planned sweep
+    after = [_decode(G.lib.grass_decode_all_noalloc, g) for _ in range(2)]
+    for got in before + after:
         np.testing.assert_array_equal(got[0], ref[0])
         np.testing.assert_array_equal(got[1], ref[1])
     if cols is not None:
