@@ -60,8 +60,9 @@ def parse():
     ap.add_argument("--khop-seeds", type=int, default=65536)
     ap.add_argument("--mode", default="LE", choices=["LE", "GT"])
     ap.add_argument("--only", default="",
-                    help="comma list: rw,khop,decode,csr,e2e,cpu,batch,serve,parity,cfg5 "
-                         "(cfg5, the 3B-edge Chung-Lu graph, runs only when named)")
+                    help="comma list: rw,khop,decode,csr,e2e,cpu,batch,serve,parity,cfg5,refgpu "
+                         "(cfg5, the 3B-edge Chung-Lu graph, and refgpu, the reference's own "
+                         "GPU rw app, run only when named)")
     ap.add_argument("--no-clocks", action="store_true")
     ap.add_argument("--batch-scale", type=int, default=24,
                     help="R-MAT scale of the batched-jobs / serving graph (edge factor 16)")
@@ -395,7 +396,9 @@ class Parity:
     def decode(self, key, prefix, mode, rowptr, cols):
         if not self.enabled:
             return
-        rp, cl = self.graph(prefix).decode_all(mode)
+        if (prefix, "decode") not in self._og:
+            self._og[(prefix, "decode")] = self.graph(prefix).decode_all(mode)
+        rp, cl = self._og[(prefix, "decode")]
         ok = (np.array_equal(rowptr.cpu().numpy().view(np.uint64), rp) and
               np.array_equal(cols.cpu().numpy().view(np.uint32), cl))
         self.put(key, ok, neighbors=int(len(cl)), vertices=int(len(rp) - 1))
@@ -513,6 +516,12 @@ def batch_bench(G, torch, graphs, n, stream, flush, K, W, parity=None, gdir=None
     draws = {0: 0, 1: 0, 2: 0}
     res = {}
     for m, g in graphs.items():
+        # the multi-RW inputs are the snapshot again (the previous mode's
+        # standalone chains walked them in place); a batch copies them at add
+        for j, (inp, outs, snap) in zip(jobs, bufs):
+            if j["type"] == 2:
+                inp.copy_(snap)
+
         def make(types):
             b = G.Batch(g)
             for j, (inp, outs, _) in zip(jobs, bufs):
@@ -664,6 +673,43 @@ def cpu_baseline(gdir, mode, n, length, seed, budget_s=12.0):
             "sample": f"{W} uniform walkers x {length} steps ({mode} decode per draw) on the "
                       f"same graph; oracle restatement of the reference decoders + app next(), "
                       f"OpenMP over walkers"}
+
+
+def reference_gpu(gdir, n, runs=3, timeout_s=600):
+    """The reference's own GPU sampler on this GPU: its unmodified `rw` app
+    (oracle/_ref/rw_gt, rw_le, built from its sources for sm_100a) against
+    this library's drop-in `rw` on the same files and the same workload, the
+    reference app's default: one walker per vertex starting at i % n, 80
+    steps (GT/src/apps/randomwalk/randomWalks.cu:4-24), `-n runs`.  Both print
+    runSamplingTime (GT/src/grass.cu:2127-2130); every walker takes every step
+    on these graphs (no isolated vertices), so a run samples 80 n edges."""
+    out = {"workload": f"{n} walkers (one per vertex, start i % n) x 80 steps, -n {runs}",
+           "edges_per_run": 80 * n}
+    bins = {"reference": {"GT": os.path.join(ROOT, "oracle", "_ref", "rw_gt"),
+                          "LE": os.path.join(ROOT, "oracle", "_ref", "rw_le")},
+            "grass_b200": {m: os.path.join(ROOT, "grass_b200", "bin", "rw") for m in ("GT", "LE")}}
+    for who, exes in bins.items():
+        for m, exe in exes.items():
+            if not os.path.exists(exe):
+                out[f"{who}_{m}"] = {"unavailable": f"{exe} not built"}
+                continue
+            cmd = [exe, "-g", os.path.join(gdir, m), "-n", str(runs)]
+            if who == "grass_b200":
+                cmd += ["--mode", m]
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s)
+            t = None
+            for line in r.stdout.splitlines():
+                if line.startswith("runSamplingTime:"):
+                    t = float(line.split()[1])
+            res = {"rc": r.returncode, "runSamplingTime_s": t}
+            if t:
+                res["edges_per_s"] = 80 * n * runs / t
+            out[f"{who}_{m}"] = res
+    for m in ("GT", "LE"):
+        a, b = out.get(f"reference_{m}", {}), out.get(f"grass_b200_{m}", {})
+        if a.get("edges_per_s") and b.get("edges_per_s"):
+            out[f"speedup_{m}"] = b["edges_per_s"] / a["edges_per_s"]
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -843,12 +889,22 @@ def main():
                                                                            stream=stream),
                             args.steps, args.warmup, flush, dist, local)
             parity.decode(f"decode_{m}", os.path.join(gdir, m), m, rp_d, cl_d)
-            stream_bytes = infos[m]["graph_file_bytes"] + (n + 1) * 8
+            stream_bytes = infos[m]["device_bytes"] - 16 * n  # the resident stream
             out[f"decode_{m}"] = {
                 "value": sum_over_ranks(dist, E * args.steps, torch) / (tot / 1000.0),
                 "unit": "decoded edges/s", "ms_per_step": tot / args.steps,
-                "algorithmic_GBps": (stream_bytes + 4 * E + 8 * (n + 1)) / (tot / args.steps)
-                / 1e6}
+                "algorithmic_GBps": (stream_bytes + 16 * n + 4 * E + 8 * (n + 1))
+                / (tot / args.steps) / 1e6}
+        # LE sweep with its chunk slots staged through shared memory (cp.async.bulk)
+        for depth in (2, 4):
+            graphs["LE"].set_tuning(decode_stage_depth=depth)
+            ms, tot = timed(torch, lambda: graphs["LE"].decode_all_device(rp_d, cl_d,
+                                                                          stream=stream),
+                            args.steps, args.warmup, flush, dist, local)
+            parity.decode(f"decode_LE_staged{depth}", os.path.join(gdir, "LE"), "LE", rp_d, cl_d)
+            out[f"decode_LE_staged{depth}"] = {"ms_per_step": tot / args.steps,
+                                               "value": E * args.steps / (tot / 1000.0)}
+        graphs["LE"].set_tuning()
         del rp_d, cl_d
 
     clk = clocks.stop()
@@ -871,6 +927,10 @@ def main():
             extra["serve"] = serve_bench(G, bgraphs[args.mode])
         out["batched_jobs_and_serving"] = extra
         del bgraphs
+
+    # ---- the reference's own GPU rw app on this GPU: only when asked for
+    if ws == 1 and rank == 0 and "refgpu" in only:
+        out["reference_gpu"] = reference_gpu(gdir, n)
 
     # ---- skewed large graph (Chung-Lu, ~3B edges): only when asked for
     if ws == 1 and "cfg5" in only:

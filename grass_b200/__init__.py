@@ -69,7 +69,8 @@ class KhopParams(C.Structure):
 class Tuning(C.Structure):
     _fields_ = [("rw_depth", C.c_uint32), ("rw_threads", C.c_uint32),
                 ("rw_blocks_per_sm", C.c_uint32), ("l2_persist", C.c_uint32),
-                ("l2_fetch_bytes", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("l2_fetch_bytes", C.c_uint32), ("decode_stage_depth", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
 
 class MrwParams(C.Structure):
@@ -188,6 +189,7 @@ def _load():
         "grass_open_mem": ([P, u64, P, u64, i32, i32, PP], i32),
         "grass_close": ([P], i32),
         "grass_get_info": ([P, C.POINTER(GraphInfo)], i32),
+        "grass_check_device_error": ([P, P], i32),
         "grass_device_view": ([P, PP, P, PP], i32),
         "grass_set_tuning": ([P, C.POINTER(Tuning)], i32),
         "grass_get_tuning": ([P, C.POINTER(Tuning)], i32),
@@ -412,8 +414,9 @@ class Graph:
         return int(self.info()["n"])
 
     def set_tuning(self, rw_depth=0, rw_threads=0, rw_blocks_per_sm=0, l2_persist=0,
-                   l2_fetch_bytes=0):
-        t = Tuning(rw_depth, rw_threads, rw_blocks_per_sm, l2_persist, l2_fetch_bytes)
+                   l2_fetch_bytes=0, decode_stage_depth=0):
+        t = Tuning(rw_depth, rw_threads, rw_blocks_per_sm, l2_persist, l2_fetch_bytes,
+                   decode_stage_depth)
         _check(lib.grass_set_tuning(self._h, C.byref(t)))
 
     def tuning(self) -> dict:
@@ -478,6 +481,11 @@ class Graph:
         p = MrwParams(walkers, steps, select, 0, seed)
         _check(lib.grass_mrw(self._h, C.byref(p), _ptr(roots), S, _ptr(src), _ptr(dst),
                              _ptr(edge_count), _stream(stream)))
+
+    def check_device_error(self, stream=None):
+        """Wait for the stream, then raise GrassError if a device-pointer call
+        flagged an error on this graph (GRASS_E_DATA / GRASS_E_TIMEOUT)."""
+        _check(lib.grass_check_device_error(self._h, _stream(stream)))
 
     def decode_all_device(self, rowptr, cols, stream=None):
         _check(lib.grass_decode_all(self._h, _ptr(rowptr), _ptr(cols), _stream(stream)))

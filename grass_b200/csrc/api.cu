@@ -264,24 +264,73 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
   cudaFree(g->d_offsets);
   g->d_offsets = nullptr;
 
-  // LE: payloads with short chunks are rewritten in neighbor order (one span
-  // per draw, le_chunked); the rewrite goes to a copy, which replaces the
-  // on-disk order stream.
+  uint64_t words_alloc = alloc_words;
+  // LE: the device layout re-chunks every vertex into sector-sized slots
+  // (le_slot_pos, device_common.cuh), built from the decoded neighbor lists.
   if (mode == GRASS_MODE_LE) {
-    Nvtx nv("LE payloads to neighbor order");
-    uint32_t *d_re = nullptr;
-    GRASS_CUDA(cudaMalloc(&d_re, alloc_words * 4));
-    tmp.dev.push_back(d_re);
-    GRASS_CUDA(cudaMemcpyAsync(d_re, g->d_words, alloc_words * 4, cudaMemcpyDeviceToDevice, st));
-    launch_le_reorder(g->d_words, d_re, g->d_recs, (uint32_t)n, st);
+    Nvtx nv("LE device layout");
+    const uint64_t E = stats[0];
+    uint64_t *d_rp = nullptr;
+    uint32_t *d_cl = nullptr, *d_meta = nullptr, *d_fp = nullptr;
+    uint64_t *d_P = nullptr;
+    GRASS_CUDA(cudaMalloc(&d_rp, (n + 1) * sizeof(uint64_t)));
+    tmp.dev.push_back(d_rp);
+    GRASS_CUDA(cudaMalloc(&d_cl, std::max<uint64_t>(E, 1) * 4));
+    tmp.dev.push_back(d_cl);
+    GRASS_CUDA(cudaMalloc(&d_meta, n * 4));
+    tmp.dev.push_back(d_meta);
+    GRASS_CUDA(cudaMalloc(&d_fp, n * 4));
+    tmp.dev.push_back(d_fp);
+    GRASS_CUDA(cudaMalloc(&d_P, n * sizeof(uint64_t)));
+    tmp.dev.push_back(d_P);
+    launch_degrees64(g->view(), d_rp, st);
+    launch_scan_u64_inplace(d_rp, n, d_scan, st);
+    launch_le_disk_decode(g->d_words, g->d_recs, (uint32_t)n, d_rp, d_cl, st);
+    launch_le_choose(d_rp, d_cl, (uint32_t)n, d_meta, d_fp, st);
+    std::vector<uint32_t> meta(n);
+    std::vector<uint64_t> rp(n + 1), P(n, 0);
+    GRASS_CUDA(cudaMemcpyAsync(meta.data(), d_meta, n * 4, cudaMemcpyDeviceToHost, st));
+    GRASS_CUDA(cudaMemcpyAsync(rp.data(), d_rp, (n + 1) * 8, cudaMemcpyDeviceToHost, st));
     GRASS_CUDA(cudaStreamSynchronize(st));
     GRASS_CUDA(cudaGetLastError());
-    tmp.dev.back() = g->d_words;  // the on-disk order copy is freed with tmp
-    g->d_words = d_re;
+    // First fit in vertex order: a vertex whose slots fit in one sector goes
+    // at the current bit if it does not cross the sector end; a larger one
+    // starts on the next sector.
+    uint64_t pos = 0;
+    for (uint64_t v = 0; v < n; v++) {
+      const uint64_t d = rp[v + 1] - rp[v];
+      if (d < 2) continue;
+      const uint32_t m = meta[v];
+      const uint64_t T = m & 0xFFu, sw = ((m >> 8) & 0xFFu) + 1, K = (m >> 16) & 0xFFu,
+                     a = m >> 24;
+      const uint64_t cb = 2 * a + (T - 1) * sw, C = (d - 2) / T + 1;
+      if (C <= K) {
+        if ((pos & 255) + C * cb > 256) pos = (pos + 255) & ~255ull;
+      } else {
+        pos = (pos + 255) & ~255ull;
+      }
+      P[v] = pos;
+      pos += (C / K) * 256 + (C % K) * cb;
+    }
+    if (pos >= (1ull << 40))
+      return set_error(GRASS_E_FORMAT, "LE device layout needs %llu bits (limit 2^40)",
+                       (unsigned long long)pos);
+    const uint64_t nw = (pos + 31) / 32;
+    words_alloc = (nw + kGuardWords + 7) / 8 * 8;
+    uint32_t *d_led = nullptr;
+    GRASS_CUDA(cudaMalloc(&d_led, words_alloc * 4));
+    tmp.dev.push_back(d_led);
+    GRASS_CUDA(cudaMemsetAsync(d_led, 0, words_alloc * 4, st));
+    GRASS_CUDA(cudaMemcpyAsync(d_P, P.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
+    launch_le_write(d_rp, d_cl, (uint32_t)n, d_meta, d_fp, d_P, d_led, g->d_recs, st);
+    GRASS_CUDA(cudaStreamSynchronize(st));
+    GRASS_CUDA(cudaGetLastError());
+    tmp.dev.back() = g->d_words;  // the on-disk stream is freed with tmp
+    g->d_words = d_led;
+    g->n_words = nw;
   }
   // GT: the stream is rebuilt with a skip field every kGtSkip gaps of a block
   // (payloads only, new offsets in the records).
-  uint64_t words_alloc = alloc_words;
   if (mode == GRASS_MODE_GT) {
     Nvtx nv("GT stream with skip fields");
     unsigned char *d_cx = nullptr;
@@ -452,6 +501,13 @@ int grass_close(grass_graph *g) {
   return GRASS_OK;
 }
 
+int grass_check_device_error(grass_graph *g, void *stream) {
+  clear_error();
+  if (!g) return set_error(GRASS_E_ARG, "null graph");
+  DeviceGuard dg(g->device);
+  return read_err_flag(g, as_stream(stream));
+}
+
 int grass_get_info(const grass_graph *g, grass_graph_info *info) {
   if (!g || !info) return set_error(GRASS_E_ARG, "null argument");
   *info = g->info;
@@ -473,6 +529,8 @@ int grass_set_tuning(grass_graph *g, const grass_tuning *t) {
     return set_error(GRASS_E_ARG, "rw_depth must be 1, 2 or 4");
   if (t->rw_threads && (t->rw_threads % 32 || t->rw_threads > 512))
     return set_error(GRASS_E_ARG, "rw_threads must be a multiple of 32 up to 512");
+  if (t->decode_stage_depth != 0 && t->decode_stage_depth != 2 && t->decode_stage_depth != 4)
+    return set_error(GRASS_E_ARG, "decode_stage_depth must be 0, 2 or 4");
   DeviceGuard dg(g->device);
   if (int rc = apply_tuning(g->device, *t, g->d_recs, g->info.n * sizeof(uint4), g->l2win))
     return rc;

@@ -422,6 +422,18 @@ __device__ __forceinline__ uint32_t gt_neighbor(const DevGraph &g, const VHdr &h
   return acc + field_sum(g.words, p, r.gaps, h.b);
 }
 
+// On-disk geometry of an LE vertex of degree d >= 2: chunk_num, chunk_len, om
+// (decoder convention, LE/src/bcg.cuh:141-146).
+__device__ __forceinline__ void le_disk_geometry(uint32_t d, uint32_t &bn, uint32_t &bl,
+                                                 uint32_t &om) {
+  const uint32_t D = d - 1;
+  const uint32_t s = isqrt_u32(D);
+  const uint32_t o = D - s * s;
+  bn = s + (o > s ? 1u : 0u);
+  bl = D / bn;
+  om = D - bn * bl;
+}
+
 // LE header: BCGVertex ctor, LE/src/bcg.cuh:130-152.
 __device__ __forceinline__ VHdr le_header(const DevGraph &g, uint32_t v) {
   VHdr h;
@@ -445,126 +457,116 @@ __device__ __forceinline__ VHdr le_header(const DevGraph &g, uint32_t v) {
   h.b = (int)c.gamma();
   h.fp = c.gamma();
   h.P = c.pos(g.words);
-  const uint32_t D = h.d - 1;
-  const uint32_t s = isqrt_u32(D);
-  const uint32_t om = D - s * s;
-  h.bn = s + (om > s ? 1u : 0u);
-  h.bl = D / h.bn;
-  h.om = D - h.bn * h.bl;
+  le_disk_geometry(h.d, h.bn, h.bl, h.om);
   return h;
 }
 
 // ---- LE payload layout in HBM ----
-// On disk an LE payload holds all chunk_num + 1 rocks, then all seas in chunk
-// order (LE/chunk_compress/compressor.hpp:352-359), so a draw reads its rock
-// pair from one place and its sea from another: two random sectors.  At load,
-// every vertex whose longest chunk spans at most kLeChunkSpan bits is rewritten
-// in neighbor order, chunk by chunk:
-//   [rock 0][seas of chunk 0][rock 1][seas of chunk 1] ... [rock chunk_num]
-// The same fields with the same widths, permuted inside the vertex's own bit
-// range (P and the payload length do not change, nor does the footprint), so a
-// draw finds its left rock, its sea and its right rock in one contiguous span
-// of at most kLeChunkSpan bits: one sector, or two when the span crosses a
-// sector end.  Vertices with longer chunks (hubs) keep the on-disk order,
-// where the rock pair is adjacent and the sea is one more sector.  Whether a
-// vertex is rewritten follows from its header alone (le_chunked).
-#ifndef GRASS_LE_CHUNK_SPAN
-#define GRASS_LE_CHUNK_SPAN 256
-#endif
-constexpr uint32_t kLeChunkSpan = GRASS_LE_CHUNK_SPAN;
+// On disk an LE vertex is chunk_num ~ sqrt(d) chunks of ~sqrt(d) neighbors:
+// all rocks, then all seas (LE/chunk_compress/compressor.hpp:352-359), so a
+// draw reads its rock pair from one 32-byte sector and its sea from another,
+// and for hubs both sit thousands of bits apart.  At load every vertex of
+// degree >= 2 is re-chunked for the device with the same method -- a chunk
+// is a left rock |n - v|, signed seas n - (r1 + id ((r2 - r1) / L)), and a
+// right rock, rocks signed by first_pos -- but with a chunk length T of its
+// own (1..32) and self-contained slots that never cross a sector:
+//   slot c = [rock c (a bits)][seas id = 1..T-1 (sw bits each)][rock c+1 (a bits)]
+//   cb = 2a + (T - 1) sw bits; K = slots per sector (<= 63);
+//   slot c starts at P + (c / K) 256 + (c % K) cb.
+// Chunk c holds neighbors cT .. cT + L - 1 with L = min(T, d - 1 - cT); the
+// last neighbor d - 1 is the right rock of chunk C - 1, C = ceil((d-1)/T).  A
+// vertex whose slots fit in one sector is packed without alignment (and then
+// lies inside one sector); a larger one starts on a sector.  T is chosen per
+// vertex for the fewest bits.  A draw reads its record and one sector.  The
+// decoded neighbors are the file's, bit for bit; the rocks of inner chunk
+// boundaries are stored twice.
+//
+// LE record (16 B): x = P low 32 bits; y = P bits 32..39 | a << 8 |
+// sea_bit << 14 | T << 20 | K << 26; z = degree; w = first_pos (degree 1: the
+// neighbor).  In VHdr: b = sea_bit, bl = T, bn = C, om = K, cx = cb.
 
-__device__ __forceinline__ bool le_chunked(const VHdr &h) {
-  if (h.d < 2) return false;
-  const uint32_t seas = h.bl - (h.om ? 0u : 1u);  // seas of the longest chunk
-  return 2u * (uint32_t)h.a + seas * (uint32_t)(h.b + 1) <= kLeChunkSpan;
+__device__ __forceinline__ uint4 pack_le_record(uint64_t P, uint32_t a, uint32_t sb, uint32_t T,
+                                                uint32_t K, uint32_t d, uint32_t fp) {
+  return make_uint4((uint32_t)P,
+                    ((uint32_t)(P >> 32) & 0xFFu) | (a & 63u) << 8 | (sb & 63u) << 14 |
+                        (T & 63u) << 20 | (K & 63u) << 26,
+                    d, fp);
 }
 
-// Chunk c and index id of neighbor i, and the chunk's length tl
-// (LE/src/bcg.cuh:198-205).
+// Bit offset of slot c.
+__device__ __forceinline__ uint64_t le_slot_pos(const VHdr &h, uint32_t c) {
+  const uint32_t q = c / h.om;
+  return h.P + (uint64_t)q * 256u + (uint64_t)(c - q * h.om) * (uint32_t)h.cx;
+}
+
+// The w (1..33) bits at bit off of one sector, the field inside it.
+__device__ __forceinline__ uint64_t sec1_field(const Sec &A, uint32_t off, int w) {
+  const uint32_t k = off >> 6, s = off & 63u;
+  const uint64_t x = sec_word(A, k);
+  const uint64_t y = k < 3 ? sec_word(A, k + 1) : 0ull;
+  const uint64_t win = s ? (x << s) | (y >> (64 - s)) : x;
+  return win >> (64 - w);
+}
+
+// Chunk c and index id of neighbor i (id == L: the last neighbor, chunk C-1's
+// right rock), and the chunk's length L.
 __device__ __forceinline__ void le_locate(const VHdr &h, uint32_t i, uint32_t &c, uint32_t &id,
-                                          uint32_t &tl) {
-  tl = h.bl + 1;
-  const uint32_t split = h.om * tl;
-  const bool flag = i >= split;
-  const uint32_t j = flag ? i - split : i;
-  if (flag) tl -= 1;
-  c = j / tl;
-  id = j - c * tl;
-  if (flag) c += h.om;
+                                          uint32_t &L) {
+  const uint32_t last = h.d - 1;
+  c = i < last ? i / h.bl : h.bn - 1;
+  id = i - c * h.bl;
+  L = min(h.bl, last - c * h.bl);
 }
 
-// Bit offset of chunk c's left rock in the neighbor-order layout: c rocks and
-// c (chunk_len - 1) + min(c, om) seas precede it.
-__device__ __forceinline__ uint64_t le_chunk_pos(const VHdr &h, uint32_t c) {
-  return h.P + (uint64_t)c * (uint64_t)h.a +
-         ((uint64_t)(h.bl - 1) * c + min(h.om, c)) * (uint64_t)(h.b + 1);
-}
-
-// LE get_vertex, LE/src/bcg.cuh:195-261: two rocks and one signed sea, from
-// either layout.  A sea field is sea_bit magnitude bits and a sign bit; with
-// sea_bit = 32 (33-bit fields, vertex ids of 2^31 and more) the magnitude is
-// the field's top 32 bits, as LE/src/bcg.cuh:245-252 reads it.
-__device__ __forceinline__ uint32_t le_neighbor(const DevGraph &g, const VHdr &h, uint32_t i) {
-  if (h.d == 1) return h.fp;
-  uint32_t c, id, tl;
-  le_locate(h, i, c, id, tl);
-  const Sec zero{0, 0, 0, 0};
-  if (le_chunked(h)) {
-    // [rock c][seas of chunk c][rock c+1]: one sector, two when it crosses
-    const uint32_t sw = (uint32_t)h.b + 1u;
-    const uint64_t X = le_chunk_pos(h, c);
-    const uint32_t off = (uint32_t)X & 255u;
-    const uint32_t need = id ? 2u * (uint32_t)h.a + (tl - 1u) * sw : (uint32_t)h.a;
-    const Sec A = load_sector(g.words, X >> 8);
-    const Sec B = off + need > 256u ? load_sector(g.words, (X >> 8) + 1) : zero;
-    const uint32_t r1m = (uint32_t)sec2_field(A, B, off, h.a);
-    const uint32_t r1 = (c < h.fp) ? h.v - r1m : h.v + r1m;
-    if (id == 0) return r1;
-    const uint64_t raw = sec2_field(A, B, off + (uint32_t)h.a + (id - 1u) * sw, (int)sw);
-    const uint32_t r2m = (uint32_t)sec2_field(A, B, off + (uint32_t)h.a + (tl - 1u) * sw, h.a);
-    const uint32_t r2 = (c + 1 < h.fp) ? h.v - r2m : h.v + r2m;
-    const uint32_t mag = (uint32_t)(raw >> 1);
-    return ((r2 - r1) / tl) * id + r1 + ((raw & 1u) ? 0u - mag : mag);
-  }
-  // On-disk order.  Rocks c and c+1 (2a <= 64 bits) and the sea (b+1 <= 33
-  // bits) are read with one 32-byte sector load each, plus the next sector
-  // only when a field crosses a sector end; the sea's position depends only
-  // on the header, so both loads are in flight together.
-  const uint64_t rpos = h.P + (uint64_t)c * (uint64_t)h.a;
-  const uint64_t rsec = rpos >> 8;
-  const uint32_t roff = (uint32_t)rpos & 255u;
-  if (id == 0) {  // the chunk's left rock itself
-    const bool cross = roff + (uint32_t)h.a > 256u;
-    const Sec A = load_sector(g.words, rsec);
-    const Sec A2 = cross ? load_sector(g.words, rsec + 1) : zero;
-    const uint32_t r1m = (uint32_t)(sec_window(A, A2, roff) >> (64 - h.a));
-    return (c < h.fp) ? h.v - r1m : h.v + r1m;
-  }
-  const bool rcross = roff + 2u * (uint32_t)h.a > 256u;
-  const uint64_t spos =
-      h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a +
-      ((uint64_t)(h.bl - 1) * c + min(h.om, c) + id - 1) * (uint64_t)(h.b + 1);
-  const uint64_t ssec = spos >> 8;
-  const uint32_t soff = (uint32_t)spos & 255u;
-  const bool scross = soff + (uint32_t)h.b + 1u > 256u;
-  // seas follow the rocks, so ssec >= rsec; sectors already requested are reused
-  const bool s_is_a = ssec == rsec, s_is_a2 = rcross && ssec == rsec + 1;
-  const bool s2_is_a2 = rcross && s_is_a;
-  const Sec A = load_sector(g.words, rsec);
-  const Sec A2 = rcross ? load_sector(g.words, rsec + 1) : zero;
-  const Sec Bl = (s_is_a || s_is_a2) ? zero : load_sector(g.words, ssec);
-  const Sec B2l = (!scross || s2_is_a2) ? zero : load_sector(g.words, ssec + 1);
-  const Sec B = s_is_a ? A : s_is_a2 ? A2 : Bl;
-  const Sec B2 = s2_is_a2 ? A2 : B2l;
-  const uint64_t rwin = sec_window(A, A2, roff);
-  const uint32_t r1m = (uint32_t)(rwin >> (64 - h.a));
-  const uint32_t r1 = (c < h.fp) ? h.v - r1m : h.v + r1m;
-  const uint32_t r2m = (uint32_t)((rwin << h.a) >> (64 - h.a));
-  const uint32_t r2 = (c + 1 < h.fp) ? h.v - r2m : h.v + r2m;
-  const uint64_t raw = sec_window(B, B2, soff) >> (63 - h.b);
+// Neighbor id of a chunk slot held in sector A at bit offset off: the left
+// rock (id 0), the right rock (id == L), or r1 + ((r2 - r1) / L) id +/- sea
+// (LE/src/bcg.cuh:195-261; with sea_bit = 32 the 33-bit field keeps its
+// whole magnitude, as LE/src/bcg.cuh:245-252 reads it).
+__device__ __forceinline__ uint32_t le_slot_value(const Sec &A, uint32_t off, const VHdr &h,
+                                                  uint32_t c, uint32_t id, uint32_t L) {
+  const int sw = h.b + 1;
+  const uint32_t r1m = (uint32_t)sec1_field(A, off, h.a);
+  const uint32_t r1 = c < h.fp ? h.v - r1m : h.v + r1m;
+  if (id == 0) return r1;
+  const uint32_t r2m = (uint32_t)sec1_field(A, off + (uint32_t)h.a + (h.bl - 1) * (uint32_t)sw, h.a);
+  const uint32_t r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
+  if (id == L) return r2;
+  const uint64_t raw = sec1_field(A, off + (uint32_t)h.a + (id - 1) * (uint32_t)sw, sw);
   const uint32_t mag = (uint32_t)(raw >> 1);
   // (r2 - r1) >= 0 for sorted rows: unsigned division is the compressor's.
-  return ((r2 - r1) / tl) * id + r1 + ((raw & 1u) ? 0u - mag : mag);
+  return ((r2 - r1) / L) * id + r1 + ((raw & 1u) ? 0u - mag : mag);
+}
+
+// Every neighbor of chunk c, its slot at bit off of sector A, into o[0..L-1]
+// (and o[L], the right rock, for the last chunk): the rocks and the step once,
+// then the seas in order.
+__device__ __forceinline__ void le_slot_decode(const Sec &A, uint32_t off, const VHdr &h,
+                                               uint32_t c, uint32_t L, bool with_right,
+                                               uint32_t *o) {
+  const int sw = h.b + 1;
+  const uint32_t r1m = (uint32_t)sec1_field(A, off, h.a);
+  const uint32_t r1 = c < h.fp ? h.v - r1m : h.v + r1m;
+  const uint32_t s0 = off + (uint32_t)h.a;
+  const uint32_t r2m = (uint32_t)sec1_field(A, s0 + (h.bl - 1) * (uint32_t)sw, h.a);
+  const uint32_t r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
+  const uint32_t step = (r2 - r1) / L;
+  o[0] = r1;
+  for (uint32_t id = 1; id < L; id++) {
+    const uint64_t raw = sec1_field(A, s0 + (id - 1) * (uint32_t)sw, sw);
+    const uint32_t mag = (uint32_t)(raw >> 1);
+    o[id] = step * id + r1 + ((raw & 1u) ? 0u - mag : mag);
+  }
+  if (with_right) o[L] = r2;
+}
+
+// LE get_vertex: one sector load.
+__device__ __forceinline__ uint32_t le_neighbor(const DevGraph &g, const VHdr &h, uint32_t i) {
+  if (h.d == 1) return h.fp;
+  uint32_t c, id, L;
+  le_locate(h, i, c, id, L);
+  const uint64_t pos = le_slot_pos(h, c);
+  const Sec A = load_sector(g.words, pos >> 8);
+  return le_slot_value(A, (uint32_t)pos & 255u, h, c, id, L);
 }
 
 // Stream headers (gamma decode at offsets[v]); used at load time only.
@@ -609,17 +611,33 @@ __device__ __forceinline__ VHdr record_header(const uint4 r, uint32_t v) {
       h.bl = h.d / h.bn;
       h.om = h.d - h.bn * h.bl;
     }
-  } else if constexpr (MODE == 1) {
-    h.bn = h.bl = h.om = 0;
+  } else if constexpr (MODE == 1) {  // the device LE layout (le_slot_pos)
+    h.P = (uint64_t)r.x | ((uint64_t)(r.y & 0xFFu) << 32);
+    h.a = (int)((r.y >> 8) & 63u);
+    h.b = (int)((r.y >> 14) & 63u);
+    h.bl = (r.y >> 20) & 63u;  // T
+    h.om = (r.y >> 26) & 63u;  // K
     if (h.d > 1) {
-      const uint32_t D = h.d - 1;
-      const uint32_t s = isqrt_u32(D);
-      const uint32_t om = D - s * s;
-      h.bn = s + (om > s ? 1u : 0u);
-      h.bl = D / h.bn;
-      h.om = D - h.bn * h.bl;
+      h.bn = (h.d - 2) / h.bl + 1;  // C = ceil((d - 1) / T)
+      h.cx = 2 * h.a + (int)(h.bl - 1) * (h.b + 1);
     }
   }
+  return h;
+}
+
+// Header of an LE vertex from its load-time record (pack_record of the stream
+// header: on-disk geometry), before the device layout is built.
+__device__ __forceinline__ VHdr le_disk_record_header(const uint4 r, uint32_t v) {
+  VHdr h;
+  h.v = v;
+  h.P = (uint64_t)r.x | ((uint64_t)(r.y & 0xFFFFu) << 32);
+  h.a = (int)((r.y >> 16) & 63u);
+  h.b = (int)((r.y >> 22) & 63u);
+  h.d = r.z;
+  h.fp = r.w;
+  h.cx = 0;
+  h.bn = h.bl = h.om = 0;
+  if (h.d > 1) le_disk_geometry(h.d, h.bn, h.bl, h.om);
   return h;
 }
 
@@ -678,10 +696,10 @@ __device__ __forceinline__ uint32_t neighbor(const DevGraph &g, const VHdr &h, u
   else return load_cold_u32(g.cols + h.P + i);
 }
 
-// Number of bits a well-formed vertex occupies given its decoded header;
-// equals offsets[v+1] - offsets[v] for files written by the reference
-// compressor (GT/chunk_compress/compressor.hpp:297-349,
-// LE/chunk_compress/compressor.hpp:329-390).
+// End bit of a vertex's payload given its header: GT in the device layout
+// (or on disk, cx = 0); LE on disk (load-time validation).  For the files
+// the reference compressor writes this is offsets[v+1]
+// (GT/chunk_compress/compressor.hpp:297-349, LE/chunk_compress/compressor.hpp:329-390).
 template <int MODE>
 __device__ __forceinline__ uint64_t payload_end(const DevGraph &g, const VHdr &h) {
   if constexpr (MODE == 0) {

@@ -154,10 +154,18 @@ void launch_scan_u32(const uint32_t *counts, uint64_t n, uint64_t *out, uint64_t
 void launch_validate(const DevGraph &g, uint32_t *deg, unsigned long long *stats,
                      cudaStream_t s);
 void launch_build_records(const DevGraph &g, uint4 *recs, cudaStream_t s);
-// LE: dst (a copy of the stream src) gets the payload of every vertex that
-// le_chunked selects rewritten in neighbor order.
-void launch_le_reorder(const uint32_t *src, uint32_t *dst, const uint4 *recs, uint32_t n,
-                       cudaStream_t s);
+// LE device layout (le_slot_pos): pass 0 decodes the on-disk stream into a
+// CSR (rowptr = scanned degrees); pass 1 picks each vertex's chunk length,
+// sea_bit, slots per sector and rock width (meta) and first_pos (fpos); the
+// host places the vertices (P, bit offsets); pass 2 writes the slots into dst
+// (zeroed) and rewrites the records in place.
+void launch_le_disk_decode(const uint32_t *words, const uint4 *recs, uint32_t n,
+                           const uint64_t *rowptr, uint32_t *cols, cudaStream_t s);
+void launch_le_choose(const uint64_t *rowptr, const uint32_t *cols, uint32_t n, uint32_t *meta,
+                      uint32_t *fpos, cudaStream_t s);
+void launch_le_write(const uint64_t *rowptr, const uint32_t *cols, uint32_t n,
+                     const uint32_t *meta, const uint32_t *fpos, const uint64_t *P, uint32_t *dst,
+                     uint4 *recs, cudaStream_t s);
 // GT stream with skip fields: pass 1 measures every vertex's skip-field
 // extra width cx[v] and rebuilt payload length len[v] (bits); pass 2 writes
 // the payloads at newP[v] into dst (zeroed) and updates the records in place.

@@ -47,63 +47,6 @@ __device__ __forceinline__ VHdr shfl_hdr(const VHdr &h, int src) {
   return o;
 }
 
-// 64 stream bits starting at bit `off`: three word loads, two funnel shifts
-// (the sweep reads the stream in order, so these hit L1).
-__device__ __forceinline__ uint64_t read_bits64(const uint32_t *w, uint64_t off) {
-  const uint32_t *q = w + (off >> 5);
-  const uint32_t s = (uint32_t)off & 31u;
-  const uint32_t x0 = ldw(q), x1 = ldw(q + 1), x2 = ldw(q + 2);
-  return ((uint64_t)__funnelshift_l(x1, x0, s) << 32) | __funnelshift_l(x2, x1, s);
-}
-
-// le_neighbor (device_common.cuh) with word reads instead of sector loads:
-// the same arithmetic, LE/src/bcg.cuh:195-261, in either payload layout.
-__device__ __forceinline__ uint32_t le_neighbor_words(const uint32_t *words, const VHdr &h,
-                                                      uint32_t i) {
-  if (h.d == 1) return h.fp;
-  uint32_t c, id, tl;
-  le_locate(h, i, c, id, tl);
-  const uint64_t sw = (uint64_t)h.b + 1;
-  uint64_t r1pos, r2pos, spos;
-  if (le_chunked(h)) {  // [rock c][seas of chunk c][rock c+1]
-    r1pos = le_chunk_pos(h, c);
-    spos = r1pos + h.a + (uint64_t)(id ? id - 1 : 0) * sw;
-    r2pos = r1pos + h.a + (uint64_t)(tl - 1) * sw;
-  } else {  // all rocks, then all seas
-    r1pos = h.P + (uint64_t)c * (uint64_t)h.a;
-    r2pos = r1pos + h.a;
-    spos = h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a +
-           ((uint64_t)(h.bl - 1) * c + min(h.om, c) + (id ? id - 1 : 0)) * sw;
-  }
-  const uint32_t r1m = (uint32_t)(read_bits64(words, r1pos) >> (64 - h.a));
-  const uint32_t r1 = (c < h.fp) ? h.v - r1m : h.v + r1m;
-  if (id == 0) return r1;
-  const uint32_t r2m = (uint32_t)(read_bits64(words, r2pos) >> (64 - h.a));
-  const uint32_t r2 = (c + 1 < h.fp) ? h.v - r2m : h.v + r2m;
-  const uint64_t raw = read_bits64(words, spos) >> (64 - sw);
-  const uint32_t mag = (uint32_t)(raw >> 1);
-  return ((r2 - r1) / tl) * id + r1 + ((raw & 1u) ? 0u - mag : mag);
-}
-
-// The next sea of a cursor (sw = sea_bit + 1 bits: magnitude, then sign;
-// sw = 33 keeps the whole 32-bit magnitude, LE/src/bcg.cuh:245-252) added to
-// its interpolated position base.
-template <class Cur>
-__device__ __forceinline__ uint32_t le_sea(Cur &cur, int sw, uint32_t base) {
-  uint32_t mag, neg;
-  if (sw > 32) {
-    const uint32_t top = cur.get(1);
-    const uint32_t rest = cur.get(32);
-    mag = (top << 31) | (rest >> 1);
-    neg = rest & 1u;
-  } else {
-    const uint32_t raw = cur.get(sw);
-    mag = raw >> 1;
-    neg = raw & 1u;
-  }
-  return base + (neg ? 0u - mag : mag);
-}
-
 // Largest v in [0, n) with rowptr[v] <= x, for x < rowptr[n].
 __device__ __forceinline__ uint32_t warp_row_of(const uint64_t *rowptr, uint32_t n, uint64_t x) {
   const int lane = threadIdx.x & 31;
@@ -224,7 +167,7 @@ __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint6
       const uint32_t i = (uint32_t)(gl - startv);
       uint32_t val = 0;
       if (MODE == 1) {
-        if (act) val = le_neighbor_words(g.words, hk, i);
+        if (act) val = le_neighbor(g, hk, i);
       } else {
         bool head = true;
         uint32_t x = 0;
@@ -302,68 +245,30 @@ constexpr uint32_t kRange = GRASS_DECODE_RANGE;  // neighbors per range item
 // Sequential decoders of one vertex (one lane each), from neighbor 0.
 struct LeSeq {
   const uint32_t *w;
-  uint64_t P;
-  uint32_t v, fp, bl, om, bn, c, id, tl, r1, r2, step;
-  int a, sw;     // rock width, sea width (magnitude + sign)
-  bool one;      // degree 1: the neighbor is stored in the header
-  bool chunked;  // neighbor-order payload (le_chunked): cur reads every field
-  BitCur cur;    // on-disk order: the seas
+  VHdr h;
+  uint32_t c, id, L;  // chunk, index in it, its length
+  uint32_t off;       // bit offset of the chunk's slot in sector A
+  Sec A;
 
-  __device__ __forceinline__ uint32_t signed_rock(uint32_t m, uint32_t k) const {
-    return k < fp ? v - m : v + m;
+  __device__ __forceinline__ void load_chunk() {
+    const uint64_t pos = le_slot_pos(h, c);
+    A = load_sector(w, pos >> 8);
+    off = (uint32_t)pos & 255u;
+    L = min(h.bl, h.d - 1 - c * h.bl);
   }
-  __device__ __forceinline__ void init(const uint32_t *words, const VHdr &h) {
+  __device__ __forceinline__ void init(const uint32_t *words, const VHdr &hd) {
     w = words;
-    P = h.P;
-    v = h.v;
-    fp = h.fp;
-    one = h.d == 1;
-    if (one) return;
-    bl = h.bl;
-    om = h.om;
-    bn = h.bn;
-    a = h.a;
-    sw = h.b + 1;
-    c = 0;
-    id = 0;
-    tl = om ? bl + 1 : bl;
-    chunked = le_chunked(h);
-    if (chunked) {
-      cur.init(w, P);
-    } else {
-      r1 = signed_rock(read_field(w, P, a), 0);
-      r2 = signed_rock(read_field(w, P + (uint64_t)a, a), 1);
-      step = (r2 - r1) / tl;
-      cur.init(w, P + (uint64_t)(bn + 1) * (uint64_t)a);
-    }
+    h = hd;
+    c = id = 0;
+    if (h.d > 1) load_chunk();
   }
   __device__ __forceinline__ uint32_t next() {
-    if (one) return fp;
-    uint32_t val;
-    if (id == 0) {
-      if (chunked) {  // this chunk's rock, then a look-ahead to the next one
-        r1 = signed_rock(cur.get(a), c);
-        if (c < bn) {
-          const uint64_t at = cur.pos(w) + (uint64_t)(tl - 1) * (uint64_t)sw;
-          r2 = signed_rock(read_field(w, at, a), c + 1);
-          step = (r2 - r1) / tl;
-        }
-      }
-      val = r1;
-    } else {
-      val = le_sea(cur, sw, step * id + r1);
-    }
-    if (++id == tl) {
+    if (h.d == 1) return h.fp;
+    const uint32_t val = le_slot_value(A, off, h, c, id, L);
+    if (++id == L && c + 1 < h.bn) {  // the next chunk's left rock is this one's right rock
       c++;
       id = 0;
-      tl = c < om ? bl + 1 : bl;
-      if (!chunked) {
-        r1 = r2;
-        if (c < bn) {
-          r2 = signed_rock(read_field(w, P + (uint64_t)(c + 1) * (uint64_t)a, a), c + 1);
-          step = (r2 - r1) / tl;
-        }
-      }
+      load_chunk();
     }
     return val;
   }
@@ -517,33 +422,31 @@ __device__ __forceinline__ void prefetch_bits(const uint32_t *words, uint64_t lo
 constexpr uint32_t kRun = GRASS_DECODE_RUN;
 static_assert(kRun % 4 == 0 && kRun <= 32, "run length");
 
-// ---- sea staging (LE ranges) ----
-// With GRASS_DECODE_STAGE, lane 0 of a warp copies the stream bytes that hold
-// a range's seas into the warp's shared-memory buffer with one bulk copy
-// (cp.async.bulk, completion counted on an mbarrier), and the lanes' sea
-// cursors read shared memory instead of global memory.  Rocks stay on the
-// global path (a few words per chunk, L1-resident).  Measured on R-MAT s22
-// ef32 (LE sweep): a 3 KB buffer per warp, with longer ranges read from
-// global memory, 1.798 ms against 1.798 ms unstaged on the same GPU; a buffer
-// for a whole range (8.5 KB per warp) 2.03 ms against 1.71 ms, from the lost
-// occupancy.  The sweep is bound by instruction issue, not by its loads.
-#ifndef GRASS_DECODE_STAGE
-#define GRASS_DECODE_STAGE 1
-#endif
-constexpr int kDecodeWarps = 8;  // warps per decode_range_kernel block
-#if GRASS_DECODE_STAGE
-// Seas of a full range (<= kRange + 1 fields of <= 33 bits), plus 16 bytes
-// of alignment at each end and 16 of cursor look-ahead.
-#ifndef GRASS_DECODE_STAGE_BYTES
-#define GRASS_DECODE_STAGE_BYTES 3072u
-#endif
-// Ranges whose seas need more than kStageBytes read them from global memory.
-constexpr uint32_t kStageBytes = GRASS_DECODE_STAGE_BYTES;
-static_assert(kStageBytes % 16 == 0, "stage buffer size");
-constexpr uint32_t kStageSmem = kDecodeWarps * (kStageBytes + 16u);
+// ---- slot staging for the LE range sweep ----
+// With a staging depth D (2 or 4), lane 0 of a warp copies the sectors that
+// hold each group of 32 chunk slots into one of the warp's D shared-memory
+// buffers with one bulk copy (cp.async.bulk, completion counted on that
+// buffer's mbarrier), D - 1 groups ahead of the group being decoded, and the
+// lanes read their slots from shared memory.  Every wait is bounded: a copy
+// that has not landed after kStagePolls polls is reported (error word bit 2,
+// GRASS_E_TIMEOUT) and the warp decodes from global memory from then on,
+// waiting once more, bounded, for its copies in flight before it exits.
+constexpr int kDecodeWarps = 8;          // warps per LE range block
+constexpr uint32_t kGroupBytes = 1024;   // 32 slots lie in at most 32 sectors
+constexpr uint32_t kOutWords = 32 * 33;  // a group's neighbors (32 chunks of <= 32, + 1)
 // Polls of the copy's mbarrier before the warp gives up (far beyond the
 // microseconds one copy takes).
-constexpr uint32_t kStagePolls = 1u << 22;
+#ifndef GRASS_STAGE_POLLS
+#define GRASS_STAGE_POLLS (1u << 22)
+#endif
+constexpr uint32_t kStagePolls = GRASS_STAGE_POLLS;
+// Test hook, off in the library: with GRASS_STAGE_NEVER_COPY the barrier is
+// armed for the copy's bytes but no copy is issued, so the phase never
+// completes and every wait runs out -- the timeout path is exercised with
+// nothing in flight.
+#ifndef GRASS_STAGE_NEVER_COPY
+#define GRASS_STAGE_NEVER_COPY 0
+#endif
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -563,6 +466,7 @@ __device__ __forceinline__ void stage_copy(void *dst, const void *src, uint32_t 
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
                "r"(bytes)
                : "memory");
+  if (GRASS_STAGE_NEVER_COPY) return;
   asm volatile(
       "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
           smem_u32(dst)),
@@ -585,107 +489,147 @@ __device__ __forceinline__ bool stage_wait(uint64_t *bar, uint32_t parity) {
   return false;
 }
 
-// BitCur over words addressed generically (shared or global memory).
-struct GenCur {
-  const uint32_t *p;
-  uint64_t buf;
-  int nb;
-  __device__ __forceinline__ void init(const uint32_t *w, uint64_t off) {
-    const uint32_t *q = w + (off >> 5);
-    const uint32_t s = (uint32_t)off & 31u;
-    buf = (((uint64_t)q[0] << 32) | q[1]) << s;
-    nb = 64 - (int)s;
-    p = q + 2;
-  }
-  __device__ __forceinline__ uint32_t get(int width) {
-    if (nb <= 32) {
-      buf |= (uint64_t)(*p) << (32 - nb);
-      p++;
-      nb += 32;
-    }
-    const uint32_t v = (uint32_t)(buf >> (64 - width));
-    buf <<= width;
-    nb -= width;
-    return v;
+// A 32-byte sector from shared memory, in stream order.
+__device__ __forceinline__ Sec smem_sector(const void *p) {
+  const uint64_t *q = static_cast<const uint64_t *>(p);
+  return Sec{swap_halves(q[0]), swap_halves(q[1]), swap_halves(q[2]), swap_halves(q[3])};
+}
+
+// Shared memory of one LE range warp: the group's decoded neighbors, then
+// DEPTH staging buffers and their barriers.
+template <int DEPTH>
+struct LeWarpSmem {
+  static constexpr uint32_t bytes() {
+    return kOutWords * 4 + DEPTH * kGroupBytes + (DEPTH ? DEPTH : 1) * 8;
   }
 };
-#endif  // GRASS_DECODE_STAGE
 
-template <int MODE>
-__global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uint64_t *rowptr,
-                                                             uint32_t *cols,
-                                                             const uint4 *__restrict__ items,
-                                                             uint64_t nitems, bool vec,
-                                                             unsigned int *err) {
+// LE range sweep on the device layout: one lane per chunk slot.  A warp takes
+// a range's chunks 32 at a time: each lane reads its slot (one 32-byte
+// sector, coalesced across the warp, or from the staged group), decodes the
+// chunk's neighbors into shared memory, and the warp writes the group's
+// neighbors to the CSR with coalesced stores.  DEPTH 0: slots from global
+// memory; 2 or 4: staged (see above).
+template <int DEPTH>
+__global__ void __launch_bounds__(256) decode_le_range_kernel(DevGraph g, const uint64_t *rowptr,
+                                                              uint32_t *cols,
+                                                              const uint4 *__restrict__ items,
+                                                              uint64_t nitems,
+                                                              unsigned int *err) {
+  extern __shared__ __align__(128) unsigned char le_smem[];
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned char *mine = le_smem + (threadIdx.x >> 5) * LeWarpSmem<DEPTH>::bytes();
+  uint32_t *out = reinterpret_cast<uint32_t *>(mine);
+  unsigned char *stage = mine + kOutWords * 4;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(stage + DEPTH * kGroupBytes);
+  uint32_t phase = 0;    // bit b: parity of buffer b's next completion
+  uint32_t pending = 0;  // bit b: buffer b has a copy issued and not yet waited for
+  bool stage_ok = DEPTH > 0;
+  if (DEPTH && lane < DEPTH) stage_bar_init(bars + lane);
+  __syncwarp();
+  bool bad = false;
+  for (uint64_t t = warp; t < nitems; t += nwarps) {
+    const uint4 it = items[t];
+    const VHdr h = header<1>(g, it.x);
+    const uint64_t base = rowptr[it.x];
+    const uint32_t T = h.bl, last = h.d - 1, i0 = it.y, i1 = it.z;
+    const uint32_t c0 = i0 < last ? i0 / T : h.bn - 1;
+    const uint32_t c1 = i1 - 1 < last ? (i1 - 1) / T : h.bn - 1;
+    const uint32_t ngroups = (c1 - c0) / 32 + 1;
+    // sectors [qa, qb] of group j's slots
+    auto group_sectors = [&](uint32_t j, uint64_t &qa, uint64_t &qb) {
+      const uint32_t ca = c0 + 32 * j, cz = min(c1, ca + 31);
+      qa = le_slot_pos(h, ca) >> 8;
+      qb = le_slot_pos(h, cz) >> 8;
+    };
+    auto issue = [&](uint32_t j) {
+      if (!DEPTH || !stage_ok) return;
+      const uint32_t b = j % (DEPTH ? DEPTH : 1);
+      uint64_t qa, qb;
+      group_sectors(j, qa, qb);
+      if (lane == 0)
+        stage_copy(stage + b * kGroupBytes, g.words + qa * 8, (uint32_t)(qb - qa + 1) * 32u,
+                   bars + b);
+      pending |= 1u << b;
+    };
+    if constexpr (DEPTH > 0)
+      for (uint32_t j = 0; j + 1 < (uint32_t)DEPTH && j < ngroups; j++) issue(j);
+    for (uint32_t j = 0; j < ngroups; j++) {  // warp-uniform
+      if (DEPTH && j + DEPTH - 1 < ngroups) issue(j + DEPTH - 1);
+      bool staged = false;
+      const uint32_t b = DEPTH ? j % DEPTH : 0;
+      if (DEPTH && stage_ok) {
+        if (__all_sync(FULL, stage_wait(bars + b, (phase >> b) & 1u))) {
+          phase ^= 1u << b;
+          pending &= ~(1u << b);
+          staged = true;
+        } else {  // the copy did not land in time: report, go on from global memory
+          if (lane == 0 && err) atomicOr(err, 2u);
+          stage_ok = false;
+        }
+      }
+      const uint32_t cg = c0 + 32 * j, c = cg + lane;
+      if (c <= c1) {
+        const uint64_t pos = le_slot_pos(h, c);
+        Sec A;
+        if (staged) {
+          uint64_t qa, qb;
+          group_sectors(j, qa, qb);
+          A = smem_sector(stage + b * kGroupBytes + ((pos >> 8) - qa) * 32u);
+        } else {
+          A = load_sector(g.words, pos >> 8);
+        }
+        // the last chunk also holds neighbor d-1, its right rock
+        le_slot_decode(A, (uint32_t)pos & 255u, h, c, min(T, last - c * T), c + 1 == h.bn,
+                       out + (c - cg) * T);
+      }
+      __syncwarp();
+      const uint32_t nb0 = cg * T, nhi = cg + 32 >= h.bn ? last + 1 : (cg + 32) * T;
+      const uint32_t lo = max(i0, nb0), hi = min(i1, nhi);
+      for (uint32_t k = lo + lane; k < hi; k += 32) {
+        const uint32_t val = out[k - nb0];
+        bad |= val >= g.n;
+        cols[base + k] = val;
+      }
+      __syncwarp();  // the group's buffers are free for the next group
+    }
+  }
+  if (DEPTH)  // copies still in flight after a timeout: one more bounded wait each
+    for (int b = 0; b < DEPTH; b++)
+      if ((pending >> b) & 1u) stage_wait(bars + b, (phase >> b) & 1u);
+  if (bad && err) atomicOr(err, 1u);
+}
+
+// GT range sweep: lane l of a warp takes run l of each group of 32 runs of
+// kRun slots, reads its fields in order with a bit cursor, and a segmented
+// warp scan carries values across runs (a run that starts inside a block
+// continues from the slot before it).
+__global__ void __launch_bounds__(256) decode_gt_range_kernel(DevGraph g, const uint64_t *rowptr,
+                                                              uint32_t *cols,
+                                                              const uint4 *__restrict__ items,
+                                                              uint64_t nitems, bool vec,
+                                                              unsigned int *err) {
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   bool bad = false;
-#if GRASS_DECODE_STAGE
-  extern __shared__ __align__(128) unsigned char stage_smem[];
-  uint32_t *stage = reinterpret_cast<uint32_t *>(stage_smem + (threadIdx.x >> 5) * kStageBytes);
-  uint64_t *bar =
-      reinterpret_cast<uint64_t *>(stage_smem + kDecodeWarps * kStageBytes) + (threadIdx.x >> 5);
-  if (MODE == 1 && lane == 0) stage_bar_init(bar);
-  __syncwarp();
-  uint32_t parity = 0;
-#endif
   for (uint64_t t = warp; t < nitems; t += nwarps) {
     const uint4 it = items[t];
-    const VHdr h = header<MODE>(g, it.x);
+    const VHdr h = header<0>(g, it.x);
     const uint64_t base = rowptr[it.x];
     const uint64_t G0 = base + it.y, G1 = base + it.z;  // CSR slots of the range
-    const uint64_t sea0 = h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a;
     const uint32_t split = h.om * (h.bl + 1);
-    const int sw = h.b + 1;
-    const bool chunked = MODE == 1 && le_chunked(h);  // neighbor-order LE payload
-    bool staged = false;  // the range's seas are in the warp's shared buffer
-#if GRASS_DECODE_STAGE
-    const uint32_t *sbuf = g.words;  // sea cursor words, and the stream bit of sbuf[0]
-    uint64_t sbase = 0;
-#endif
     {  // ask L2 for the range's stream bits (read in order below), within the payload
       const uint32_t i0 = it.y, i1 = it.z;
-      const uint64_t pend = payload_end<MODE>(g, h);
+      const uint64_t pend = payload_end<0>(g, h);
       const uint32_t c0 = i0 < split ? i0 / (h.bl + 1) : h.om + (i0 - split) / max(h.bl, 1u);
       const uint64_t cl = c0 + (i1 - i0) / max(h.bl, 1u) + 2;
-      if (chunked) {  // the range's fields are contiguous
-        prefetch_bits(g.words, le_chunk_pos(h, c0),
-                      min(pend, le_chunk_pos(h, (uint32_t)min(cl, (uint64_t)h.bn)) + h.a));
-      } else if (MODE == 1) {
-        prefetch_bits(g.words, h.P + (uint64_t)c0 * h.a,
-                      min(pend, h.P + min(cl, (uint64_t)h.bn + 1) * h.a));
-        const uint64_t lo = sea0 + (uint64_t)(i0 > c0 ? i0 - c0 - 1 : 0) * sw;
-        const uint64_t hi = min(pend, sea0 + (uint64_t)i1 * sw);
-#if GRASS_DECODE_STAGE
-        // the seas [lo, hi) in whole 16-byte units, plus 16 bytes the
-        // cursors may read ahead (inside the stream's zero guard)
-        const uint64_t b0 = (lo >> 3) & ~(uint64_t)15;
-        const uint64_t b1 = ((((hi + 7) >> 3) + 16) + 15) & ~(uint64_t)15;
-        staged = hi > lo && b1 - b0 <= kStageBytes;
-        if (staged) {
-          __syncwarp();  // every lane is done with the previous range's seas
-          if (lane == 0)
-            stage_copy(stage, reinterpret_cast<const char *>(g.words) + b0, (uint32_t)(b1 - b0),
-                       bar);
-          const bool ok = __all_sync(FULL, stage_wait(bar, parity));
-          parity ^= 1u;
-          if (!ok) {  // the copy did not land: report, wait once more, stop
-            if (lane == 0 && err) atomicOr(err, 2u);
-            stage_wait(bar, parity ^ 1u);
-            return;
-          }
-          sbuf = stage;
-          sbase = b0 * 8;
-        }
-#endif
-        if (!staged) prefetch_bits(g.words, lo, hi);
-      } else {
-        prefetch_bits(g.words, gt_block_pos(h, c0),
-                      min(pend, gt_block_pos(h, (uint32_t)min(cl, (uint64_t)h.bn))));
-      }
+      prefetch_bits(g.words, gt_block_pos(h, c0),
+                    min(pend, gt_block_pos(h, (uint32_t)min(cl, (uint64_t)h.bn))));
     }
-    uint32_t carry = 0;  // GT: value of the slot before the current group
+    uint32_t carry = 0;  // value of the slot before the current group
     bool carry_ok = false;
     for (uint64_t gs = G0 & ~(uint64_t)(kRun - 1); gs < G1; gs += 32 * kRun) {
       const uint64_t rs = gs + (uint64_t)lane * kRun;  // this lane's run [rs, rs + 8)
@@ -693,174 +637,89 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
       const uint32_t cnt = a1 > a0 ? (uint32_t)(a1 - a0) : 0u;
       const uint32_t s = cnt ? (uint32_t)(a0 - base) : it.y;  // first neighbor of the run
       uint32_t vals[kRun];
-      // chunk / block c of neighbor s, index id within it, length tl
+      // block c of neighbor s, index id within it, length tl
       const bool hi = s < split;
       uint32_t tl = hi ? h.bl + 1 : h.bl;
       const uint32_t j = hi ? s : s - split;
       uint32_t c = tl ? j / tl : 0u;
       uint32_t id = j - c * tl;
       if (!hi) c += h.om;
-      if (chunked) {
-        // neighbor order: the cursor reads every field (rock c, its seas,
-        // rock c+1, ...); each chunk's right rock is a look-ahead read
-        uint32_t r1 = 0, r2 = 0, step = 0;
-        BitCur cur;
-        if (cnt) {
-          const uint64_t X = le_chunk_pos(h, c);
-          if (id) {
-            const uint32_t r1m = read_field(g.words, X, h.a);
-            r1 = c < h.fp ? h.v - r1m : h.v + r1m;
-            const uint32_t r2m =
-                read_field(g.words, X + h.a + (uint64_t)(tl - 1) * (uint64_t)sw, h.a);
-            r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
-            step = (r2 - r1) / tl;
-            cur.init(g.words, X + h.a + (uint64_t)(id - 1) * (uint64_t)sw);
-          } else {
-            cur.init(g.words, X);
-          }
-        }
-#pragma unroll
-        for (uint32_t k = 0; k < kRun; k++) {
-          if (k >= cnt) break;
-          uint32_t val;
-          if (id == 0) {
-            const uint32_t r1m = cur.get(h.a);
-            r1 = c < h.fp ? h.v - r1m : h.v + r1m;
-            if (c < h.bn) {
-              const uint64_t at = cur.pos(g.words) + (uint64_t)(tl - 1) * (uint64_t)sw;
-              const uint32_t r2m = read_field(g.words, at, h.a);
-              r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
-              step = (r2 - r1) / tl;
-            }
-            val = r1;
-          } else {
-            val = le_sea(cur, sw, step * id + r1);
-          }
-          vals[k] = val;
-          if (++id == tl) {
-            c++;
-            id = 0;
-            tl = c < h.om ? h.bl + 1 : h.bl;
-          }
-        }
-      } else if (MODE == 1) {
-        uint32_t r1 = 0, r2 = 0, step = 0;
-#if GRASS_DECODE_STAGE
-        GenCur sea;
-#else
-        BitCur sea;
-#endif
-        if (cnt) {
-          const uint64_t rw = read_bits64(g.words, h.P + (uint64_t)c * (uint64_t)h.a);
-          const uint32_t r1m = (uint32_t)(rw >> (64 - h.a));
-          r1 = c < h.fp ? h.v - r1m : h.v + r1m;
-          if (c < h.bn) {
-            const uint32_t r2m = (uint32_t)((rw << h.a) >> (64 - h.a));
-            r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
-            step = (r2 - r1) / tl;
-          }
-          // next sea in neighbor order: index s - c - 1 (id > 0) or s - c (id == 0)
-#if GRASS_DECODE_STAGE
-          sea.init(sbuf, sea0 + (uint64_t)(s - c - (id ? 1u : 0u)) * (uint64_t)sw - sbase);
-#else
-          sea.init(g.words, sea0 + (uint64_t)(s - c - (id ? 1u : 0u)) * (uint64_t)sw);
-#endif
-        }
-#pragma unroll
-        for (uint32_t k = 0; k < kRun; k++) {
-          if (k >= cnt) break;
-          const uint32_t val = id == 0 ? r1 : le_sea(sea, sw, step * id + r1);
-          vals[k] = val;
-          if (++id == tl) {  // next chunk: its left rock is this chunk's right rock
-            c++;
-            id = 0;
-            tl = c < h.om ? h.bl + 1 : h.bl;
-            r1 = r2;
-            if (c < h.bn) {
-              const uint32_t r2m = read_field(g.words, h.P + (uint64_t)(c + 1) * h.a, h.a);
-              r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
-              step = (r2 - r1) / tl;
-            }
-          }
-        }
-      } else {
-        // Fields in order: block c holds its head (a bits), then tl - 1 gaps,
-        // with a skip field (an absolute value relative to the head) at every
-        // kGtSkip-th position.  Slots before the run's first head or skip field
-        // are relative to the slot before the run, whose value a segmented
-        // warp scan over the runs supplies.
-        BitCur cur;
-        const int sk = h.b + h.cx;  // skip-field width
-        uint64_t hp = 0;            // bit offset of block c
-        if (cnt) {
-          hp = gt_block_pos(h, c);
-          cur.init(g.words, id ? gt_field_pos(h, hp, id) : hp);
-        }
-        uint32_t x = 0, rel = 0;  // rel: bit k set when slot k is relative
-        bool seen = false;         // an absolute value has been read in this run
-        uint32_t hv0 = 0;          // head value of block c, once known
-        bool hk = false;
-#pragma unroll
-        for (uint32_t k = 0; k < kRun; k++) {
-          if (k >= cnt) break;
-          if (id == 0) {
-            const uint32_t hv = (h.a ? cur.get(h.a) : 0u) + 1u;
-            x = hv0 = c >= h.fp ? h.v + hv : h.v - hv;
-            hk = seen = true;
-          } else if (id % kGtSkip == 0) {
-            if (!hk) {  // the run started inside the block: read its head
-              const uint32_t hv = read_field(g.words, hp, h.a) + 1u;
-              hv0 = c >= h.fp ? h.v + hv : h.v - hv;
-              hk = true;
-            }
-            x = hv0 + id + (sk ? cur.get(sk) : 0u);
-            seen = true;
-          } else {
-            x += (h.b ? cur.get(h.b) : 0u) + 1u;
-            if (!seen) rel |= 1u << k;
-          }
-          vals[k] = x;
-          if (++id == tl) {
-            c++;
-            id = 0;
-            tl = c < h.om ? h.bl + 1 : h.bl;
-          }
-        }
-        // (absolute?, last value) of runs 0..lane; empty runs are the identity
-        uint32_t sx = cnt ? x : 0u;
-        bool sf = cnt && seen;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const uint32_t y = __shfl_up_sync(FULL, sx, o);
-          const bool f = __shfl_up_sync(FULL, (int)sf, o);
-          if (lane >= o && !sf) {
-            sx += y;
-            sf = f;
-          }
-        }
-        uint32_t bx = __shfl_up_sync(FULL, sx, 1);
-        bool bf = __shfl_up_sync(FULL, (int)sf, 1);
-        if (lane == 0) {
-          bx = 0;
-          bf = false;
-        }
-        if (!carry_ok) {  // first group: the slot before G0 (used when G0 is inside a block)
-          uint32_t y = 0;
-          if (lane == 0 && it.y > 0) y = gt_neighbor(g, h, it.y - 1);
-          carry = __shfl_sync(FULL, y, 0);
-          carry_ok = true;
-        }
-        const uint32_t in = bf ? bx : carry + bx;  // value of the slot before the run
-#pragma unroll
-        for (uint32_t k = 0; k < kRun; k++)
-          if ((rel >> k) & 1u) vals[k] += in;
-        const unsigned has = __ballot_sync(FULL, cnt > 0);
-        uint32_t lastv = 0;
-#pragma unroll
-        for (uint32_t k = 0; k < kRun; k++)
-          if (k + 1 == cnt) lastv = vals[k];
-        carry = __shfl_sync(FULL, lastv, 31 - __clz(has));
+      // Fields in order: block c holds its head (a bits), then tl - 1 gaps,
+      // with a skip field (an absolute value relative to the head) at every
+      // kGtSkip-th position.  Slots before the run's first head or skip field
+      // are relative to the slot before the run, whose value a segmented
+      // warp scan over the runs supplies.
+      BitCur cur;
+      const int sk = h.b + h.cx;  // skip-field width
+      uint64_t hp = 0;            // bit offset of block c
+      if (cnt) {
+        hp = gt_block_pos(h, c);
+        cur.init(g.words, id ? gt_field_pos(h, hp, id) : hp);
       }
+      uint32_t x = 0, rel = 0;  // rel: bit k set when slot k is relative
+      bool seen = false;         // an absolute value has been read in this run
+      uint32_t hv0 = 0;          // head value of block c, once known
+      bool hk = false;
+#pragma unroll
+      for (uint32_t k = 0; k < kRun; k++) {
+        if (k >= cnt) break;
+        if (id == 0) {
+          const uint32_t hv = (h.a ? cur.get(h.a) : 0u) + 1u;
+          x = hv0 = c >= h.fp ? h.v + hv : h.v - hv;
+          hk = seen = true;
+        } else if (id % kGtSkip == 0) {
+          if (!hk) {  // the run started inside the block: read its head
+            const uint32_t hv = read_field(g.words, hp, h.a) + 1u;
+            hv0 = c >= h.fp ? h.v + hv : h.v - hv;
+            hk = true;
+          }
+          x = hv0 + id + (sk ? cur.get(sk) : 0u);
+          seen = true;
+        } else {
+          x += (h.b ? cur.get(h.b) : 0u) + 1u;
+          if (!seen) rel |= 1u << k;
+        }
+        vals[k] = x;
+        if (++id == tl) {
+          c++;
+          id = 0;
+          tl = c < h.om ? h.bl + 1 : h.bl;
+        }
+      }
+      // (absolute?, last value) of runs 0..lane; empty runs are the identity
+      uint32_t sx = cnt ? x : 0u;
+      bool sf = cnt && seen;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL, sx, o);
+        const bool f = __shfl_up_sync(FULL, (int)sf, o);
+        if (lane >= o && !sf) {
+          sx += y;
+          sf = f;
+        }
+      }
+      uint32_t bx = __shfl_up_sync(FULL, sx, 1);
+      bool bf = __shfl_up_sync(FULL, (int)sf, 1);
+      if (lane == 0) {
+        bx = 0;
+        bf = false;
+      }
+      if (!carry_ok) {  // first group: the slot before G0 (used when G0 is inside a block)
+        uint32_t y = 0;
+        if (lane == 0 && it.y > 0) y = gt_neighbor(g, h, it.y - 1);
+        carry = __shfl_sync(FULL, y, 0);
+        carry_ok = true;
+      }
+      const uint32_t in = bf ? bx : carry + bx;  // value of the slot before the run
+#pragma unroll
+      for (uint32_t k = 0; k < kRun; k++)
+        if ((rel >> k) & 1u) vals[k] += in;
+      const unsigned has = __ballot_sync(FULL, cnt > 0);
+      uint32_t lastv = 0;
+#pragma unroll
+      for (uint32_t k = 0; k < kRun; k++)
+        if (k + 1 == cnt) lastv = vals[k];
+      carry = __shfl_sync(FULL, lastv, 31 - __clz(has));
       if (cnt) {
         uint32_t *o = cols + a0;
         if (cnt == kRun && vec) {  // aligned full run: 16-byte stores
@@ -915,11 +774,24 @@ __global__ void __launch_bounds__(256) decode_small_kernel(DevGraph g, const uin
 static void launch_plan_kernels(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
                                 unsigned int *err, cudaStream_t s);
 
+template <int DEPTH>
+static void launch_le_range(const DevGraph &v, const uint64_t *rowptr, uint32_t *cols,
+                            const grass_graph *g, unsigned grid, unsigned int *err,
+                            cudaStream_t s) {
+  const uint32_t smem = kDecodeWarps * LeWarpSmem<DEPTH>::bytes();
+  static std::once_flag once;  // opt in to more than 48 KB of dynamic shared memory
+  std::call_once(once, [&] {
+    cudaFuncSetAttribute(decode_le_range_kernel<DEPTH>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  });
+  decode_le_range_kernel<DEPTH><<<grid, 32 * kDecodeWarps, smem, s>>>(
+      v, rowptr, cols, g->d_plan_big, g->plan_nbig, err);
+}
+
 int launch_decode_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
                           unsigned int *err, cudaStream_t s) {
   const uint32_t n = (uint32_t)g->info.n;
   if (!g->info.num_edges) return GRASS_OK;
-  const int dev = g->device;
   {
     std::lock_guard<std::mutex> lk(g->plan_mu);
     if (!g->plan_ok) {
@@ -1000,23 +872,15 @@ static void launch_plan_kernels(const grass_graph *g, const uint64_t *rowptr, ui
     const unsigned grid = (unsigned)std::max<uint64_t>(
         1, std::min<uint64_t>((g->plan_nbig + 7) / 8, (uint64_t)sm_count(dev) * per_sm));
     const bool vec = (reinterpret_cast<uintptr_t>(cols) & 15u) == 0;  // 16-byte stores allowed
-    if (g->mode == GRASS_MODE_GT)
-      decode_range_kernel<0><<<grid, 256, 0, s>>>(v, rowptr, cols, g->d_plan_big, g->plan_nbig,
-                                                   vec, err);
-    else {
-#if GRASS_DECODE_STAGE
-      static bool attr = false;
-      if (!attr) {
-        cudaFuncSetAttribute(decode_range_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kStageSmem);
-        attr = true;
+    if (g->mode == GRASS_MODE_GT) {
+      decode_gt_range_kernel<<<grid, 256, 0, s>>>(v, rowptr, cols, g->d_plan_big, g->plan_nbig,
+                                                  vec, err);
+    } else {
+      switch (g->tuning.decode_stage_depth) {
+        case 2: launch_le_range<2>(v, rowptr, cols, g, grid, err, s); break;
+        case 4: launch_le_range<4>(v, rowptr, cols, g, grid, err, s); break;
+        default: launch_le_range<0>(v, rowptr, cols, g, grid, err, s);
       }
-      const uint32_t smem = kStageSmem;
-#else
-      const uint32_t smem = 0;
-#endif
-      decode_range_kernel<1><<<grid, 32 * kDecodeWarps, smem, s>>>(
-          v, rowptr, cols, g->d_plan_big, g->plan_nbig, vec, err);
     }
     count_launch();
   }

@@ -223,47 +223,152 @@ __device__ __forceinline__ void or_bits(uint32_t *w, uint64_t off, uint64_t val,
   if (lo) atomicOr(w + (off >> 5) + 1, lo);
 }
 
-// LE payloads in neighbor order (le_chunked, device_common.cuh): one warp per
-// vertex.  dst starts as a copy of src; the lanes clear the vertex's payload
-// bits [P, end) in dst, then move every field from its on-disk position
-// (rock c at P + c a; sea k at P + (chunk_num + 1) a + k (sea_bit + 1),
-// LE/src/bcg.cuh:211, 237) to its neighbor-order position.  Words shared with
-// another vertex's header or payload are changed with atomicAnd / atomicOr on
-// this vertex's bits only; the warp's clears are ordered before its writes by
-// __syncwarp.
-__global__ void __launch_bounds__(256) le_reorder_kernel(const uint32_t *__restrict__ src,
-                                                         uint32_t *dst,
-                                                         const uint4 *__restrict__ recs,
-                                                         uint32_t n) {
+// ---- LE device layout (le_slot_pos, device_common.cuh) ----
+
+// Neighbor i of an LE vertex in the on-disk layout: rocks at P + c a, seas at
+// P + (chunk_num + 1) a + k (sea_bit + 1) (LE/src/bcg.cuh:195-261).
+__device__ __forceinline__ uint32_t le_disk_neighbor(const uint32_t *words, const VHdr &h,
+                                                     uint32_t i) {
+  if (h.d == 1) return h.fp;
+  uint32_t tl = h.bl + 1;
+  const uint32_t split = h.om * tl;
+  const bool flag = i >= split;
+  const uint32_t j = flag ? i - split : i;
+  if (flag) tl -= 1;
+  uint32_t c = j / tl;
+  const uint32_t id = j - c * tl;
+  if (flag) c += h.om;
+  const uint64_t rpos = h.P + (uint64_t)c * (uint64_t)h.a;
+  const uint32_t r1m = (uint32_t)bits_at(words, rpos, h.a);
+  const uint32_t r1 = c < h.fp ? h.v - r1m : h.v + r1m;
+  if (id == 0) return r1;
+  const uint32_t r2m = (uint32_t)bits_at(words, rpos + h.a, h.a);
+  const uint32_t r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
+  const uint64_t k = (uint64_t)(h.bl - 1) * c + min(h.om, c) + id - 1;
+  const uint64_t raw =
+      bits_at(words, h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a + k * (uint64_t)(h.b + 1), h.b + 1);
+  const uint32_t mag = (uint32_t)(raw >> 1);
+  return ((r2 - r1) / tl) * id + r1 + ((raw & 1u) ? 0u - mag : mag);
+}
+
+// Pass 0: every LE neighbor list, decoded from the on-disk stream into a
+// temporary CSR (one warp per vertex).
+__global__ void __launch_bounds__(256) le_disk_decode_kernel(const uint32_t *__restrict__ words,
+                                                             const uint4 *__restrict__ recs,
+                                                             uint32_t n,
+                                                             const uint64_t *__restrict__ rowptr,
+                                                             uint32_t *__restrict__ cols) {
   const int lane = threadIdx.x & 31;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t v = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
-    const VHdr h = record_header<1>(recs[v], (uint32_t)v);
-    if (!le_chunked(h)) continue;  // warp-uniform
-    const uint32_t sw = (uint32_t)h.b + 1u;
-    const uint64_t end = payload_end<1>(DevGraph{}, h);
-    const uint64_t w0 = h.P >> 5, w1 = (end - 1) >> 5;
-    for (uint64_t k = w0 + lane; k <= w1; k += 32) {
-      uint32_t m = 0xFFFFFFFFu;  // bits of word k inside [P, end), MSB first
-      if (k == w0) m &= 0xFFFFFFFFu >> ((uint32_t)h.P & 31u);
-      if (k == w1) m &= 0xFFFFFFFFu << (31u - ((uint32_t)(end - 1) & 31u));
-      if (m == 0xFFFFFFFFu) dst[k] = 0u;
-      else atomicAnd(dst + k, ~m);
+    const VHdr h = le_disk_record_header(recs[v], (uint32_t)v);
+    uint32_t *out = cols + rowptr[v];
+    for (uint32_t i = lane; i < h.d; i += 32) out[i] = le_disk_neighbor(words, h, i);
+  }
+}
+
+__device__ __forceinline__ uint32_t bit_len64(uint64_t x) { return x ? 64u - __clzll(x) : 1u; }
+
+// Chunk lengths tried per vertex; slots must fit a sector (cb <= 256).
+__constant__ uint8_t kLeChunkLens[] = {1, 2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 16, 20, 24, 28, 32};
+constexpr int kNumChunkLens = sizeof(kLeChunkLens);
+constexpr uint32_t kLeMaxSlots = 63;  // K is stored in 6 bits
+
+// Pass 1: per vertex of degree >= 2, the chunk length T with the fewest
+// bits (a vertex of one sector: C cb; larger: whole sectors), its sea_bit
+// (largest residual magnitude's bit count, as get_bit_num), K, rock width a
+// (bits of max(|n_0 - v|, |n_{d-1} - v|), LE/chunk_compress/compressor.hpp:69)
+// and first_pos (rocks below v).  meta[v] = T | sea_bit << 8 | K << 16 | a << 24.
+__global__ void __launch_bounds__(256) le_choose_kernel(const uint64_t *__restrict__ rowptr,
+                                                        const uint32_t *__restrict__ cols,
+                                                        uint32_t n, uint32_t *__restrict__ meta,
+                                                        uint32_t *__restrict__ fpos) {
+  const int lane = threadIdx.x & 31;
+  const unsigned FULLM = 0xFFFFFFFFu;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
+    const uint64_t base = rowptr[v];
+    const uint32_t d = (uint32_t)(rowptr[v + 1] - base);
+    if (d < 2) {
+      if (lane == 0) meta[v] = 0, fpos[v] = 0;
+      continue;
     }
-    __syncwarp();
-    const uint64_t sea0 = h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a;
-    for (uint32_t i = lane; i < h.d; i += 32) {
-      uint32_t c, id, tl;
-      le_locate(h, i, c, id, tl);
-      const uint64_t X = le_chunk_pos(h, c);
-      if (id == 0) {
-        or_bits(dst, X, bits_at(src, h.P + (uint64_t)c * h.a, h.a), h.a);
-      } else {
-        const uint64_t k = (uint64_t)(h.bl - 1) * c + min(h.om, c) + id - 1;
-        or_bits(dst, X + h.a + (uint64_t)(id - 1) * sw, bits_at(src, sea0 + k * sw, (int)sw),
-                (int)sw);
+    const uint32_t *nb = cols + base;
+    const int64_t vv = (int64_t)v;
+    const uint32_t a = bit_len64((uint64_t)max(llabs((int64_t)nb[0] - vv),
+                                               llabs((int64_t)nb[d - 1] - vv)));
+    const uint32_t last = d - 1;
+    uint64_t best = ~0ull;
+    uint32_t bT = 1, bsb = 0, bK = 1;
+    for (int t = 0; t < kNumChunkLens; t++) {
+      const uint32_t T = kLeChunkLens[t];
+      if (T > 1 && T >= d) break;  // one chunk already holds every neighbor
+      uint32_t sb = 0;
+      for (uint32_t i = lane; i < last; i += 32) {
+        const uint32_t c = i / T, id = i - c * T;
+        if (!id) continue;
+        const uint32_t L = min(T, last - c * T);
+        const uint32_t r1 = nb[c * T], r2 = nb[c * T + L];
+        const int64_t res = (int64_t)nb[i] - ((int64_t)r1 + (int64_t)id * ((r2 - r1) / L));
+        sb = max(sb, bit_len64((uint64_t)llabs(res)));
       }
+      sb = __reduce_max_sync(FULLM, sb);
+      const uint32_t cb = 2 * a + (T - 1) * (sb + 1);
+      if (cb > 256) continue;
+      const uint32_t K = min(256u / cb, kLeMaxSlots);
+      const uint32_t C = (last - 1) / T + 1;
+      const uint64_t cost = C <= K ? (uint64_t)C * cb : (uint64_t)((C + K - 1) / K) * 256u;
+      if (cost < best) best = cost, bT = T, bsb = sb, bK = K;
     }
+    // first_pos: the rocks (n[cT] for c < C, and n[d-1]) below v
+    const uint32_t C = (last - 1) / bT + 1;
+    uint32_t below = 0;
+    for (uint32_t c = lane; c <= C; c += 32) below += (c < C ? nb[c * bT] : nb[last]) < v;
+    below = __reduce_add_sync(FULLM, below);
+    if (lane == 0) {
+      meta[v] = bT | bsb << 8 | bK << 16 | a << 24;
+      fpos[v] = below;
+    }
+  }
+}
+
+// Pass 2: every vertex's slots at its offset P[v] in dst (zeroed), and its
+// record rewritten in place in the device format.
+__global__ void __launch_bounds__(256) le_write_kernel(const uint64_t *__restrict__ rowptr,
+                                                       const uint32_t *__restrict__ cols,
+                                                       uint32_t n,
+                                                       const uint32_t *__restrict__ meta,
+                                                       const uint32_t *__restrict__ fpos,
+                                                       const uint64_t *__restrict__ P,
+                                                       uint32_t *dst, uint4 *recs) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
+    const uint64_t base = rowptr[v];
+    const uint32_t d = (uint32_t)(rowptr[v + 1] - base);
+    if (d < 2) {
+      if (lane == 0) recs[v] = d ? pack_le_record(0, 0, 0, 0, 0, 1, cols[base]) : make_uint4(0, 0, 0, 0);
+      continue;
+    }
+    const uint32_t *nb = cols + base;
+    const uint32_t m = meta[v];
+    const uint32_t T = m & 0xFFu, sb = (m >> 8) & 0xFFu, K = (m >> 16) & 0xFFu, a = m >> 24;
+    const uint32_t sw = sb + 1, cb = 2 * a + (T - 1) * sw, last = d - 1, C = (last - 1) / T + 1;
+    for (uint32_t c = lane; c < C; c += 32) {
+      const uint32_t q = c / K;
+      const uint64_t at = P[v] + (uint64_t)q * 256u + (uint64_t)(c - q * K) * cb;
+      const uint32_t L = min(T, last - c * T);
+      const uint32_t r1 = nb[c * T], r2 = nb[c * T + L];
+      or_bits(dst, at, (uint64_t)llabs((int64_t)r1 - (int64_t)v), a);
+      const uint32_t step = (r2 - r1) / L;
+      for (uint32_t id = 1; id < L; id++) {
+        const int64_t res = (int64_t)nb[c * T + id] - ((int64_t)r1 + (int64_t)id * step);
+        const uint64_t f = ((uint64_t)llabs(res) << 1) | (res < 0 ? 1u : 0u);
+        if (f) or_bits(dst, at + a + (uint64_t)(id - 1) * sw, f, sw);
+      }
+      or_bits(dst, at + a + (uint64_t)(T - 1) * sw, (uint64_t)llabs((int64_t)r2 - (int64_t)v), a);
+    }
+    if (lane == 0) recs[v] = pack_le_record(P[v], a, sb, T, K, d, fpos[v]);
   }
 }
 
@@ -402,11 +507,29 @@ void launch_build_records(const DevGraph &g, uint4 *recs, cudaStream_t s) {
   count_launch();
 }
 
-void launch_le_reorder(const uint32_t *src, uint32_t *dst, const uint4 *recs, uint32_t n,
-                       cudaStream_t s) {
+void launch_le_disk_decode(const uint32_t *words, const uint4 *recs, uint32_t n,
+                           const uint64_t *rowptr, uint32_t *cols, cudaStream_t s) {
   int dev = 0;
   cudaGetDevice(&dev);
-  le_reorder_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(src, dst, recs, n);
+  le_disk_decode_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(words, recs, n, rowptr, cols);
+  count_launch();
+}
+
+void launch_le_choose(const uint64_t *rowptr, const uint32_t *cols, uint32_t n, uint32_t *meta,
+                      uint32_t *fpos, cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  le_choose_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(rowptr, cols, n, meta, fpos);
+  count_launch();
+}
+
+void launch_le_write(const uint64_t *rowptr, const uint32_t *cols, uint32_t n,
+                     const uint32_t *meta, const uint32_t *fpos, const uint64_t *P, uint32_t *dst,
+                     uint4 *recs, cudaStream_t s) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  le_write_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(rowptr, cols, n, meta, fpos, P, dst,
+                                                              recs);
   count_launch();
 }
 

@@ -110,29 +110,14 @@ __device__ __forceinline__ void draw_footprint(const DevGraph &g, const VHdr &h,
       r0[nr] = r.spos;
       r1[nr++] = e;
     }
-  } else if (h.d > 1 && le_chunked(h)) {
-    // neighbor order: rock c, the sea, rock c+1 lie in one span (le_neighbor
-    // loads the sectors of the span)
-    uint32_t c, id, tl;
-    le_locate(h, i, c, id, tl);
-    const uint64_t X = le_chunk_pos(h, c);
-    const uint64_t span = id ? 2ull * h.a + (uint64_t)(tl - 1) * (h.b + 1) : (uint64_t)h.a;
-    bits = id ? 2ull * h.a + h.b + 1 : (uint64_t)h.a;
-    sectors = ((X + span - 1) >> 8) - (X >> 8) + 1;
-    return;
   } else if (h.d > 1) {
-    uint32_t c, id, tl;
-    le_locate(h, i, c, id, tl);
-    const uint64_t rp = h.P + (uint64_t)c * h.a;
-    r0[nr] = rp;
-    r1[nr++] = rp + (id ? 2u : 1u) * (uint64_t)h.a;
-    if (id) {
-      const uint64_t spos =
-          h.P + (uint64_t)(h.bn + 1) * (uint64_t)h.a +
-          ((uint64_t)(h.bl - 1) * c + min(h.om, c) + id - 1) * (uint64_t)(h.b + 1);
-      r0[nr] = spos;
-      r1[nr++] = spos + h.b + 1;
-    }
+    // the device layout: the chunk's slot, inside one sector; the bits read
+    // are the left rock, and for an inner neighbor the right rock and a sea
+    uint32_t c, id, L;
+    le_locate(h, i, c, id, L);
+    bits = id == 0 ? (uint64_t)h.a : id == L ? 2ull * h.a : 2ull * h.a + h.b + 1;
+    sectors = 1;
+    return;
   }
   bits = 0;
   sectors = 0;

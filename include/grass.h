@@ -134,6 +134,14 @@ int grass_open_mem(const void *graph_bytes, uint64_t graph_size, const void *off
                    uint64_t offset_size, int mode, int device, grass_graph **out);
 int grass_close(grass_graph *g);
 int grass_get_info(const grass_graph *g, grass_graph_info *info);
+/* Waits for `stream`, then reads and clears the graph's device error word,
+ * which the asynchronous device-pointer calls (samplers, decode) set instead
+ * of aborting (the reference asserts, GT/src/utils.hpp:17, 108-119):
+ * GRASS_E_DATA when a decoded id was out of range (corrupt payload),
+ * GRASS_E_TIMEOUT when a decode warp's staged copy did not land within its
+ * bounded wait (that range was decoded from global memory instead), else
+ * GRASS_OK.  The _host calls check it themselves. */
+int grass_check_device_error(grass_graph *g, void *stream);
 /* Device view of the resident graph (for callers that launch their own
  * kernels): the stream words (n_words + at least 16 zero guard words, each
  * word the next 32 stream bits MSB-first) and the n vertex records, 16 bytes
@@ -167,7 +175,10 @@ typedef struct {
                                  access-policy window                               */
   uint32_t l2_fetch_bytes;    /* 0 = leave as is; 32/64/128: this process's
                                  cudaLimitMaxL2FetchGranularity hint                 */
-  uint32_t reserved[3];
+  uint32_t decode_stage_depth;/* LE decode sweep: 0 = chunk slots read from global
+                                 memory; 2 or 4 = groups of 32 slots copied into
+                                 shared memory (cp.async.bulk) that many ahead       */
+  uint32_t reserved[2];
 } grass_tuning;
 int grass_set_tuning(grass_graph *g, const grass_tuning *t);
 int grass_get_tuning(const grass_graph *g, grass_tuning *t);
