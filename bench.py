@@ -677,7 +677,7 @@ def cpu_baseline(gdir, mode, n, length, seed, budget_s=12.0):
 
 def reference_gpu(gdir, n, runs=3, timeout_s=600):
     """The reference's own GPU sampler on this GPU: its unmodified `rw` app
-    (oracle/_ref/rw_gt, rw_le, built from its sources for sm_100a) against
+    (baseline/_ref/rw_gt, rw_le, built from its sources for sm_100a) against
     this library's drop-in `rw` on the same files and the same workload, the
     reference app's default: one walker per vertex starting at i % n, 80
     steps (GT/src/apps/randomwalk/randomWalks.cu:4-24), `-n runs`.  Both print
@@ -685,8 +685,8 @@ def reference_gpu(gdir, n, runs=3, timeout_s=600):
     on these graphs (no isolated vertices), so a run samples 80 n edges."""
     out = {"workload": f"{n} walkers (one per vertex, start i % n) x 80 steps, -n {runs}",
            "edges_per_run": 80 * n}
-    bins = {"reference": {"GT": os.path.join(ROOT, "oracle", "_ref", "rw_gt"),
-                          "LE": os.path.join(ROOT, "oracle", "_ref", "rw_le")},
+    bins = {"reference": {"GT": os.path.join(ROOT, "baseline", "_ref", "rw_gt"),
+                          "LE": os.path.join(ROOT, "baseline", "_ref", "rw_le")},
             "grass_b200": {m: os.path.join(ROOT, "grass_b200", "bin", "rw") for m in ("GT", "LE")}}
     for who, exes in bins.items():
         for m, exe in exes.items():

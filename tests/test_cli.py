@@ -128,3 +128,17 @@ def test_auto_mode_detects_the_format(binaries):
         r = run(binaries["rw"], "-g", os.path.join(d, mode), "--walkers", "10")
         assert r.returncode == 0, r.stderr
         assert f"Format: {mode}," in r.stdout
+
+
+@pytest.mark.parametrize("args", [(), ("-n", "2"), ("--help",)])
+def test_usage_matches_the_reference_binary(binaries, args):
+    """Where the reference's own rw app has been built (baseline/_ref/rw_gt,
+    from its sources), its usage lines and exit status are ours."""
+    ref = os.path.join(ROOT, "baseline", "_ref", "rw_gt")
+    if not os.path.exists(ref):
+        pytest.skip("reference rw app not built here")
+    r_ref, r_ours = run(ref, *args), run(binaries["rw"], *args)
+    assert r_ref.returncode == r_ours.returncode == 0
+    ref_lines = [ln.rstrip() for ln in r_ref.stdout.splitlines() if ln.strip()]
+    ours = [ln.rstrip() for ln in r_ours.stdout.splitlines() if ln.strip()]
+    assert ours[:len(ref_lines)] == ref_lines
