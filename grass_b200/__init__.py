@@ -93,7 +93,8 @@ class Job(C.Structure):
 class BatchConfig(C.Structure):
     _fields_ = [("walker_tile", C.c_uint32), ("depth", C.c_uint32),
                 ("warps_per_block", C.c_uint32), ("khop_seeds", C.c_uint32),
-                ("use_graph", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+                ("use_graph", C.c_uint32), ("warps_per_vertex", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}

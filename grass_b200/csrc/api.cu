@@ -264,15 +264,15 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
   cudaFree(g->d_offsets);
   g->d_offsets = nullptr;
 
+  // The device layout: every vertex re-chunked into sector-sized slots
+  // (device_common.cuh), built from the decoded neighbor lists; it replaces
+  // the on-disk stream.
   uint64_t words_alloc = alloc_words;
-  // LE: the device layout re-chunks every vertex into sector-sized slots
-  // (le_slot_pos, device_common.cuh), built from the decoded neighbor lists.
-  if (mode == GRASS_MODE_LE) {
-    Nvtx nv("LE device layout");
+  {
+    Nvtx nv("device layout");
     const uint64_t E = stats[0];
-    uint64_t *d_rp = nullptr;
+    uint64_t *d_rp = nullptr, *d_P = nullptr;
     uint32_t *d_cl = nullptr, *d_meta = nullptr, *d_fp = nullptr;
-    uint64_t *d_P = nullptr;
     GRASS_CUDA(cudaMalloc(&d_rp, (n + 1) * sizeof(uint64_t)));
     tmp.dev.push_back(d_rp);
     GRASS_CUDA(cudaMalloc(&d_cl, std::max<uint64_t>(E, 1) * 4));
@@ -285,8 +285,8 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
     tmp.dev.push_back(d_P);
     launch_degrees64(g->view(), d_rp, st);
     launch_scan_u64_inplace(d_rp, n, d_scan, st);
-    launch_le_disk_decode(g->d_words, g->d_recs, (uint32_t)n, d_rp, d_cl, st);
-    launch_le_choose(d_rp, d_cl, (uint32_t)n, d_meta, d_fp, st);
+    launch_disk_decode(mode, g->d_words, g->d_recs, (uint32_t)n, d_rp, d_cl, st);
+    launch_slot_choose(mode, d_rp, d_cl, (uint32_t)n, d_meta, d_fp, st);
     std::vector<uint32_t> meta(n);
     std::vector<uint64_t> rp(n + 1), P(n, 0);
     GRASS_CUDA(cudaMemcpyAsync(meta.data(), d_meta, n * 4, cudaMemcpyDeviceToHost, st));
@@ -295,15 +295,17 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
     GRASS_CUDA(cudaGetLastError());
     // First fit in vertex order: a vertex whose slots fit in one sector goes
     // at the current bit if it does not cross the sector end; a larger one
-    // starts on the next sector.
+    // starts on the next sector.  Slots: GT ceil(d / T), LE ceil((d - 1) / T)
+    // (an LE vertex of degree 1 keeps its neighbor in the record).
+    const bool gt = mode == GRASS_MODE_GT;
     uint64_t pos = 0;
     for (uint64_t v = 0; v < n; v++) {
       const uint64_t d = rp[v + 1] - rp[v];
-      if (d < 2) continue;
+      if (d < (gt ? 1u : 2u)) continue;
       const uint32_t m = meta[v];
-      const uint64_t T = m & 0xFFu, sw = ((m >> 8) & 0xFFu) + 1, K = (m >> 16) & 0xFFu,
-                     a = m >> 24;
-      const uint64_t cb = 2 * a + (T - 1) * sw, C = (d - 2) / T + 1;
+      const uint64_t T = m & 0xFFu, b = (m >> 8) & 0xFFu, K = (m >> 16) & 0xFFu, a = m >> 24;
+      const uint64_t cb = gt ? a + (T - 1) * b : 2 * a + (T - 1) * (b + 1);
+      const uint64_t C = gt ? (d - 1) / T + 1 : (d - 2) / T + 1;
       if (C <= K) {
         if ((pos & 255) + C * cb > 256) pos = (pos + 255) & ~255ull;
       } else {
@@ -313,50 +315,20 @@ int open_impl(ByteSource &src, const uint8_t *ob, uint64_t osize, int mode, int 
       pos += (C / K) * 256 + (C % K) * cb;
     }
     if (pos >= (1ull << 40))
-      return set_error(GRASS_E_FORMAT, "LE device layout needs %llu bits (limit 2^40)",
+      return set_error(GRASS_E_FORMAT, "device layout needs %llu bits (limit 2^40)",
                        (unsigned long long)pos);
     const uint64_t nw = (pos + 31) / 32;
     words_alloc = (nw + kGuardWords + 7) / 8 * 8;
-    uint32_t *d_led = nullptr;
-    GRASS_CUDA(cudaMalloc(&d_led, words_alloc * 4));
-    tmp.dev.push_back(d_led);
-    GRASS_CUDA(cudaMemsetAsync(d_led, 0, words_alloc * 4, st));
+    uint32_t *d_slots = nullptr;
+    GRASS_CUDA(cudaMalloc(&d_slots, words_alloc * 4));
+    tmp.dev.push_back(d_slots);
+    GRASS_CUDA(cudaMemsetAsync(d_slots, 0, words_alloc * 4, st));
     GRASS_CUDA(cudaMemcpyAsync(d_P, P.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, st));
-    launch_le_write(d_rp, d_cl, (uint32_t)n, d_meta, d_fp, d_P, d_led, g->d_recs, st);
+    launch_slot_write(mode, d_rp, d_cl, (uint32_t)n, d_meta, d_fp, d_P, d_slots, g->d_recs, st);
     GRASS_CUDA(cudaStreamSynchronize(st));
     GRASS_CUDA(cudaGetLastError());
     tmp.dev.back() = g->d_words;  // the on-disk stream is freed with tmp
-    g->d_words = d_led;
-    g->n_words = nw;
-  }
-  // GT: the stream is rebuilt with a skip field every kGtSkip gaps of a block
-  // (payloads only, new offsets in the records).
-  if (mode == GRASS_MODE_GT) {
-    Nvtx nv("GT stream with skip fields");
-    unsigned char *d_cx = nullptr;
-    uint64_t *d_len = nullptr, *d_stmp = nullptr;
-    GRASS_CUDA(cudaMalloc(&d_cx, n));
-    tmp.dev.push_back(d_cx);
-    GRASS_CUDA(cudaMalloc(&d_len, (n + 1) * sizeof(uint64_t)));
-    tmp.dev.push_back(d_len);
-    GRASS_CUDA(cudaMalloc(&d_stmp, (scan_tmp_words(n) + 1) * sizeof(uint64_t)));
-    tmp.dev.push_back(d_stmp);
-    launch_gt_skip_measure(g->d_words, g->d_recs, (uint32_t)n, d_cx, d_len, st);
-    launch_scan_u64_inplace(d_len, n, d_stmp, st);  // new payload offsets, total in d_len[n]
-    uint64_t bits = 0;
-    GRASS_CUDA(cudaMemcpyAsync(&bits, d_len + n, sizeof bits, cudaMemcpyDeviceToHost, st));
-    GRASS_CUDA(cudaStreamSynchronize(st));
-    const uint64_t nw = (bits + 31) / 32;
-    words_alloc = (nw + kGuardWords + 7) / 8 * 8;
-    uint32_t *d_sk = nullptr;
-    GRASS_CUDA(cudaMalloc(&d_sk, words_alloc * 4));
-    tmp.dev.push_back(d_sk);
-    GRASS_CUDA(cudaMemsetAsync(d_sk, 0, words_alloc * 4, st));
-    launch_gt_skip_write(g->d_words, d_sk, g->d_recs, (uint32_t)n, d_cx, d_len, st);
-    GRASS_CUDA(cudaStreamSynchronize(st));
-    GRASS_CUDA(cudaGetLastError());
-    tmp.dev.back() = g->d_words;  // the on-disk stream is freed with tmp
-    g->d_words = d_sk;
+    g->d_words = d_slots;
     g->n_words = nw;
   }
 

@@ -262,91 +262,56 @@ __device__ __forceinline__ VHdr gt_header(const DevGraph &g, uint32_t v) {
   return h;
 }
 
-// ---- GT payload layout in HBM ----
-// On disk a GT block is its head and then len - 1 gaps, so neighbor id of a
-// block costs id sequential gap reads (GT/src/bcg.cuh:153-168), O(sqrt d) for
-// hubs.  At load the stream is rebuilt with a skip field in every block at
-// each position t = g * kGtSkip (g >= 1): in place of gap t it holds the sum
-// of the block's raw gaps 1..t, in b + cx bits (cx per vertex, in its record).
-// Neighbor id of a block is then
-//   head value + id + (id >= kGtSkip ? skip field g = id / kGtSkip : 0)
-//              + the raw gaps after that skip field (fewer than kGtSkip),
-// the sum being the reference's head + sum of (gap + 1) regrouped.  Blocks of
-// at most kGtSkip neighbors are unchanged.  The rebuilt stream holds the
-// payloads only, back to back in vertex order (the headers live in the
-// records).  Footprint: cx bits per kGtSkip gaps of long blocks.
-#ifndef GRASS_GT_SKIP
-#define GRASS_GT_SKIP 16
-#endif
-constexpr uint32_t kGtSkip = GRASS_GT_SKIP;
+// ---- sector slots: the device layout of both formats ----
+// On disk a vertex is ~sqrt(d) blocks (GT) or chunks (LE) of ~sqrt(d)
+// neighbors, so a random draw in a hub touches several 32-byte sectors: GT
+// adds up to sqrt(d) gaps (GT/src/bcg.cuh:153-168), LE reads its rock pair
+// and its sea from two places (LE/src/bcg.cuh:195-261).  At load every
+// vertex is re-chunked for the device with its format's own method but a
+// chunk length T (1..32) of its own, each chunk in a self-contained slot that
+// never crosses a sector:
+//   slot c of cb bits starts at P + (c / K) 256 + (c % K) cb, K <= 63 slots
+//   per sector; a vertex whose slots fit in one sector is packed without
+//   alignment (and lies inside one sector), a larger one starts on a sector.
+// A draw reads its record and one sector.  T is chosen per vertex for the
+// fewest bits.  Decoded neighbors are the file's, bit for bit.
+//
+// Record (16 B): x = P low 32 bits; y = P bits 32..39 | a << 8 | b << 14 |
+// T << 20 | K << 26; z = degree; w = first_pos (LE degree 1: the neighbor).
+// In VHdr: bl = T, om = K, bn = C (number of slots), cx = cb.
 
-// Bits of a block of L >= 1 neighbors.
-__device__ __host__ __forceinline__ uint64_t gt_block_bits(const VHdr &h, uint32_t L) {
-  return (uint64_t)h.a + (uint64_t)(L - 1) * (uint64_t)h.b +
-         (uint64_t)((L - 1) / kGtSkip) * (uint64_t)h.cx;
+__device__ __forceinline__ uint4 pack_slot_record(uint64_t P, uint32_t a, uint32_t b, uint32_t T,
+                                                  uint32_t K, uint32_t d, uint32_t fp) {
+  return make_uint4((uint32_t)P,
+                    ((uint32_t)(P >> 32) & 0xFFu) | (a & 63u) << 8 | (b & 63u) << 14 |
+                        (T & 63u) << 20 | (K & 63u) << 26,
+                    d, fp);
 }
 
-// Bit offset of block blk (blocks before om hold bl + 1 neighbors, the rest bl).
-__device__ __forceinline__ uint64_t gt_block_pos(const VHdr &h, uint32_t blk) {
-  const uint32_t lo = min(blk, h.om);
-  return h.P + (uint64_t)lo * gt_block_bits(h, h.bl + 1) +
-         (uint64_t)(blk - lo) * gt_block_bits(h, h.bl);
+// Bit offset of slot c.
+__device__ __forceinline__ uint64_t slot_pos(const VHdr &h, uint32_t c) {
+  const uint32_t q = c / h.om;
+  return h.P + (uint64_t)q * 256u + (uint64_t)(c - q * h.om) * (uint32_t)h.cx;
 }
 
-// Bit offset of field t >= 1 (a gap, or a skip field when t % kGtSkip == 0)
-// of the block at bit offset bpos.
-__device__ __forceinline__ uint64_t gt_field_pos(const VHdr &h, uint64_t bpos, uint32_t t) {
-  return bpos + (uint64_t)h.a + (uint64_t)(t - 1) * (uint64_t)h.b +
-         (uint64_t)((t - 1) / kGtSkip) * (uint64_t)h.cx;
+// The w (1..33) bits at bit off of one sector, the field inside it.
+__device__ __forceinline__ uint64_t sec1_field(const Sec &A, uint32_t off, int w) {
+  const uint32_t k = off >> 6, s = off & 63u;
+  const uint64_t x = sec_word(A, k);
+  const uint64_t y = k < 3 ? sec_word(A, k + 1) : 0ull;
+  const uint64_t win = s ? (x << s) | (y >> (64 - s)) : x;
+  return win >> (64 - w);
 }
 
-// Block blk and index id of neighbor i (GT/src/bcg.cuh:153-160).
-__device__ __forceinline__ void gt_block_of(const VHdr &h, uint32_t i, uint32_t &blk,
-                                            uint32_t &id) {
-  const uint32_t split = (h.bl + 1) * h.om;
-  const bool flag = i < split;
-  const uint32_t j = flag ? i : i - split;
-  const uint32_t len = h.bl + (flag ? 1u : 0u);
-  blk = j / len;
-  id = j - blk * len;
-  if (!flag) blk += h.om;
-}
-
-// A GT draw of neighbor i, located: the head field, the skip field (when id
-// >= kGtSkip), and the run of raw gaps to add after it.
-struct GtRun {
-  uint64_t pos;   // bit offset of the head field
-  uint64_t spos;  // bit offset of the skip field (skip) or of the first gap
-  uint32_t id;    // index within the block
-  uint32_t gaps;  // raw gaps after the skip field (or after the head)
-  bool up;        // head counts upward from v (block >= first_pos)
-  bool skip;
-};
-
-__device__ __forceinline__ GtRun gt_locate(const VHdr &h, uint32_t i) {
-  uint32_t blk, id;
-  gt_block_of(h, i, blk, id);
-  GtRun r;
-  r.pos = gt_block_pos(h, blk);
-  r.id = id;
-  r.up = blk >= h.fp;
-  const uint32_t q = id / kGtSkip;
-  r.skip = q != 0;
-  r.gaps = id - q * kGtSkip;
-  r.spos = q ? gt_field_pos(h, r.pos, q * kGtSkip) : r.pos + (uint64_t)h.a;
-  return r;
-}
-
-// Sum of n w-bit fields starting at bit off (< 512) of the 512-bit window
-// A:B, all inside it; a 128-bit shift window pulls the next word when needed.
-__device__ __forceinline__ uint32_t sec2_sum(const Sec &A, const Sec &B, uint32_t off, uint32_t n,
-                                             int w) {
+// Sum of n w-bit fields from bit off of one sector (off + n w <= 256): a
+// 128-bit shift window pulls the next word when needed.
+__device__ __forceinline__ uint32_t sec1_sum(const Sec &A, uint32_t off, uint32_t n, int w) {
   if (!n || !w) return 0;
   uint32_t k = off >> 6;
   const uint32_t sh = off & 63u;
-  uint64_t buf = sec2_word(A, B, k) << sh;
+  uint64_t buf = sec_word(A, k) << sh;
   int nb = 64 - (int)sh;
-  uint64_t nxt = sec2_word(A, B, ++k);
+  uint64_t nxt = k < 3 ? sec_word(A, ++k) : 0ull;
   uint32_t s = 0;
   for (uint32_t j = 0; j < n; j++) {
     uint32_t v;
@@ -359,67 +324,48 @@ __device__ __forceinline__ uint32_t sec2_sum(const Sec &A, const Sec &B, uint32_
       v = (uint32_t)(((nb ? buf >> (64 - nb) : 0ull) << r) | (nxt >> (64 - r)));
       buf = nxt << r;
       nb = 64 - r;
-      nxt = sec2_word(A, B, ++k);
+      nxt = k < 3 ? sec_word(A, ++k) : 0ull;
     }
     s += v;
   }
   return s;
 }
 
-// Sum of n >= 0 consecutive w-bit fields at bit pos through a sequential
-// cursor (the first load is one memory round trip, the rest hit L1).
-__device__ __forceinline__ uint32_t field_sum(const uint32_t *words, uint64_t pos, uint32_t n,
-                                              int w) {
-  if (!n || !w) return 0;
-  BitCur c;
-  c.init(words, pos);
-  uint32_t s = 0;
-  for (uint32_t k = 0; k < n; k++) s += c.get(w);
-  return s;
+// ---- GT ----
+// Slot c: the head |n_cT - v| - 1 (a bits), then the gaps n_i - n_{i-1} - 1
+// (b bits) of neighbors cT+1 .. cT+L-1, L = min(T, d - cT); the head counts
+// up from v when c >= first_pos (the reference's encoding per block,
+// GT/chunk_compress/compressor.hpp:245-282, on chunks of T).
+
+// On-disk block geometry, load time only: block blk starts at
+// P + blk (a + (bl - 1) b) + min(blk, om) b (GT/src/bcg.cuh:153-163).
+__device__ __forceinline__ uint64_t gt_disk_block_pos(const VHdr &h, uint32_t blk) {
+  return h.P + (uint64_t)blk * ((uint64_t)h.a + (uint64_t)(h.bl - 1) * h.b) +
+         (uint64_t)min(blk, h.om) * h.b;
 }
 
-// GT get_vertex, GT/src/bcg.cuh:153-168, on the skip-field layout: the head
-// from its sector(s); the skip field and the gaps after it from theirs (the
-// same two sectors when they lie within 512 bits of the head's sector).
+// GT get_vertex on the device layout: one sector; neighbor id of slot c is
+// the head value + id + the sum of its id gaps.
 __device__ __forceinline__ uint32_t gt_neighbor(const DevGraph &g, const VHdr &h, uint32_t i) {
-  const GtRun r = gt_locate(h, i);
-  const int sw = h.b + h.cx;  // skip field width
-  const uint64_t end = r.spos + (r.skip ? (uint64_t)sw : 0ull) + (uint64_t)r.gaps * h.b;
-  const uint64_t s0 = r.pos >> 8;
-  const uint32_t off = (uint32_t)r.pos & 255u;
-  const Sec zero{0, 0, 0, 0};
-  const bool near = end - (s0 << 8) <= 512u;  // head, skip field and gaps in s0, s0 + 1
-  const bool two = near ? end - (s0 << 8) > 256u : off + (uint32_t)h.a > 256u;
-  const Sec A = load_sector(g.words, s0);
-  const Sec A2 = two ? load_sector(g.words, s0 + 1) : zero;
-  const uint32_t hv = (uint32_t)sec2_field(A, A2, off, h.a) + 1u;
-  uint32_t acc = (r.up ? h.v + hv : h.v - hv) + r.id;
-  if (near) {
-    uint32_t o = (uint32_t)(r.spos - (s0 << 8));
-    if (r.skip) {
-      acc += (uint32_t)sec2_field(A, A2, o, sw);
-      o += (uint32_t)sw;
-    }
-    return acc + sec2_sum(A, A2, o, r.gaps, h.b);
+  const uint32_t c = i / h.bl, id = i - c * h.bl;
+  const uint64_t pos = slot_pos(h, c);
+  const Sec A = load_sector(g.words, pos >> 8);
+  const uint32_t off = (uint32_t)pos & 255u;
+  const uint32_t hv = (uint32_t)sec1_field(A, off, h.a) + 1u;
+  return (c >= h.fp ? h.v + hv : h.v - hv) + id + sec1_sum(A, off + (uint32_t)h.a, id, h.b);
+}
+
+// Every neighbor of slot c (at bit off of sector A) into o[0..L-1].
+__device__ __forceinline__ void gt_slot_decode(const Sec &A, uint32_t off, const VHdr &h,
+                                               uint32_t c, uint32_t L, uint32_t *o) {
+  const uint32_t hv = (uint32_t)sec1_field(A, off, h.a) + 1u;
+  uint32_t x = c >= h.fp ? h.v + hv : h.v - hv;
+  o[0] = x;
+  uint32_t p = off + (uint32_t)h.a;
+  for (uint32_t t = 1; t < L; t++, p += (uint32_t)h.b) {
+    x += (h.b ? (uint32_t)sec1_field(A, p, h.b) : 0u) + 1u;
+    o[t] = x;
   }
-  const uint64_t t0 = r.spos >> 8;
-  const uint32_t toff = (uint32_t)r.spos & 255u;
-  if (end - (t0 << 8) <= 512u) {  // the skip field and its gaps in two sectors
-    const Sec B = load_sector(g.words, t0);
-    const Sec B2 = end - (t0 << 8) > 256u ? load_sector(g.words, t0 + 1) : zero;
-    uint32_t o = toff;
-    if (r.skip) {
-      acc += (uint32_t)sec2_field(B, B2, o, sw);
-      o += (uint32_t)sw;
-    }
-    return acc + sec2_sum(B, B2, o, r.gaps, h.b);
-  }
-  uint64_t p = r.spos;  // wide fields: a sequential cursor
-  if (r.skip) {
-    acc += read_field(g.words, p, sw);
-    p += (uint64_t)sw;
-  }
-  return acc + field_sum(g.words, p, r.gaps, h.b);
 }
 
 // On-disk geometry of an LE vertex of degree d >= 2: chunk_num, chunk_len, om
@@ -461,52 +407,14 @@ __device__ __forceinline__ VHdr le_header(const DevGraph &g, uint32_t v) {
   return h;
 }
 
-// ---- LE payload layout in HBM ----
-// On disk an LE vertex is chunk_num ~ sqrt(d) chunks of ~sqrt(d) neighbors:
-// all rocks, then all seas (LE/chunk_compress/compressor.hpp:352-359), so a
-// draw reads its rock pair from one 32-byte sector and its sea from another,
-// and for hubs both sit thousands of bits apart.  At load every vertex of
-// degree >= 2 is re-chunked for the device with the same method -- a chunk
-// is a left rock |n - v|, signed seas n - (r1 + id ((r2 - r1) / L)), and a
-// right rock, rocks signed by first_pos -- but with a chunk length T of its
-// own (1..32) and self-contained slots that never cross a sector:
-//   slot c = [rock c (a bits)][seas id = 1..T-1 (sw bits each)][rock c+1 (a bits)]
-//   cb = 2a + (T - 1) sw bits; K = slots per sector (<= 63);
-//   slot c starts at P + (c / K) 256 + (c % K) cb.
-// Chunk c holds neighbors cT .. cT + L - 1 with L = min(T, d - 1 - cT); the
-// last neighbor d - 1 is the right rock of chunk C - 1, C = ceil((d-1)/T).  A
-// vertex whose slots fit in one sector is packed without alignment (and then
-// lies inside one sector); a larger one starts on a sector.  T is chosen per
-// vertex for the fewest bits.  A draw reads its record and one sector.  The
-// decoded neighbors are the file's, bit for bit; the rocks of inner chunk
-// boundaries are stored twice.
-//
-// LE record (16 B): x = P low 32 bits; y = P bits 32..39 | a << 8 |
-// sea_bit << 14 | T << 20 | K << 26; z = degree; w = first_pos (degree 1: the
-// neighbor).  In VHdr: b = sea_bit, bl = T, bn = C, om = K, cx = cb.
-
-__device__ __forceinline__ uint4 pack_le_record(uint64_t P, uint32_t a, uint32_t sb, uint32_t T,
-                                                uint32_t K, uint32_t d, uint32_t fp) {
-  return make_uint4((uint32_t)P,
-                    ((uint32_t)(P >> 32) & 0xFFu) | (a & 63u) << 8 | (sb & 63u) << 14 |
-                        (T & 63u) << 20 | (K & 63u) << 26,
-                    d, fp);
-}
-
-// Bit offset of slot c.
-__device__ __forceinline__ uint64_t le_slot_pos(const VHdr &h, uint32_t c) {
-  const uint32_t q = c / h.om;
-  return h.P + (uint64_t)q * 256u + (uint64_t)(c - q * h.om) * (uint32_t)h.cx;
-}
-
-// The w (1..33) bits at bit off of one sector, the field inside it.
-__device__ __forceinline__ uint64_t sec1_field(const Sec &A, uint32_t off, int w) {
-  const uint32_t k = off >> 6, s = off & 63u;
-  const uint64_t x = sec_word(A, k);
-  const uint64_t y = k < 3 ? sec_word(A, k + 1) : 0ull;
-  const uint64_t win = s ? (x << s) | (y >> (64 - s)) : x;
-  return win >> (64 - w);
-}
+// ---- LE ----
+// Slot c (the sector slots above): [rock c (a bits)][seas id = 1..T-1 (sea_bit
+// + 1 bits each)][rock c+1 (a bits)]; chunk c holds neighbors cT .. cT+L-1, L
+// = min(T, d - 1 - cT), and the last neighbor d - 1 is the right rock of slot
+// C - 1, C = ceil((d-1)/T).  A chunk is the reference's: a left rock |n - v|,
+// signed seas n - (r1 + id ((r2 - r1) / L)), a right rock, rocks signed by
+// first_pos (LE/chunk_compress/compressor.hpp:288-359), on chunks of T; the
+// rocks of inner chunk boundaries are stored twice.  In VHdr b = sea_bit.
 
 // Chunk c and index id of neighbor i (id == L: the last neighbor, chunk C-1's
 // right rock), and the chunk's length L.
@@ -564,7 +472,7 @@ __device__ __forceinline__ uint32_t le_neighbor(const DevGraph &g, const VHdr &h
   if (h.d == 1) return h.fp;
   uint32_t c, id, L;
   le_locate(h, i, c, id, L);
-  const uint64_t pos = le_slot_pos(h, c);
+  const uint64_t pos = slot_pos(h, c);
   const Sec A = load_sector(g.words, pos >> 8);
   return le_slot_value(A, (uint32_t)pos & 255u, h, c, id, L);
 }
@@ -582,7 +490,7 @@ __device__ __forceinline__ uint4 pack_record(const VHdr &h) {
   r.y = ((uint32_t)(h.P >> 32) & 0xFFFFu) | ((uint32_t)h.a & 63u) << 16 |
         ((uint32_t)h.b & 63u) << 22;
   r.z = h.d;
-  r.w = h.fp | ((uint32_t)h.cx & 63u) << 16;  // cx: GT only (0 elsewhere)
+  r.w = h.fp;
   return r;
 }
 
@@ -599,28 +507,44 @@ __device__ __forceinline__ VHdr record_header(const uint4 r, uint32_t v) {
   h.fp = r.w;
   h.cx = 0;
   h.bn = h.bl = h.om = 0;  // (CSR, mode 2: no chunk geometry)
-  if constexpr (MODE == 0) {
-    h.fp = r.w & 0xFFFFu;  // GT: first_pos <= 46342, skip-field extra width above it
-    h.cx = (int)((r.w >> 16) & 63u);
-    const uint32_t s = isqrt_u32(h.d);
-    if (s * s == h.d) {
-      h.bn = h.bl = s;
-      h.om = 0;
-    } else {
-      h.bn = s + 1;
-      h.bl = h.d / h.bn;
-      h.om = h.d - h.bn * h.bl;
-    }
-  } else if constexpr (MODE == 1) {  // the device LE layout (le_slot_pos)
+  if constexpr (MODE == 0 || MODE == 1) {  // the device layouts (slot_pos)
     h.P = (uint64_t)r.x | ((uint64_t)(r.y & 0xFFu) << 32);
     h.a = (int)((r.y >> 8) & 63u);
     h.b = (int)((r.y >> 14) & 63u);
     h.bl = (r.y >> 20) & 63u;  // T
     h.om = (r.y >> 26) & 63u;  // K
-    if (h.d > 1) {
+    if constexpr (MODE == 0) {
+      if (h.d) {
+        h.bn = (h.d - 1) / h.bl + 1;  // C = ceil(d / T)
+        h.cx = h.a + (int)(h.bl - 1) * h.b;
+      }
+    } else if (h.d > 1) {
       h.bn = (h.d - 2) / h.bl + 1;  // C = ceil((d - 1) / T)
       h.cx = 2 * h.a + (int)(h.bl - 1) * (h.b + 1);
     }
+  }
+  return h;
+}
+
+// Header of a GT vertex from its load-time record (pack_record of the stream
+// header: on-disk block geometry), before the device layout is built.
+__device__ __forceinline__ VHdr gt_disk_record_header(const uint4 r, uint32_t v) {
+  VHdr h;
+  h.v = v;
+  h.P = (uint64_t)r.x | ((uint64_t)(r.y & 0xFFFFu) << 32);
+  h.a = (int)((r.y >> 16) & 63u);
+  h.b = (int)((r.y >> 22) & 63u);
+  h.d = r.z;
+  h.fp = r.w;
+  h.cx = 0;
+  const uint32_t s = isqrt_u32(h.d);
+  if (s * s == h.d) {
+    h.bn = h.bl = s;
+    h.om = 0;
+  } else {
+    h.bn = s + 1;
+    h.bl = h.d / h.bn;
+    h.om = h.d - h.bn * h.bl;
   }
   return h;
 }
@@ -696,14 +620,13 @@ __device__ __forceinline__ uint32_t neighbor(const DevGraph &g, const VHdr &h, u
   else return load_cold_u32(g.cols + h.P + i);
 }
 
-// End bit of a vertex's payload given its header: GT in the device layout
-// (or on disk, cx = 0); LE on disk (load-time validation).  For the files
-// the reference compressor writes this is offsets[v+1]
+// End bit of a vertex's on-disk payload given its stream header (load-time
+// validation).  For the files the reference compressor writes this is offsets[v+1]
 // (GT/chunk_compress/compressor.hpp:297-349, LE/chunk_compress/compressor.hpp:329-390).
 template <int MODE>
 __device__ __forceinline__ uint64_t payload_end(const DevGraph &g, const VHdr &h) {
   if constexpr (MODE == 0) {
-    return gt_block_pos(h, h.bn);
+    return gt_disk_block_pos(h, h.bn);
   } else {
     if (h.d <= 1) return 0;  // caller checks via the header cursor instead
     return h.P + (uint64_t)(h.bn + 1) * h.a + (uint64_t)(h.d - h.bn - 1) * (h.b + 1);

@@ -154,25 +154,18 @@ void launch_scan_u32(const uint32_t *counts, uint64_t n, uint64_t *out, uint64_t
 void launch_validate(const DevGraph &g, uint32_t *deg, unsigned long long *stats,
                      cudaStream_t s);
 void launch_build_records(const DevGraph &g, uint4 *recs, cudaStream_t s);
-// LE device layout (le_slot_pos): pass 0 decodes the on-disk stream into a
-// CSR (rowptr = scanned degrees); pass 1 picks each vertex's chunk length,
-// sea_bit, slots per sector and rock width (meta) and first_pos (fpos); the
-// host places the vertices (P, bit offsets); pass 2 writes the slots into dst
-// (zeroed) and rewrites the records in place.
-void launch_le_disk_decode(const uint32_t *words, const uint4 *recs, uint32_t n,
-                           const uint64_t *rowptr, uint32_t *cols, cudaStream_t s);
-void launch_le_choose(const uint64_t *rowptr, const uint32_t *cols, uint32_t n, uint32_t *meta,
-                      uint32_t *fpos, cudaStream_t s);
-void launch_le_write(const uint64_t *rowptr, const uint32_t *cols, uint32_t n,
-                     const uint32_t *meta, const uint32_t *fpos, const uint64_t *P, uint32_t *dst,
-                     uint4 *recs, cudaStream_t s);
-// GT stream with skip fields: pass 1 measures every vertex's skip-field
-// extra width cx[v] and rebuilt payload length len[v] (bits); pass 2 writes
-// the payloads at newP[v] into dst (zeroed) and updates the records in place.
-void launch_gt_skip_measure(const uint32_t *src, const uint4 *recs, uint32_t n,
-                            unsigned char *cx, uint64_t *len, cudaStream_t s);
-void launch_gt_skip_write(const uint32_t *src, uint32_t *dst, uint4 *recs, uint32_t n,
-                          const unsigned char *cx, const uint64_t *newP, cudaStream_t s);
+// Device layout (sector slots, device_common.cuh) of mode GT or LE: pass 0
+// decodes the on-disk stream into a CSR (rowptr = scanned degrees); pass 1
+// picks each vertex's chunk length, field widths and slots per sector (meta)
+// and first_pos (fpos); the host places the vertices (P, bit offsets); pass 2
+// writes the slots into dst (zeroed) and rewrites the records in place.
+void launch_disk_decode(int mode, const uint32_t *words, const uint4 *recs, uint32_t n,
+                        const uint64_t *rowptr, uint32_t *cols, cudaStream_t s);
+void launch_slot_choose(int mode, const uint64_t *rowptr, const uint32_t *cols, uint32_t n,
+                        uint32_t *meta, uint32_t *fpos, cudaStream_t s);
+void launch_slot_write(int mode, const uint64_t *rowptr, const uint32_t *cols, uint32_t n,
+                       const uint32_t *meta, const uint32_t *fpos, const uint64_t *P,
+                       uint32_t *dst, uint4 *recs, cudaStream_t s);
 void launch_degrees(const DevGraph &g, uint32_t *deg, cudaStream_t s);
 void launch_degrees64(const DevGraph &g, uint64_t *deg, cudaStream_t s);
 // In-place exclusive scan of vals[0..n) into vals[0..n]; tmp as above.

@@ -82,8 +82,9 @@ __global__ void __launch_bounds__(256, MODE == 1 ? GRASS_BATCH_MIN_BLOCKS_LE
       rw_warp<MODE, DEPTH>(g, jb.in, jb.count, jb.length, jb.seed, 0, (int)jb.layout, jb.out0,
                            tk.begin, tk.end, cnt, bad);
     } else if (jb.type == GRASS_JOB_KHOP) {
+      const uint32_t parts = max(1u, tk.pad >> 8), part = tk.pad & 0xFFu;
       for (uint64_t s = tk.begin; s < tk.end; s++)
-        khop_seed_warp<MODE>(g, jb.in, jb.khop, s, my, cnt, bad);
+        khop_seed_warp<MODE>(g, jb.in, jb.khop, s, my, cnt, bad, part, parts);
     } else {
       for (uint64_t s = tk.begin; s < tk.end; s++) {
         if (jb.gen_roots) {
@@ -124,7 +125,8 @@ grass_batch_config resolve(const grass_batch_config &c, int mode) {
 
 bool same_shape(const grass_batch_config &a, const grass_batch_config &b) {
   return a.walker_tile == b.walker_tile && a.depth == b.depth &&
-         a.warps_per_block == b.warps_per_block && a.khop_seeds == b.khop_seeds;
+         a.warps_per_block == b.warps_per_block && a.khop_seeds == b.khop_seeds &&
+         a.warps_per_vertex == b.warps_per_vertex;
 }
 
 }  // namespace
@@ -141,6 +143,7 @@ grass_batch_config resolve_batch_config(const grass_batch_config &c, int mode) {
   if (!r.warps_per_block) r.warps_per_block = 8;
   if (!r.khop_seeds) r.khop_seeds = 1;
   if (!r.use_graph) r.use_graph = 1;
+  if (!r.warps_per_vertex) r.warps_per_vertex = 1;
   return r;
 }
 
@@ -179,8 +182,11 @@ void split_job(const grass_job &j, uint32_t ji, const grass_batch_config &c,
                std::vector<BatchTask> &cta, std::vector<BatchTask> &mrw,
                std::vector<BatchTask> &khop, std::vector<BatchTask> &rw) {
   if (j.type == GRASS_JOB_KHOP) {
+    // pad = part | parts << 8: warps_per_vertex items per seed group
+    const uint32_t parts = c.warps_per_vertex;
     for (uint64_t s = 0; s < j.count; s += c.khop_seeds)
-      khop.push_back({ji, 0, s, std::min<uint64_t>(j.count, s + c.khop_seeds)});
+      for (uint32_t p = 0; p < parts; p++)
+        khop.push_back({ji, p | parts << 8, s, std::min<uint64_t>(j.count, s + c.khop_seeds)});
   } else if (j.type == GRASS_JOB_MRW) {
     auto &q = j.select == GRASS_SELECT_DEGREE ? mrw : cta;
     for (uint64_t s = 0; s < j.count; s++) q.push_back({ji, 0, s, s + 1});
@@ -434,11 +440,13 @@ int grass_batch_clear(grass_batch *b) {
 
 int grass_batch_set_config(grass_batch *b, const grass_batch_config *cfg) {
   if (!b || !cfg) return set_error(GRASS_E_ARG, "null argument");
-  const uint32_t t = cfg->walker_tile, d = cfg->depth, w = cfg->warps_per_block;
+  const uint32_t t = cfg->walker_tile, d = cfg->depth, w = cfg->warps_per_block,
+                 v = cfg->warps_per_vertex;
   if ((t && (t % 32 || t > 4096)) || (d && d != 1 && d != 2 && d != 4) ||
-      (w && w != 1 && w != 2 && w != 4 && w != 8) || cfg->use_graph > 2)
+      (w && w != 1 && w != 2 && w != 4 && w != 8) || cfg->use_graph > 2 ||
+      (v && v != 1 && v != 2 && v != 4 && v != 8))
     return set_error(GRASS_E_ARG, "batch config: walker_tile multiple of 32 <= 4096, depth 1/2/4, "
-                                  "warps_per_block 1/2/4/8");
+                                  "warps_per_block 1/2/4/8, warps_per_vertex 1/2/4/8");
   std::lock_guard<std::mutex> lk(b->mu);
   b->cfg = *cfg;
   if (!same_shape(resolve(b->cfg, b->mode()), b->built_cfg)) b->dirty = true;
@@ -504,14 +512,17 @@ int grass_batch_autotune(grass_batch *b, void *stream, grass_batch_config *best,
     GRASS_CUDA(cudaEventCreate(&e1));
   }
   const uint32_t tiles[] = {64, 128, 256}, depths[] = {1, 2, 4}, wpbs[] = {1, 2, 4, 8};
+  const uint32_t wpvs[] = {1, 2, 4, 8};
   int rc = GRASS_OK;
   for (uint32_t t : tiles) {
     for (uint32_t d : depths) {
-      for (uint32_t w : wpbs) {
+      for (uint32_t idx = 0; idx < 16 && !rc; idx++) {
+        const uint32_t w = wpbs[idx & 3], v = wpvs[idx >> 2];
         grass_batch_config c = keep;
         c.walker_tile = t;
         c.depth = d;
         c.warps_per_block = w;
+        c.warps_per_vertex = v;
         if ((rc = grass_batch_set_config(b, &c))) break;
         if ((rc = grass_batch_run(b, stream, nullptr))) break;  // build + warm-up
         float ms = 1e30f;

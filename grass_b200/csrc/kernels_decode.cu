@@ -88,19 +88,6 @@ __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint6
     const uint64_t g0 = t * kTaskNeighbors;
     const uint64_t g1 = min(E, g0 + kTaskNeighbors);
     uint32_t vr = warp_row_of(rowptr, g.n, g0);
-    uint32_t carry = 0;
-    if (MODE == 0) {
-      // a task that starts inside a block needs the value of neighbor g0-1
-      const uint32_t i0 = (uint32_t)(g0 - rowptr[vr]);
-      if (i0 > 0) {
-        uint32_t c = 0;
-        if (lane == 0) {
-          const VHdr h0 = header<0>(g, vr);
-          if (gt_locate(h0, i0).gaps > 0) c = gt_neighbor(g, h0, i0 - 1);
-        }
-        carry = __shfl_sync(FULL, c, 0);
-      }
-    }
     // Header of the vertex that holds the whole current round (fast path),
     // kept across rounds of the same vertex.
     uint32_t cv = 0xFFFFFFFFu;
@@ -164,44 +151,8 @@ __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint6
           startv = rowptr[v];
         }
       }
-      const uint32_t i = (uint32_t)(gl - startv);
-      uint32_t val = 0;
-      if (MODE == 1) {
-        if (act) val = le_neighbor(g, hk, i);
-      } else {
-        bool head = true;
-        uint32_t x = 0;
-        if (act) {
-          const GtRun run = gt_locate(hk, i);
-          if (far) {
-            x = gt_neighbor(g, hk, i);  // complete value; starts its own segment
-          } else if (run.gaps == 0) {  // a head or a skip field: an absolute value
-            const uint32_t hv = read_field(g.words, run.pos, hk.a) + 1u;
-            x = run.up ? hk.v + hv : hk.v - hv;
-            if (run.skip) x += run.id + read_field(g.words, run.spos, hk.b + hk.cx);
-          } else {
-            head = false;
-            const uint64_t at = run.spos + (run.skip ? (uint64_t)(hk.b + hk.cx) : 0ull) +
-                                (uint64_t)(run.gaps - 1) * hk.b;
-            x = (hk.b ? read_field(g.words, at, hk.b) : 0u) + 1u;
-          }
-        }
-        if (lane == 0 && !head) {
-          x += carry;
-          head = true;
-        }
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {  // segmented inclusive scan
-          const uint32_t y = __shfl_up_sync(FULL, x, o);
-          const int f = __shfl_up_sync(FULL, (int)head, o);
-          if (lane >= o && !head) {
-            x += y;
-            head = f;
-          }
-        }
-        carry = __shfl_sync(FULL, x, 31);
-        val = x;
-      }
+      // each neighbor is one independent draw of one sector slot
+      const uint32_t val = act ? neighbor<MODE>(g, hk, (uint32_t)(gl - startv)) : 0u;
       if (act) {
         if (val >= g.n) bad = true;
         cols[gl] = val;
@@ -225,17 +176,10 @@ __global__ void __launch_bounds__(256) decode_all_kernel(DevGraph g, const uint6
 // Planned sweep.  The first sweep of a graph builds a plan once: vertices of
 // degree >= 32 become neighbor ranges of at most 2048 (hubs are split), the
 // others are grouped by floor(log2(degree)).  Then
-//  * a range is decoded by one warp in rounds of 32 consecutive neighbors
-//    (coalesced stores).  The round's chunk / block position is carried from
-//    round to round and each lane steps to its own with a few compares, so
-//    there is no per-neighbor division: LE divides once per chunk
-//    ((r2 - r1) / L_c, by the lane that starts the chunk, then shuffled), GT
-//    runs a segmented warp scan of gaps (LE/src/bcg.cuh:195-261,
-//    GT/src/bcg.cuh:153-168);
-//  * a small vertex is decoded by one lane, sequentially with bit cursors
-//    (seas, or heads and gaps, are contiguous in neighbor order); a warp
-//    takes 32 vertices of one degree class, so its lanes run for similar
-//    lengths.
+//  * a range is decoded by one warp, one lane per chunk slot, 32 slots at a
+//    time (decode_range_kernel);
+//  * a small vertex is decoded by one lane, slot after slot; a warp takes 32
+//    vertices of one degree class, so its lanes run for similar lengths.
 constexpr uint32_t kBigDegree = 32;
 #ifndef GRASS_DECODE_RANGE
 #define GRASS_DECODE_RANGE 2048
@@ -251,7 +195,7 @@ struct LeSeq {
   Sec A;
 
   __device__ __forceinline__ void load_chunk() {
-    const uint64_t pos = le_slot_pos(h, c);
+    const uint64_t pos = slot_pos(h, c);
     A = load_sector(w, pos >> 8);
     off = (uint32_t)pos & 255u;
     L = min(h.bl, h.d - 1 - c * h.bl);
@@ -275,41 +219,38 @@ struct LeSeq {
 };
 
 struct GtSeq {
-  uint32_t v, fp, bl, om, blk, id, len, prev, head;
-  int a, b, sw;  // head, gap and skip-field widths
-  BitCur cur;
+  const uint32_t *w;
+  VHdr h;
+  uint32_t c, id, L;  // slot, index in it, its length
+  uint32_t off, x;    // bit offset of the slot in sector A; the previous value
+  Sec A;
 
-  __device__ __forceinline__ void init(const uint32_t *words, const VHdr &h) {
-    v = h.v;
-    fp = h.fp;
-    bl = h.bl;
-    om = h.om;
-    a = h.a;
-    b = h.b;
-    sw = h.b + h.cx;
-    blk = 0;
-    id = 0;
-    len = om ? bl + 1 : bl;
-    prev = head = 0;
-    cur.init(words, h.P);
+  __device__ __forceinline__ void load_chunk() {
+    const uint64_t pos = slot_pos(h, c);
+    A = load_sector(w, pos >> 8);
+    off = (uint32_t)pos & 255u;
+    L = min(h.bl, h.d - c * h.bl);
+  }
+  __device__ __forceinline__ void init(const uint32_t *words, const VHdr &hd) {
+    w = words;
+    h = hd;
+    c = id = 0;
+    if (h.d) load_chunk();
   }
   __device__ __forceinline__ uint32_t next() {
-    uint32_t val;
     if (id == 0) {
-      const uint32_t hv = (a ? cur.get(a) : 0u) + 1u;
-      val = head = blk >= fp ? v + hv : v - hv;
-    } else if (id % kGtSkip == 0) {  // skip field: the block's raw gaps 1..id summed
-      val = head + id + (sw ? cur.get(sw) : 0u);
+      const uint32_t hv = (uint32_t)sec1_field(A, off, h.a) + 1u;
+      x = c >= h.fp ? h.v + hv : h.v - hv;
     } else {
-      val = prev + (b ? cur.get(b) : 0u) + 1u;
+      x += (h.b ? (uint32_t)sec1_field(A, off + (uint32_t)h.a + (id - 1) * (uint32_t)h.b, h.b)
+                : 0u) + 1u;
     }
-    prev = val;
-    if (++id == len) {
-      blk++;
+    if (++id == L && c + 1 < h.bn) {
+      c++;
       id = 0;
-      len = blk < om ? bl + 1 : bl;
+      load_chunk();
     }
-    return val;
+    return x;
   }
 };
 
@@ -397,32 +338,7 @@ __global__ void plan_fill_kernel(const uint4 *__restrict__ recs, uint32_t n, uin
   }
 }
 
-// The warp asks L2 for every 128-byte line of stream bits [lo, hi): a range
-// reads its stream in order, so without this each new line is a full DRAM
-// round trip with nothing else in flight for the warp.
-__device__ __forceinline__ void prefetch_bits(const uint32_t *words, uint64_t lo, uint64_t hi) {
-  const int lane = threadIdx.x & 31;
-  if (hi <= lo) return;
-  const char *base = reinterpret_cast<const char *>(words);
-  const uint64_t l0 = (lo >> 3) >> 7, l1 = ((hi - 1) >> 3) >> 7;  // lines holding bits lo..hi-1
-  for (uint64_t l = l0 + lane; l <= l1; l += 32)
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(base + (l << 7)));
-}
-
-// A neighbor range is cut into runs of 8 consecutive CSR slots aligned to 8
-// (32 bytes); lane l of a warp takes run l of each group of 32 runs, decodes
-// it in order with a bit cursor and stores a full run with two 16-byte
-// writes, so the warp writes 1 KB contiguous per group.
-#ifndef GRASS_DECODE_RUN
-#define GRASS_DECODE_RUN 8
-#endif
-// Slots per lane run (multiple of 4, <= 32).  Measured on R-MAT s22 ef32:
-// 8 -> LE 1.70 ms; 16 -> 2.52 ms; 4 -> 11.6 ms.  Range length (2048 or 4096)
-// made no difference.
-constexpr uint32_t kRun = GRASS_DECODE_RUN;
-static_assert(kRun % 4 == 0 && kRun <= 32, "run length");
-
-// ---- slot staging for the LE range sweep ----
+// ---- slot staging for the range sweep ----
 // With a staging depth D (2 or 4), lane 0 of a warp copies the sectors that
 // hold each group of 32 chunk slots into one of the warp's D shared-memory
 // buffers with one bulk copy (cp.async.bulk, completion counted on that
@@ -431,7 +347,7 @@ static_assert(kRun % 4 == 0 && kRun <= 32, "run length");
 // that has not landed after kStagePolls polls is reported (error word bit 2,
 // GRASS_E_TIMEOUT) and the warp decodes from global memory from then on,
 // waiting once more, bounded, for its copies in flight before it exits.
-constexpr int kDecodeWarps = 8;          // warps per LE range block
+constexpr int kDecodeWarps = 8;          // warps per range block
 constexpr uint32_t kGroupBytes = 1024;   // 32 slots lie in at most 32 sectors
 constexpr uint32_t kOutWords = 32 * 33;  // a group's neighbors (32 chunks of <= 32, + 1)
 // Polls of the copy's mbarrier before the warp gives up (far beyond the
@@ -495,32 +411,31 @@ __device__ __forceinline__ Sec smem_sector(const void *p) {
   return Sec{swap_halves(q[0]), swap_halves(q[1]), swap_halves(q[2]), swap_halves(q[3])};
 }
 
-// Shared memory of one LE range warp: the group's decoded neighbors, then
+// Shared memory of one range warp: the group's decoded neighbors, then
 // DEPTH staging buffers and their barriers.
 template <int DEPTH>
-struct LeWarpSmem {
+struct WarpSmem {
   static constexpr uint32_t bytes() {
     return kOutWords * 4 + DEPTH * kGroupBytes + (DEPTH ? DEPTH : 1) * 8;
   }
 };
 
-// LE range sweep on the device layout: one lane per chunk slot.  A warp takes
-// a range's chunks 32 at a time: each lane reads its slot (one 32-byte
-// sector, coalesced across the warp, or from the staged group), decodes the
-// chunk's neighbors into shared memory, and the warp writes the group's
-// neighbors to the CSR with coalesced stores.  DEPTH 0: slots from global
-// memory; 2 or 4: staged (see above).
-template <int DEPTH>
-__global__ void __launch_bounds__(256) decode_le_range_kernel(DevGraph g, const uint64_t *rowptr,
-                                                              uint32_t *cols,
-                                                              const uint4 *__restrict__ items,
-                                                              uint64_t nitems,
-                                                              unsigned int *err) {
+// Range sweep on the device layout (GT or LE): one lane per chunk slot.  A
+// warp takes a range's slots 32 at a time: each lane reads its slot (one
+// 32-byte sector, coalesced across the warp, or from the staged group),
+// decodes the chunk's neighbors into shared memory, and the warp writes the
+// group's neighbors to the CSR with coalesced stores.  DEPTH 0: slots from
+// global memory; 2 or 4: staged (see above).
+template <int MODE, int DEPTH>
+__global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uint64_t *rowptr,
+                                                           uint32_t *cols,
+                                                           const uint4 *__restrict__ items,
+                                                           uint64_t nitems, unsigned int *err) {
   extern __shared__ __align__(128) unsigned char le_smem[];
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned char *mine = le_smem + (threadIdx.x >> 5) * LeWarpSmem<DEPTH>::bytes();
+  unsigned char *mine = le_smem + (threadIdx.x >> 5) * WarpSmem<DEPTH>::bytes();
   uint32_t *out = reinterpret_cast<uint32_t *>(mine);
   unsigned char *stage = mine + kOutWords * 4;
   uint64_t *bars = reinterpret_cast<uint64_t *>(stage + DEPTH * kGroupBytes);
@@ -532,17 +447,18 @@ __global__ void __launch_bounds__(256) decode_le_range_kernel(DevGraph g, const 
   bool bad = false;
   for (uint64_t t = warp; t < nitems; t += nwarps) {
     const uint4 it = items[t];
-    const VHdr h = header<1>(g, it.x);
+    const VHdr h = header<MODE>(g, it.x);
     const uint64_t base = rowptr[it.x];
     const uint32_t T = h.bl, last = h.d - 1, i0 = it.y, i1 = it.z;
-    const uint32_t c0 = i0 < last ? i0 / T : h.bn - 1;
-    const uint32_t c1 = i1 - 1 < last ? (i1 - 1) / T : h.bn - 1;
+    // slot of neighbor i: i / T (LE: the last neighbor is slot C-1's right rock)
+    const uint32_t c0 = MODE == 0 || i0 < last ? i0 / T : h.bn - 1;
+    const uint32_t c1 = MODE == 0 || i1 - 1 < last ? (i1 - 1) / T : h.bn - 1;
     const uint32_t ngroups = (c1 - c0) / 32 + 1;
     // sectors [qa, qb] of group j's slots
     auto group_sectors = [&](uint32_t j, uint64_t &qa, uint64_t &qb) {
       const uint32_t ca = c0 + 32 * j, cz = min(c1, ca + 31);
-      qa = le_slot_pos(h, ca) >> 8;
-      qb = le_slot_pos(h, cz) >> 8;
+      qa = slot_pos(h, ca) >> 8;
+      qb = slot_pos(h, cz) >> 8;
     };
     auto issue = [&](uint32_t j) {
       if (!DEPTH || !stage_ok) return;
@@ -572,7 +488,7 @@ __global__ void __launch_bounds__(256) decode_le_range_kernel(DevGraph g, const 
       }
       const uint32_t cg = c0 + 32 * j, c = cg + lane;
       if (c <= c1) {
-        const uint64_t pos = le_slot_pos(h, c);
+        const uint64_t pos = slot_pos(h, c);
         Sec A;
         if (staged) {
           uint64_t qa, qb;
@@ -581,12 +497,15 @@ __global__ void __launch_bounds__(256) decode_le_range_kernel(DevGraph g, const 
         } else {
           A = load_sector(g.words, pos >> 8);
         }
-        // the last chunk also holds neighbor d-1, its right rock
-        le_slot_decode(A, (uint32_t)pos & 255u, h, c, min(T, last - c * T), c + 1 == h.bn,
-                       out + (c - cg) * T);
+        if constexpr (MODE == 0) {
+          gt_slot_decode(A, (uint32_t)pos & 255u, h, c, min(T, h.d - c * T), out + (c - cg) * T);
+        } else {  // the last chunk also holds neighbor d-1, its right rock
+          le_slot_decode(A, (uint32_t)pos & 255u, h, c, min(T, last - c * T), c + 1 == h.bn,
+                         out + (c - cg) * T);
+        }
       }
       __syncwarp();
-      const uint32_t nb0 = cg * T, nhi = cg + 32 >= h.bn ? last + 1 : (cg + 32) * T;
+      const uint32_t nb0 = cg * T, nhi = cg + 32 >= h.bn ? h.d : (cg + 32) * T;
       const uint32_t lo = max(i0, nb0), hi = min(i1, nhi);
       for (uint32_t k = lo + lane; k < hi; k += 32) {
         const uint32_t val = out[k - nb0];
@@ -599,145 +518,6 @@ __global__ void __launch_bounds__(256) decode_le_range_kernel(DevGraph g, const 
   if (DEPTH)  // copies still in flight after a timeout: one more bounded wait each
     for (int b = 0; b < DEPTH; b++)
       if ((pending >> b) & 1u) stage_wait(bars + b, (phase >> b) & 1u);
-  if (bad && err) atomicOr(err, 1u);
-}
-
-// GT range sweep: lane l of a warp takes run l of each group of 32 runs of
-// kRun slots, reads its fields in order with a bit cursor, and a segmented
-// warp scan carries values across runs (a run that starts inside a block
-// continues from the slot before it).
-__global__ void __launch_bounds__(256) decode_gt_range_kernel(DevGraph g, const uint64_t *rowptr,
-                                                              uint32_t *cols,
-                                                              const uint4 *__restrict__ items,
-                                                              uint64_t nitems, bool vec,
-                                                              unsigned int *err) {
-  const int lane = threadIdx.x & 31;
-  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  bool bad = false;
-  for (uint64_t t = warp; t < nitems; t += nwarps) {
-    const uint4 it = items[t];
-    const VHdr h = header<0>(g, it.x);
-    const uint64_t base = rowptr[it.x];
-    const uint64_t G0 = base + it.y, G1 = base + it.z;  // CSR slots of the range
-    const uint32_t split = h.om * (h.bl + 1);
-    {  // ask L2 for the range's stream bits (read in order below), within the payload
-      const uint32_t i0 = it.y, i1 = it.z;
-      const uint64_t pend = payload_end<0>(g, h);
-      const uint32_t c0 = i0 < split ? i0 / (h.bl + 1) : h.om + (i0 - split) / max(h.bl, 1u);
-      const uint64_t cl = c0 + (i1 - i0) / max(h.bl, 1u) + 2;
-      prefetch_bits(g.words, gt_block_pos(h, c0),
-                    min(pend, gt_block_pos(h, (uint32_t)min(cl, (uint64_t)h.bn))));
-    }
-    uint32_t carry = 0;  // value of the slot before the current group
-    bool carry_ok = false;
-    for (uint64_t gs = G0 & ~(uint64_t)(kRun - 1); gs < G1; gs += 32 * kRun) {
-      const uint64_t rs = gs + (uint64_t)lane * kRun;  // this lane's run [rs, rs + 8)
-      const uint64_t a0 = max(rs, G0), a1 = min(rs + kRun, G1);
-      const uint32_t cnt = a1 > a0 ? (uint32_t)(a1 - a0) : 0u;
-      const uint32_t s = cnt ? (uint32_t)(a0 - base) : it.y;  // first neighbor of the run
-      uint32_t vals[kRun];
-      // block c of neighbor s, index id within it, length tl
-      const bool hi = s < split;
-      uint32_t tl = hi ? h.bl + 1 : h.bl;
-      const uint32_t j = hi ? s : s - split;
-      uint32_t c = tl ? j / tl : 0u;
-      uint32_t id = j - c * tl;
-      if (!hi) c += h.om;
-      // Fields in order: block c holds its head (a bits), then tl - 1 gaps,
-      // with a skip field (an absolute value relative to the head) at every
-      // kGtSkip-th position.  Slots before the run's first head or skip field
-      // are relative to the slot before the run, whose value a segmented
-      // warp scan over the runs supplies.
-      BitCur cur;
-      const int sk = h.b + h.cx;  // skip-field width
-      uint64_t hp = 0;            // bit offset of block c
-      if (cnt) {
-        hp = gt_block_pos(h, c);
-        cur.init(g.words, id ? gt_field_pos(h, hp, id) : hp);
-      }
-      uint32_t x = 0, rel = 0;  // rel: bit k set when slot k is relative
-      bool seen = false;         // an absolute value has been read in this run
-      uint32_t hv0 = 0;          // head value of block c, once known
-      bool hk = false;
-#pragma unroll
-      for (uint32_t k = 0; k < kRun; k++) {
-        if (k >= cnt) break;
-        if (id == 0) {
-          const uint32_t hv = (h.a ? cur.get(h.a) : 0u) + 1u;
-          x = hv0 = c >= h.fp ? h.v + hv : h.v - hv;
-          hk = seen = true;
-        } else if (id % kGtSkip == 0) {
-          if (!hk) {  // the run started inside the block: read its head
-            const uint32_t hv = read_field(g.words, hp, h.a) + 1u;
-            hv0 = c >= h.fp ? h.v + hv : h.v - hv;
-            hk = true;
-          }
-          x = hv0 + id + (sk ? cur.get(sk) : 0u);
-          seen = true;
-        } else {
-          x += (h.b ? cur.get(h.b) : 0u) + 1u;
-          if (!seen) rel |= 1u << k;
-        }
-        vals[k] = x;
-        if (++id == tl) {
-          c++;
-          id = 0;
-          tl = c < h.om ? h.bl + 1 : h.bl;
-        }
-      }
-      // (absolute?, last value) of runs 0..lane; empty runs are the identity
-      uint32_t sx = cnt ? x : 0u;
-      bool sf = cnt && seen;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(FULL, sx, o);
-        const bool f = __shfl_up_sync(FULL, (int)sf, o);
-        if (lane >= o && !sf) {
-          sx += y;
-          sf = f;
-        }
-      }
-      uint32_t bx = __shfl_up_sync(FULL, sx, 1);
-      bool bf = __shfl_up_sync(FULL, (int)sf, 1);
-      if (lane == 0) {
-        bx = 0;
-        bf = false;
-      }
-      if (!carry_ok) {  // first group: the slot before G0 (used when G0 is inside a block)
-        uint32_t y = 0;
-        if (lane == 0 && it.y > 0) y = gt_neighbor(g, h, it.y - 1);
-        carry = __shfl_sync(FULL, y, 0);
-        carry_ok = true;
-      }
-      const uint32_t in = bf ? bx : carry + bx;  // value of the slot before the run
-#pragma unroll
-      for (uint32_t k = 0; k < kRun; k++)
-        if ((rel >> k) & 1u) vals[k] += in;
-      const unsigned has = __ballot_sync(FULL, cnt > 0);
-      uint32_t lastv = 0;
-#pragma unroll
-      for (uint32_t k = 0; k < kRun; k++)
-        if (k + 1 == cnt) lastv = vals[k];
-      carry = __shfl_sync(FULL, lastv, 31 - __clz(has));
-      if (cnt) {
-        uint32_t *o = cols + a0;
-        if (cnt == kRun && vec) {  // aligned full run: 16-byte stores
-#pragma unroll
-          for (uint32_t q = 0; q < kRun / 4; q++)
-            reinterpret_cast<uint4 *>(o)[q] =
-                make_uint4(vals[4 * q], vals[4 * q + 1], vals[4 * q + 2], vals[4 * q + 3]);
-        } else {
-#pragma unroll
-          for (uint32_t k = 0; k < kRun; k++)
-            if (k < cnt) o[k] = vals[k];
-        }
-#pragma unroll
-        for (uint32_t k = 0; k < kRun; k++)
-          if (k < cnt) bad |= vals[k] >= g.n;
-      }
-    }
-  }
   if (bad && err) atomicOr(err, 1u);
 }
 
@@ -774,18 +554,28 @@ __global__ void __launch_bounds__(256) decode_small_kernel(DevGraph g, const uin
 static void launch_plan_kernels(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
                                 unsigned int *err, cudaStream_t s);
 
-template <int DEPTH>
-static void launch_le_range(const DevGraph &v, const uint64_t *rowptr, uint32_t *cols,
-                            const grass_graph *g, unsigned grid, unsigned int *err,
-                            cudaStream_t s) {
-  const uint32_t smem = kDecodeWarps * LeWarpSmem<DEPTH>::bytes();
+template <int MODE, int DEPTH>
+static void launch_range(const DevGraph &v, const uint64_t *rowptr, uint32_t *cols,
+                         const grass_graph *g, unsigned grid, unsigned int *err, cudaStream_t s) {
+  const uint32_t smem = kDecodeWarps * WarpSmem<DEPTH>::bytes();
   static std::once_flag once;  // opt in to more than 48 KB of dynamic shared memory
   std::call_once(once, [&] {
-    cudaFuncSetAttribute(decode_le_range_kernel<DEPTH>,
+    cudaFuncSetAttribute(decode_range_kernel<MODE, DEPTH>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   });
-  decode_le_range_kernel<DEPTH><<<grid, 32 * kDecodeWarps, smem, s>>>(
+  decode_range_kernel<MODE, DEPTH><<<grid, 32 * kDecodeWarps, smem, s>>>(
       v, rowptr, cols, g->d_plan_big, g->plan_nbig, err);
+}
+
+template <int MODE>
+static void launch_range_depth(const DevGraph &v, const uint64_t *rowptr, uint32_t *cols,
+                               const grass_graph *g, unsigned grid, unsigned int *err,
+                               cudaStream_t s) {
+  switch (g->tuning.decode_stage_depth) {
+    case 2: launch_range<MODE, 2>(v, rowptr, cols, g, grid, err, s); break;
+    case 4: launch_range<MODE, 4>(v, rowptr, cols, g, grid, err, s); break;
+    default: launch_range<MODE, 0>(v, rowptr, cols, g, grid, err, s);
+  }
 }
 
 int launch_decode_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
@@ -871,17 +661,8 @@ static void launch_plan_kernels(const grass_graph *g, const uint64_t *rowptr, ui
   if (g->plan_nbig) {
     const unsigned grid = (unsigned)std::max<uint64_t>(
         1, std::min<uint64_t>((g->plan_nbig + 7) / 8, (uint64_t)sm_count(dev) * per_sm));
-    const bool vec = (reinterpret_cast<uintptr_t>(cols) & 15u) == 0;  // 16-byte stores allowed
-    if (g->mode == GRASS_MODE_GT) {
-      decode_gt_range_kernel<<<grid, 256, 0, s>>>(v, rowptr, cols, g->d_plan_big, g->plan_nbig,
-                                                  vec, err);
-    } else {
-      switch (g->tuning.decode_stage_depth) {
-        case 2: launch_le_range<2>(v, rowptr, cols, g, grid, err, s); break;
-        case 4: launch_le_range<4>(v, rowptr, cols, g, grid, err, s); break;
-        default: launch_le_range<0>(v, rowptr, cols, g, grid, err, s);
-      }
-    }
+    if (g->mode == GRASS_MODE_GT) launch_range_depth<0>(v, rowptr, cols, g, grid, err, s);
+    else launch_range_depth<1>(v, rowptr, cols, g, grid, err, s);
     count_launch();
   }
   if (g->plan_nsmall) {

@@ -223,7 +223,7 @@ __device__ __forceinline__ void or_bits(uint32_t *w, uint64_t off, uint64_t val,
   if (lo) atomicOr(w + (off >> 5) + 1, lo);
 }
 
-// ---- LE device layout (le_slot_pos, device_common.cuh) ----
+// ---- LE device layout (sector slots, device_common.cuh) ----
 
 // Neighbor i of an LE vertex in the on-disk layout: rocks at P + c a, seas at
 // P + (chunk_num + 1) a + k (sea_bit + 1) (LE/src/bcg.cuh:195-261).
@@ -270,9 +270,9 @@ __global__ void __launch_bounds__(256) le_disk_decode_kernel(const uint32_t *__r
 __device__ __forceinline__ uint32_t bit_len64(uint64_t x) { return x ? 64u - __clzll(x) : 1u; }
 
 // Chunk lengths tried per vertex; slots must fit a sector (cb <= 256).
-__constant__ uint8_t kLeChunkLens[] = {1, 2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 16, 20, 24, 28, 32};
-constexpr int kNumChunkLens = sizeof(kLeChunkLens);
-constexpr uint32_t kLeMaxSlots = 63;  // K is stored in 6 bits
+__constant__ uint8_t kChunkLens[] = {1, 2, 3, 4, 5, 6, 7, 8, 10, 12, 14, 16, 20, 24, 28, 32};
+constexpr int kNumChunkLens = sizeof(kChunkLens);
+constexpr uint32_t kMaxSlots = 63;  // K is stored in 6 bits
 
 // Pass 1: per vertex of degree >= 2, the chunk length T with the fewest
 // bits (a vertex of one sector: C cb; larger: whole sectors), its sea_bit
@@ -301,7 +301,7 @@ __global__ void __launch_bounds__(256) le_choose_kernel(const uint64_t *__restri
     uint64_t best = ~0ull;
     uint32_t bT = 1, bsb = 0, bK = 1;
     for (int t = 0; t < kNumChunkLens; t++) {
-      const uint32_t T = kLeChunkLens[t];
+      const uint32_t T = kChunkLens[t];
       if (T > 1 && T >= d) break;  // one chunk already holds every neighbor
       uint32_t sb = 0;
       for (uint32_t i = lane; i < last; i += 32) {
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(256) le_choose_kernel(const uint64_t *__restri
       sb = __reduce_max_sync(FULLM, sb);
       const uint32_t cb = 2 * a + (T - 1) * (sb + 1);
       if (cb > 256) continue;
-      const uint32_t K = min(256u / cb, kLeMaxSlots);
+      const uint32_t K = min(256u / cb, kMaxSlots);
       const uint32_t C = (last - 1) / T + 1;
       const uint64_t cost = C <= K ? (uint64_t)C * cb : (uint64_t)((C + K - 1) / K) * 256u;
       if (cost < best) best = cost, bT = T, bsb = sb, bK = K;
@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(256) le_write_kernel(const uint64_t *__restric
     const uint64_t base = rowptr[v];
     const uint32_t d = (uint32_t)(rowptr[v + 1] - base);
     if (d < 2) {
-      if (lane == 0) recs[v] = d ? pack_le_record(0, 0, 0, 0, 0, 1, cols[base]) : make_uint4(0, 0, 0, 0);
+      if (lane == 0) recs[v] = d ? pack_slot_record(0, 0, 0, 0, 0, 1, cols[base]) : make_uint4(0, 0, 0, 0);
       continue;
     }
     const uint32_t *nb = cols + base;
@@ -368,95 +368,130 @@ __global__ void __launch_bounds__(256) le_write_kernel(const uint64_t *__restric
       }
       or_bits(dst, at + a + (uint64_t)(T - 1) * sw, (uint64_t)llabs((int64_t)r2 - (int64_t)v), a);
     }
-    if (lane == 0) recs[v] = pack_le_record(P[v], a, sb, T, K, d, fpos[v]);
+    if (lane == 0) recs[v] = pack_slot_record(P[v], a, sb, T, K, d, fpos[v]);
   }
 }
 
-// ---- GT stream with skip fields (gt_block_pos, device_common.cuh) ----
-// Both kernels take one warp per vertex and one lane per block, reading the
-// on-disk stream through each block's cursor: head (a bits), then len - 1
-// raw gaps (b bits), GT/chunk_compress/compressor.hpp:297-349.
+// ---- GT device layout (sector slots, device_common.cuh) ----
 
-__device__ __forceinline__ uint32_t bit_len(uint32_t x) { return x ? 32u - __clz(x) : 1u; }
-
-// Pass 1: per vertex the skip-field extra width cx (bits of the largest
-// running gap sum at a skip position, beyond b) and the rebuilt payload's
-// length in bits.
-__global__ void __launch_bounds__(256) gt_skip_measure_kernel(const uint32_t *__restrict__ src,
-                                                              const uint4 *__restrict__ recs,
-                                                              uint32_t n,
-                                                              unsigned char *__restrict__ cx,
-                                                              uint64_t *__restrict__ len) {
+// Pass 0: every GT neighbor list, decoded from the on-disk stream into a
+// temporary CSR: one warp per vertex, one lane per block, each block's head
+// and gaps read in order (GT/src/bcg.cuh:153-168).
+__global__ void __launch_bounds__(256) gt_disk_decode_kernel(const uint32_t *__restrict__ words,
+                                                             const uint4 *__restrict__ recs,
+                                                             uint32_t n,
+                                                             const uint64_t *__restrict__ rowptr,
+                                                             uint32_t *__restrict__ cols) {
   const int lane = threadIdx.x & 31;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   for (uint64_t v = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
-    const VHdr h = record_header<0>(recs[v], (uint32_t)v);  // on-disk layout (cx = 0)
-    if (h.d == 0) {
-      if (lane == 0) cx[v] = 0, len[v] = 0;
-      continue;
-    }
-    const uint32_t longest = h.bl + (h.om ? 1u : 0u);
-    uint32_t mx = 0;  // bits of the largest gap sum at a skip position
-    if (longest - 1 >= kGtSkip) {
-      for (uint32_t blk = lane; blk < h.bn; blk += 32) {
-        const uint32_t L = blk < h.om ? h.bl + 1 : h.bl;
-        BitCur c;
-        c.init(src, gt_block_pos(h, blk) + h.a);
-        uint32_t sum = 0;
-        for (uint32_t t = 1; t < L; t++) {
-          sum += h.b ? c.get(h.b) : 0u;
-          if (t % kGtSkip == 0) mx = max(mx, bit_len(sum));
-        }
-      }
-      mx = __reduce_max_sync(0xFFFFFFFFu, mx);
-    }
-    if (lane == 0) {
-      const uint32_t x = mx > (uint32_t)h.b ? mx - (uint32_t)h.b : 0u;
-      VHdr hn = h;
-      hn.cx = (int)x;
-      cx[v] = (unsigned char)x;
-      len[v] = payload_end<0>(DevGraph{}, hn) - h.P;
-    }
-  }
-}
-
-// Pass 2: the rebuilt payload of every vertex at its new offset newP[v] in
-// dst (zeroed), and its record updated in place (P, and cx above first_pos).
-__global__ void __launch_bounds__(256) gt_skip_write_kernel(const uint32_t *__restrict__ src,
-                                                            uint32_t *dst, uint4 *recs,
-                                                            uint32_t n,
-                                                            const unsigned char *__restrict__ cx,
-                                                            const uint64_t *__restrict__ newP) {
-  const int lane = threadIdx.x & 31;
-  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  for (uint64_t v = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
-    const VHdr h = record_header<0>(recs[v], (uint32_t)v);
-    VHdr hn = h;
-    hn.P = newP[v];
-    hn.cx = cx[v];
-    const int sk = hn.b + hn.cx;
+    const VHdr h = gt_disk_record_header(recs[v], (uint32_t)v);
+    uint32_t *out = cols + rowptr[v];
     for (uint32_t blk = lane; blk < h.bn; blk += 32) {
       const uint32_t L = blk < h.om ? h.bl + 1 : h.bl;
+      const uint32_t i0 = blk * h.bl + min(blk, h.om);
       BitCur c;
-      c.init(src, gt_block_pos(h, blk));
-      uint64_t at = gt_block_pos(hn, blk);
-      or_bits(dst, at, c.get(h.a), h.a);
-      at += h.a;
-      uint32_t sum = 0;
+      c.init(words, gt_disk_block_pos(h, blk));
+      const uint32_t hv = c.get(h.a) + 1u;
+      uint32_t x = blk >= h.fp ? h.v + hv : h.v - hv;
+      out[i0] = x;
       for (uint32_t t = 1; t < L; t++) {
-        const uint32_t gap = h.b ? c.get(h.b) : 0u;
-        sum += gap;
-        if (t % kGtSkip == 0) {
-          if (sk) or_bits(dst, at, sum, sk);
-          at += sk;
-        } else {
-          if (h.b) or_bits(dst, at, gap, h.b);
-          at += h.b;
-        }
+        x += (h.b ? c.get(h.b) : 0u) + 1u;
+        out[i0 + t] = x;
       }
     }
-    __syncwarp();  // every lane has read the old record
-    if (lane == 0) recs[v] = pack_record(hn);
+  }
+}
+
+// Pass 1: per vertex of degree >= 1, the chunk length T with the fewest bits
+// (as for LE), the head width a (bits of the largest |n_cT - v| - 1), the gap
+// width b (bits of the largest n_i - n_{i-1} - 1 inside a chunk; 0 without
+// gaps), K, and first_pos (chunks whose head lies below v).
+// meta[v] = T | b << 8 | K << 16 | a << 24.
+__global__ void __launch_bounds__(256) gt_choose_kernel(const uint64_t *__restrict__ rowptr,
+                                                        const uint32_t *__restrict__ cols,
+                                                        uint32_t n, uint32_t *__restrict__ meta,
+                                                        uint32_t *__restrict__ fpos) {
+  const int lane = threadIdx.x & 31;
+  const unsigned FULLM = 0xFFFFFFFFu;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
+    const uint64_t base = rowptr[v];
+    const uint32_t d = (uint32_t)(rowptr[v + 1] - base);
+    if (d == 0) {
+      if (lane == 0) meta[v] = 0, fpos[v] = 0;
+      continue;
+    }
+    const uint32_t *nb = cols + base;
+    const int64_t vv = (int64_t)v;
+    uint64_t best = ~0ull;
+    uint32_t bT = 1, bb = 0, bK = 1, ba = 1;
+    for (int t = 0; t < kNumChunkLens; t++) {
+      const uint32_t T = kChunkLens[t];
+      if (T > 1 && T > d) break;  // one chunk already holds every neighbor
+      uint32_t a = 1, b = 0;
+      for (uint32_t i = lane; i < d; i += 32) {
+        if (i % T == 0) {
+          a = max(a, bit_len64((uint64_t)(llabs((int64_t)nb[i] - vv) - 1)));
+        } else {
+          b = max(b, bit_len64((uint64_t)(nb[i] - nb[i - 1] - 1)));
+        }
+      }
+      a = __reduce_max_sync(FULLM, a);
+      b = __reduce_max_sync(FULLM, b);
+      const uint32_t cb = a + (T - 1) * b;
+      if (cb > 256) continue;
+      const uint32_t K = min(256u / cb, kMaxSlots);
+      const uint32_t C = (d - 1) / T + 1;
+      const uint64_t cost = C <= K ? (uint64_t)C * cb : (uint64_t)((C + K - 1) / K) * 256u;
+      if (cost < best) best = cost, bT = T, bb = b, bK = K, ba = a;
+    }
+    const uint32_t C = (d - 1) / bT + 1;
+    uint32_t below = 0;
+    for (uint32_t c = lane; c < C; c += 32) below += nb[c * bT] < v;
+    below = __reduce_add_sync(FULLM, below);
+    if (lane == 0) {
+      meta[v] = bT | bb << 8 | bK << 16 | ba << 24;
+      fpos[v] = below;
+    }
+  }
+}
+
+// Pass 2: every vertex's slots at its offset P[v] in dst (zeroed), and its
+// record rewritten in place in the device format.
+__global__ void __launch_bounds__(256) gt_write_kernel(const uint64_t *__restrict__ rowptr,
+                                                       const uint32_t *__restrict__ cols,
+                                                       uint32_t n,
+                                                       const uint32_t *__restrict__ meta,
+                                                       const uint32_t *__restrict__ fpos,
+                                                       const uint64_t *__restrict__ P,
+                                                       uint32_t *dst, uint4 *recs) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t v = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; v < n; v += nwarps) {
+    const uint64_t base = rowptr[v];
+    const uint32_t d = (uint32_t)(rowptr[v + 1] - base);
+    if (d == 0) {
+      if (lane == 0) recs[v] = make_uint4(0, 0, 0, 0);
+      continue;
+    }
+    const uint32_t *nb = cols + base;
+    const uint32_t m = meta[v];
+    const uint32_t T = m & 0xFFu, b = (m >> 8) & 0xFFu, K = (m >> 16) & 0xFFu, a = m >> 24;
+    const uint32_t cb = a + (T - 1) * b, C = (d - 1) / T + 1;
+    for (uint32_t c = lane; c < C; c += 32) {
+      const uint32_t q = c / K;
+      uint64_t at = P[v] + (uint64_t)q * 256u + (uint64_t)(c - q * K) * cb;
+      const uint32_t i0 = c * T, L = min(T, d - i0);
+      const uint64_t head = (uint64_t)(llabs((int64_t)nb[i0] - (int64_t)v) - 1);
+      if (head) or_bits(dst, at, head, a);
+      at += a;
+      for (uint32_t t = 1; t < L; t++, at += b) {
+        const uint32_t gap = nb[i0 + t] - nb[i0 + t - 1] - 1;
+        if (gap) or_bits(dst, at, gap, b);
+      }
+    }
+    if (lane == 0) recs[v] = pack_slot_record(P[v], a, b, T, K, d, fpos[v]);
   }
 }
 
@@ -507,45 +542,36 @@ void launch_build_records(const DevGraph &g, uint4 *recs, cudaStream_t s) {
   count_launch();
 }
 
-void launch_le_disk_decode(const uint32_t *words, const uint4 *recs, uint32_t n,
-                           const uint64_t *rowptr, uint32_t *cols, cudaStream_t s) {
+void launch_disk_decode(int mode, const uint32_t *words, const uint4 *recs, uint32_t n,
+                        const uint64_t *rowptr, uint32_t *cols, cudaStream_t s) {
   int dev = 0;
   cudaGetDevice(&dev);
-  le_disk_decode_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(words, recs, n, rowptr, cols);
+  const unsigned grid = (unsigned)sm_count(dev) * 8;
+  if (mode == GRASS_MODE_GT) gt_disk_decode_kernel<<<grid, 256, 0, s>>>(words, recs, n, rowptr, cols);
+  else le_disk_decode_kernel<<<grid, 256, 0, s>>>(words, recs, n, rowptr, cols);
   count_launch();
 }
 
-void launch_le_choose(const uint64_t *rowptr, const uint32_t *cols, uint32_t n, uint32_t *meta,
-                      uint32_t *fpos, cudaStream_t s) {
+void launch_slot_choose(int mode, const uint64_t *rowptr, const uint32_t *cols, uint32_t n,
+                        uint32_t *meta, uint32_t *fpos, cudaStream_t s) {
   int dev = 0;
   cudaGetDevice(&dev);
-  le_choose_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(rowptr, cols, n, meta, fpos);
+  const unsigned grid = (unsigned)sm_count(dev) * 8;
+  if (mode == GRASS_MODE_GT) gt_choose_kernel<<<grid, 256, 0, s>>>(rowptr, cols, n, meta, fpos);
+  else le_choose_kernel<<<grid, 256, 0, s>>>(rowptr, cols, n, meta, fpos);
   count_launch();
 }
 
-void launch_le_write(const uint64_t *rowptr, const uint32_t *cols, uint32_t n,
-                     const uint32_t *meta, const uint32_t *fpos, const uint64_t *P, uint32_t *dst,
-                     uint4 *recs, cudaStream_t s) {
+void launch_slot_write(int mode, const uint64_t *rowptr, const uint32_t *cols, uint32_t n,
+                       const uint32_t *meta, const uint32_t *fpos, const uint64_t *P,
+                       uint32_t *dst, uint4 *recs, cudaStream_t s) {
   int dev = 0;
   cudaGetDevice(&dev);
-  le_write_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(rowptr, cols, n, meta, fpos, P, dst,
-                                                              recs);
-  count_launch();
-}
-
-void launch_gt_skip_measure(const uint32_t *src, const uint4 *recs, uint32_t n,
-                            unsigned char *cx, uint64_t *len, cudaStream_t s) {
-  int dev = 0;
-  cudaGetDevice(&dev);
-  gt_skip_measure_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(src, recs, n, cx, len);
-  count_launch();
-}
-
-void launch_gt_skip_write(const uint32_t *src, uint32_t *dst, uint4 *recs, uint32_t n,
-                          const unsigned char *cx, const uint64_t *newP, cudaStream_t s) {
-  int dev = 0;
-  cudaGetDevice(&dev);
-  gt_skip_write_kernel<<<(unsigned)sm_count(dev) * 8, 256, 0, s>>>(src, dst, recs, n, cx, newP);
+  const unsigned grid = (unsigned)sm_count(dev) * 8;
+  if (mode == GRASS_MODE_GT)
+    gt_write_kernel<<<grid, 256, 0, s>>>(rowptr, cols, n, meta, fpos, P, dst, recs);
+  else
+    le_write_kernel<<<grid, 256, 0, s>>>(rowptr, cols, n, meta, fpos, P, dst, recs);
   count_launch();
 }
 

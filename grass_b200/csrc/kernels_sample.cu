@@ -99,35 +99,17 @@ __global__ void __launch_bounds__(512, MODE == 0 ? GRASS_RW_GT_MIN_BLOCKS : GRAS
 template <int MODE>
 __device__ __forceinline__ void draw_footprint(const DevGraph &g, const VHdr &h, uint32_t i,
                                                uint64_t &bits, uint64_t &sectors) {
-  uint64_t r0[3], r1[3];  // half-open bit ranges, in stream order
-  int nr = 0;
-  if (MODE == 0) {  // the head; the skip field and the gaps after it
-    const GtRun r = gt_locate(h, i);
-    r0[nr] = r.pos;
-    r1[nr++] = r.pos + h.a;
-    const uint64_t e = r.spos + (r.skip ? (uint64_t)(h.b + h.cx) : 0ull) + (uint64_t)r.gaps * h.b;
-    if (e > r.spos) {
-      r0[nr] = r.spos;
-      r1[nr++] = e;
-    }
-  } else if (h.d > 1) {
-    // the device layout: the chunk's slot, inside one sector; the bits read
-    // are the left rock, and for an inner neighbor the right rock and a sea
+  (void)g;
+  sectors = 1;  // a chunk slot never crosses a sector
+  if (MODE == 0) {  // the slot's head and the gaps up to neighbor i
+    bits = (uint64_t)h.a + (uint64_t)(i % h.bl) * h.b;
+  } else if (h.d > 1) {  // the left rock; for an inner neighbor the right rock and a sea
     uint32_t c, id, L;
     le_locate(h, i, c, id, L);
     bits = id == 0 ? (uint64_t)h.a : id == L ? 2ull * h.a : 2ull * h.a + h.b + 1;
-    sectors = 1;
-    return;
-  }
-  bits = 0;
-  sectors = 0;
-  uint64_t last = ~0ull;
-  for (int k = 0; k < nr; k++) {
-    if (r1[k] <= r0[k]) continue;
-    bits += r1[k] - r0[k];
-    const uint64_t s0 = r0[k] >> 8, s1 = (r1[k] - 1) >> 8;
-    sectors += s1 - s0 + 1 - (s0 == last ? 1 : 0);
-    last = s1;
+  } else {  // LE degree 1: the neighbor is in the record
+    bits = 0;
+    sectors = 0;
   }
 }
 

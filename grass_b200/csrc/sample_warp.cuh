@@ -103,20 +103,34 @@ struct SmemHdr {
   }
 };
 
+// With parts > 1, `parts` warps share the seed: warp `part` takes the subtrees
+// of the first hop's children part, part + parts, ... for every later hop.
+// Every part draws the first hop itself (the same values: each writes them,
+// only part 0 counts them), so no warp waits for another.  Draws keep their
+// Philox slot, so the output is the same for any number of parts.
 template <int MODE>
 __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t *seeds,
                                                const KhopArgs &A, uint64_t s, SmemHdr &my,
-                                               uint64_t &cnt, bool &bad) {
+                                               uint64_t &cnt, bool &bad, uint32_t part = 0,
+                                               uint32_t parts = 1) {
   const int lane = threadIdx.x & 31;
   for (uint32_t hop = 0; hop < A.hops; hop++) {
     const uint32_t f = A.fan[hop];
-    const uint64_t P = hop ? A.width[hop - 1] : 1;
+    const uint64_t Pall = hop ? A.width[hop - 1] : 1;
+    // this part's parents: Q consecutive ones under each of its first-hop children
+    const uint64_t Q = hop ? Pall / A.fan[0] : 1;
+    const uint64_t mine = hop ? (part < A.fan[0] ? (A.fan[0] - part + parts - 1) / parts : 0) : 1;
+    const uint64_t P = mine * Q;
+    auto parent = [&](uint64_t k) -> uint64_t {
+      return hop ? (part + (k / Q) * parts) * Q + k % Q : 0;
+    };
+    const bool count = hop || part == 0;
     uint32_t *out = A.out[hop] + s * A.width[hop];
     const uint32_t *prev = hop ? A.out[hop - 1] + s * A.width[hop - 1] : nullptr;
     for (uint64_t pc = 0; pc < P; pc += 32) {
       const uint64_t p = pc + lane;
       uint32_t t = INVALID_VERTEX;
-      if (p < P) t = hop ? prev[p] : seeds[s];
+      if (p < P) t = hop ? prev[parent(p)] : seeds[s];
       VHdr h;
       if (t < g.n) {
         h = header<MODE>(g, t);
@@ -140,7 +154,7 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
         uint32_t nv = INVALID_VERTEX;
         if (act) {
           const uint32_t pl = (uint32_t)(j / f);
-          slot = pc * f + j;
+          slot = parent(pc + pl) * f + (j - (uint64_t)pl * f);
           const VHdr hk = my.get(pl);
           if (hk.d) {
             draw = true;
@@ -154,7 +168,7 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
             if (nv >= g.n) {
               bad = true;
               nv = INVALID_VERTEX;
-            } else {
+            } else if (count) {
               cnt++;
             }
           }

@@ -354,14 +354,18 @@ typedef struct {
 } grass_job;
 
 /* Launch shape of the batched kernel; zero fields take defaults.  The
- * autotuner sweeps walker_tile x depth x warps_per_block. */
+ * autotuner sweeps walker_tile x depth x warps_per_block x warps_per_vertex. */
 typedef struct {
   uint32_t walker_tile;      /* RW walkers per work item: 64, 128, 256 (default 64)           */
   uint32_t depth;            /* RW walkers in flight per lane: 1, 2, 4 (default 1)            */
   uint32_t warps_per_block;  /* 1, 2, 4, 8 (default 8)                                        */
   uint32_t khop_seeds;       /* k-hop seeds per work item (default 1)                         */
   uint32_t use_graph;        /* 1 (default): replay a captured CUDA graph; 2: plain launches  */
-  uint32_t reserved[3];
+  uint32_t warps_per_vertex; /* k-hop: warps sharing one seed vertex's expansion, split by
+                                its first hop's subtrees: 1, 2, 4, 8 (default 1); the
+                                counterpart of the reference's per-transit thread-block /
+                                grid kernels (GT/src/grass.cu:884-1083)                   */
+  uint32_t reserved[2];
 } grass_batch_config;
 
 typedef struct grass_batch grass_batch;

@@ -109,12 +109,15 @@ def test_batch_configs_and_autotune(mode):
     d, rowptr, cols, meta = golden_graph("rmat_s10_e8")
     g = G.Graph(os.path.join(d, mode), mode)
     m = Mix(torch, g, g.n)
-    for tile, depth, wpb in [(64, 1, 1), (256, 4, 8), (96, 2, 2)]:
-        m.batch.set_config(walker_tile=tile, depth=depth, warps_per_block=wpb, khop_seeds=3)
-        m.check()
+    for tile, depth, wpb, wpv in [(64, 1, 1, 1), (256, 4, 8, 2), (96, 2, 2, 4), (64, 1, 8, 8)]:
+        m.batch.set_config(walker_tile=tile, depth=depth, warps_per_block=wpb, khop_seeds=3,
+                           warps_per_vertex=wpv)
+        m.check()  # k-hop seeds split over wpv warps: the same frontiers and edge counts
     best, ms = m.batch.autotune()
     assert ms > 0 and best["walker_tile"] in (64, 128, 256)
+    assert best["warps_per_vertex"] in (1, 2, 4, 8)
     assert m.batch.config()["walker_tile"] == best["walker_tile"]
+    assert m.batch.config()["warps_per_vertex"] == best["warps_per_vertex"]
     m.check()
 
 
@@ -128,5 +131,6 @@ def test_batch_on_csr_equals_compressed(mode):
     csr = g.csr()
     m = Mix(torch, g, g.n, on=csr)
     m.check(runs=2)
-    m.batch.set_config(walker_tile=64, depth=2, warps_per_block=4, khop_seeds=2)
+    m.batch.set_config(walker_tile=64, depth=2, warps_per_block=4, khop_seeds=2,
+                       warps_per_vertex=4)
     m.check()

@@ -1,6 +1,6 @@
 """Bounded device waits: the decode sweep's staged-copy wait runs out, the
-warp reports GRASS_E_TIMEOUT through the graph's error word and decodes the
-range from global memory instead, and the context stays usable.
+warp reports GRASS_E_TIMEOUT through the graph's error word and decodes its
+slots from global memory instead, and the context stays usable.
 
 The wait is made to run out without a GPU fault: the test build of the
 library (grass_b200/lib/libgrass_b200_stagetest.so, GRASS_STAGE_NEVER_COPY)
@@ -26,15 +26,18 @@ def test_staged_wait_runs_out_and_is_reported(tmp_path):
     for name, args in {"grass_open": [C.c_char_p, C.c_int, C.c_int, C.POINTER(P)],
                        "grass_decode_all": [P, P, P, P],
                        "grass_check_device_error": [P, P], "grass_close": [P],
+                       "grass_set_tuning": [P, P],
                        "grass_rw": [P, P, P, C.c_uint64, P, P, P]}.items():
         getattr(lib, name).argtypes = args
         getattr(lib, name).restype = C.c_int
-    # R-MAT scale 16: hubs whose LE chunks span more than 256 bits keep the
-    # on-disk order, and their decode ranges stage their seas
+    # R-MAT scale 16: its vertices of degree >= 32 are decoded by the range
+    # sweep, which stages their slots
     rp, cols = G.rmat_graph(16, 16, seed=42)
     G.compress_to_files(rp, cols, "LE", str(tmp_path / "LE"))
     g = P()
     assert lib.grass_open(str(tmp_path / "LE").encode(), G.MODE_LE, 0, C.byref(g)) == G.OK
+    tune = G.Tuning(decode_stage_depth=2)  # the range sweep stages its slots
+    assert lib.grass_set_tuning(g, C.cast(C.byref(tune), P)) == G.OK
     n, E = len(rp) - 1, len(cols)
     rp_d = torch.empty(n + 1, dtype=torch.int64, device="cuda")
     cl_d = torch.empty(E, dtype=torch.int32, device="cuda")
@@ -62,13 +65,16 @@ def test_staged_wait_runs_out_and_is_reported(tmp_path):
     assert lib.grass_close(g) == G.OK
 
 
-def test_library_decode_reports_no_error():
-    """The shipped library on the same kind of graph: no timeout."""
-    import torch
+@pytest.mark.parametrize("mode", ["LE", "GT"])
+@pytest.mark.parametrize("depth", [0, 2, 4])
+def test_library_decode_staged_reports_no_error(mode, depth):
+    """The shipped library, slots staged or not: the same CSR, no error."""
     rp, cols = G.rmat_graph(16, 16, seed=42)
-    gb, ob = G.compress(rp, cols, "LE")
-    g = G.Graph.from_bytes(gb, ob, "LE")
-    r, c = g.decode_all()
-    np.testing.assert_array_equal(c, cols)
-    g.check_device_error()
-    torch.cuda.synchronize()
+    gb, ob = G.compress(rp, cols, mode)
+    g = G.Graph.from_bytes(gb, ob, mode)
+    g.set_tuning(decode_stage_depth=depth)
+    for _ in range(2):
+        r, c = g.decode_all()
+        np.testing.assert_array_equal(r, rp.astype(np.uint64))
+        np.testing.assert_array_equal(c, cols)
+        g.check_device_error()
