@@ -485,8 +485,12 @@ int grass_server_wait(grass_server *s, uint64_t ticket, uint32_t timeout_ms, gra
 /* Frees a finished request's result memory. */
 int grass_server_release(grass_server *s, uint64_t ticket);
 int grass_server_stats_get(grass_server *s, grass_server_stats *st);
-/* Finishes the running batches (bounded by timeout_ms), fails waiting
- * requests with GRASS_E_TIMEOUT and frees everything. */
+/* Fails the requests not yet launched with GRASS_E_TIMEOUT, waits up to
+ * timeout_ms for the running batches, then stops the dispatcher thread and
+ * frees the streams, arenas and results.  If batches are still running when
+ * timeout_ms ends it returns GRASS_E_TIMEOUT and frees nothing (the
+ * dispatcher and the batches' callbacks still use the server): the server
+ * accepts no new requests and the caller calls grass_server_destroy again. */
 int grass_server_destroy(grass_server *s, uint32_t timeout_ms);
 
 /* Open-loop load generator for the serving loop: Poisson arrivals at `rate`
