@@ -501,8 +501,8 @@ int grass_set_tuning(grass_graph *g, const grass_tuning *t) {
     return set_error(GRASS_E_ARG, "rw_depth must be 1, 2 or 4");
   if (t->rw_threads && (t->rw_threads % 32 || t->rw_threads > 512))
     return set_error(GRASS_E_ARG, "rw_threads must be a multiple of 32 up to 512");
-  if (t->decode_stage_depth != 0 && t->decode_stage_depth != 2 && t->decode_stage_depth != 4)
-    return set_error(GRASS_E_ARG, "decode_stage_depth must be 0, 2 or 4");
+  if (t->decode_stage_depth > 4 || t->decode_stage_depth == 3)
+    return set_error(GRASS_E_ARG, "decode_stage_depth must be 0 (default), 1, 2 or 4");
   DeviceGuard dg(g->device);
   if (int rc = apply_tuning(g->device, *t, g->d_recs, g->info.n * sizeof(uint4), g->l2win))
     return rc;

@@ -467,6 +467,63 @@ __device__ __forceinline__ void le_slot_decode(const Sec &A, uint32_t off, const
   if (with_right) o[L] = r2;
 }
 
+// ---- slot decoders on 32-bit words (shared or global memory) ----
+// w points at the slot's sector as stream words (each the next 32 bits MSB
+// first), with one more readable word after it; off is the bit offset of the
+// slot in it.  One funnel shift per field of up to 32 bits.
+__device__ __forceinline__ uint32_t word_field(const uint32_t *w, uint32_t off, int width) {
+  const uint32_t q = off >> 5, s = off & 31u;
+  const uint32_t x = __funnelshift_l(w[q + 1], w[q], s);
+  return width ? x >> (32 - width) : 0u;
+}
+
+// An LE sea (width sw = sea_bit + 1 <= 33) added to its interpolated base.
+__device__ __forceinline__ uint32_t word_sea(const uint32_t *w, uint32_t off, int sw,
+                                             uint32_t base) {
+  uint32_t mag, neg;
+  if (sw > 32) {  // sea_bit 32: the magnitude is the field's top 32 bits
+    mag = word_field(w, off, 32);
+    neg = word_field(w, off + 32, 1);
+  } else {
+    const uint32_t raw = word_field(w, off, sw);
+    mag = raw >> 1;
+    neg = raw & 1u;
+  }
+  return base + (neg ? 0u - mag : mag);
+}
+
+// le_slot_decode / gt_slot_decode on words.
+__device__ __forceinline__ void le_slot_decode_w(const uint32_t *w, uint32_t off, const VHdr &h,
+                                                 uint32_t c, uint32_t L, bool with_right,
+                                                 uint32_t *o) {
+  const int sw = h.b + 1;
+  const uint32_t r1m = word_field(w, off, h.a);
+  const uint32_t r1 = c < h.fp ? h.v - r1m : h.v + r1m;
+  const uint32_t s0 = off + (uint32_t)h.a;
+  const uint32_t r2m = word_field(w, s0 + (h.bl - 1) * (uint32_t)sw, h.a);
+  const uint32_t r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
+  const uint32_t step = (r2 - r1) / L;
+  o[0] = r1;
+  uint32_t at = s0, base = r1;
+  for (uint32_t id = 1; id < L; id++, at += (uint32_t)sw) {
+    base += step;
+    o[id] = word_sea(w, at, sw, base);
+  }
+  if (with_right) o[L] = r2;
+}
+
+__device__ __forceinline__ void gt_slot_decode_w(const uint32_t *w, uint32_t off, const VHdr &h,
+                                                 uint32_t c, uint32_t L, uint32_t *o) {
+  const uint32_t hv = word_field(w, off, h.a) + 1u;
+  uint32_t x = c >= h.fp ? h.v + hv : h.v - hv;
+  o[0] = x;
+  uint32_t at = off + (uint32_t)h.a;
+  for (uint32_t t = 1; t < L; t++, at += (uint32_t)h.b) {
+    x += word_field(w, at, h.b) + 1u;
+    o[t] = x;
+  }
+}
+
 // LE get_vertex: one sector load.
 __device__ __forceinline__ uint32_t le_neighbor(const DevGraph &g, const VHdr &h, uint32_t i) {
   if (h.d == 1) return h.fp;
@@ -618,6 +675,40 @@ __device__ __forceinline__ uint32_t neighbor(const DevGraph &g, const VHdr &h, u
   if constexpr (MODE == 0) return gt_neighbor(g, h, i);
   else if constexpr (MODE == 1) return le_neighbor(g, h, i);
   else return load_cold_u32(g.cols + h.P + i);
+}
+
+// A compressed draw (GT or LE) in two halves, so that a lane can have the
+// sector loads of several draws in flight before it decodes any: where its
+// slot is (draw_at), then its value from the loaded sector (draw_value).
+struct DrawAt {
+  uint64_t pos;       // bit offset of the slot
+  uint32_t c, id, L;  // slot, index in it, slot length (LE)
+};
+
+template <int MODE>
+__device__ __forceinline__ DrawAt draw_at(const VHdr &h, uint32_t i) {
+  DrawAt at;
+  if constexpr (MODE == 0) {
+    at.c = i / h.bl;
+    at.id = i - at.c * h.bl;
+    at.L = 0;
+  } else {
+    le_locate(h, i, at.c, at.id, at.L);
+  }
+  at.pos = slot_pos(h, at.c);
+  return at;
+}
+
+template <int MODE>
+__device__ __forceinline__ uint32_t draw_value(const Sec &A, const DrawAt &at, const VHdr &h) {
+  const uint32_t off = (uint32_t)at.pos & 255u;
+  if constexpr (MODE == 0) {
+    const uint32_t hv = (uint32_t)sec1_field(A, off, h.a) + 1u;
+    return (at.c >= h.fp ? h.v + hv : h.v - hv) + at.id +
+           sec1_sum(A, off + (uint32_t)h.a, at.id, h.b);
+  } else {
+    return le_slot_value(A, off, h, at.c, at.id, at.L);
+  }
 }
 
 // End bit of a vertex's on-disk payload given its stream header (load-time

@@ -339,16 +339,18 @@ __global__ void plan_fill_kernel(const uint4 *__restrict__ recs, uint32_t n, uin
 }
 
 // ---- slot staging for the range sweep ----
-// With a staging depth D (2 or 4), lane 0 of a warp copies the sectors that
-// hold each group of 32 chunk slots into one of the warp's D shared-memory
-// buffers with one bulk copy (cp.async.bulk, completion counted on that
-// buffer's mbarrier), D - 1 groups ahead of the group being decoded, and the
-// lanes read their slots from shared memory.  Every wait is bounded: a copy
-// that has not landed after kStagePolls polls is reported (error word bit 2,
-// GRASS_E_TIMEOUT) and the warp decodes from global memory from then on,
-// waiting once more, bounded, for its copies in flight before it exits.
+// Lane 0 of a warp copies the sectors that hold each group of 32 chunk slots
+// into one of the warp's D shared-memory buffers with one bulk copy
+// (cp.async.bulk, completion counted on that buffer's mbarrier), D - 1 groups
+// ahead of the group being decoded (D = 1: copy, then decode), and the lanes
+// read their fields from shared memory, one funnel shift per field.  Every
+// wait is bounded: a copy that has not landed after kStagePolls polls is
+// reported (error word bit 2, GRASS_E_TIMEOUT) and the warp reads global
+// memory from then on, waiting once more, bounded, for its copies in flight
+// before it exits.
 constexpr int kDecodeWarps = 8;          // warps per range block
-constexpr uint32_t kGroupBytes = 1024;   // 32 slots lie in at most 32 sectors
+constexpr uint32_t kGroupBytes = 1056;   // 32 slots lie in at most 32 sectors; + one
+                                         // sector that field reads may touch
 constexpr uint32_t kOutWords = 32 * 33;  // a group's neighbors (32 chunks of <= 32, + 1)
 // Polls of the copy's mbarrier before the warp gives up (far beyond the
 // microseconds one copy takes).
@@ -405,27 +407,18 @@ __device__ __forceinline__ bool stage_wait(uint64_t *bar, uint32_t parity) {
   return false;
 }
 
-// A 32-byte sector from shared memory, in stream order.
-__device__ __forceinline__ Sec smem_sector(const void *p) {
-  const uint64_t *q = static_cast<const uint64_t *>(p);
-  return Sec{swap_halves(q[0]), swap_halves(q[1]), swap_halves(q[2]), swap_halves(q[3])};
-}
-
 // Shared memory of one range warp: the group's decoded neighbors, then
 // DEPTH staging buffers and their barriers.
 template <int DEPTH>
 struct WarpSmem {
-  static constexpr uint32_t bytes() {
-    return kOutWords * 4 + DEPTH * kGroupBytes + (DEPTH ? DEPTH : 1) * 8;
-  }
+  static constexpr uint32_t bytes() { return kOutWords * 4 + DEPTH * kGroupBytes + DEPTH * 8; }
 };
 
 // Range sweep on the device layout (GT or LE): one lane per chunk slot.  A
-// warp takes a range's slots 32 at a time: each lane reads its slot (one
-// 32-byte sector, coalesced across the warp, or from the staged group),
-// decodes the chunk's neighbors into shared memory, and the warp writes the
-// group's neighbors to the CSR with coalesced stores.  DEPTH 0: slots from
-// global memory; 2 or 4: staged (see above).
+// warp takes a range's slots 32 at a time, staged in shared memory (DEPTH
+// groups in flight, see above): each lane decodes its chunk's neighbors into
+// shared memory, and the warp writes the group's neighbors to the CSR with
+// coalesced stores.
 template <int MODE, int DEPTH>
 __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uint64_t *rowptr,
                                                            uint32_t *cols,
@@ -441,8 +434,8 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
   uint64_t *bars = reinterpret_cast<uint64_t *>(stage + DEPTH * kGroupBytes);
   uint32_t phase = 0;    // bit b: parity of buffer b's next completion
   uint32_t pending = 0;  // bit b: buffer b has a copy issued and not yet waited for
-  bool stage_ok = DEPTH > 0;
-  if (DEPTH && lane < DEPTH) stage_bar_init(bars + lane);
+  bool stage_ok = true;
+  if (lane < DEPTH) stage_bar_init(bars + lane);
   __syncwarp();
   bool bad = false;
   for (uint64_t t = warp; t < nitems; t += nwarps) {
@@ -461,8 +454,8 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
       qb = slot_pos(h, cz) >> 8;
     };
     auto issue = [&](uint32_t j) {
-      if (!DEPTH || !stage_ok) return;
-      const uint32_t b = j % (DEPTH ? DEPTH : 1);
+      if (!stage_ok) return;
+      const uint32_t b = j % DEPTH;
       uint64_t qa, qb;
       group_sectors(j, qa, qb);
       if (lane == 0)
@@ -470,13 +463,12 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
                    bars + b);
       pending |= 1u << b;
     };
-    if constexpr (DEPTH > 0)
-      for (uint32_t j = 0; j + 1 < (uint32_t)DEPTH && j < ngroups; j++) issue(j);
+    for (uint32_t j = 0; j + 1 < (uint32_t)DEPTH && j < ngroups; j++) issue(j);
     for (uint32_t j = 0; j < ngroups; j++) {  // warp-uniform
-      if (DEPTH && j + DEPTH - 1 < ngroups) issue(j + DEPTH - 1);
+      if (j + DEPTH - 1 < ngroups) issue(j + DEPTH - 1);
       bool staged = false;
-      const uint32_t b = DEPTH ? j % DEPTH : 0;
-      if (DEPTH && stage_ok) {
+      const uint32_t b = j % DEPTH;
+      if (stage_ok) {
         if (__all_sync(FULL, stage_wait(bars + b, (phase >> b) & 1u))) {
           phase ^= 1u << b;
           pending &= ~(1u << b);
@@ -489,19 +481,21 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
       const uint32_t cg = c0 + 32 * j, c = cg + lane;
       if (c <= c1) {
         const uint64_t pos = slot_pos(h, c);
-        Sec A;
+        // the slot's sector as words: from the staged group, or (after a
+        // timeout) from global memory
+        const uint32_t *w;
         if (staged) {
           uint64_t qa, qb;
           group_sectors(j, qa, qb);
-          A = smem_sector(stage + b * kGroupBytes + ((pos >> 8) - qa) * 32u);
+          w = reinterpret_cast<const uint32_t *>(stage + b * kGroupBytes + ((pos >> 8) - qa) * 32u);
         } else {
-          A = load_sector(g.words, pos >> 8);
+          w = g.words + (pos >> 8) * 8;
         }
         if constexpr (MODE == 0) {
-          gt_slot_decode(A, (uint32_t)pos & 255u, h, c, min(T, h.d - c * T), out + (c - cg) * T);
+          gt_slot_decode_w(w, (uint32_t)pos & 255u, h, c, min(T, h.d - c * T), out + (c - cg) * T);
         } else {  // the last chunk also holds neighbor d-1, its right rock
-          le_slot_decode(A, (uint32_t)pos & 255u, h, c, min(T, last - c * T), c + 1 == h.bn,
-                         out + (c - cg) * T);
+          le_slot_decode_w(w, (uint32_t)pos & 255u, h, c, min(T, last - c * T), c + 1 == h.bn,
+                           out + (c - cg) * T);
         }
       }
       __syncwarp();
@@ -515,9 +509,9 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
       __syncwarp();  // the group's buffers are free for the next group
     }
   }
-  if (DEPTH)  // copies still in flight after a timeout: one more bounded wait each
-    for (int b = 0; b < DEPTH; b++)
-      if ((pending >> b) & 1u) stage_wait(bars + b, (phase >> b) & 1u);
+  // copies still in flight after a timeout: one more bounded wait each
+  for (int b = 0; b < DEPTH; b++)
+    if ((pending >> b) & 1u) stage_wait(bars + b, (phase >> b) & 1u);
   if (bad && err) atomicOr(err, 1u);
 }
 
@@ -574,7 +568,7 @@ static void launch_range_depth(const DevGraph &v, const uint64_t *rowptr, uint32
   switch (g->tuning.decode_stage_depth) {
     case 2: launch_range<MODE, 2>(v, rowptr, cols, g, grid, err, s); break;
     case 4: launch_range<MODE, 4>(v, rowptr, cols, g, grid, err, s); break;
-    default: launch_range<MODE, 0>(v, rowptr, cols, g, grid, err, s);
+    default: launch_range<MODE, 1>(v, rowptr, cols, g, grid, err, s);
   }
 }
 

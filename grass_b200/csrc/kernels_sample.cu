@@ -230,6 +230,12 @@ __global__ void __launch_bounds__(512, GRASS_RW_CSR_MIN_BLOCKS) rw_csr_kernel(De
 }
 
 // ---------------------------------------------------------------------------
+// Draws a lane of the standalone compressed k-hop has in flight at once (the
+// batched kernel keeps one: its register budget is shared with the walks).
+#ifndef GRASS_KHOP_INFLIGHT
+#define GRASS_KHOP_INFLIGHT 4
+#endif
+
 // k-hop.  One warp per sample.  For each hop, the frontier is taken in
 // chunks of 32 transits: lane p decodes the header of transit p into shared
 // memory, then the chunk's f*32 draws are spread over the lanes.
@@ -244,7 +250,8 @@ __global__ void __launch_bounds__(256) khop_kernel(DevGraph g, const uint32_t *_
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   uint64_t cnt = 0;
   bool bad = false;
-  for (uint64_t s = warp; s < S; s += nwarps) khop_seed_warp<MODE>(g, seeds, A, s, my, cnt, bad);
+  for (uint64_t s = warp; s < S; s += nwarps)
+    khop_seed_warp<MODE, GRASS_KHOP_INFLIGHT>(g, seeds, A, s, my, cnt, bad);
   warp_add_u64(edges, cnt);
   if (bad && err) atomicOr(err, 1u);
 }

@@ -108,7 +108,9 @@ struct SmemHdr {
 // Every part draws the first hop itself (the same values: each writes them,
 // only part 0 counts them), so no warp waits for another.  Draws keep their
 // Philox slot, so the output is the same for any number of parts.
-template <int MODE>
+// INFLIGHT: draws a lane of a compressed k-hop has in flight at once (every
+// slot sector is requested before any is decoded).
+template <int MODE, int INFLIGHT = 1>
 __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t *seeds,
                                                const KhopArgs &A, uint64_t s, SmemHdr &my,
                                                uint64_t &cnt, bool &bad, uint32_t part = 0,
@@ -146,33 +148,79 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
       __syncwarp();
       const uint64_t nP = min((uint64_t)32, P - pc);
       const uint64_t total = nP * f;
-      for (uint64_t j0 = 0; j0 < total; j0 += 32) {  // warp-uniform
-        const uint64_t j = j0 + lane;
-        const bool act = j < total;
-        uint64_t slot = 0;
-        bool draw = false;
-        uint32_t nv = INVALID_VERTEX;
-        if (act) {
-          const uint32_t pl = (uint32_t)(j / f);
-          slot = parent(pc + pl) * f + (j - (uint64_t)pl * f);
-          const VHdr hk = my.get(pl);
-          if (hk.d) {
-            draw = true;
-            const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(slot >> 2), (uint32_t)s,
-                                           (uint32_t)(s >> 32), TAG_KHOP | hop);
-            nv = neighbor<MODE>(g, hk, mulhi_u32(pick(rr, (int)(slot & 3)), hk.d));
-          }
-        }
-        if (act) {
-          if (draw) {
-            if (nv >= g.n) {
-              bad = true;
-              nv = INVALID_VERTEX;
-            } else if (count) {
-              cnt++;
+      if constexpr (MODE != 2) {
+        for (uint64_t j0 = 0; j0 < total; j0 += 32 * INFLIGHT) {  // warp-uniform
+          Sec sec[INFLIGHT];
+          DrawAt at[INFLIGHT];
+          uint32_t pl[INFLIGHT];
+          bool dr[INFLIGHT];
+#pragma unroll
+          for (int u = 0; u < INFLIGHT; u++) {
+            const uint64_t j = j0 + (uint64_t)u * 32 + lane;
+            dr[u] = false;
+            pl[u] = 0;
+            if (j < total) {
+              pl[u] = (uint32_t)(j / f);
+              const VHdr hk = my.get(pl[u]);
+              const uint64_t slot = parent(pc + pl[u]) * f + (j - (uint64_t)pl[u] * f);
+              if (hk.d > (MODE == 1 ? 1u : 0u)) {  // (LE degree 1: the record holds it)
+                dr[u] = true;
+                const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(slot >> 2), (uint32_t)s,
+                                               (uint32_t)(s >> 32), TAG_KHOP | hop);
+                at[u] = draw_at<MODE>(hk, mulhi_u32(pick(rr, (int)(slot & 3)), hk.d));
+                sec[u] = load_sector(g.words, at[u].pos >> 8);
+              }
             }
           }
-          out[slot] = nv;
+#pragma unroll
+          for (int u = 0; u < INFLIGHT; u++) {
+            const uint64_t j = j0 + (uint64_t)u * 32 + lane;
+            if (j >= total) continue;
+            const VHdr hk = my.get(pl[u]);
+            const uint64_t slot = parent(pc + pl[u]) * f + (j - (uint64_t)pl[u] * f);
+            uint32_t nv = INVALID_VERTEX;
+            if (dr[u]) nv = draw_value<MODE>(sec[u], at[u], hk);
+            else if (hk.d == 1) nv = hk.fp;  // LE degree 1
+            if (hk.d) {
+              if (nv >= g.n) {
+                bad = true;
+                nv = INVALID_VERTEX;
+              } else if (count) {
+                cnt++;
+              }
+            }
+            out[slot] = nv;
+          }
+        }
+      } else {  // CSR: one column load per draw
+        for (uint64_t j0 = 0; j0 < total; j0 += 32) {  // warp-uniform
+          const uint64_t j = j0 + lane;
+          const bool act = j < total;
+          uint64_t slot = 0;
+          bool draw = false;
+          uint32_t nv = INVALID_VERTEX;
+          if (act) {
+            const uint32_t pl = (uint32_t)(j / f);
+            slot = parent(pc + pl) * f + (j - (uint64_t)pl * f);
+            const VHdr hk = my.get(pl);
+            if (hk.d) {
+              draw = true;
+              const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(slot >> 2), (uint32_t)s,
+                                             (uint32_t)(s >> 32), TAG_KHOP | hop);
+              nv = neighbor<MODE>(g, hk, mulhi_u32(pick(rr, (int)(slot & 3)), hk.d));
+            }
+          }
+          if (act) {
+            if (draw) {
+              if (nv >= g.n) {
+                bad = true;
+                nv = INVALID_VERTEX;
+              } else if (count) {
+                cnt++;
+              }
+            }
+            out[slot] = nv;
+          }
         }
       }
       __syncwarp();

@@ -66,7 +66,7 @@ def test_staged_wait_runs_out_and_is_reported(tmp_path):
 
 
 @pytest.mark.parametrize("mode", ["LE", "GT"])
-@pytest.mark.parametrize("depth", [0, 2, 4])
+@pytest.mark.parametrize("depth", [0, 1, 2, 4])
 def test_library_decode_staged_reports_no_error(mode, depth):
     """The shipped library, slots staged or not: the same CSR, no error."""
     rp, cols = G.rmat_graph(16, 16, seed=42)
