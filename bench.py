@@ -405,12 +405,17 @@ class Parity:
 
 
 def ncu_traffic(workload_key: str):
-    """Per-launch DRAM bytes of the RW kernel from the committed ncu summary."""
+    """Per-launch DRAM bytes of the walk kernel from the committed ncu summary
+    (profiles/traffic.json: dram__bytes_read.sum + dram__bytes_write.sum of one
+    capture, scaled to a full launch by draws), and where they come from."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     if not os.path.exists(p):
-        return None
+        return None, None
     d = json.load(open(p))
-    return d.get(workload_key)
+    e = d.get(workload_key)
+    if not isinstance(e, dict):
+        return None, None
+    return e.get("bytes_per_launch"), e.get("capture")
 
 
 def random_sector_ceiling(G, torch, dev, flush, K=5, W=3):
@@ -945,7 +950,7 @@ def main():
     avg_s = head["ms_per_step"] / 1000.0
     peak, peak_kind = peaks()
     achieved = alg_bytes / avg_s / 1e9
-    traffic = ncu_traffic(f"rw_{args.mode}_s{args.scale}_e{args.edge_factor}_W{W}_L{L}")
+    traffic, traffic_src = ncu_traffic(f"rw_{args.mode}_s{args.scale}_e{args.edge_factor}_L{L}")
     # random-access context: 32-byte sectors a walk reads per second, beside
     # the rate of uniform random 4-byte reads over 2 GiB (no locality at all)
     ceil = random_sector_ceiling(G, torch, dev, flush) if "rw" in only else None
@@ -1006,7 +1011,7 @@ def main():
             "config": workload_config(args, meta),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
-                         "traffic": traffic,
+                         "traffic": traffic, "traffic_capture": traffic_src,
                          "algorithmic_bytes_per_launch": alg_bytes,
                          "sector_bytes_per_launch": sectors * 32,
                          "sector_GBps": sectors * 32 / avg_s / 1e9,
