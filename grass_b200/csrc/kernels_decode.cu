@@ -407,12 +407,18 @@ __device__ __forceinline__ bool stage_wait(uint64_t *bar, uint32_t parity) {
   return false;
 }
 
-// Shared memory of one range warp: the group's decoded neighbors, then
-// DEPTH staging buffers and their barriers.
+// Shared memory of one range warp, in a block of its own that starts on a
+// 128-byte boundary: DEPTH staging buffers (each a multiple of 16 bytes, as
+// cp.async.bulk requires of its destination), the group's decoded neighbors,
+// then the buffers' mbarriers (8-byte aligned).
 template <int DEPTH>
 struct WarpSmem {
-  static constexpr uint32_t bytes() { return kOutWords * 4 + DEPTH * kGroupBytes + DEPTH * 8; }
+  static constexpr uint32_t stage_off() { return 0; }
+  static constexpr uint32_t out_off() { return DEPTH * kGroupBytes; }
+  static constexpr uint32_t bar_off() { return out_off() + kOutWords * 4; }
+  static constexpr uint32_t bytes() { return (bar_off() + DEPTH * 8 + 127) / 128 * 128; }
 };
+static_assert(kGroupBytes % 16 == 0 && (kOutWords * 4) % 16 == 0, "staging alignment");
 
 // Range sweep on the device layout (GT or LE): one lane per chunk slot.  A
 // warp takes a range's slots 32 at a time, staged in shared memory (DEPTH
@@ -428,10 +434,12 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
   const int lane = threadIdx.x & 31;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-  unsigned char *mine = le_smem + (threadIdx.x >> 5) * WarpSmem<DEPTH>::bytes();
-  uint32_t *out = reinterpret_cast<uint32_t *>(mine);
-  unsigned char *stage = mine + kOutWords * 4;
-  uint64_t *bars = reinterpret_cast<uint64_t *>(stage + DEPTH * kGroupBytes);
+  using WS = WarpSmem<DEPTH>;
+  static_assert(WS::bytes() % 128 == 0 && WS::bar_off() % 8 == 0, "warp block alignment");
+  unsigned char *mine = le_smem + (threadIdx.x >> 5) * WS::bytes();
+  unsigned char *stage = mine + WS::stage_off();
+  uint32_t *out = reinterpret_cast<uint32_t *>(mine + WS::out_off());
+  uint64_t *bars = reinterpret_cast<uint64_t *>(mine + WS::bar_off());
   uint32_t phase = 0;    // bit b: parity of buffer b's next completion
   uint32_t pending = 0;  // bit b: buffer b has a copy issued and not yet waited for
   bool stage_ok = true;
