@@ -763,6 +763,24 @@ def run_reference(args):
     return 0
 
 
+def footprint_config1(G):
+    """BASELINE config 1's graph (R-MAT s16 ef16, seed 42, graph_sort): the
+    resident bytes of each format and of its files against the CSR."""
+    gdir, meta = build_graph(16, 16)
+    n, E = meta["n"], meta["num_edges"]
+    csr = (n + 1) * 8 + 4 * E
+    out = {"graph": f"R-MAT scale 16 edge factor 16: {n} vertices, {E} directed edges",
+           "CSR": csr}
+    for m in ("LE", "GT"):
+        g = G.Graph(os.path.join(gdir, m), m)
+        inf = g.info()
+        out[m] = {"device_bytes": inf["device_bytes"], "ratio_device": csr / inf["device_bytes"],
+                  "file_bytes": inf["graph_file_bytes"] + inf["offset_file_bytes"],
+                  "ratio_files": csr / (inf["graph_file_bytes"] + inf["offset_file_bytes"])}
+        g.close()
+    return out
+
+
 def workload_config(args, meta):
     return {
         "workload": f"random walk, {args.walkers} uniform walkers x L={args.length}, "
@@ -787,7 +805,8 @@ def main():
     import grass_b200 as G
 
     only = set(args.only.split(",")) if args.only else {"rw", "khop", "decode", "csr", "e2e",
-                                                         "cpu", "batch", "serve", "parity"}
+                                                         "cpu", "batch", "serve", "parity",
+                                                         "footprint"}
     gdir, meta = build_graph(args.scale, args.edge_factor)
     n, E = meta["n"], meta["num_edges"]
     W, L = args.walkers, args.length
@@ -1029,6 +1048,10 @@ def main():
                                 **{f"ratio_{m}": csr_bytes / infos[m]["device_bytes"]
                                    for m in infos}},
             "load_seconds": {m: infos[m]["upload_seconds"] for m in infos},
+            "footprint_files": {f"ratio_{m}": csr_bytes / (infos[m]["graph_file_bytes"] +
+                                                         infos[m]["offset_file_bytes"])
+                                for m in infos},
+            "footprint_config1": footprint_config1(G) if "footprint" in only else None,
             "parity": ({k: v["ok"] for k, v in parity.res.items()} if parity.enabled else None),
             "parity_detail": parity.res if parity.enabled else None,
         }
