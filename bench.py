@@ -680,6 +680,80 @@ def cpu_baseline(gdir, mode, n, length, seed, budget_s=12.0):
                       f"OpenMP over walkers"}
 
 
+def two_sample_chi2(a, b, min_count=10):
+    """Two-sample chi-square of two count vectors over the same vertices.
+    Conditional on each bin's combined count c, a's share is Binomial(c, p),
+    p = sum(a) / (sum(a) + sum(b)), under the null of one law.  Vertices with
+    c >= min_count are bins of their own; the others are pooled in vertex
+    order into bins of combined count >= 2 min_count.  Returns (stat, df, p)."""
+    from scipy.stats import chi2
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    c = a + b
+    big = c >= min_count
+    A, Cc = [a[big]], [c[big]]
+    sa, sc = a[~big], c[~big]
+    if sc.size:
+        cut = np.floor(np.cumsum(sc) / (2 * min_count)).astype(np.int64)
+        cut = np.minimum(cut, max(int(cut[-1]) - 1, 0))  # fold a short tail into the last bin
+        A.append(np.bincount(cut, weights=sa))
+        Cc.append(np.bincount(cut, weights=sc))
+    A, Cc = np.concatenate(A), np.concatenate(Cc)
+    keep = Cc > 0
+    A, Cc = A[keep], Cc[keep]
+    p = a.sum() / c.sum()
+    stat = float(((A - Cc * p) ** 2 / (Cc * p * (1 - p))).sum())
+    df = int(A.size - 1)
+    return stat, df, float(chi2.sf(stat, df))
+
+
+def reference_visits(G, torch, gdir, n, positions=(1, 10, 40, 79), timeout_s=600):
+    """Per-vertex visit counts of the reference's own GPU sampler against this
+    library's, two-sample chi-square per position.  The reference's rw app is
+    run, one walker per vertex, from baseline/_ref/rw_{gt,le}_visits (its
+    sources with baseline/visit_hook.h force-included, which writes the
+    transits after the chosen steps); this library walks the same starts
+    (i % n) for 80 steps.  Each walker adds one visit per position, so each
+    position's counts are a sample of n independent walkers; ended walks are
+    not counted."""
+    import tempfile
+    out = {"positions": list(positions), "walkers": n}
+    dev = torch.device("cuda", torch.cuda.current_device())
+    for m in ("GT", "LE"):
+        exe = os.path.join(ROOT, "baseline", "_ref", f"rw_{m.lower()}_visits")
+        if not os.path.exists(exe):
+            out[m] = {"unavailable": f"{exe} not built"}
+            continue
+        with tempfile.TemporaryDirectory() as td:
+            env = dict(os.environ, GRASS_VISIT_DUMP=os.path.join(td, "v"),
+                       GRASS_VISIT_STEPS=",".join(map(str, positions)))
+            r = subprocess.run([exe, "-g", os.path.join(gdir, m), "-n", "1"], env=env,
+                               capture_output=True, text=True, timeout=timeout_s)
+            ref = {}
+            for pos in positions:
+                f = os.path.join(td, f"v.{pos}.i32")
+                ref[pos] = np.fromfile(f, dtype=np.int32) if os.path.exists(f) else None
+        g = G.Graph(os.path.join(gdir, m), m)
+        starts = torch.arange(n, dtype=torch.int32, device=dev)
+        paths = torch.empty(n * 81, dtype=torch.int32, device=dev)
+        g.rw_device(starts, n, 80, 20241203, paths, layout=1)
+        ours = paths.view(81, n).cpu().numpy()
+        g.close()
+        res = {"rc": r.returncode}
+        for pos in positions:
+            if ref[pos] is None:
+                res[str(pos)] = {"unavailable": "no dump"}
+                continue
+            rv = ref[pos][(ref[pos] >= 0) & (ref[pos] < n)]
+            ov = ours[pos][(ours[pos] >= 0) & (ours[pos] < n)]
+            stat, df, pv = two_sample_chi2(np.bincount(rv, minlength=n),
+                                           np.bincount(ov, minlength=n))
+            res[str(pos)] = {"visits_reference": int(rv.size), "visits_grass_b200": int(ov.size),
+                             "chi2": stat, "df": df, "p": pv}
+        out[m] = res
+    return out
+
+
 def reference_gpu(gdir, n, runs=3, timeout_s=600):
     """The reference's own GPU sampler on this GPU: its unmodified `rw` app
     (baseline/_ref/rw_gt, rw_le, built from its sources for sm_100a) against
@@ -955,6 +1029,9 @@ def main():
     # ---- the reference's own GPU rw app on this GPU: only when asked for
     if ws == 1 and rank == 0 and "refgpu" in only:
         out["reference_gpu"] = reference_gpu(gdir, n)
+        g1dir, meta1 = build_graph(16, 16)
+        out["reference_gpu"]["visits_rmat_s16"] = reference_visits(G, torch, g1dir, meta1["n"])
+        out["reference_gpu"]["visits_rmat_s22"] = reference_visits(G, torch, gdir, n)
 
     # ---- skewed large graph (Chung-Lu, ~3B edges): only when asked for
     if ws == 1 and "cfg5" in only:
