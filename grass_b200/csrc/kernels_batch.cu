@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(256, MODE == 1 ? GRASS_BATCH_MIN_BLOCKS_LE
                                                     unsigned int *err) {
   __shared__ SmemHdr sh[8];
   __shared__ CtaSmem<8> csm;
+  __shared__ __align__(16) uint32_t dbuf[8][32 * kDrawBufWords];  // k-hop draw staging
   SmemHdr &my = sh[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   uint64_t all = 0;
@@ -84,7 +85,8 @@ __global__ void __launch_bounds__(256, MODE == 1 ? GRASS_BATCH_MIN_BLOCKS_LE
     } else if (jb.type == GRASS_JOB_KHOP) {
       const uint32_t parts = max(1u, tk.pad >> 8), part = tk.pad & 0xFFu;
       for (uint64_t s = tk.begin; s < tk.end; s++)
-        khop_seed_warp<MODE>(g, jb.in, jb.khop, s, my, cnt, bad, part, parts);
+        khop_seed_warp<MODE>(g, jb.in, jb.khop, s, my, dbuf[threadIdx.x >> 5], cnt, bad, part,
+                             parts);
     } else {
       for (uint64_t s = tk.begin; s < tk.end; s++) {
         if (jb.gen_roots) {

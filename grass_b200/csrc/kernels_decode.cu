@@ -407,22 +407,35 @@ __device__ __forceinline__ bool stage_wait(uint64_t *bar, uint32_t parity) {
   return false;
 }
 
+// Metadata of the 32 range items a warp takes at a time (lane k loads item k's
+// record and row start once; the group loop reads them back by broadcast).
+struct RangeMeta {
+  uint4 rec[32];
+  uint64_t base[32];
+  uint32_t v[32], i0[32], i1[32];
+};
+
 // Shared memory of one range warp, in a block of its own that starts on a
 // 128-byte boundary: DEPTH staging buffers (each a multiple of 16 bytes, as
 // cp.async.bulk requires of its destination), the group's decoded neighbors,
-// then the buffers' mbarriers (8-byte aligned).
+// the item metadata, then the buffers' mbarriers (8-byte aligned).
 template <int DEPTH>
 struct WarpSmem {
   static constexpr uint32_t stage_off() { return 0; }
   static constexpr uint32_t out_off() { return DEPTH * kGroupBytes; }
-  static constexpr uint32_t bar_off() { return out_off() + kOutWords * 4; }
+  static constexpr uint32_t meta_off() { return out_off() + kOutWords * 4; }
+  static constexpr uint32_t bar_off() { return meta_off() + (uint32_t)sizeof(RangeMeta); }
   static constexpr uint32_t bytes() { return (bar_off() + DEPTH * 8 + 127) / 128 * 128; }
 };
-static_assert(kGroupBytes % 16 == 0 && (kOutWords * 4) % 16 == 0, "staging alignment");
+static_assert(kGroupBytes % 16 == 0 && (kOutWords * 4) % 16 == 0 && sizeof(RangeMeta) % 16 == 0,
+              "staging alignment");
 
 // Range sweep on the device layout (GT or LE): one lane per chunk slot.  A
-// warp takes a range's slots 32 at a time, staged in shared memory (DEPTH
-// groups in flight, see above): each lane decodes its chunk's neighbors into
+// warp takes 32 range items at a time: lane k loads item k's record and row
+// start, and a scan over the lanes numbers the items' groups of 32 slots
+// 0 .. total-1 in item order.  The warp then walks that sequence, staging
+// each group's sectors in shared memory DEPTH - 1 groups ahead (across item
+// boundaries, see above): each lane decodes its chunk's neighbors into
 // shared memory, and the warp writes the group's neighbors to the CSR with
 // coalesced stores.
 template <int MODE, int DEPTH>
@@ -435,10 +448,12 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   using WS = WarpSmem<DEPTH>;
-  static_assert(WS::bytes() % 128 == 0 && WS::bar_off() % 8 == 0, "warp block alignment");
+  static_assert(WS::bytes() % 128 == 0 && WS::bar_off() % 8 == 0 && WS::meta_off() % 16 == 0,
+                "warp block alignment");
   unsigned char *mine = le_smem + (threadIdx.x >> 5) * WS::bytes();
   unsigned char *stage = mine + WS::stage_off();
   uint32_t *out = reinterpret_cast<uint32_t *>(mine + WS::out_off());
+  RangeMeta &m = *reinterpret_cast<RangeMeta *>(mine + WS::meta_off());
   uint64_t *bars = reinterpret_cast<uint64_t *>(mine + WS::bar_off());
   uint32_t phase = 0;    // bit b: parity of buffer b's next completion
   uint32_t pending = 0;  // bit b: buffer b has a copy issued and not yet waited for
@@ -446,36 +461,79 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
   if (lane < DEPTH) stage_bar_init(bars + lane);
   __syncwarp();
   bool bad = false;
-  for (uint64_t t = warp; t < nitems; t += nwarps) {
-    const uint4 it = items[t];
-    const VHdr h = header<MODE>(g, it.x);
-    const uint64_t base = rowptr[it.x];
-    const uint32_t T = h.bl, last = h.d - 1, i0 = it.y, i1 = it.z;
-    // slot of neighbor i: i / T (LE: the last neighbor is slot C-1's right rock)
-    const uint32_t c0 = MODE == 0 || i0 < last ? i0 / T : h.bn - 1;
-    const uint32_t c1 = MODE == 0 || i1 - 1 < last ? (i1 - 1) / T : h.bn - 1;
-    const uint32_t ngroups = (c1 - c0) / 32 + 1;
-    // sectors [qa, qb] of group j's slots
-    auto group_sectors = [&](uint32_t j, uint64_t &qa, uint64_t &qb) {
-      const uint32_t ca = c0 + 32 * j, cz = min(c1, ca + 31);
-      qa = slot_pos(h, ca) >> 8;
-      qb = slot_pos(h, cz) >> 8;
+  for (uint64_t tb = warp * 32; tb < nitems; tb += nwarps * 32) {
+    // lane k: item tb + k, its slots [c0, c1] and their group count
+    const uint64_t t = tb + lane;
+    uint32_t c0 = 0, c1 = 0, ng = 0;
+    if (t < nitems) {
+      const uint4 it = items[t];
+      const uint4 r = graph_record<MODE>(g, it.x);
+      const VHdr h = record_header<MODE>(r, it.x);
+      m.rec[lane] = r;
+      m.v[lane] = it.x;
+      m.base[lane] = rowptr[it.x];
+      m.i0[lane] = it.y;
+      m.i1[lane] = it.z;
+      // slot of neighbor i: i / T (LE: the last neighbor is slot C-1's right rock)
+      const uint32_t last = h.d - 1;
+      c0 = MODE == 0 || it.y < last ? it.y / h.bl : h.bn - 1;
+      c1 = MODE == 0 || it.z - 1 < last ? (it.z - 1) / h.bl : h.bn - 1;
+      ng = (c1 - c0) / 32 + 1;
+    }
+    uint32_t incl = ng;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const uint32_t excl = incl - ng;  // this item's first group in the sequence
+    const uint32_t total = __shfl_sync(FULL, incl, 31);
+    __syncwarp();
+    // the item holding group s of the sequence (items with groups come first)
+    auto item_of = [&](uint32_t s) -> int {
+      return __popc(__ballot_sync(FULL, ng > 0 && excl <= s)) - 1;
     };
-    auto issue = [&](uint32_t j) {
+    // sectors [qa, qb] of group s
+    auto group_sectors = [&](uint32_t s, uint64_t &qa, uint64_t &qb) {
+      const int k = item_of(s);
+      const uint32_t j = s - __shfl_sync(FULL, excl, k);
+      const uint32_t kc0 = __shfl_sync(FULL, c0, k), kc1 = __shfl_sync(FULL, c1, k);
+      const VHdr hk = record_header<MODE>(m.rec[k], m.v[k]);
+      const uint32_t ca = kc0 + 32 * j, cz = min(kc1, ca + 31);
+      qa = slot_pos(hk, ca) >> 8;
+      qb = slot_pos(hk, cz) >> 8;
+    };
+    auto issue = [&](uint32_t s) {
       if (!stage_ok) return;
-      const uint32_t b = j % DEPTH;
+      const uint32_t b = s % DEPTH;
       uint64_t qa, qb;
-      group_sectors(j, qa, qb);
+      group_sectors(s, qa, qb);
       if (lane == 0)
         stage_copy(stage + b * kGroupBytes, g.words + qa * 8, (uint32_t)(qb - qa + 1) * 32u,
                    bars + b);
       pending |= 1u << b;
     };
-    for (uint32_t j = 0; j + 1 < (uint32_t)DEPTH && j < ngroups; j++) issue(j);
-    for (uint32_t j = 0; j < ngroups; j++) {  // warp-uniform
-      if (j + DEPTH - 1 < ngroups) issue(j + DEPTH - 1);
+    for (uint32_t s = 0; s + 1 < (uint32_t)DEPTH && s < total; s++) issue(s);
+    int kcur = -1;
+    VHdr h;
+    uint64_t base = 0;
+    uint32_t i0 = 0, i1 = 0, kc0 = 0, kc1 = 0, kex = 0;
+    for (uint32_t s = 0; s < total; s++) {  // warp-uniform
+      if (s + DEPTH - 1 < total) issue(s + DEPTH - 1);
+      const int k = item_of(s);
+      if (k != kcur) {  // the next item: its header and range from the metadata
+        kcur = k;
+        h = record_header<MODE>(m.rec[k], m.v[k]);
+        base = m.base[k];
+        i0 = m.i0[k];
+        i1 = m.i1[k];
+        kc0 = __shfl_sync(FULL, c0, k);
+        kc1 = __shfl_sync(FULL, c1, k);
+        kex = __shfl_sync(FULL, excl, k);
+      }
+      const uint32_t T = h.bl, last = h.d - 1, j = s - kex;
       bool staged = false;
-      const uint32_t b = j % DEPTH;
+      const uint32_t b = s % DEPTH;
       if (stage_ok) {
         if (__all_sync(FULL, stage_wait(bars + b, (phase >> b) & 1u))) {
           phase ^= 1u << b;
@@ -486,15 +544,14 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
           stage_ok = false;
         }
       }
-      const uint32_t cg = c0 + 32 * j, c = cg + lane;
-      if (c <= c1) {
+      const uint32_t cg = kc0 + 32 * j, c = cg + lane;
+      if (c <= kc1) {
         const uint64_t pos = slot_pos(h, c);
         // the slot's sector as words: from the staged group, or (after a
         // timeout) from global memory
         const uint32_t *w;
         if (staged) {
-          uint64_t qa, qb;
-          group_sectors(j, qa, qb);
+          const uint64_t qa = slot_pos(h, cg) >> 8;
           w = reinterpret_cast<const uint32_t *>(stage + b * kGroupBytes + ((pos >> 8) - qa) * 32u);
         } else {
           w = g.words + (pos >> 8) * 8;
@@ -509,13 +566,14 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
       __syncwarp();
       const uint32_t nb0 = cg * T, nhi = cg + 32 >= h.bn ? h.d : (cg + 32) * T;
       const uint32_t lo = max(i0, nb0), hi = min(i1, nhi);
-      for (uint32_t k = lo + lane; k < hi; k += 32) {
-        const uint32_t val = out[k - nb0];
+      for (uint32_t q = lo + lane; q < hi; q += 32) {
+        const uint32_t val = out[q - nb0];
         bad |= val >= g.n;
-        cols[base + k] = val;
+        cols[base + q] = val;
       }
       __syncwarp();  // the group's buffers are free for the next group
     }
+    __syncwarp();  // the metadata is free for the next batch
   }
   // copies still in flight after a timeout: one more bounded wait each
   for (int b = 0; b < DEPTH; b++)

@@ -12,6 +12,8 @@
 #include "mrw_cta.cuh"
 #include "sample_warp.cuh"
 
+#include <mutex>
+
 // Resident 512-thread blocks per SM each walk kernel is compiled for (its
 // register budget), as measured on the 1M x 80 walk: the LE walk keeps all
 // the registers it wants (100 at one walker per thread, 123 at four; 64
@@ -230,66 +232,58 @@ __global__ void __launch_bounds__(512, GRASS_RW_CSR_MIN_BLOCKS) rw_csr_kernel(De
 }
 
 // ---------------------------------------------------------------------------
-// Draws a lane of the standalone compressed k-hop has in flight at once (the
-// batched kernel keeps one: its register budget is shared with the walks).
+// Draws a lane of the standalone k-hop has in flight at once (the batched
+// kernel keeps one: its register budget is shared with the walks), and the
+// k-hop kernels' resident blocks per SM (256 threads each).  Measured on
+// R-MAT s22 ef32, 65,536 seeds x (25, 10): (2, 4) beat (4, 2), (4, 3), (2, 3)
+// and (1, 4) for GT, LE and the CSR.
 #ifndef GRASS_KHOP_INFLIGHT
-#define GRASS_KHOP_INFLIGHT 4
+#define GRASS_KHOP_INFLIGHT 2
 #endif
+#ifndef GRASS_KHOP_MIN_BLOCKS
+#define GRASS_KHOP_MIN_BLOCKS 4
+#endif
+// Words of a warp's draw-staging buffers (dynamic shared memory).
+constexpr uint32_t kKhopBufWords = GRASS_KHOP_INFLIGHT * 32 * kDrawBufWords;
 
-// k-hop.  One warp per sample.  For each hop, the frontier is taken in
-// chunks of 32 transits: lane p decodes the header of transit p into shared
-// memory, then the chunk's f*32 draws are spread over the lanes.
+// k-hop.  One warp per seed (khop_seed_warp).
 
 template <int MODE>
-__global__ void __launch_bounds__(256) khop_kernel(DevGraph g, const uint32_t *__restrict__ seeds,
+__global__ void __launch_bounds__(256, GRASS_KHOP_MIN_BLOCKS) khop_kernel(DevGraph g, const uint32_t *__restrict__ seeds,
                                                    uint64_t S, KhopArgs A,
                                                    unsigned long long *edges, unsigned int *err) {
   __shared__ SmemHdr sh[8];
+  extern __shared__ __align__(16) uint32_t khop_dbuf[];  // 8 warps x kKhopBufWords
   SmemHdr &my = sh[threadIdx.x >> 5];
+  uint32_t *dbuf = khop_dbuf + (threadIdx.x >> 5) * kKhopBufWords;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   uint64_t cnt = 0;
   bool bad = false;
   for (uint64_t s = warp; s < S; s += nwarps)
-    khop_seed_warp<MODE, GRASS_KHOP_INFLIGHT>(g, seeds, A, s, my, cnt, bad);
+    khop_seed_warp<MODE, GRASS_KHOP_INFLIGHT>(g, seeds, A, s, my, dbuf, cnt, bad);
   warp_add_u64(edges, cnt);
   if (bad && err) atomicOr(err, 1u);
 }
 
-__global__ void __launch_bounds__(256) khop_csr_kernel(DevCsr c, const uint32_t *__restrict__ seeds,
+// The CSR twin of khop_kernel: the same warp routine and draws, one column
+// load per draw.
+__global__ void __launch_bounds__(256, GRASS_KHOP_MIN_BLOCKS) khop_csr_kernel(DevCsr c, const uint32_t *__restrict__ seeds,
                                                        uint64_t S, KhopArgs A,
                                                        unsigned long long *edges) {
-  const int lane = threadIdx.x & 31;
+  __shared__ SmemHdr sh[8];
+  SmemHdr &my = sh[threadIdx.x >> 5];
+  DevGraph g{};
+  g.n = c.n;
+  g.mode = GRASS_MODE_CSR_INTERNAL;
+  g.rowptr = c.rowptr;
+  g.cols = c.cols;
   const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
   const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
   uint64_t cnt = 0;
-  for (uint64_t s = warp; s < S; s += nwarps) {
-    for (uint32_t hop = 0; hop < A.hops; hop++) {
-      const uint32_t f = A.fan[hop];
-      const uint64_t P = hop ? A.width[hop - 1] : 1;
-      uint32_t *out = A.out[hop] + s * A.width[hop];
-      const uint32_t *prev = hop ? A.out[hop - 1] + s * A.width[hop - 1] : nullptr;
-      const uint64_t total = P * f;
-      for (uint64_t j = lane; j < total; j += 32) {
-        const uint64_t p = j / f;
-        const uint32_t t = hop ? prev[p] : seeds[s];
-        uint32_t nv = INVALID_VERTEX;
-        if (t < c.n) {
-          uint64_t b, e;
-          csr_row(c.rowptr, t, b, e);
-          const uint64_t d = e - b;
-          if (d) {
-            const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(j >> 2), (uint32_t)s,
-                                           (uint32_t)(s >> 32), TAG_KHOP | hop);
-            nv = c.cols[b + mulhi_u32(pick(rr, (int)(j & 3)), (uint32_t)d)];
-            cnt++;
-          }
-        }
-        out[j] = nv;
-      }
-      __syncwarp();
-    }
-  }
+  bool bad = false;
+  for (uint64_t s = warp; s < S; s += nwarps)
+    khop_seed_warp<2, GRASS_KHOP_INFLIGHT>(g, seeds, A, s, my, nullptr, cnt, bad);
   warp_add_u64(edges, cnt);
 }
 
@@ -592,10 +586,16 @@ void launch_khop(const DevGraph &g, const grass_khop_params &p, const uint32_t *
   if (!S) return;
   const KhopArgs A = khop_args(p, hop_out);
   const unsigned grid = grid_warps(S, 8, cur_dev(), 8);
+  const uint32_t smem = 8 * kKhopBufWords * 4;
+  static std::once_flag once;  // opt in to more than 48 KB of shared memory
+  std::call_once(once, [&] {
+    cudaFuncSetAttribute(khop_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(khop_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  });
   if (g.mode == GRASS_MODE_GT)
-    khop_kernel<0><<<grid, 256, 0, s>>>(g, seeds, S, A, edges, err);
+    khop_kernel<0><<<grid, 256, smem, s>>>(g, seeds, S, A, edges, err);
   else
-    khop_kernel<1><<<grid, 256, 0, s>>>(g, seeds, S, A, edges, err);
+    khop_kernel<1><<<grid, 256, smem, s>>>(g, seeds, S, A, edges, err);
   count_launch();
 }
 

@@ -91,6 +91,7 @@ struct SmemHdr {
   uint64_t P[32];
   uint32_t v[32], d[32], bn[32], bl[32], om[32], fp[32];
   int a[32], b[32], cx[32];
+  uint64_t ob[32];  // k-hop: first output slot of transit i (parent index * fanout)
   __device__ __forceinline__ void put(int i, const VHdr &h) {
     P[i] = h.P; v[i] = h.v; d[i] = h.d; bn[i] = h.bn; bl[i] = h.bl; om[i] = h.om; fp[i] = h.fp;
     a[i] = h.a; b[i] = h.b; cx[i] = h.cx;
@@ -103,21 +104,107 @@ struct SmemHdr {
   }
 };
 
+// Exact x / d for x < 2^32 and 2 <= d < 2^32 by one 64-bit multiply-high.
+// M = floor((2^64 - 1) / d) + 1 = 2^64 / d + e with 0 <= e < 1, so
+// x M / 2^64 = x / d + x e / 2^64, and x e / 2^64 < 2^-32 < 1 / d never
+// carries the quotient past the next integer.  d = 1 passes x through.
+__host__ __device__ __forceinline__ uint64_t div_magic(uint32_t d) {
+  return d >= 2 ? ~0ull / d + 1 : 0ull;
+}
+__device__ __forceinline__ uint32_t div_by(uint32_t x, uint32_t d, uint64_t M) {
+  return d >= 2 ? (uint32_t)__umul64hi((uint64_t)x, M) : x;
+}
+
+// Word k (0..3) of a Philox block held as four values.
+__device__ __forceinline__ uint32_t pick4(uint32_t x, uint32_t y, uint32_t z, uint32_t w, int k) {
+  return k == 0 ? x : k == 1 ? y : k == 2 ? z : w;
+}
+
+// div_magic(d) for the small divisors of the slot layout (chunk length T,
+// slots per sector K, chunk length L: all below 64), read through L1.
+struct DivMagic64 {
+  uint64_t m[64];
+};
+__host__ __device__ constexpr DivMagic64 make_div_magic64() {
+  DivMagic64 t{};
+  for (uint32_t d = 2; d < 64; d++) t.m[d] = ~0ull / d + 1;
+  return t;
+}
+__device__ const DivMagic64 kDivMagic64 = make_div_magic64();
+__device__ __forceinline__ uint32_t div_small(uint32_t x, uint32_t d) {  // d in [1, 63]
+  return div_by(x, d, __ldg(&kDivMagic64.m[d]));
+}
+
+// Per-lane staging of a k-hop draw's slot sector: 32 bytes copied by two
+// 16-byte cp.async (no registers held while the copy is in flight), in a
+// buffer of kDrawBufWords words (the sector, and the words that field reads
+// past its end may touch; a multiple of 16 bytes).
+constexpr uint32_t kDrawBufWords = 12;
+__device__ __forceinline__ void draw_copy(uint32_t *dst, const uint32_t *words, uint64_t sector) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  const uint32_t *src = words + sector * 8;
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d + 16), "l"(src + 4) : "memory");
+}
+__device__ __forceinline__ void draw_copy_wait() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// A GT neighbor from its slot's words (slot at bit off): the head, then id gaps.
+__device__ __forceinline__ uint32_t gt_draw_w(const uint32_t *w, uint32_t off, uint32_t v,
+                                              uint32_t fp, int a, int b, uint32_t c,
+                                              uint32_t id) {
+  const uint32_t hv = word_field(w, off, a) + 1u;
+  uint32_t x = (c >= fp ? v + hv : v - hv) + id;
+  uint32_t at = off + (uint32_t)a;
+  for (uint32_t t = 0; t < id; t++, at += (uint32_t)b) x += word_field(w, at, b);
+  return x;
+}
+
+// An LE neighbor from its slot's words: the left rock (id 0), the right rock
+// (id == L), or the interpolated base plus the signed sea.
+__device__ __forceinline__ uint32_t le_draw_w(const uint32_t *w, uint32_t off, uint32_t v,
+                                              uint32_t fp, int a, int sb, uint32_t T, uint32_t c,
+                                              uint32_t id, uint32_t L) {
+  const uint32_t sw = (uint32_t)sb + 1u;
+  const uint32_t r1m = word_field(w, off, a);
+  const uint32_t r1 = c < fp ? v - r1m : v + r1m;
+  if (id == 0) return r1;
+  const uint32_t s0 = off + (uint32_t)a;
+  const uint32_t r2m = word_field(w, s0 + (T - 1) * sw, a);
+  const uint32_t r2 = c + 1 < fp ? v - r2m : v + r2m;
+  if (id == L) return r2;
+  // (r2 - r1) >= 0 for sorted rows: unsigned division is the compressor's
+  return word_sea(w, s0 + (id - 1) * sw, (int)sw, div_small(r2 - r1, L) * id + r1);
+}
+
 // With parts > 1, `parts` warps share the seed: warp `part` takes the subtrees
 // of the first hop's children part, part + parts, ... for every later hop.
 // Every part draws the first hop itself (the same values: each writes them,
 // only part 0 counts them), so no warp waits for another.  Draws keep their
 // Philox slot, so the output is the same for any number of parts.
-// INFLIGHT: draws a lane of a compressed k-hop has in flight at once (every
-// slot sector is requested before any is decoded).
+//
+// Draw slot k of hop h (its index in the seed's hop-h output row) uses word
+// k & 3 of Philox(seed; k >> 2, s, s >> 32, TAG_KHOP | h).  The frontier is
+// taken G transits at a time (G = 32, fewer only for fanouts above 2^27, so
+// that a group's draw count fits 32 bits): lane p loads the header of transit
+// p, then the group's G f draws are spread over the lanes.  With one part and
+// G = 32 a group's slots are contiguous (pc f + j, pc a multiple of 32), so the
+// lanes compute the group's Philox blocks once per 128 draws, lane l block l of
+// the window, and hand the words out by shuffles; otherwise each draw
+// computes its own block.  INFLIGHT: draws a lane has in flight at once (every
+// load is issued before any is decoded).  MODE 2 is the CSR (one column load
+// per draw).
 template <int MODE, int INFLIGHT = 1>
 __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t *seeds,
                                                const KhopArgs &A, uint64_t s, SmemHdr &my,
-                                               uint64_t &cnt, bool &bad, uint32_t part = 0,
-                                               uint32_t parts = 1) {
+                                               uint32_t *dbuf, uint64_t &cnt, bool &bad,
+                                               uint32_t part = 0, uint32_t parts = 1) {
+  static_assert(INFLIGHT == 1 || INFLIGHT == 2 || INFLIGHT == 4, "INFLIGHT in {1, 2, 4}");
   const int lane = threadIdx.x & 31;
   for (uint32_t hop = 0; hop < A.hops; hop++) {
     const uint32_t f = A.fan[hop];
+    const uint64_t Mf = div_magic(f);
     const uint64_t Pall = hop ? A.width[hop - 1] : 1;
     // this part's parents: Q consecutive ones under each of its first-hop children
     const uint64_t Q = hop ? Pall / A.fan[0] : 1;
@@ -127,12 +214,20 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
       return hop ? (part + (k / Q) * parts) * Q + k % Q : 0;
     };
     const bool count = hop || part == 0;
+    const bool last_hop = hop + 1 == A.hops;
+    const uint32_t G = f < (1u << 27) ? 32u : (uint32_t)max(1ull, 0xFFFFFFFFull / f);
+    const bool contig = parts == 1 && G == 32;
     uint32_t *out = A.out[hop] + s * A.width[hop];
     const uint32_t *prev = hop ? A.out[hop - 1] + s * A.width[hop - 1] : nullptr;
-    for (uint64_t pc = 0; pc < P; pc += 32) {
+    for (uint64_t pc = 0; pc < P; pc += G) {
       const uint64_t p = pc + lane;
       uint32_t t = INVALID_VERTEX;
-      if (p < P) t = hop ? prev[parent(p)] : seeds[s];
+      uint64_t ob = 0;
+      if (lane < (int)G && p < P) {
+        const uint64_t par = parent(p);
+        ob = par * f;
+        t = hop ? prev[par] : seeds[s];
+      }
       VHdr h;
       if (t < g.n) {
         h = header<MODE>(g, t);
@@ -145,30 +240,108 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
         h.a = h.b = 0;
       }
       my.put(lane, h);
+      my.ob[lane] = ob;
       __syncwarp();
-      const uint64_t nP = min((uint64_t)32, P - pc);
-      const uint64_t total = nP * f;
-      if constexpr (MODE != 2) {
-        for (uint64_t j0 = 0; j0 < total; j0 += 32 * INFLIGHT) {  // warp-uniform
-          Sec sec[INFLIGHT];
-          DrawAt at[INFLIGHT];
-          uint32_t pl[INFLIGHT];
-          bool dr[INFLIGHT];
+      const uint32_t nP = (uint32_t)min((uint64_t)G, P - pc);
+      const uint32_t total = nP * f;  // < 2^32 by the choice of G
+      const uint64_t sbase = pc * f;  // contiguous groups: slot = sbase + j
+      u32x4 rw = u32x4{0, 0, 0, 0};
+      for (uint64_t j0 = 0; j0 < total; j0 += 32 * INFLIGHT) {  // warp-uniform
+        if (contig && (j0 & 127u) == 0)
+          rw = philox4x32_10(A.seed, (uint32_t)(((sbase + j0) >> 2) + (uint64_t)lane), (uint32_t)s,
+                             (uint32_t)(s >> 32), TAG_KHOP | hop);
+        uint32_t rnd[INFLIGHT];
+#pragma unroll
+        for (int u = 0; u < INFLIGHT; u++) {
+          rnd[u] = 0;
+          if (contig) {  // warp-uniform
+            // block ((j0 mod 128) + 32 u + lane) / 4 of the window, word lane & 3
+            const int src = (int)((((uint32_t)j0 & 127u) + 32u * u + (uint32_t)lane) >> 2);
+            const uint32_t x = __shfl_sync(kFull, rw.x, src), y = __shfl_sync(kFull, rw.y, src);
+            const uint32_t z = __shfl_sync(kFull, rw.z, src), w = __shfl_sync(kFull, rw.w, src);
+            rnd[u] = pick4(x, y, z, w, lane & 3);
+          }
+        }
+        if constexpr (MODE != 2) {
+          // phase 1: each draw's slot, its sector copied into this lane's buffer u
+          uint32_t di[INFLIGHT], dc[INFLIGHT], doff[INFLIGHT];
 #pragma unroll
           for (int u = 0; u < INFLIGHT; u++) {
             const uint64_t j = j0 + (uint64_t)u * 32 + lane;
-            dr[u] = false;
-            pl[u] = 0;
+            di[u] = dc[u] = doff[u] = 0;
             if (j < total) {
-              pl[u] = (uint32_t)(j / f);
-              const VHdr hk = my.get(pl[u]);
-              const uint64_t slot = parent(pc + pl[u]) * f + (j - (uint64_t)pl[u] * f);
-              if (hk.d > (MODE == 1 ? 1u : 0u)) {  // (LE degree 1: the record holds it)
-                dr[u] = true;
-                const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(slot >> 2), (uint32_t)s,
-                                               (uint32_t)(s >> 32), TAG_KHOP | hop);
-                at[u] = draw_at<MODE>(hk, mulhi_u32(pick(rr, (int)(slot & 3)), hk.d));
-                sec[u] = load_sector(g.words, at[u].pos >> 8);
+              const uint32_t pl = div_by((uint32_t)j, f, Mf);
+              const uint32_t d = my.d[pl];
+              if (d > (MODE == 1 ? 1u : 0u)) {  // (LE degree 1: the record holds it)
+                if (!contig) {
+                  const uint64_t slot = my.ob[pl] + ((uint32_t)j - pl * f);
+                  rnd[u] = pick(philox4x32_10(A.seed, (uint32_t)(slot >> 2), (uint32_t)s,
+                                              (uint32_t)(s >> 32), TAG_KHOP | hop),
+                                (int)(slot & 3));
+                }
+                const uint32_t i = mulhi_u32(rnd[u], d), T = my.bl[pl], K = my.om[pl];
+                // slot c of neighbor i (LE: neighbor d-1 is slot C-1's right rock)
+                const uint32_t c = div_small(MODE == 1 ? min(i, d - 2) : i, T);
+                const uint32_t q = div_small(c, K);
+                const uint64_t pos = my.P[pl] + (uint64_t)q * 256u + (uint64_t)(c - q * K) * (uint32_t)my.cx[pl];
+                draw_copy(dbuf + ((uint32_t)u * 32 + lane) * kDrawBufWords, g.words, pos >> 8);
+                di[u] = i;
+                dc[u] = c;
+                doff[u] = (uint32_t)pos & 255u;
+              }
+            }
+          }
+          draw_copy_wait();
+          // phase 2: decode from the buffers, store
+#pragma unroll
+          for (int u = 0; u < INFLIGHT; u++) {
+            const uint64_t j = j0 + (uint64_t)u * 32 + lane;
+            if (j >= total) continue;
+            const uint32_t pl = div_by((uint32_t)j, f, Mf);
+            const uint32_t d = my.d[pl];
+            const uint64_t slot = contig ? sbase + j : my.ob[pl] + ((uint32_t)j - pl * f);
+            uint32_t nv = INVALID_VERTEX;
+            if (d > (MODE == 1 ? 1u : 0u)) {
+              const uint32_t *w = dbuf + ((uint32_t)u * 32 + lane) * kDrawBufWords;
+              const uint32_t T = my.bl[pl], id = di[u] - dc[u] * T;
+              if constexpr (MODE == 0) {
+                nv = gt_draw_w(w, doff[u], my.v[pl], my.fp[pl], my.a[pl], my.b[pl], dc[u], id);
+              } else {
+                const uint32_t L = min(T, d - 1 - dc[u] * T);
+                nv = le_draw_w(w, doff[u], my.v[pl], my.fp[pl], my.a[pl], my.b[pl], T, dc[u], id,
+                               L);
+              }
+            } else if (d == 1) {
+              nv = my.fp[pl];  // LE degree 1
+            }
+            if (d) {
+              if (nv >= g.n) {
+                bad = true;
+                nv = INVALID_VERTEX;
+              } else if (count) {
+                cnt++;
+              }
+            }
+            if (last_hop) store_out_u32(out + slot, nv);
+            else out[slot] = nv;  // read back by the next hop
+          }
+        } else {  // CSR: one column load per draw
+          uint32_t col[INFLIGHT];
+#pragma unroll
+          for (int u = 0; u < INFLIGHT; u++) {
+            const uint64_t j = j0 + (uint64_t)u * 32 + lane;
+            col[u] = INVALID_VERTEX;
+            if (j < total) {
+              const uint32_t pl = div_by((uint32_t)j, f, Mf);
+              const uint32_t d = my.d[pl];
+              if (d) {
+                if (!contig) {
+                  const uint64_t slot = my.ob[pl] + ((uint32_t)j - pl * f);
+                  rnd[u] = pick(philox4x32_10(A.seed, (uint32_t)(slot >> 2), (uint32_t)s,
+                                              (uint32_t)(s >> 32), TAG_KHOP | hop),
+                                (int)(slot & 3));
+                }
+                col[u] = load_cold_u32(g.cols + my.P[pl] + mulhi_u32(rnd[u], d));
               }
             }
           }
@@ -176,12 +349,10 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
           for (int u = 0; u < INFLIGHT; u++) {
             const uint64_t j = j0 + (uint64_t)u * 32 + lane;
             if (j >= total) continue;
-            const VHdr hk = my.get(pl[u]);
-            const uint64_t slot = parent(pc + pl[u]) * f + (j - (uint64_t)pl[u] * f);
-            uint32_t nv = INVALID_VERTEX;
-            if (dr[u]) nv = draw_value<MODE>(sec[u], at[u], hk);
-            else if (hk.d == 1) nv = hk.fp;  // LE degree 1
-            if (hk.d) {
+            const uint32_t pl = div_by((uint32_t)j, f, Mf);
+            const uint64_t slot = contig ? sbase + j : my.ob[pl] + ((uint32_t)j - pl * f);
+            uint32_t nv = col[u];
+            if (my.d[pl]) {
               if (nv >= g.n) {
                 bad = true;
                 nv = INVALID_VERTEX;
@@ -189,37 +360,8 @@ __device__ __forceinline__ void khop_seed_warp(const DevGraph &g, const uint32_t
                 cnt++;
               }
             }
-            out[slot] = nv;
-          }
-        }
-      } else {  // CSR: one column load per draw
-        for (uint64_t j0 = 0; j0 < total; j0 += 32) {  // warp-uniform
-          const uint64_t j = j0 + lane;
-          const bool act = j < total;
-          uint64_t slot = 0;
-          bool draw = false;
-          uint32_t nv = INVALID_VERTEX;
-          if (act) {
-            const uint32_t pl = (uint32_t)(j / f);
-            slot = parent(pc + pl) * f + (j - (uint64_t)pl * f);
-            const VHdr hk = my.get(pl);
-            if (hk.d) {
-              draw = true;
-              const u32x4 rr = philox4x32_10(A.seed, (uint32_t)(slot >> 2), (uint32_t)s,
-                                             (uint32_t)(s >> 32), TAG_KHOP | hop);
-              nv = neighbor<MODE>(g, hk, mulhi_u32(pick(rr, (int)(slot & 3)), hk.d));
-            }
-          }
-          if (act) {
-            if (draw) {
-              if (nv >= g.n) {
-                bad = true;
-                nv = INVALID_VERTEX;
-              } else if (count) {
-                cnt++;
-              }
-            }
-            out[slot] = nv;
+            if (last_hop) store_out_u32(out + slot, nv);
+            else out[slot] = nv;  // read back by the next hop
           }
         }
       }
