@@ -994,7 +994,7 @@ def main():
                 "algorithmic_GBps": (stream_bytes + 16 * n + 4 * E + 8 * (n + 1))
                 / (tot / args.steps) / 1e6}
         # LE sweep with its chunk slots staged through shared memory (cp.async.bulk)
-        for depth in (2, 4):
+        for depth in (1, 2, 4):
             graphs["LE"].set_tuning(decode_stage_depth=depth)
             ms, tot = timed(torch, lambda: graphs["LE"].decode_all_device(rp_d, cl_d,
                                                                           stream=stream),

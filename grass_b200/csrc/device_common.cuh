@@ -288,9 +288,35 @@ __device__ __forceinline__ uint4 pack_slot_record(uint64_t P, uint32_t a, uint32
                     d, fp);
 }
 
+// Exact x / d for x < 2^32 and 2 <= d < 2^32 by one 64-bit multiply-high.
+// M = floor((2^64 - 1) / d) + 1 = 2^64 / d + e with 0 <= e < 1, so
+// x M / 2^64 = x / d + x e / 2^64, and x e / 2^64 < 2^-32 < 1 / d never
+// carries the quotient past the next integer.  d = 1 passes x through.
+__host__ __device__ __forceinline__ uint64_t div_magic(uint32_t d) {
+  return d >= 2 ? ~0ull / d + 1 : 0ull;
+}
+__device__ __forceinline__ uint32_t div_by(uint32_t x, uint32_t d, uint64_t M) {
+  return d >= 2 ? (uint32_t)__umul64hi((uint64_t)x, M) : x;
+}
+
+// div_magic(d) for the small divisors of the slot layout (chunk length T,
+// slots per sector K, chunk length L: all below 64), read through L1.
+struct DivMagic64 {
+  uint64_t m[64];
+};
+__host__ __device__ constexpr DivMagic64 make_div_magic64() {
+  DivMagic64 t{};
+  for (uint32_t d = 2; d < 64; d++) t.m[d] = ~0ull / d + 1;
+  return t;
+}
+__device__ const DivMagic64 kDivMagic64 = make_div_magic64();
+__device__ __forceinline__ uint32_t div_small(uint32_t x, uint32_t d) {  // d in [1, 63]
+  return div_by(x, d, __ldg(&kDivMagic64.m[d & 63u]));
+}
+
 // Bit offset of slot c.
 __device__ __forceinline__ uint64_t slot_pos(const VHdr &h, uint32_t c) {
-  const uint32_t q = c / h.om;
+  const uint32_t q = div_small(c, h.om);
   return h.P + (uint64_t)q * 256u + (uint64_t)(c - q * h.om) * (uint32_t)h.cx;
 }
 
@@ -347,7 +373,7 @@ __device__ __forceinline__ uint64_t gt_disk_block_pos(const VHdr &h, uint32_t bl
 // GT get_vertex on the device layout: one sector; neighbor id of slot c is
 // the head value + id + the sum of its id gaps.
 __device__ __forceinline__ uint32_t gt_neighbor(const DevGraph &g, const VHdr &h, uint32_t i) {
-  const uint32_t c = i / h.bl, id = i - c * h.bl;
+  const uint32_t c = div_small(i, h.bl), id = i - c * h.bl;
   const uint64_t pos = slot_pos(h, c);
   const Sec A = load_sector(g.words, pos >> 8);
   const uint32_t off = (uint32_t)pos & 255u;
@@ -421,7 +447,7 @@ __device__ __forceinline__ VHdr le_header(const DevGraph &g, uint32_t v) {
 __device__ __forceinline__ void le_locate(const VHdr &h, uint32_t i, uint32_t &c, uint32_t &id,
                                           uint32_t &L) {
   const uint32_t last = h.d - 1;
-  c = i < last ? i / h.bl : h.bn - 1;
+  c = i < last ? div_small(i, h.bl) : h.bn - 1;
   id = i - c * h.bl;
   L = min(h.bl, last - c * h.bl);
 }
@@ -442,7 +468,7 @@ __device__ __forceinline__ uint32_t le_slot_value(const Sec &A, uint32_t off, co
   const uint64_t raw = sec1_field(A, off + (uint32_t)h.a + (id - 1) * (uint32_t)sw, sw);
   const uint32_t mag = (uint32_t)(raw >> 1);
   // (r2 - r1) >= 0 for sorted rows: unsigned division is the compressor's.
-  return ((r2 - r1) / L) * id + r1 + ((raw & 1u) ? 0u - mag : mag);
+  return div_small(r2 - r1, L) * id + r1 + ((raw & 1u) ? 0u - mag : mag);
 }
 
 // Every neighbor of chunk c, its slot at bit off of sector A, into o[0..L-1]
@@ -457,7 +483,7 @@ __device__ __forceinline__ void le_slot_decode(const Sec &A, uint32_t off, const
   const uint32_t s0 = off + (uint32_t)h.a;
   const uint32_t r2m = (uint32_t)sec1_field(A, s0 + (h.bl - 1) * (uint32_t)sw, h.a);
   const uint32_t r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
-  const uint32_t step = (r2 - r1) / L;
+  const uint32_t step = div_small(r2 - r1, L);
   o[0] = r1;
   for (uint32_t id = 1; id < L; id++) {
     const uint64_t raw = sec1_field(A, s0 + (id - 1) * (uint32_t)sw, sw);
@@ -502,7 +528,7 @@ __device__ __forceinline__ void le_slot_decode_w(const uint32_t *w, uint32_t off
   const uint32_t s0 = off + (uint32_t)h.a;
   const uint32_t r2m = word_field(w, s0 + (h.bl - 1) * (uint32_t)sw, h.a);
   const uint32_t r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
-  const uint32_t step = (r2 - r1) / L;
+  const uint32_t step = div_small(r2 - r1, L);
   o[0] = r1;
   uint32_t at = s0, base = r1;
   for (uint32_t id = 1; id < L; id++, at += (uint32_t)sw) {
@@ -572,11 +598,11 @@ __device__ __forceinline__ VHdr record_header(const uint4 r, uint32_t v) {
     h.om = (r.y >> 26) & 63u;  // K
     if constexpr (MODE == 0) {
       if (h.d) {
-        h.bn = (h.d - 1) / h.bl + 1;  // C = ceil(d / T)
+        h.bn = div_small(h.d - 1, h.bl) + 1;  // C = ceil(d / T)
         h.cx = h.a + (int)(h.bl - 1) * h.b;
       }
     } else if (h.d > 1) {
-      h.bn = (h.d - 2) / h.bl + 1;  // C = ceil((d - 1) / T)
+      h.bn = div_small(h.d - 2, h.bl) + 1;  // C = ceil((d - 1) / T)
       h.cx = 2 * h.a + (int)(h.bl - 1) * (h.b + 1);
     }
   }
@@ -689,7 +715,7 @@ template <int MODE>
 __device__ __forceinline__ DrawAt draw_at(const VHdr &h, uint32_t i) {
   DrawAt at;
   if constexpr (MODE == 0) {
-    at.c = i / h.bl;
+    at.c = div_small(i, h.bl);
     at.id = i - at.c * h.bl;
     at.L = 0;
   } else {

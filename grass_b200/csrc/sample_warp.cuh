@@ -104,35 +104,9 @@ struct SmemHdr {
   }
 };
 
-// Exact x / d for x < 2^32 and 2 <= d < 2^32 by one 64-bit multiply-high.
-// M = floor((2^64 - 1) / d) + 1 = 2^64 / d + e with 0 <= e < 1, so
-// x M / 2^64 = x / d + x e / 2^64, and x e / 2^64 < 2^-32 < 1 / d never
-// carries the quotient past the next integer.  d = 1 passes x through.
-__host__ __device__ __forceinline__ uint64_t div_magic(uint32_t d) {
-  return d >= 2 ? ~0ull / d + 1 : 0ull;
-}
-__device__ __forceinline__ uint32_t div_by(uint32_t x, uint32_t d, uint64_t M) {
-  return d >= 2 ? (uint32_t)__umul64hi((uint64_t)x, M) : x;
-}
-
 // Word k (0..3) of a Philox block held as four values.
 __device__ __forceinline__ uint32_t pick4(uint32_t x, uint32_t y, uint32_t z, uint32_t w, int k) {
   return k == 0 ? x : k == 1 ? y : k == 2 ? z : w;
-}
-
-// div_magic(d) for the small divisors of the slot layout (chunk length T,
-// slots per sector K, chunk length L: all below 64), read through L1.
-struct DivMagic64 {
-  uint64_t m[64];
-};
-__host__ __device__ constexpr DivMagic64 make_div_magic64() {
-  DivMagic64 t{};
-  for (uint32_t d = 2; d < 64; d++) t.m[d] = ~0ull / d + 1;
-  return t;
-}
-__device__ const DivMagic64 kDivMagic64 = make_div_magic64();
-__device__ __forceinline__ uint32_t div_small(uint32_t x, uint32_t d) {  // d in [1, 63]
-  return div_by(x, d, __ldg(&kDivMagic64.m[d]));
 }
 
 // Per-lane staging of a k-hop draw's slot sector: 32 bytes copied by two

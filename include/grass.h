@@ -175,9 +175,10 @@ typedef struct {
                                  access-policy window                               */
   uint32_t l2_fetch_bytes;    /* 0 = leave as is; 32/64/128: this process's
                                  cudaLimitMaxL2FetchGranularity hint                 */
-  uint32_t decode_stage_depth;/* decode sweep: groups of 32 chunk slots copied into
-                                 shared memory (cp.async.bulk) 1 (default), 2 or 4
-                                 groups ahead of the one being decoded              */
+  uint32_t decode_stage_depth;/* decode sweep: 0 (default) reads chunk slots
+                                 through L1; 1, 2 or 4 copies groups of 32 slots into
+                                 shared memory (cp.async.bulk) that many groups ahead
+                                 of the one being decoded (measured slower)          */
   uint32_t reserved[2];
 } grass_tuning;
 int grass_set_tuning(grass_graph *g, const grass_tuning *t);
