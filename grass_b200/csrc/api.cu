@@ -469,6 +469,7 @@ int grass_close(grass_graph *g) {
   cudaFree(g->d_err);
   cudaFree(g->d_plan_big);
   cudaFree(g->d_plan_small);
+  cudaFree(g->d_plan_flat);
   delete g;
   return GRASS_OK;
 }

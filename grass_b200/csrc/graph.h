@@ -64,6 +64,11 @@ struct grass_graph {
   mutable uint32_t *d_plan_small = nullptr;
   mutable uint64_t plan_nbig = 0, plan_nsmall = 0;
   mutable bool plan_ok = false;
+  // The flat plan of the default (unstaged) sweep: runs of consecutive
+  // vertices (v0, v1, 0, 0) and hub neighbor ranges (v, v + 1, i0, i1).
+  mutable uint4 *d_plan_flat = nullptr;
+  mutable uint64_t plan_nflat = 0;
+  mutable bool plan_flat_ok = false;
   grass::DevGraph view() const {
     grass::DevGraph g;
     g.words = d_words;

@@ -585,6 +585,192 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
   if (bad && err) atomicOr(err, 1u);
 }
 
+// ---- the flat sweep (the default) ----
+// A warp takes one item of the flat plan: a run of consecutive vertices
+// [v0, v1) (i1 == 0), or one vertex's neighbor range [i0, i1) (hubs, degree
+// >= kRange).  The item's output is one contiguous stretch of the CSR, and
+// its chunk slots, taken in vertex order, fill it in order.  So the warp
+// walks the item 32 vertices at a time (lane k loads vertex k's record and
+// counts its slots), numbers their slots by a warp scan, and decodes them 32
+// at a time, one slot per lane, whatever vertex each belongs to: a group of
+// 32 slots is a contiguous stretch of at most 32 * 33 neighbors, decoded into
+// shared memory and written with coalesced stores.  A lane reads its slot's
+// fields as 32-bit words from global memory through L1 (one funnel shift per
+// field); measured faster than loading the sector into registers and reading
+// the fields in order from there (LE 1.00 against 1.04 ms, GT 1.16 against
+// 1.43 ms on R-MAT s22 ef32).  LE vertices of degree 1 count as one slot (the
+// neighbor is in the record).
+constexpr uint32_t kFlatHub = kRange;  // degree from which a vertex is split into ranges
+
+template <int MODE>
+__global__ void __launch_bounds__(256) decode_flat_kernel(DevGraph g, const uint64_t *rowptr,
+                                                          uint32_t *cols,
+                                                          const uint4 *__restrict__ items,
+                                                          uint64_t nitems, unsigned int *err) {
+  __shared__ __align__(16) uint32_t out_all[8][kOutWords];
+  uint32_t *out = out_all[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  bool bad = false;
+  for (uint64_t t = warp; t < nitems; t += nwarps) {
+    const uint4 it = items[t];
+    const bool run = it.w == 0;
+    const uint32_t v0 = it.x, v1 = run ? it.y : it.x + 1;
+    for (uint32_t vb = v0; vb < v1; vb += 32) {
+      // lane k: vertex vb + k, its slots [c0, c0 + ns) and first output position
+      const uint32_t v = vb + lane;
+      const bool vok = v < v1;
+      uint4 r = make_uint4(0, 0, 0, 0);
+      uint32_t c0 = 0, ns = 0;
+      uint64_t ob = 0;  // output position of the vertex's slot c0's first neighbor
+      if (vok) {
+        r = graph_record<MODE>(g, v);
+        const VHdr h = record_header<MODE>(r, v);
+        const uint32_t i0 = run ? 0u : it.z, i1 = run ? h.d : it.w;
+        if (MODE == 1 && h.d == 1) {
+          ns = 1;
+        } else if (h.d) {
+          const uint32_t last = h.d - 1;
+          c0 = MODE == 0 || i0 < last ? div_small(i0, h.bl) : h.bn - 1;
+          const uint32_t c1 = MODE == 0 || i1 - 1 < last ? div_small(i1 - 1, h.bl) : h.bn - 1;
+          ns = c1 - c0 + 1;
+        }
+        ob = rowptr[v] + (uint64_t)c0 * h.bl;
+      }
+      uint32_t sincl = ns;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(FULL, sincl, o);
+        if (lane >= o) sincl += y;
+      }
+      const uint32_t sexcl = sincl - ns, stot = __shfl_sync(FULL, sincl, 31);
+      // the item's stored stretch: [lo, hi) of the CSR
+      const uint64_t v_lo = run ? __shfl_sync(FULL, ob, 0) : rowptr[v0] + it.z;
+      const uint64_t v_hi = run ? rowptr[min(v1, vb + 32)] : rowptr[v0] + it.w;
+      for (uint32_t sg = 0; sg < stot; sg += 32) {  // warp-uniform
+        const uint32_t sl = sg + lane;
+        // the lane's vertex: the last k with sexcl_k <= sl
+        int k = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+          const uint32_t e = __shfl_sync(FULL, sexcl, k + step);
+          if (k + step < 32 && e <= sl) k += step;
+        }
+        const uint32_t kx = __shfl_sync(FULL, r.x, k), ky = __shfl_sync(FULL, r.y, k);
+        const uint32_t kz = __shfl_sync(FULL, r.z, k), kw = __shfl_sync(FULL, r.w, k);
+        const uint32_t kc0 = __shfl_sync(FULL, c0, k), kse = __shfl_sync(FULL, sexcl, k);
+        const uint64_t kob = __shfl_sync(FULL, ob, k);
+        const bool act = sl < stot;
+        const VHdr h = record_header<MODE>(make_uint4(kx, ky, kz, kw), vb + (uint32_t)k);
+        const uint32_t c = kc0 + (sl - kse);
+        const uint64_t pos0 = kob + (uint64_t)(sl - kse) * h.bl;  // slot's first output position
+        const uint64_t g_lo = __shfl_sync(FULL, pos0, 0);
+        // the slot's neighbors: GT min(T, d - cT); LE min(T, d-1-cT) (+ the right
+        // rock in the last slot); LE degree 1: the record's neighbor
+        uint32_t len = 0;
+        if (act) {
+          if (MODE == 1 && h.d == 1) {
+            len = 1;
+            out[pos0 - g_lo] = h.fp;
+          } else {
+            const uint64_t p = slot_pos(h, c);
+            const uint32_t *w = g.words + (p >> 8) * 8;
+            if constexpr (MODE == 0) {
+              len = min(h.bl, h.d - c * h.bl);
+              gt_slot_decode_w(w, (uint32_t)p & 255u, h, c, len, out + (pos0 - g_lo));
+            } else {
+              const uint32_t L = min(h.bl, h.d - 1 - c * h.bl);
+              const bool right = c + 1 == h.bn;
+              le_slot_decode_w(w, (uint32_t)p & 255u, h, c, L, right, out + (pos0 - g_lo));
+              len = L + (right ? 1u : 0u);
+            }
+          }
+        }
+        const uint64_t g_hi = __reduce_max_sync(FULL, act ? (uint32_t)(pos0 - g_lo) + len : 0u) + g_lo;
+        __syncwarp();
+        const uint64_t lo = max(g_lo, v_lo), hi = min(g_hi, v_hi);
+        for (uint64_t q = lo + lane; q < hi; q += 32) {
+          const uint32_t val = out[q - g_lo];
+          bad |= val >= g.n;
+          cols[q] = val;
+        }
+        __syncwarp();  // the group's buffer is free for the next group
+      }
+    }
+  }
+  if (bad && err) atomicOr(err, 1u);
+}
+
+// Flat plan: items in vertex order.  One warp per chunk of kPlanChunk
+// vertices.  A vertex of degree >= kFlatHub becomes ceil(d / kRange) range
+// items (v, v + 1, i0, i1); the others form runs, a run starting at the
+// chunk's first vertex, after a hub, and wherever the chunk's running degree
+// sum crosses a multiple of kRange.  Runs get (v0, 0, 0, 0) here; their end
+// is the next item's first vertex (flat_plan_link_kernel).
+template <bool FILL>
+__global__ void flat_plan_kernel(const uint4 *__restrict__ recs, uint32_t n, uint32_t nchunks,
+                                 uint32_t *counts, const unsigned long long *cursors,
+                                 uint4 *items) {
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (warp >= nchunks) return;
+  const uint32_t v0 = warp * kPlanChunk, v1 = min(n, v0 + kPlanChunk);
+  unsigned long long cur = FILL ? cursors[warp] : 0ull;
+  uint32_t tot = 0;
+  uint64_t carry = 0;       // degree sum of the chunk's vertices before this sub-chunk
+  bool prev_hub = true;     // (the chunk's first vertex starts a run)
+  uint64_t prev_win = 0;
+  for (uint32_t b = v0; b < v1; b += 32) {
+    const uint32_t v = b + lane;
+    const uint32_t d = v < v1 ? recs[v].z : 0u;
+    const bool hub = v < v1 && d >= kFlatHub;
+    uint64_t incl = d;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint64_t y = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const uint64_t pre = carry + incl - d;  // chunk degree sum before v
+    const uint64_t win = pre / kRange;
+    const uint32_t hub_up = __shfl_up_sync(FULL, (uint32_t)hub, 1);
+    const bool ph = lane ? hub_up != 0u : prev_hub;
+    const uint64_t pw_up = __shfl_up_sync(FULL, win, 1);
+    const uint64_t pw = lane ? pw_up : prev_win;
+    const bool start = v < v1 && !hub && (ph || win != pw);
+    const uint32_t w_items = hub ? (d + kRange - 1) / kRange : (start ? 1u : 0u);
+    uint32_t wi = w_items;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(FULL, wi, o);
+      if (lane >= o) wi += y;
+    }
+    if (FILL && w_items) {
+      const unsigned long long at = cur + wi - w_items;
+      if (hub) {
+        for (uint32_t j = 0; j < w_items; j++)
+          items[at + j] = make_uint4(v, v + 1, j * kRange, min(d, (j + 1) * kRange));
+      } else {
+        items[at] = make_uint4(v, 0u, 0u, 0u);
+      }
+    }
+    const uint32_t wsum = __shfl_sync(FULL, wi, 31);
+    cur += wsum;
+    tot += wsum;
+    carry += __shfl_sync(FULL, incl, 31);
+    prev_hub = __shfl_sync(FULL, (uint32_t)hub, 31) != 0u;
+    prev_win = __shfl_sync(FULL, win, 31);
+  }
+  if (!FILL && lane == 0) counts[warp] = tot;
+}
+
+// A run ends where the next item starts (or at n).
+__global__ void flat_plan_link_kernel(uint4 *items, uint64_t nitems, uint32_t n) {
+  const uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+  if (k >= nitems) return;
+  if (items[k].w == 0) items[k].y = k + 1 < nitems ? items[k + 1].x : n;
+}
+
 template <int MODE>
 __global__ void __launch_bounds__(256) decode_small_kernel(DevGraph g, const uint64_t *rowptr,
                                                              uint32_t *cols,
@@ -643,10 +829,84 @@ static void launch_range_depth(const DevGraph &v, const uint64_t *rowptr, uint32
   }
 }
 
+// Builds the flat plan (once) on stream s.
+static int build_flat_plan(const grass_graph *g, cudaStream_t s) {
+  const uint32_t n = (uint32_t)g->info.n;
+  const uint32_t nchunks = (n + kPlanChunk - 1) / kPlanChunk;
+  const unsigned pgrid = (nchunks + 7) / 8;  // 8 warps (chunks) per block
+  uint32_t *cnt = nullptr;
+  unsigned long long *cur = nullptr;
+  GRASS_CUDA(cudaMalloc(&cnt, (uint64_t)nchunks * sizeof(uint32_t)));
+  cudaError_t e = cudaMalloc(&cur, (uint64_t)nchunks * sizeof(unsigned long long));
+  std::vector<uint32_t> hc(nchunks);
+  std::vector<unsigned long long> hcur(nchunks);
+  uint64_t tot = 0;
+  if (e == cudaSuccess) {
+    flat_plan_kernel<false><<<pgrid, 256, 0, s>>>(g->d_recs, n, nchunks, cnt, nullptr, nullptr);
+    count_launch();
+    e = cudaMemcpyAsync(hc.data(), cnt, hc.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) {
+    for (uint32_t ch = 0; ch < nchunks; ch++) {
+      hcur[ch] = tot;
+      tot += hc[ch];
+    }
+    e = cudaMalloc(&g->d_plan_flat, std::max<uint64_t>(tot, 1) * sizeof(uint4));
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(cur, hcur.data(), hcur.size() * sizeof(unsigned long long),
+                        cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    flat_plan_kernel<true><<<pgrid, 256, 0, s>>>(g->d_recs, n, nchunks, nullptr, cur,
+                                                 g->d_plan_flat);
+    count_launch();
+    if (tot) {
+      flat_plan_link_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, s>>>(g->d_plan_flat, tot, n);
+      count_launch();
+    }
+    e = cudaStreamSynchronize(s);
+  }
+  cudaFree(cnt);
+  cudaFree(cur);
+  if (e != cudaSuccess) {
+    cudaFree(g->d_plan_flat);
+    g->d_plan_flat = nullptr;
+    return cuda_fail(e, "flat decode plan build");
+  }
+  g->plan_nflat = tot;
+  g->plan_flat_ok = true;
+  return GRASS_OK;
+}
+
+static void launch_flat(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
+                        unsigned int *err, cudaStream_t s) {
+  if (!g->plan_nflat) return;
+  const DevGraph v = g->view();
+  const unsigned grid = (unsigned)std::max<uint64_t>(
+      1, std::min<uint64_t>((g->plan_nflat + 7) / 8, (uint64_t)sm_count(g->device) * 8));
+  if (g->mode == GRASS_MODE_GT)
+    decode_flat_kernel<0><<<grid, 256, 0, s>>>(v, rowptr, cols, g->d_plan_flat, g->plan_nflat, err);
+  else
+    decode_flat_kernel<1><<<grid, 256, 0, s>>>(v, rowptr, cols, g->d_plan_flat, g->plan_nflat, err);
+  count_launch();
+}
+
 int launch_decode_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
                           unsigned int *err, cudaStream_t s) {
   const uint32_t n = (uint32_t)g->info.n;
   if (!g->info.num_edges) return GRASS_OK;
+  if (g->tuning.decode_stage_depth == 0) {  // the flat sweep
+    {
+      std::lock_guard<std::mutex> lk(g->plan_mu);
+      if (!g->plan_flat_ok) {
+        const int rc = build_flat_plan(g, s);
+        if (rc) return rc;
+      }
+    }
+    launch_flat(g, rowptr, cols, err, s);
+    return GRASS_OK;
+  }
   {
     std::lock_guard<std::mutex> lk(g->plan_mu);
     if (!g->plan_ok) {
@@ -709,11 +969,14 @@ int launch_decode_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t
 
 bool launch_decode_if_planned(const grass_graph *g, const uint64_t *rowptr, uint32_t *cols,
                               unsigned int *err, cudaStream_t s) {
+  const bool flat = g->tuning.decode_stage_depth == 0;
   {
     std::lock_guard<std::mutex> lk(g->plan_mu);
-    if (!g->plan_ok) return false;
+    if (flat ? !g->plan_flat_ok : !g->plan_ok) return false;
   }
-  if (g->info.num_edges) launch_plan_kernels(g, rowptr, cols, err, s);
+  if (!g->info.num_edges) return true;
+  if (flat) launch_flat(g, rowptr, cols, err, s);
+  else launch_plan_kernels(g, rowptr, cols, err, s);
   return true;
 }
 
