@@ -16,9 +16,9 @@
 
 // Resident 512-thread blocks per SM each walk kernel is compiled for (its
 // register budget), as measured on the 1M x 80 walk: the LE walk keeps all
-// the registers it wants (100 at one walker per thread, 123 at four; 64
-// spill and ran 5% slower, and 256-thread blocks at 3 per SM ran 3-5%
-// slower), the GT walk is 23% faster at 64 registers, the CSR walk 2% faster.
+// the registers it wants (79 at one walker per thread; launched as 256-thread
+// blocks, three per SM, which ran 17% faster than 512-thread blocks), the GT
+// walk is 23% faster at 64 registers or fewer, the CSR walk 2% faster.
 #ifndef GRASS_RW_LE_MIN_BLOCKS
 #define GRASS_RW_LE_MIN_BLOCKS 1
 #endif
