@@ -1003,6 +1003,22 @@ def main():
             out[f"decode_LE_staged{depth}"] = {"ms_per_step": tot / args.steps,
                                                "value": E * args.steps / (tot / 1000.0)}
         graphs["LE"].set_tuning()
+        # the allocation-free entry point on a graph without a decode plan
+        # (its unplanned sweep), then with one (the planned sweep)
+        import ctypes
+        fresh = G.Graph(os.path.join(gdir, "LE"), "LE")
+        st_ptr = ctypes.c_void_p(stream.cuda_stream) if stream is not None else None
+
+        def noalloc():
+            rc = G.lib.grass_decode_all_noalloc(fresh.handle, ctypes.c_void_p(rp_d.data_ptr()),
+                                                ctypes.c_void_p(cl_d.data_ptr()), st_ptr)
+            assert rc == G.OK, G.last_error()
+
+        ms, tot = timed(torch, noalloc, args.steps, args.warmup, flush, dist, local)
+        parity.decode("decode_LE_noalloc_unplanned", os.path.join(gdir, "LE"), "LE", rp_d, cl_d)
+        out["decode_LE_noalloc_unplanned"] = {"ms_per_step": tot / args.steps,
+                                              "value": E * args.steps / (tot / 1000.0)}
+        fresh.close()
         del rp_d, cl_d
 
     clk = clocks.stop()
