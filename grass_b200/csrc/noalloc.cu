@@ -67,7 +67,7 @@ extern "C" int grass_decode_all_noalloc(const grass_graph *g, uint64_t *d_rowptr
   launch_scan_u64_inplace(d_rowptr, n, scratch, st);
   // The planned sweep once an earlier grass_decode_all has built the graph's
   // plan (launching it allocates nothing); until then the unplanned sweep,
-  // which needs no plan and is about 2.4x slower.
+  // which needs no plan and is about 3x slower.
   if (!launch_decode_if_planned(g, d_rowptr, d_cols, g->d_err, st))
     launch_decode_all(g->view(), d_rowptr, d_cols, g->info.num_edges, g->d_err, st);
   const cudaError_t e = cudaGetLastError();
