@@ -254,11 +254,16 @@ def cfg5_bench(G, torch, stream, flush, K, parity=None):
 # ---------------------------------------------------------------------------
 # clocks during the timed region
 
+# host wall-clock windows of the timed regions (time.time(), start and end),
+# recorded by timed() so that the clock samples taken inside them can be told apart
+TIMED_WINDOWS = []
+
+
 class Clocks:
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,"
-              "utilization.gpu")
+              "utilization.gpu,timestamp")
 
     def __init__(self, gpu_index: int, enabled: bool = True):
         self.p = None
@@ -284,32 +289,40 @@ class Clocks:
         except Exception:
             self.p.kill()
         self.f.close()
-        sm, mx, pw, busy = [], [], [], []
+        import datetime
+        sm, mx, pw, busy, inside = [], [], [], [], []
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in open(self.path):
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 10:
+            if len(parts) < 11:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx.append(float(parts[2]))
-                pw.append(float(parts[3]))
-                busy.append(float(parts[9]) >= 50.0)
+                c, m, w = float(parts[1]), float(parts[2]), float(parts[3])
+                b = float(parts[9]) >= 50.0
+                ts = datetime.datetime.strptime(parts[10], "%Y/%m/%d %H:%M:%S.%f").timestamp()
             except ValueError:
                 continue
+            sm.append(c)
+            mx.append(m)
+            pw.append(w)
+            busy.append(b)
+            # a sample within 50 ms of a timed region counts as taken during it
+            inside.append(any(t0 - 0.05 <= ts <= t1 + 0.05 for t0, t1 in TIMED_WINDOWS))
             for nm, val in zip(names, parts[5:9]):
                 if val.lower().startswith("active"):
                     reasons.add(nm)
         os.unlink(self.path)
         if not sm:
             return None
-        # median under load: samples with the GPU busy (the sampler also runs
+        # median under load: the samples taken during the timed regions, else
+        # those with the GPU busy (the sampler also runs while graphs load and
         # while the host checks outputs between timed regions)
-        loaded = [c for c, b in zip(sm, busy) if b] or sm
+        loaded = ([c for c, t in zip(sm, inside) if t] or [c for c, b in zip(sm, busy) if b]
+                  or sm)
         return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx), "samples": len(sm),
-                "samples_under_load": sum(busy), "power_w_max": max(pw),
-                "reasons": sorted(reasons)}
+                "samples_in_timed_regions": sum(inside), "samples_under_load": sum(busy),
+                "power_w_max": max(pw), "reasons": sorted(reasons)}
 
 
 def peaks():
@@ -451,12 +464,14 @@ def timed(torch, fn, K, W, flush, dist=None, dev=None):
     st = torch.cuda.current_stream()
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
            for _ in range(K)]
+    t_start = time.time()
     for a, b in evs:
         flush()
         a.record(st)
         fn()
         b.record(st)
     torch.cuda.synchronize()
+    TIMED_WINDOWS.append((t_start, time.time()))
     barrier(dist, dev)
     torch.cuda.synchronize()
     ms = [a.elapsed_time(b) for a, b in evs]

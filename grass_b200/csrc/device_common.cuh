@@ -494,11 +494,6 @@ __device__ __forceinline__ void le_slot_decode(const Sec &A, uint32_t off, const
 }
 
 // ---- slot decoders on 32-bit words (shared or global memory) ----
-// Unroll factor of their per-neighbor loops (more field reads in flight).
-#ifndef GRASS_DECODE_UNROLL
-#define GRASS_DECODE_UNROLL 1
-#endif
-constexpr int kDecodeUnroll = GRASS_DECODE_UNROLL;
 // w points at the slot's sector as stream words (each the next 32 bits MSB
 // first), with one more readable word after it; off is the bit offset of the
 // slot in it.  One funnel shift per field of up to 32 bits.
@@ -536,7 +531,6 @@ __device__ __forceinline__ void le_slot_decode_w(const uint32_t *w, uint32_t off
   const uint32_t step = div_small(r2 - r1, L);
   o[0] = r1;
   uint32_t at = s0, base = r1;
-#pragma unroll kDecodeUnroll
   for (uint32_t id = 1; id < L; id++, at += (uint32_t)sw) {
     base += step;
     o[id] = word_sea(w, at, sw, base);
@@ -550,7 +544,6 @@ __device__ __forceinline__ void gt_slot_decode_w(const uint32_t *w, uint32_t off
   uint32_t x = c >= h.fp ? h.v + hv : h.v - hv;
   o[0] = x;
   uint32_t at = off + (uint32_t)h.a;
-#pragma unroll kDecodeUnroll
   for (uint32_t t = 1; t < L; t++, at += (uint32_t)h.b) {
     x += word_field(w, at, h.b) + 1u;
     o[t] = x;
