@@ -602,8 +602,12 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
 // neighbor is in the record).
 constexpr uint32_t kFlatHub = kRange;  // degree from which a vertex is split into ranges
 
+#ifndef GRASS_DECODE_FLAT_MIN_BLOCKS
+#define GRASS_DECODE_FLAT_MIN_BLOCKS 1
+#endif
+
 template <int MODE>
-__global__ void __launch_bounds__(256) decode_flat_kernel(DevGraph g, const uint64_t *rowptr,
+__global__ void __launch_bounds__(256, GRASS_DECODE_FLAT_MIN_BLOCKS) decode_flat_kernel(DevGraph g, const uint64_t *rowptr,
                                                           uint32_t *cols,
                                                           const uint4 *__restrict__ items,
                                                           uint64_t nitems, unsigned int *err) {
