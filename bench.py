@@ -729,42 +729,62 @@ def reference_visits(G, torch, gdir, n, positions=(1, 10, 40, 79), timeout_s=600
     sources with baseline/visit_hook.h force-included, which writes the
     transits after the chosen steps); this library walks the same starts
     (i % n) for 80 steps.  Each walker adds one visit per position, so each
-    position's counts are a sample of n independent walkers; ended walks are
-    not counted."""
+    position's counts are a sample of n walkers; ended walks are not counted.
+    Calibration beside it: this library against itself (two Philox seeds),
+    and, for LE, whose reference states are seeded from the clock, the
+    reference against itself (two runs).  The test assumes independent
+    walkers; a sample whose walkers are correlated fails it even against
+    itself."""
     import tempfile
     out = {"positions": list(positions), "walkers": n}
     dev = torch.device("cuda", torch.cuda.current_device())
+
+    def ref_counts(exe, gpath):
+        with tempfile.TemporaryDirectory() as td:
+            env = dict(os.environ, GRASS_VISIT_DUMP=os.path.join(td, "v"),
+                       GRASS_VISIT_STEPS=",".join(map(str, positions)))
+            r = subprocess.run([exe, "-g", gpath, "-n", "1"], env=env, capture_output=True,
+                               text=True, timeout=timeout_s)
+            cnt = {}
+            for pos in positions:
+                f = os.path.join(td, f"v.{pos}.i32")
+                if os.path.exists(f):
+                    a = np.fromfile(f, dtype=np.int32)
+                    cnt[pos] = np.bincount(a[(a >= 0) & (a < n)], minlength=n)
+            return r.returncode, cnt
+
+    def chi(a, b):
+        stat, df, pv = two_sample_chi2(a, b)
+        return {"chi2_over_df": stat / max(df, 1), "df": df, "p": pv}
+
     for m in ("GT", "LE"):
         exe = os.path.join(ROOT, "baseline", "_ref", f"rw_{m.lower()}_visits")
         if not os.path.exists(exe):
             out[m] = {"unavailable": f"{exe} not built"}
             continue
-        with tempfile.TemporaryDirectory() as td:
-            env = dict(os.environ, GRASS_VISIT_DUMP=os.path.join(td, "v"),
-                       GRASS_VISIT_STEPS=",".join(map(str, positions)))
-            r = subprocess.run([exe, "-g", os.path.join(gdir, m), "-n", "1"], env=env,
-                               capture_output=True, text=True, timeout=timeout_s)
-            ref = {}
-            for pos in positions:
-                f = os.path.join(td, f"v.{pos}.i32")
-                ref[pos] = np.fromfile(f, dtype=np.int32) if os.path.exists(f) else None
-        g = G.Graph(os.path.join(gdir, m), m)
+        gpath = os.path.join(gdir, m)
+        rc, ref = ref_counts(exe, gpath)
+        ref2 = ref_counts(exe, gpath)[1] if m == "LE" else None
+        g = G.Graph(gpath, m)
         starts = torch.arange(n, dtype=torch.int32, device=dev)
         paths = torch.empty(n * 81, dtype=torch.int32, device=dev)
-        g.rw_device(starts, n, 80, 20241203, paths, layout=1)
-        ours = paths.view(81, n).cpu().numpy()
+        ours = []
+        for seed in (20241203, 777):
+            g.rw_device(starts, n, 80, seed, paths, layout=1)
+            ours.append(paths.view(81, n).cpu().numpy())
         g.close()
-        res = {"rc": r.returncode}
+        res = {"rc": rc}
         for pos in positions:
-            if ref[pos] is None:
+            if pos not in ref:
                 res[str(pos)] = {"unavailable": "no dump"}
                 continue
-            rv = ref[pos][(ref[pos] >= 0) & (ref[pos] < n)]
-            ov = ours[pos][(ours[pos] >= 0) & (ours[pos] < n)]
-            stat, df, pv = two_sample_chi2(np.bincount(rv, minlength=n),
-                                           np.bincount(ov, minlength=n))
-            res[str(pos)] = {"visits_reference": int(rv.size), "visits_grass_b200": int(ov.size),
-                             "chi2": stat, "df": df, "p": pv}
+            oc = [np.bincount(o[pos][(o[pos] >= 0) & (o[pos] < n)], minlength=n) for o in ours]
+            e = {"visits_reference": int(ref[pos].sum()), "visits_grass_b200": int(oc[0].sum()),
+                 "reference_vs_grass_b200": chi(ref[pos], oc[0]),
+                 "grass_b200_vs_itself": chi(oc[0], oc[1])}
+            if ref2 is not None and pos in ref2:
+                e["reference_vs_itself"] = chi(ref[pos], ref2[pos])
+            res[str(pos)] = e
         out[m] = res
     return out
 
