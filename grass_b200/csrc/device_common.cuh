@@ -519,33 +519,73 @@ __device__ __forceinline__ uint32_t word_sea(const uint32_t *w, uint32_t off, in
 }
 
 // le_slot_decode / gt_slot_decode on words.
+// Fields of up to 32 bits read in order from words: a two-word window, one
+// funnel shift per field, the next word loaded one ahead.  Reads up to three
+// words past the last field's word.
+struct WordStream {
+  const uint32_t *w;
+  uint32_t q, pos, lo, hi, nx;
+  __device__ __forceinline__ void init(const uint32_t *words, uint32_t at) {
+    w = words;
+    q = at >> 5;
+    pos = at & 31u;
+    lo = w[q];
+    hi = w[q + 1];
+    nx = w[q + 2];
+  }
+  __device__ __forceinline__ uint32_t get(int width) {  // width 0..32
+    const uint32_t x = __funnelshift_l(hi, lo, pos);
+    pos += (uint32_t)width;
+    if (pos >= 32) {
+      pos -= 32;
+      lo = hi;
+      hi = nx;
+      nx = w[q + 3];
+      q++;
+    }
+    return width ? x >> (32 - width) : 0u;
+  }
+};
+
 __device__ __forceinline__ void le_slot_decode_w(const uint32_t *w, uint32_t off, const VHdr &h,
                                                  uint32_t c, uint32_t L, bool with_right,
                                                  uint32_t *o) {
   const int sw = h.b + 1;
-  const uint32_t r1m = word_field(w, off, h.a);
-  const uint32_t r1 = c < h.fp ? h.v - r1m : h.v + r1m;
   const uint32_t s0 = off + (uint32_t)h.a;
   const uint32_t r2m = word_field(w, s0 + (h.bl - 1) * (uint32_t)sw, h.a);
   const uint32_t r2 = c + 1 < h.fp ? h.v - r2m : h.v + r2m;
+  WordStream S;
+  S.init(w, off);
+  const uint32_t r1m = S.get(h.a);
+  const uint32_t r1 = c < h.fp ? h.v - r1m : h.v + r1m;
   const uint32_t step = div_small(r2 - r1, L);
   o[0] = r1;
-  uint32_t at = s0, base = r1;
-  for (uint32_t id = 1; id < L; id++, at += (uint32_t)sw) {
+  uint32_t base = r1;
+  for (uint32_t id = 1; id < L; id++) {
     base += step;
-    o[id] = word_sea(w, at, sw, base);
+    uint32_t mag, neg;
+    if (sw > 32) {  // sea_bit 32: the magnitude is the field's top 32 bits
+      mag = S.get(32);
+      neg = S.get(1);
+    } else {
+      const uint32_t raw = S.get(sw);
+      mag = raw >> 1;
+      neg = raw & 1u;
+    }
+    o[id] = base + (neg ? 0u - mag : mag);
   }
   if (with_right) o[L] = r2;
 }
 
 __device__ __forceinline__ void gt_slot_decode_w(const uint32_t *w, uint32_t off, const VHdr &h,
                                                  uint32_t c, uint32_t L, uint32_t *o) {
-  const uint32_t hv = word_field(w, off, h.a) + 1u;
+  WordStream S;
+  S.init(w, off);
+  const uint32_t hv = S.get(h.a) + 1u;
   uint32_t x = c >= h.fp ? h.v + hv : h.v - hv;
   o[0] = x;
-  uint32_t at = off + (uint32_t)h.a;
-  for (uint32_t t = 1; t < L; t++, at += (uint32_t)h.b) {
-    x += word_field(w, at, h.b) + 1u;
+  for (uint32_t t = 1; t < L; t++) {
+    x += S.get(h.b) + 1u;
     o[t] = x;
   }
 }
