@@ -254,6 +254,14 @@ def cfg5_bench(G, torch, stream, flush, K, parity=None):
 # ---------------------------------------------------------------------------
 # clocks during the timed region
 
+_T0 = time.time()
+
+
+def progress(msg: str):
+    """One line per phase on stderr, with the seconds since the bench started."""
+    print(f"[bench +{time.time() - _T0:7.1f}s] {msg}", file=sys.stderr, flush=True)
+
+
 # host wall-clock windows of the timed regions (time.time(), start and end),
 # recorded by timed() so that the clock samples taken inside them can be told apart
 TIMED_WINDOWS = []
@@ -916,10 +924,12 @@ def main():
     only = set(args.only.split(",")) if args.only else {"rw", "khop", "decode", "csr", "e2e",
                                                          "cpu", "batch", "serve", "parity",
                                                          "footprint"}
+    progress("graph build / cache")
     gdir, meta = build_graph(args.scale, args.edge_factor)
     n, E = meta["n"], meta["num_edges"]
     W, L = args.walkers, args.length
     dev = torch.device("cuda", local)
+    progress("open graphs")
     stream = torch.cuda.current_stream()
     flush_buf = torch.empty(64 << 20, dtype=torch.int32, device=dev)
 
@@ -944,6 +954,7 @@ def main():
         return lambda: obj.rw_device(starts, W, L, replica_seed(7, rank), paths, ecount, layout=LAYOUT,
                                      stream=stream)
 
+    progress("random walks")
     # ---- (a) random walk: headline mode first
     order = [args.mode] + [m for m in ("LE", "GT") if m != args.mode]
     launches0 = G.launch_count()
@@ -970,6 +981,7 @@ def main():
         all_edges = sum_over_ranks(dist, e1 * args.steps, torch)
         out["rw_CSR"] = {"value": all_edges / (tot / 1000.0), "ms_per_step": tot / args.steps}
 
+    progress("k-hop")
     # ---- (b) k-hop (25, 10)
     if "khop" in only:
         S, fan = args.khop_seeds, (25, 10)
@@ -1013,6 +1025,7 @@ def main():
             "achieved_gbs": alg / (tot / args.steps / 1000.0) / 1e9}
         del hops, csrc, cdst
 
+    progress("decode sweep")
     # ---- (c) decode-only sweep
     if "decode" in only:
         rp_d = torch.empty(n + 1, dtype=torch.int64, device=dev)
@@ -1058,6 +1071,7 @@ def main():
 
     clk = clocks.stop()
 
+    progress("batched jobs and serving")
     # ---- batched uneven jobs and the serving loop (R-MAT s24 ef16), 1 GPU runs
     if ws == 1 and ({"batch", "serve"} & only):
         bdir, bmeta = build_graph(args.batch_scale, 16)
@@ -1067,12 +1081,14 @@ def main():
                           f"(undirected): "
                           f"{bn} vertices, {bmeta['num_edges']} directed edges"}
         if "batch" in only:
+            progress("batch: 256-job mix, autotune + timed runs (LE, GT, CSR)")
             bcsr = bgraphs["LE"].csr()  # uncompressed baseline of the same graph
             extra["batch"] = batch_bench(G, torch, {**bgraphs, "CSR": bcsr}, bn, stream, flush,
                                          5, 3, parity, bdir)
             bcsr.close()
             del bcsr
         if "serve" in only:
+            progress("serving: peak and latency sweeps")
             extra["serve"] = serve_bench(G, bgraphs[args.mode])
         out["batched_jobs_and_serving"] = extra
         del bgraphs
@@ -1088,6 +1104,7 @@ def main():
     if ws == 1 and "cfg5" in only:
         out["chung_lu_100M"] = cfg5_bench(G, torch, stream, flush, 3, parity)
 
+    progress("roofline accounting, random-read probe")
     # ---- accounting for the roofline of the headline kernel
     acct = torch.zeros(3, dtype=torch.int64, device=dev)
     graphs[args.mode].rw_account(starts, W, L, replica_seed(7, rank), acct, stream=stream)
@@ -1112,6 +1129,7 @@ def main():
             rand.update({"CSR_sectors_per_draw": 2.0,
                          "CSR_sectors_per_s": 2 * draws / (out["rw_CSR"]["ms_per_step"] / 1000.0)})
 
+    progress("e2e")
     # ---- e2e through the host API, pinned buffers, copies inside the region
     e2e = None
     if "e2e" in only:
@@ -1142,6 +1160,7 @@ def main():
                "ms_per_step": 1000 * el / args.steps, "api": "grass_rw_host (pinned host buffers)"}
 
     cpu = None
+    progress("cpu baseline")
     if rank == 0 and "cpu" in only:
         try:
             cpu = cpu_baseline(gdir, args.mode, n, L, 7)
