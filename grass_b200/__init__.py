@@ -128,7 +128,8 @@ class ServerStats(C.Structure):
                                           "batches", "edges", "waiting", "running",
                                           "scratch_in_use", "scratch_peak")] + \
                [("busy_us", C.c_double), ("issue_us", C.c_double),
-                ("staging_alloc_us", C.c_double), ("phase_us", C.c_double * 6)]
+                ("staging_alloc_us", C.c_double), ("phase_us", C.c_double * 6),
+                ("staging_fallbacks", C.c_uint64)]
 
     def as_dict(self):
         return {k: list(getattr(self, k)) if k == "phase_us" else getattr(self, k)

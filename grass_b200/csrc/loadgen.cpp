@@ -12,6 +12,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <list>
 #include <thread>
 #include <vector>
 
@@ -153,18 +154,12 @@ int run_server(const grass_graph *g, const grass_loadgen_config &c, std::vector<
   for (auto &s : state) s.store(0);
   Clock::time_point t0;
   std::atomic<bool> started{false};
+  // The collector takes results as they finish and releases each at once,
+  // oldest first but not only in order: a request still queued must not keep
+  // later, finished results (and the staging or scratch they hold) alive.
   std::thread collector([&] {
     while (!started.load(std::memory_order_acquire)) std::this_thread::yield();
-    for (size_t i = 0; i < N; i++) {
-      int sv;
-      while ((sv = state[i].load(std::memory_order_acquire)) == 0) std::this_thread::yield();
-      if (sv == 2) continue;
-      grass_result res;
-      const int rc = grass_server_wait(srv, ticket[i], c.timeout_ms, &res);
-      if (rc == GRASS_E_TIMEOUT) {
-        o.failed++;
-        continue;
-      }
+    auto record = [&](size_t i, int rc, const grass_result &res) {
       if (rc || res.status) {
         o.failed++;
       } else {
@@ -180,6 +175,52 @@ int run_server(const grass_graph *g, const grass_loadgen_config &c, std::vector<
         o.last = std::max(o.last, submit_at[i] + (res.done_us - res.submit_us));
       }
       grass_server_release(srv, ticket[i]);
+    };
+    std::list<size_t> open;  // submitted, not yet collected, in ticket order
+    size_t next = 0, closed = 0;
+    double oldest_since = -1;  // when the collector started waiting on open.front()
+    constexpr size_t kScan = 1024;  // later requests checked while the oldest runs
+    while (closed < N) {
+      while (next < N) {
+        const int sv = state[next].load(std::memory_order_acquire);
+        if (sv == 0) break;
+        if (sv == 2) closed++;
+        else open.push_back(next);
+        next++;
+      }
+      if (open.empty()) {
+        std::this_thread::yield();
+        continue;
+      }
+      const size_t i = open.front();
+      if (oldest_since < 0) oldest_since = since_us(t0);
+      grass_result res;
+      const int rc = grass_server_wait(srv, ticket[i], 1, &res);
+      if (rc != GRASS_E_TIMEOUT) {
+        record(i, rc, res);
+        open.pop_front();
+        closed++;
+        oldest_since = -1;
+        continue;
+      }
+      size_t k = 0;
+      for (auto it = std::next(open.begin()); it != open.end() && k < kScan; k++) {
+        int d = 0;
+        if (grass_server_poll(srv, ticket[*it], &d) == GRASS_OK && d) {
+          grass_result r2;
+          record(*it, grass_server_wait(srv, ticket[*it], 0, &r2), r2);
+          it = open.erase(it);
+          closed++;
+        } else {
+          ++it;
+        }
+      }
+      if (since_us(t0) - oldest_since > 1e3 * c.timeout_ms) {  // give the oldest up
+        o.failed++;
+        open.pop_front();
+        closed++;
+        oldest_since = -1;
+      }
     }
   });
   t0 = Clock::now();

@@ -49,6 +49,7 @@ namespace {
 using Clock = std::chrono::steady_clock;
 constexpr uint64_t kAlign = 256;
 constexpr uint32_t kMaxSlots = 16;
+constexpr double kFallbackUs = 5000;  // staging wait with nothing in flight before the fallback
 
 inline uint64_t align_up(uint64_t x) { return (x + kAlign - 1) & ~(kAlign - 1); }
 
@@ -222,6 +223,7 @@ struct grass_server {
   uint64_t in_use = 0;
   grass_server_stats st{};
   double busy_since = 0;
+  double staging_blocked_since = -1;  // first failed staging take with nothing in flight
   grass::Clock::time_point t0;
 
   double now_us() const {
@@ -379,20 +381,36 @@ Batch *grass_server::form(double now, int cls) {
   b->work_bytes = b->bytes - b->out_bytes;
   b->in_cap = table_bytes(b->reqs.size(), ntasks) + sin;
   b->out_cap = align_up(b->reqs.size() * 8 + 4) + (dev_out ? 0 : sout);
-  bool ok = true;
+  bool fallback = false;
   if (Arena::round(b->in_cap) + Arena::round(b->out_cap) > staging.size) {
     b->oversize = true;  // a single request larger than the arena
   } else {
     b->in_host = staging.take(b->in_cap);
     b->out_host = b->in_host ? staging.take(b->out_cap) : nullptr;
-    ok = b->out_host != nullptr;
+    if (!b->out_host) {
+      staging.give(b->in_host, b->in_cap);
+      b->in_host = nullptr;
+      // With batches in flight their finish frees staging (and wakes this
+      // loop): wait.  With none, the arena is held by results their callers
+      // have not released.  Releases usually follow within microseconds, but
+      // waiting for them could wait for good (a caller may hold one result
+      // while it waits for the next), so after kFallbackUs with nothing in
+      // flight this batch stages through the pinned fallback pool instead.
+      if (running == 0) {
+        if (staging_blocked_since < 0) staging_blocked_since = now;
+        if (now - staging_blocked_since >= kFallbackUs) b->oversize = fallback = true;
+      } else {
+        staging_blocked_since = -1;
+      }
+    }
   }
+  bool ok = b->oversize || b->out_host;
   if (ok) {
     b->d_work = static_cast<uint8_t *>(scratch.take(b->work_bytes));
     b->d_out = !b->d_work || !b->out_bytes ? nullptr : static_cast<uint8_t *>(scratch.take(b->out_bytes));
     ok = b->d_work && (b->d_out || !b->out_bytes);
   }
-  if (!ok) {  // wait for releases (fragmented arenas); requests go back in order
+  if (!ok) {  // wait for a finish or releases (fragmented arenas); requests go back in order
     if (!b->oversize) {
       staging.give(b->in_host, b->in_cap);
       staging.give(b->out_host, b->out_cap);
@@ -406,6 +424,8 @@ Batch *grass_server::form(double now, int cls) {
     delete b;
     return nullptr;
   }
+  if (fallback) st.staging_fallbacks++;
+  staging_blocked_since = -1;
   b->slot = slot;
   b->cls = cls;
   running_cls[cls]++;
@@ -647,7 +667,7 @@ void grass_server::loop() {
     }
     // Sleep until a window closes, or a submit/finish.  A batch that was due
     // but not formed waits for scratch or a stream: only a finish helps.
-    double wait_us = 50000;
+    double wait_us = staging_blocked_since >= 0 && running == 0 ? kFallbackUs / 4 : 50000;
     for (int c = 0; c < 2; c++) {
       if (waiting[c].empty() || free_slot(c) == kMaxSlots) continue;
       const double left = window_left(c, now);

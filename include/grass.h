@@ -414,7 +414,11 @@ int grass_batch_destroy(grass_batch *b);
  * Results are copied to pinned host memory owned by the server (or, with
  * results_on_device, stay in device memory) and stay valid until
  * grass_server_release.  Each request's result equals the standalone call
- * with the same parameters and seed.
+ * with the same parameters and seed.  Unreleased host results never stall
+ * new batches: when they fill the staging arena, batches stage through a
+ * pinned fallback pool (counted in staging_fallbacks).  Results kept on the
+ * device count against scratch_budget until released, so a caller that holds
+ * them must release some before waiting on requests that need the room.
  * ========================================================================= */
 typedef struct {
   uint64_t scratch_budget;   /* device bytes for launched requests, allocated at create
@@ -471,6 +475,9 @@ typedef struct {
   double phase_us[6];                       /* issue time by step: pool allocation,
                                                staging fill, H2D enqueue, kernel launch,
                                                D2H enqueue, free + completion callback  */
+  uint64_t staging_fallbacks;               /* batches staged through the pinned fallback
+                                               pool because unreleased results held the
+                                               staging arena                             */
 } grass_server_stats;
 
 typedef struct grass_server grass_server;
