@@ -179,7 +179,11 @@ int run_server(const grass_graph *g, const grass_loadgen_config &c, std::vector<
     std::list<size_t> open;  // submitted, not yet collected, in ticket order
     size_t next = 0, closed = 0;
     double oldest_since = -1;  // when the collector started waiting on open.front()
-    constexpr size_t kScan = 1024;  // later requests checked while the oldest runs
+    // Later requests are checked only while the oldest has been waited for a
+    // while (a queued request, not merely a long one), and a bounded number
+    // per pass, so that polling does not compete with the dispatcher.
+    constexpr size_t kScan = 256;
+    constexpr double kScanAfterUs = 10000;
     while (closed < N) {
       while (next < N) {
         const int sv = state[next].load(std::memory_order_acquire);
@@ -195,7 +199,7 @@ int run_server(const grass_graph *g, const grass_loadgen_config &c, std::vector<
       const size_t i = open.front();
       if (oldest_since < 0) oldest_since = since_us(t0);
       grass_result res;
-      const int rc = grass_server_wait(srv, ticket[i], 1, &res);
+      const int rc = grass_server_wait(srv, ticket[i], 2, &res);
       if (rc != GRASS_E_TIMEOUT) {
         record(i, rc, res);
         open.pop_front();
@@ -203,7 +207,7 @@ int run_server(const grass_graph *g, const grass_loadgen_config &c, std::vector<
         oldest_since = -1;
         continue;
       }
-      size_t k = 0;
+      size_t k = since_us(t0) - oldest_since < kScanAfterUs ? kScan : 0;
       for (auto it = std::next(open.begin()); it != open.end() && k < kScan; k++) {
         int d = 0;
         if (grass_server_poll(srv, ticket[*it], &d) == GRASS_OK && d) {

@@ -692,7 +692,7 @@ int grass_server_create(const grass_graph *g, const grass_server_config *cfg,
   if (cfg) s->cfg = *cfg;
   grass_server_config &c = s->cfg;
   if (!c.scratch_budget) c.scratch_budget = 8ull << 30;
-  if (!c.target_draws) c.target_draws = 1ull << 22;
+  if (!c.target_draws) c.target_draws = 1ull << 20;
   if (!c.staging_bytes) c.staging_bytes = 1ull << 30;
   if (!c.window_min_us) c.window_min_us = 200;
   if (!c.window_max_us) c.window_max_us = 1000;

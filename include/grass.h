@@ -423,7 +423,7 @@ int grass_batch_destroy(grass_batch *b);
 typedef struct {
   uint64_t scratch_budget;   /* device bytes for launched requests, allocated at create
                                 (0: 8 GiB)                                            */
-  uint64_t target_draws;     /* close a batch at this much waiting work (0: 2^22)     */
+  uint64_t target_draws;     /* close a batch at this much waiting work (0: 2^20)     */
   uint64_t staging_bytes;    /* pinned host arena for inputs and results, made at
                                 create (0: 1 GiB); a batch carries at most 1/8 of it
                                 unless one request is larger.  Results hold their

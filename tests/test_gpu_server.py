@@ -225,3 +225,31 @@ def test_requests_overlap_a_running_batch(mode):
     np.testing.assert_array_equal(res["outputs"][1], dst.reshape(-1))
     assert res["edges"] == e2
     srv.close()
+
+
+@pytest.mark.parametrize("mode", ["GT", "LE"])
+def test_held_results_do_not_stall_later_requests(mode):
+    """A caller holds every result while it waits for the next, and the
+    results together are far larger than the pinned staging arena.  Waiting
+    for releases would stall for good; the server stages the later batches
+    through its fallback pool and every request finishes, with the
+    standalone result."""
+    d, *_ = golden_graph("rmat_s10_e8")
+    g = G.Graph(os.path.join(d, mode), mode)
+    n = g.n
+    rng = np.random.default_rng(9)
+    srv = G.Server(g, staging_bytes=1 << 20, max_inflight=2, window_min_us=1, window_max_us=1)
+    reqs = []
+    for i in range(12):  # each result ~160-320 KB: the 1 MiB arena holds a few at most
+        starts = rng.integers(0, n, 1000 + 100 * i).astype(np.uint32)
+        reqs.append((starts, 39, 500 + i, srv.submit_rw(starts, 39, 500 + i)))
+    held = []
+    for starts, L, seed, t in reqs:
+        held.append((starts, L, seed, srv.wait(t, timeout_ms=20000, release=False)))
+    for starts, L, seed, r in held:
+        p, _ = g.rw(starts, L, seed)
+        np.testing.assert_array_equal(r["outputs"][0], p.reshape(-1))
+    assert srv.stats()["staging_fallbacks"] >= 1
+    for _, _, _, t in reqs:
+        G.lib.grass_server_release(srv._h, t)
+    srv.close()
