@@ -373,6 +373,16 @@ class Parity:
         got = P.contiguous().cpu().numpy().view(np.uint32)
         self.put(key, np.array_equal(got, ref), walkers=k, steps=L)
 
+    def node2vec(self, key, prefix, mode, starts, W, L, seed, p, q, paths, layout, k=8192):
+        if not self.enabled:
+            return
+        k = min(k, W)
+        st = starts[:k].cpu().numpy().view(np.uint32)
+        ref, _ = self.graph(prefix).node2vec(mode, st, L, seed, p, q)
+        P = paths.view(L + 1, W)[:, :k].T if layout == 1 else paths.view(W, L + 1)[:k]
+        got = P.contiguous().cpu().numpy().view(np.uint32)
+        self.put(key, np.array_equal(got, ref), walkers=k, steps=L, p=p, q=q)
+
     def khop(self, key, prefix, mode, seeds, S, fan, seed, hops, k=4096):
         if not self.enabled:
             return
@@ -1024,6 +1034,29 @@ def main():
             "algorithmic_bytes": alg,
             "achieved_gbs": alg / (tot / args.steps / 1000.0) / 1e9}
         del hops, csrc, cdst
+
+    # ---- second-order (node2vec) walk, beyond the reference: only when asked for
+    if "n2v" in only:
+        progress("node2vec walks")
+        for name, obj in [("LE", graphs["LE"]), ("GT", graphs["GT"])] + (
+                [("CSR", csr)] if csr is not None else []):
+            for (p, q) in ((1.0, 0.5), (4.0, 0.25)):
+                ecount.zero_()
+                obj.node2vec_device(starts, W, L, replica_seed(7, rank), p, q, paths, ecount, layout=LAYOUT,
+                                    stream=stream)
+                torch.cuda.synchronize()
+                e1 = int(ecount.item())
+                ms, tot = timed(torch, lambda o=obj: o.node2vec_device(
+                    starts, W, L, replica_seed(7, rank), p, q, paths, ecount, layout=LAYOUT,
+                    stream=stream),
+                    args.steps, args.warmup, flush, dist, local)
+                out[f"node2vec_{name}_p{p:g}_q{q:g}"] = {
+                    "value": sum_over_ranks(dist, e1 * args.steps, torch) / (tot / 1000.0),
+                    "unit": UNIT, "ms_per_step": tot / args.steps, "edges_per_step": e1}
+                if name != "CSR":
+                    parity.node2vec(f"node2vec_{name}_p{p:g}_q{q:g}", os.path.join(gdir, name),
+                                    name, starts, W, L, replica_seed(7, rank), p, q, paths,
+                                    LAYOUT)
 
     progress("decode sweep")
     # ---- (c) decode-only sweep

@@ -62,6 +62,12 @@ class RwParams(C.Structure):
     _fields_ = [("length", C.c_uint32), ("layout", C.c_uint32), ("seed", C.c_uint64)]
 
 
+class Node2vecParams(C.Structure):
+    _fields_ = [("length", C.c_uint32), ("layout", C.c_uint32), ("seed", C.c_uint64),
+                ("p", C.c_double), ("q", C.c_double), ("max_tries", C.c_uint32),
+                ("reserved", C.c_uint32 * 3)]
+
+
 class KhopParams(C.Structure):
     _fields_ = [("hops", C.c_uint32), ("fanouts", C.c_uint32 * MAX_HOPS), ("seed", C.c_uint64)]
 
@@ -201,6 +207,8 @@ def _load():
         "grass_decode_all_noalloc": ([P, P, P, P], i32),
         "grass_uniform_starts": ([u64, u64, u64, P, P], i32),
         "grass_rw": ([P, C.POINTER(RwParams), P, u64, P, P, P], i32),
+        "grass_node2vec": ([P, C.POINTER(Node2vecParams), P, u64, P, P, P], i32),
+        "grass_csr_node2vec": ([P, C.POINTER(Node2vecParams), P, u64, P, P, P], i32),
         "grass_rw_host": ([P, C.POINTER(RwParams), P, u64, P, P], i32),
         "grass_rw_account": ([P, C.POINTER(RwParams), P, u64, P, P], i32),
         "grass_random_read_probe": ([P, u64, u64, u64, P, C.POINTER(u64), P], i32),
@@ -464,6 +472,13 @@ class Graph:
         p = RwParams(length, layout, seed)
         _check(lib.grass_rw(self._h, C.byref(p), _ptr(starts), W, _ptr(paths), _ptr(edge_count),
                             _stream(stream)))
+
+    def node2vec_device(self, starts, W: int, length: int, seed: int, p: float, q: float,
+                        paths, edge_count=None, max_tries: int = 0,
+                        layout: int = LAYOUT_WALK_MAJOR, stream=None):
+        prm = Node2vecParams(length, layout, seed, p, q, max_tries)
+        _check(lib.grass_node2vec(self._h, C.byref(prm), _ptr(starts), W, _ptr(paths),
+                                  _ptr(edge_count), _stream(stream)))
 
     def rw_account(self, starts, W: int, length: int, seed: int, out3, stream=None):
         """Adds [algorithmic bytes, 32B sectors, draws] of the walk to out3."""
@@ -806,6 +821,13 @@ class Csr:
         n, nnz, b = C.c_uint64(), C.c_uint64(), C.c_uint64()
         _check(lib.grass_csr_info(self._h, C.byref(n), C.byref(nnz), C.byref(b)))
         return {"n": n.value, "nnz": nnz.value, "device_bytes": b.value}
+
+    def node2vec_device(self, starts, W: int, length: int, seed: int, p: float, q: float,
+                        paths, edge_count=None, max_tries: int = 0,
+                        layout: int = LAYOUT_WALK_MAJOR, stream=None):
+        prm = Node2vecParams(length, layout, seed, p, q, max_tries)
+        _check(lib.grass_csr_node2vec(self._h, C.byref(prm), _ptr(starts), W, _ptr(paths),
+                                      _ptr(edge_count), _stream(stream)))
 
     def rw_device(self, starts, W: int, length: int, seed: int, paths, edge_count=None,
                   layout: int = LAYOUT_WALK_MAJOR, stream=None):

@@ -5,6 +5,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <mutex>
 #include <string>
@@ -634,6 +635,38 @@ int grass_rw(const grass_graph *g, const grass_rw_params *p, const uint32_t *d_s
   return check_launch();
 }
 
+// node2vec acceptance thresholds: floor(alpha / alpha_max * 2^32) for alpha
+// = 1/p (return), 1 (a neighbor of the previous vertex), 1/q (farther); the
+// largest is exactly 2^32 (always accepted).  The oracle computes the same.
+static int node2vec_args(const grass_node2vec_params *p, grass_node2vec_params &r,
+                         uint64_t t[3]) {
+  if (!p || p->layout > 1 || !(p->p > 0.0) || !(p->q > 0.0) || !std::isfinite(p->p) ||
+      !std::isfinite(p->q) || p->max_tries > 65536u)
+    return set_error(GRASS_E_ARG, "node2vec: bad parameters");
+  r = *p;
+  if (!r.max_tries) r.max_tries = 64;
+  const double a[3] = {1.0 / r.p, 1.0, 1.0 / r.q};
+  const double amax = std::max(a[0], std::max(a[1], a[2]));
+  for (int k = 0; k < 3; k++) t[k] = (uint64_t)(a[k] / amax * 4294967296.0);
+  return GRASS_OK;
+}
+
+int grass_node2vec(const grass_graph *g, const grass_node2vec_params *p,
+                   const uint32_t *d_starts, uint64_t W, uint32_t *d_paths,
+                   unsigned long long *d_edge_count, void *stream) {
+  grass::Nvtx nvtx_("grass_node2vec");
+  clear_error();
+  if (int rc = check_graph(g)) return rc;
+  grass_node2vec_params r;
+  uint64_t t[3];
+  if (int rc = node2vec_args(p, r, t)) return rc;
+  if (W && (!d_starts || !d_paths)) return set_error(GRASS_E_ARG, "node2vec: null buffers");
+  DeviceGuard dg(g->device);
+  launch_node2vec(g->view(), r, t, d_starts, W, d_paths, d_edge_count, g->d_err,
+                  as_stream(stream));
+  return check_launch();
+}
+
 int grass_rw_account(const grass_graph *g, const grass_rw_params *p, const uint32_t *d_starts,
                      uint64_t W, unsigned long long *d_out, void *stream) {
   clear_error();
@@ -930,6 +963,26 @@ int grass_csr_khop(const grass_csr *c, const grass_khop_params *p, const uint32_
   if (S && (!d_seeds || !d_hop_out)) return set_error(GRASS_E_ARG, "k-hop: null buffers");
   DeviceGuard dg(c->device);
   launch_khop_csr(c->view(), *p, d_seeds, S, d_hop_out, d_edge_count, as_stream(stream));
+  return check_launch();
+}
+
+int grass_csr_node2vec(const grass_csr *c, const grass_node2vec_params *p,
+                       const uint32_t *d_starts, uint64_t W, uint32_t *d_paths,
+                       unsigned long long *d_edge_count, void *stream) {
+  grass::Nvtx nvtx_("grass_csr_node2vec");
+  clear_error();
+  if (!c) return set_error(GRASS_E_ARG, "null csr");
+  grass_node2vec_params r;
+  uint64_t t[3];
+  if (int rc = node2vec_args(p, r, t)) return rc;
+  if (W && (!d_starts || !d_paths)) return set_error(GRASS_E_ARG, "node2vec: null buffers");
+  DeviceGuard dg(c->device);
+  grass::DevGraph v{};
+  v.n = (uint32_t)c->n;
+  v.mode = grass::GRASS_MODE_CSR_INTERNAL;
+  v.rowptr = c->d_rowptr;
+  v.cols = c->d_cols;
+  launch_node2vec(v, r, t, d_starts, W, d_paths, d_edge_count, nullptr, as_stream(stream));
   return check_launch();
 }
 

@@ -139,14 +139,18 @@ __device__ __forceinline__ uint64_t policy_evict_first() {
   return p;
 }
 
+// The loads below are inline PTX, marked volatile: a non-volatile asm
+// statement counts as a pure function of its inputs, so the compiler may
+// execute it speculatively -- hoisted above the branch that guards its
+// address (a record load for an invalid vertex id, say) -- and fault.
 __device__ __forceinline__ uint4 load_record(const uint4 *p) {
   uint4 r;
 #if GRASS_HOT_POLICY
-  asm("ld.global.nc.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
+  asm volatile("ld.global.nc.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%4], %5;"
       : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
       : "l"(p), "l"(policy_evict_last()));
 #else
-  asm("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
+  asm volatile("ld.global.nc.v4.u32 {%0,%1,%2,%3}, [%4];"
       : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
       : "l"(p));
 #endif
@@ -157,7 +161,7 @@ __device__ __forceinline__ uint4 load_record(const uint4 *p) {
 __device__ __forceinline__ uint32_t load_cold_u32(const uint32_t *p) {
 #if GRASS_COLD_POLICY
   uint32_t v;
-  asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy_evict_first()));
+  asm volatile("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(policy_evict_first()));
   return v;
 #else
   return __ldg(p);
@@ -179,11 +183,11 @@ __device__ __forceinline__ Sec load_sector(const uint32_t *words, uint64_t secto
   const uint64_t *p = reinterpret_cast<const uint64_t *>(words) + sector * 4;
   uint64_t a0, a1, a2, a3;
 #if GRASS_COLD_POLICY
-  asm("ld.global.nc.L2::evict_first.v4.b64 {%0,%1,%2,%3}, [%4];"
+  asm volatile("ld.global.nc.L2::evict_first.v4.b64 {%0,%1,%2,%3}, [%4];"
       : "=l"(a0), "=l"(a1), "=l"(a2), "=l"(a3)
       : "l"(p));
 #else
-  asm("ld.global.nc.v4.b64 {%0,%1,%2,%3}, [%4];"
+  asm volatile("ld.global.nc.v4.b64 {%0,%1,%2,%3}, [%4];"
       : "=l"(a0), "=l"(a1), "=l"(a2), "=l"(a3)
       : "l"(p));
 #endif
@@ -696,11 +700,11 @@ __device__ __forceinline__ void csr_row(const uint64_t *rowptr, uint32_t v, uint
   const uint64_t *p = rowptr + (v & ~3u);
   uint64_t a0, a1, a2, a3;
 #if GRASS_HOT_POLICY
-  asm("ld.global.nc.L2::evict_last.v4.b64 {%0,%1,%2,%3}, [%4];"
+  asm volatile("ld.global.nc.L2::evict_last.v4.b64 {%0,%1,%2,%3}, [%4];"
       : "=l"(a0), "=l"(a1), "=l"(a2), "=l"(a3)
       : "l"(p));
 #else
-  asm("ld.global.nc.v4.b64 {%0,%1,%2,%3}, [%4];"
+  asm volatile("ld.global.nc.v4.b64 {%0,%1,%2,%3}, [%4];"
       : "=l"(a0), "=l"(a1), "=l"(a2), "=l"(a3)
       : "l"(p));
 #endif

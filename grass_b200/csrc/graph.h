@@ -219,6 +219,12 @@ grass_tuning resolve_tuning(const grass_tuning &t, int kind);
 void launch_khop(const DevGraph &g, const grass_khop_params &p, const uint32_t *seeds,
                  uint64_t S, uint32_t *const *hop_out, unsigned long long *edges,
                  unsigned int *err, cudaStream_t s);
+// Second-order walk (MODE of g: GT, LE, or 2 for a CSR view); t: the
+// acceptance thresholds {return, in, out} in [0, 2^32].
+void launch_node2vec(const DevGraph &g, const grass_node2vec_params &p, const uint64_t t[3],
+                     const uint32_t *starts, uint64_t W, uint32_t *paths,
+                     unsigned long long *edges, unsigned int *err, cudaStream_t s,
+                     uint64_t w0 = 0);
 void launch_khop_csr(const DevCsr &c, const grass_khop_params &p, const uint32_t *seeds,
                      uint64_t S, uint32_t *const *hop_out, unsigned long long *edges,
                      cudaStream_t s);

@@ -96,6 +96,107 @@ __global__ void __launch_bounds__(512, MODE == 0 ? GRASS_RW_GT_MIN_BLOCKS : GRAS
   if (bad && err) atomicOr(err, 1u);
 }
 
+// ---------------------------------------------------------------------------
+// Second-order (node2vec) walk.  One walker per thread.  Try k of step s
+// draws Philox(seed; s, w, w >> 32, TAG_N2V | k): word 0 picks the candidate
+// from N(v), word 1 is compared with the candidate's acceptance threshold
+// (return to u, a neighbor of u, or farther).  The membership test is a
+// binary search of u's sorted neighbor list (has_neighbor).
+struct N2vArgs {
+  uint32_t L, max_tries;
+  int layout;
+  uint64_t seed, w0;
+  uint64_t t_ret, t_in, t_out;  // acceptance thresholds in [0, 2^32]
+};
+
+// The first neighbor of slot c (GT: its head; LE: its left rock), from the
+// one sector that holds the slot.
+template <int MODE>
+__device__ __forceinline__ uint32_t slot_first(const DevGraph &g, const VHdr &h, uint32_t c) {
+  const uint64_t pos = slot_pos(h, c);
+  const Sec A = load_sector(g.words, pos >> 8);
+  const uint32_t m = (uint32_t)sec1_field(A, (uint32_t)pos & 255u, h.a);
+  if constexpr (MODE == 0) return c >= h.fp ? h.v + m + 1u : h.v - m - 1u;
+  else return c < h.fp ? h.v - m : h.v + m;
+}
+
+// Whether x is a neighbor of u.  Compressed: a binary search over the slots'
+// first neighbors (one sector each), then over the indices of the one slot
+// that can hold x (its sector again, so L1).  CSR: over the row.
+template <int MODE>
+__device__ __forceinline__ bool has_neighbor(const DevGraph &g, const VHdr &h, uint32_t x) {
+  if (h.d == 0) return false;
+  uint32_t lo = 0, hi = h.d - 1;  // index range that can hold x
+  if constexpr (MODE != 2) {
+    if (MODE == 1 && h.d == 1) return h.fp == x;
+    if (slot_first<MODE>(g, h, 0) > x) return false;
+    uint32_t cl = 0, ch = h.bn - 1;  // the last slot whose first neighbor is <= x
+    while (cl < ch) {
+      const uint32_t mid = cl + (ch - cl + 1) / 2;
+      if (slot_first<MODE>(g, h, mid) <= x) cl = mid;
+      else ch = mid - 1;
+    }
+    lo = cl * h.bl;
+    hi = cl + 1 == h.bn ? h.d - 1 : (cl + 1) * h.bl - 1;
+  } else {
+    if (neighbor<MODE>(g, h, 0) > x) return false;
+  }
+  while (lo < hi) {  // the last index in [lo, hi] whose neighbor is <= x
+    const uint32_t mid = lo + (hi - lo + 1) / 2;
+    if (neighbor<MODE>(g, h, mid) <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return neighbor<MODE>(g, h, lo) == x;
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) n2v_kernel(DevGraph g, const uint32_t *__restrict__ starts,
+                                                  uint64_t W, N2vArgs a,
+                                                  uint32_t *__restrict__ paths,
+                                                  unsigned long long *edges, unsigned int *err) {
+  const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  uint64_t cnt = 0;
+  bool bad = false;
+  for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < W; w += nthreads) {
+    const uint64_t id = a.w0 + w;
+    const uint32_t s0 = starts[w];
+    store_path(paths, a.layout, W, a.L, w, 0, s0);
+    uint32_t v = s0 < g.n ? s0 : INVALID_VERTEX, u = INVALID_VERTEX;
+    VHdr hu;  // the previous vertex's header (kept from the step that left it)
+    hu.d = 0;
+    for (uint32_t s = 0; s < a.L; s++) {
+      if (v != INVALID_VERTEX) {
+        const VHdr h = header<MODE>(g, v);
+        if (h.d == 0) {
+          v = INVALID_VERTEX;
+        } else {
+          uint32_t x = INVALID_VERTEX;
+          for (uint32_t k = 0; k < a.max_tries; k++) {
+            const u32x4 r =
+                philox4x32_10(a.seed, s, (uint32_t)id, (uint32_t)(id >> 32), TAG_N2V | k);
+            x = neighbor<MODE>(g, h, mulhi_u32(r.x, h.d));
+            if (s == 0 || k + 1 == a.max_tries) break;  // first step: uniform
+            const uint64_t t = x == u ? a.t_ret : has_neighbor<MODE>(g, hu, x) ? a.t_in : a.t_out;
+            if ((uint64_t)r.y < t) break;
+          }
+          if (x >= g.n) {
+            bad = true;
+            v = INVALID_VERTEX;
+          } else {
+            u = v;
+            hu = h;
+            v = x;
+            cnt++;
+          }
+        }
+      }
+      store_path(paths, a.layout, W, a.L, w, s + 1, v);
+    }
+  }
+  warp_add_u64(edges, cnt);
+  if (bad && err) atomicOr(err, 1u);
+}
+
 // Stream bits a draw of neighbor i reads (the payload fields; the header is
 // in the vertex record), and the 32-byte sectors those reads span.
 template <int MODE>
@@ -596,6 +697,26 @@ void launch_khop(const DevGraph &g, const grass_khop_params &p, const uint32_t *
     khop_kernel<0><<<grid, 256, smem, s>>>(g, seeds, S, A, edges, err);
   else
     khop_kernel<1><<<grid, 256, smem, s>>>(g, seeds, S, A, edges, err);
+  count_launch();
+}
+
+void launch_node2vec(const DevGraph &g, const grass_node2vec_params &p, const uint64_t t[3],
+                     const uint32_t *starts, uint64_t W, uint32_t *paths,
+                     unsigned long long *edges, unsigned int *err, cudaStream_t s, uint64_t w0) {
+  if (!W) return;
+  N2vArgs a;
+  a.L = p.length;
+  a.max_tries = p.max_tries;
+  a.layout = (int)p.layout;
+  a.seed = p.seed;
+  a.w0 = w0;
+  a.t_ret = t[0];
+  a.t_in = t[1];
+  a.t_out = t[2];
+  const unsigned grid = grid_warps(W, 256, cur_dev(), 8);
+  if (g.mode == GRASS_MODE_GT) n2v_kernel<0><<<grid, 256, 0, s>>>(g, starts, W, a, paths, edges, err);
+  else if (g.mode == GRASS_MODE_LE) n2v_kernel<1><<<grid, 256, 0, s>>>(g, starts, W, a, paths, edges, err);
+  else n2v_kernel<2><<<grid, 256, 0, s>>>(g, starts, W, a, paths, edges, err);
   count_launch();
 }
 

@@ -15,6 +15,8 @@
 //                   word 0 (+ word 2 as high half) picks the walker, word 1 the neighbor
 //   uniform starts  c0 = i >> 2,     id = 0,       tag = TAG_START,       word i & 3
 //   multi-RW roots  c0 = i >> 2,     id = 0,       tag = TAG_MRW_ROOT,    word i & 3
+//   node2vec        c0 = step,       id = walker,  tag = TAG_N2V | try,
+//                   word 0 picks the candidate, word 1 is the acceptance draw
 //   multi-RW, continuous time (select 2): counter {k, sample, walker, TAG_MRW_CT}
 //                   for event k of a walker: words 0-1 its holding time, word 2
 //                   its neighbor
@@ -37,6 +39,7 @@ constexpr uint32_t TAG_START = 0x53540001u;
 constexpr uint32_t TAG_MRW_ROOT = 0x4d520002u;
 constexpr uint32_t TAG_GEN = 0x47454e01u;
 constexpr uint32_t TAG_MRW_CT = 0x4d520003u;
+constexpr uint32_t TAG_N2V = 0x4e320000u;  // | try (16 bits)
 
 struct u32x4 {
   uint32_t x, y, z, w;

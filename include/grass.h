@@ -242,6 +242,31 @@ int grass_rw_host(const grass_graph *g, const grass_rw_params *p, const uint32_t
  * for the offset) and to d_out[2] the number of draws. */
 int grass_rw_account(const grass_graph *g, const grass_rw_params *p, const uint32_t *d_starts,
                      uint64_t W, unsigned long long *d_out, void *stream);
+/* Second-order (node2vec) walk: a biased walk beyond the reference, whose
+ * apps are first-order only (its compressor has no edge weights, so a walk
+ * is biased by its previous vertex, not weighted; GT/src/apps/randomwalk/
+ * randomWalks.cu:49-81 is the first-order step this generalises).  The
+ * first step is uniform.  A later step from v, having come from u, draws a
+ * candidate x uniformly from N(v) and accepts it with probability
+ * alpha(x) / max(1/p, 1, 1/q), alpha = 1/p if x == u, 1 if x is a neighbor
+ * of u, 1/q otherwise; after max_tries rejected candidates the last one is
+ * taken.  Try k of step s of walker w draws Philox(seed; s, w, w >> 32,
+ * GRASS_N2V tag | k): word 0 picks the candidate ((r * d) >> 32), word 1 is
+ * compared with the integer threshold floor(alpha / alpha_max * 2^32).
+ * Membership in N(u) is a binary search of u's sorted neighbor list.  Paths
+ * as grass_rw. */
+typedef struct {
+  uint32_t length;     /* steps per walk                                      */
+  uint32_t layout;     /* GRASS_LAYOUT_*                                      */
+  uint64_t seed;       /* Philox key                                          */
+  double p, q;         /* return and in-out parameters (> 0)                  */
+  uint32_t max_tries;  /* candidates per step, 1..65536 (0: 64)               */
+  uint32_t reserved[3];
+} grass_node2vec_params;
+int grass_node2vec(const grass_graph *g, const grass_node2vec_params *p,
+                   const uint32_t *d_starts, uint64_t W, uint32_t *d_paths,
+                   unsigned long long *d_edge_count, void *stream);
+
 /* Random-read probe (no reference counterpart): about `reads` independent
  * random 4-byte reads from d_buf[0, n_words) (n_words a power of two), eight
  * in flight per thread, with the loaded values summed into *d_sink; *issued
@@ -557,6 +582,9 @@ int grass_csr_rw(const grass_csr *c, const grass_rw_params *p, const uint32_t *d
 int grass_csr_khop(const grass_csr *c, const grass_khop_params *p, const uint32_t *d_seeds,
                    uint64_t S, uint32_t *const *d_hop_out, unsigned long long *d_edge_count,
                    void *stream);
+int grass_csr_node2vec(const grass_csr *c, const grass_node2vec_params *p,
+                       const uint32_t *d_starts, uint64_t W, uint32_t *d_paths,
+                       unsigned long long *d_edge_count, void *stream);
 
 #ifdef __cplusplus
 }

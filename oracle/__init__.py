@@ -73,6 +73,9 @@ def lib():
         L.og_rw.restype = u64
         L.og_rw_csr.argtypes = [P, P, u32, P, u64, u32, u64, P, i32]
         L.og_rw_csr.restype = u64
+        L.og_node2vec.argtypes = [G, i32, P, u64, u32, u64, C.c_double, C.c_double, u32, P,
+                                  i32]
+        L.og_node2vec.restype = u64
         L.og_khop.argtypes = [G, i32, P, u64, P, i32, u64, P, i32]
         L.og_khop.restype = u64
         L.og_mrw.argtypes = [G, i32, P, u64, u32, u32, u64, i32, P, P, i32]
@@ -188,6 +191,14 @@ class OracleGraph:
         paths = np.zeros((len(starts), L + 1), dtype=np.uint32)
         tot = lib().og_rw(C.byref(self._g), MODES.get(mode, mode), _p(starts), len(starts), L,
                           seed, _p(paths), threads)
+        return paths, int(tot)
+
+    def node2vec(self, mode, starts: np.ndarray, L: int, seed: int, p: float, q: float,
+                 max_tries: int = 0, threads: int = 0):
+        starts = np.ascontiguousarray(starts, dtype=np.uint32)
+        paths = np.zeros((len(starts), L + 1), dtype=np.uint32)
+        tot = lib().og_node2vec(C.byref(self._g), MODES.get(mode, mode), _p(starts), len(starts),
+                                L, seed, p, q, max_tries, _p(paths), threads)
         return paths, int(tot)
 
     def khop(self, mode, seeds: np.ndarray, fanouts, seed: int, threads: int = 0):

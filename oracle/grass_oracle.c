@@ -437,6 +437,67 @@ uint64_t og_rw(const og_graph *g, int mode, const uint32_t *starts, uint64_t W, 
   return total;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Second-order (node2vec) walk, beyond the reference (its apps are first
+ * order, GT/src/apps/randomwalk/randomWalks.cu:49-81).  Membership of x in
+ * N(u): a binary search of u's sorted list through get_vertex. */
+static int og_has_neighbor(const og_graph *g, int mode, uint32_t u, uint32_t x) {
+  if (u >= g->n) return 0;
+  hdr_t h = header(g, mode, u);
+  if (!h.ok || h.d == 0 || getv(g, mode, &h, 0) > x) return 0;
+  uint32_t lo = 0, hi = h.d - 1;
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo + 1) / 2;
+    if (getv(g, mode, &h, mid) <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return getv(g, mode, &h, lo) == x;
+}
+
+uint64_t og_node2vec(const og_graph *g, int mode, const uint32_t *starts, uint64_t W,
+                     uint32_t L, uint64_t seed, double p, double q, uint32_t max_tries,
+                     uint32_t *paths, int threads) {
+  set_threads(threads);
+  if (!max_tries) max_tries = 64;
+  const double a[3] = {1.0 / p, 1.0, 1.0 / q};
+  double amax = a[0] > a[1] ? a[0] : a[1];
+  if (a[2] > amax) amax = a[2];
+  uint64_t t[3];
+  for (int k = 0; k < 3; k++) t[k] = (uint64_t)(a[k] / amax * 4294967296.0);
+  uint64_t total = 0;
+  const uint64_t pitch = (uint64_t)L + 1;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : total)
+  for (int64_t w = 0; w < (int64_t)W; w++) {
+    uint32_t *row = paths + (uint64_t)w * pitch;
+    uint32_t v = starts[w], u = OG_INVALID;
+    if (v >= g->n) v = OG_INVALID;
+    row[0] = starts[w];
+    for (uint32_t s = 0; s < L; s++) {
+      if (v != OG_INVALID) {
+        hdr_t h = header(g, mode, v);
+        if (!h.ok || h.d == 0) {
+          v = OG_INVALID;
+        } else {
+          uint32_t x = OG_INVALID;
+          for (uint32_t k = 0; k < max_tries; k++) {
+            uint32_t c[4] = {s, (uint32_t)w, (uint32_t)((uint64_t)w >> 32), OG_TAG_N2V | k}, o[4];
+            og_philox4x32_10((uint32_t)seed, (uint32_t)(seed >> 32), c, o);
+            x = getv(g, mode, &h, mulhi32(o[0], h.d));
+            if (s == 0 || k + 1 == max_tries) break;
+            const uint64_t th = x == u ? t[0] : og_has_neighbor(g, mode, u, x) ? t[1] : t[2];
+            if ((uint64_t)o[1] < th) break;
+          }
+          u = v;
+          v = x;
+          total++;
+        }
+      }
+      row[s + 1] = v;
+    }
+  }
+  return total;
+}
+
 uint64_t og_rw_csr(const uint64_t *rowptr, const uint32_t *cols, uint32_t n,
                    const uint32_t *starts, uint64_t W, uint32_t L, uint64_t seed,
                    uint32_t *paths, int threads) {

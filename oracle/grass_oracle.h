@@ -50,6 +50,7 @@ extern "C" {
 #define OG_TAG_START 0x53540001u
 #define OG_TAG_MRW_ROOT 0x4d520002u
 #define OG_TAG_MRW_CT 0x4d520003u
+#define OG_TAG_N2V 0x4e320000u /* | try */
 
 typedef struct {
   uint32_t *words;    /* big-endian packed graph words + 2 zero guard words */
@@ -93,6 +94,15 @@ uint64_t og_rw(const og_graph *g, int mode, const uint32_t *starts, uint64_t W,
 uint64_t og_rw_csr(const uint64_t *rowptr, const uint32_t *cols, uint32_t n,
                    const uint32_t *starts, uint64_t W, uint32_t L, uint64_t seed,
                    uint32_t *paths, int threads);
+/* Second-order (node2vec) walk beyond the reference: first step uniform;
+ * later steps draw candidates from N(v) and accept with probability
+ * alpha / alpha_max (alpha = 1/p back to u, 1 for a neighbor of u, 1/q
+ * otherwise), taking the last candidate after max_tries.  Try k of step s of
+ * walker w: Philox(seed; s, w, w >> 32, OG_TAG_N2V | k), word 0 the candidate,
+ * word 1 against floor(alpha / alpha_max * 2^32).  Paths [W][L+1]. */
+uint64_t og_node2vec(const og_graph *g, int mode, const uint32_t *starts, uint64_t W,
+                     uint32_t L, uint64_t seed, double p, double q, uint32_t max_tries,
+                     uint32_t *paths, int threads);
 
 /* k-hop with replacement.  hop_out[h] is [S][prod_{j<=h} fanouts[j]]. */
 uint64_t og_khop(const og_graph *g, int mode, const uint32_t *seeds, uint64_t S,
