@@ -100,8 +100,8 @@ __global__ void __launch_bounds__(512, MODE == 0 ? GRASS_RW_GT_MIN_BLOCKS : GRAS
 // Second-order (node2vec) walk.  One walker per thread.  Try k of step s
 // draws Philox(seed; s, w, w >> 32, TAG_N2V | k): word 0 picks the candidate
 // from N(v), word 1 is compared with the candidate's acceptance threshold
-// (return to u, a neighbor of u, or farther).  The membership test is a
-// binary search of u's sorted neighbor list (has_neighbor).
+// (return to u, a neighbor of u, or farther).  The membership test searches
+// u's sorted neighbor list (has_neighbor).
 struct N2vArgs {
   uint32_t L, max_tries;
   int layout;
@@ -109,44 +109,68 @@ struct N2vArgs {
   uint64_t t_ret, t_in, t_out;  // acceptance thresholds in [0, 2^32]
 };
 
-// The first neighbor of slot c (GT: its head; LE: its left rock), from the
-// one sector that holds the slot.
+// The first neighbor of slot c (GT: its head; LE: its left rock): one field
+// of at most 32 bits, read as one or two 32-bit words (the second only when
+// the field crosses into it).
 template <int MODE>
 __device__ __forceinline__ uint32_t slot_first(const DevGraph &g, const VHdr &h, uint32_t c) {
   const uint64_t pos = slot_pos(h, c);
-  const Sec A = load_sector(g.words, pos >> 8);
-  const uint32_t m = (uint32_t)sec1_field(A, (uint32_t)pos & 255u, h.a);
+  const uint32_t *q = g.words + (pos >> 5);
+  const uint32_t s = (uint32_t)pos & 31u, w = (uint32_t)h.a;
+  const uint32_t hi = ldw(q), lo = s + w > 32u ? ldw(q + 1) : 0u;
+  const uint32_t m = w ? __funnelshift_l(lo, hi, s) >> (32u - w) : 0u;
   if constexpr (MODE == 0) return c >= h.fp ? h.v + m + 1u : h.v - m - 1u;
   else return c < h.fp ? h.v - m : h.v + m;
 }
 
-// Whether x is a neighbor of u.  Compressed: a binary search over the slots'
-// first neighbors (one sector each), then over the indices of the one slot
-// that can hold x (its sector again, so L1).  CSR: over the row.
+// The last index in [lo, hi] whose key is <= x, given key(lo) <= x, for
+// nondecreasing keys: a binary search, one probe per round.  (An 8-way
+// search, seven independent probes per round, was slower: with a million
+// walkers in flight latency is hidden anyway, and it loads more.)
+template <class Key>
+__device__ __forceinline__ uint32_t last_le(uint32_t lo, uint32_t hi, uint32_t x, Key key) {
+  while (lo < hi) {
+    const uint32_t mid = lo + (hi - lo + 1) / 2;
+    if (key(mid) <= x) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Whether x is a neighbor of the vertex of header h.  Compressed: a search
+// over the slots' first neighbors for the one slot that can hold x, then a
+// search of that slot inside its sector, in registers (GT: a scan of the
+// gaps; LE: a binary search of the closed-form values).  CSR: a search of
+// the row.
 template <int MODE>
 __device__ __forceinline__ bool has_neighbor(const DevGraph &g, const VHdr &h, uint32_t x) {
   if (h.d == 0) return false;
-  uint32_t lo = 0, hi = h.d - 1;  // index range that can hold x
-  if constexpr (MODE != 2) {
+  if constexpr (MODE == 2) {
+    if (neighbor<MODE>(g, h, 0) > x) return false;
+    const uint32_t i = last_le(0u, h.d - 1, x, [&](uint32_t k) { return neighbor<MODE>(g, h, k); });
+    return neighbor<MODE>(g, h, i) == x;
+  } else {
     if (MODE == 1 && h.d == 1) return h.fp == x;
     if (slot_first<MODE>(g, h, 0) > x) return false;
-    uint32_t cl = 0, ch = h.bn - 1;  // the last slot whose first neighbor is <= x
-    while (cl < ch) {
-      const uint32_t mid = cl + (ch - cl + 1) / 2;
-      if (slot_first<MODE>(g, h, mid) <= x) cl = mid;
-      else ch = mid - 1;
+    const uint32_t c = last_le(0u, h.bn - 1, x, [&](uint32_t k) { return slot_first<MODE>(g, h, k); });
+    // slot c holds indices c bl .. c bl + last
+    const uint32_t last = c + 1 == h.bn ? h.d - 1 - c * h.bl : h.bl - 1;
+    const uint64_t pos = slot_pos(h, c);
+    const Sec A = load_sector(g.words, pos >> 8);
+    const uint32_t off = (uint32_t)pos & 255u;
+    if constexpr (MODE == 0) {
+      const uint32_t hv = (uint32_t)sec1_field(A, off, h.a) + 1u;
+      uint32_t y = c >= h.fp ? h.v + hv : h.v - hv;
+      uint32_t p = off + (uint32_t)h.a;
+      for (uint32_t t = 0; y < x && t < last; t++, p += (uint32_t)h.b)
+        y += (h.b ? (uint32_t)sec1_field(A, p, h.b) : 0u) + 1u;
+      return y == x;
+    } else {
+      const uint32_t L = min(h.bl, h.d - 1 - c * h.bl);
+      const uint32_t id = last_le(0u, last, x, [&](uint32_t k) { return le_slot_value(A, off, h, c, k, L); });
+      return le_slot_value(A, off, h, c, id, L) == x;
     }
-    lo = cl * h.bl;
-    hi = cl + 1 == h.bn ? h.d - 1 : (cl + 1) * h.bl - 1;
-  } else {
-    if (neighbor<MODE>(g, h, 0) > x) return false;
   }
-  while (lo < hi) {  // the last index in [lo, hi] whose neighbor is <= x
-    const uint32_t mid = lo + (hi - lo + 1) / 2;
-    if (neighbor<MODE>(g, h, mid) <= x) lo = mid;
-    else hi = mid - 1;
-  }
-  return neighbor<MODE>(g, h, lo) == x;
 }
 
 template <int MODE>
@@ -155,6 +179,7 @@ __global__ void __launch_bounds__(256) n2v_kernel(DevGraph g, const uint32_t *__
                                                   uint32_t *__restrict__ paths,
                                                   unsigned long long *edges, unsigned int *err) {
   const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+  const uint64_t t_lo = min(a.t_in, a.t_out), t_hi = max(a.t_in, a.t_out);
   uint64_t cnt = 0;
   bool bad = false;
   for (uint64_t w = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; w < W; w += nthreads) {
@@ -176,8 +201,17 @@ __global__ void __launch_bounds__(256) n2v_kernel(DevGraph g, const uint32_t *__
                 philox4x32_10(a.seed, s, (uint32_t)id, (uint32_t)(id >> 32), TAG_N2V | k);
             x = neighbor<MODE>(g, h, mulhi_u32(r.x, h.d));
             if (s == 0 || k + 1 == a.max_tries) break;  // first step: uniform
-            const uint64_t t = x == u ? a.t_ret : has_neighbor<MODE>(g, hu, x) ? a.t_in : a.t_out;
-            if ((uint64_t)r.y < t) break;
+            const uint64_t y = r.y;
+            if (x == u) {
+              if (y < a.t_ret) break;
+              continue;
+            }
+            // below both thresholds the candidate is taken, at or above both it
+            // is not, whether or not it is a neighbor of u: only in between does
+            // the membership search run (never when t_in == t_out, i.e. q = 1)
+            if (y < t_lo) break;
+            if (y >= t_hi) continue;
+            if (y < (has_neighbor<MODE>(g, hu, x) ? a.t_in : a.t_out)) break;
           }
           if (x >= g.n) {
             bad = true;
