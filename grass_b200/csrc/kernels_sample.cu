@@ -173,8 +173,22 @@ __device__ __forceinline__ bool has_neighbor(const DevGraph &g, const VHdr &h, u
   }
 }
 
+// Resident 256-thread blocks per SM the node2vec kernels are compiled for.
+// The walk is latency-bound (dependent sector reads, divergent tries), so
+// resident warps matter more than registers: on the 1M x 80 walk the
+// compressed kernels at 4 blocks (64 registers) ran 1.6x faster than at 118
+// registers (2 blocks; unbounded builds also came out at 134, 1 block), 1.2x
+// faster than at 3 blocks, and 1.1-1.2x faster than at 5 or 6, where spills
+// grow.  The CSR kernel needs no cap (69 registers, 3 blocks).
+#ifndef GRASS_N2V_MIN_BLOCKS
+#define GRASS_N2V_MIN_BLOCKS 4
+#endif
+#ifndef GRASS_N2V_CSR_MIN_BLOCKS
+#define GRASS_N2V_CSR_MIN_BLOCKS 1
+#endif
+
 template <int MODE>
-__global__ void __launch_bounds__(256) n2v_kernel(DevGraph g, const uint32_t *__restrict__ starts,
+__global__ void __launch_bounds__(256, MODE == 2 ? GRASS_N2V_CSR_MIN_BLOCKS : GRASS_N2V_MIN_BLOCKS) n2v_kernel(DevGraph g, const uint32_t *__restrict__ starts,
                                                   uint64_t W, N2vArgs a,
                                                   uint32_t *__restrict__ paths,
                                                   unsigned long long *edges, unsigned int *err) {
