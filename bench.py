@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--scale", type=int, default=22)
     ap.add_argument("--edge-factor", type=int, default=32)
     ap.add_argument("--walkers", type=int, default=1 << 20)
+    ap.add_argument("--mrw-samples", type=int, default=1 << 18,
+                    help="multi-RW samples (80 walkers x 100 steps each) for --only mrw")
     ap.add_argument("--length", type=int, default=80)
     ap.add_argument("--khop-seeds", type=int, default=65536)
     ap.add_argument("--mode", default="LE", choices=["LE", "GT"])
@@ -394,6 +396,17 @@ class Parity:
             got = hops[h].view(S, int(w))[:k].cpu().numpy().view(np.uint32)
             ok = ok and np.array_equal(got, refs[h])
         self.put(key, ok, seeds=k, fanouts=list(fan))
+
+    def mrw(self, key, prefix, mode, roots0, R, T, seed, src, dst, roots, k=256):
+        """Samples 0..k-1 of a multi-RW launch: edges taken and final roots."""
+        if not self.enabled:
+            return
+        r0 = roots0[:k * R].cpu().numpy().view(np.uint32).reshape(k, R)
+        rs, rd, fin, _ = self.graph(prefix).mrw(mode, r0, T, seed, 0)
+        ok = (np.array_equal(src[:k * T].cpu().numpy().view(np.uint32).reshape(k, T), rs) and
+              np.array_equal(dst[:k * T].cpu().numpy().view(np.uint32).reshape(k, T), rd) and
+              np.array_equal(roots[:k * R].cpu().numpy().view(np.uint32).reshape(k, R), fin))
+        self.put(key, ok, samples=k, walkers=R, steps=T)
 
     def batch(self, key, prefix, mode, jobs, bufs, per_type=(3, 3, 2)):
         """The first per_type[t] jobs of each type of a batched run: RW paths
@@ -1057,6 +1070,36 @@ def main():
                     parity.node2vec(f"node2vec_{name}_p{p:g}_q{q:g}", os.path.join(gdir, name),
                                     name, starts, W, L, replica_seed(7, rank), p, q, paths,
                                     LAYOUT)
+
+    # ---- multi-RW in the reference mrw app's shape, beyond the headline: only when asked for
+    if "mrw" in only:
+        progress("multi-RW")
+        S_m, R_m, T_m = args.mrw_samples, 80, 100
+        roots0 = torch.empty(S_m * R_m, dtype=torch.int32, device=dev)
+        G.mrw_roots_device(n, S_m, R_m, replica_seed(11, rank), roots0, stream=stream)
+        torch.cuda.synchronize()
+        mroots = torch.empty_like(roots0)
+        msrc = torch.empty(S_m * T_m, dtype=torch.int32, device=dev)
+        mdst = torch.empty(S_m * T_m, dtype=torch.int32, device=dev)
+        for name in ("LE", "GT"):
+            obj = graphs[name]
+
+            def mrun(o=obj):  # the roots are updated in place: restore them (S x R x 4 bytes)
+                mroots.copy_(roots0)
+                o.mrw_device(mroots, S_m, R_m, T_m, replica_seed(11, rank), msrc, mdst,
+                             edge_count=ecount, stream=stream)
+            ecount.zero_()
+            mrun()
+            torch.cuda.synchronize()
+            e1 = int(ecount.item())
+            ms, tot = timed(torch, mrun, args.steps, args.warmup, flush, dist, local)
+            out[f"mrw_{name}"] = {
+                "value": sum_over_ranks(dist, e1 * args.steps, torch) / (tot / 1000.0),
+                "unit": UNIT, "ms_per_step": tot / args.steps, "edges_per_step": e1,
+                "samples": S_m, "walkers": R_m, "steps": T_m}
+            parity.mrw(f"mrw_{name}", os.path.join(gdir, name), name, roots0, R_m, T_m,
+                       replica_seed(11, rank), msrc, mdst, mroots)
+        del roots0, mroots, msrc, mdst
 
     progress("decode sweep")
     # ---- (c) decode-only sweep

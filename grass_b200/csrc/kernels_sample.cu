@@ -449,8 +449,18 @@ struct MrwLayout {
 };
 
 // Multi random walk, one sample per warp, the sample's state in shared memory.
+// Resident 256-thread blocks per SM it is compiled for: each warp's step chain
+// waits on dependent record and sector reads, so resident warps pay.  On
+// 262,144 samples of 80 walkers x 100 steps (R-MAT s22 ef32) 4 blocks (64
+// registers) ran 1.6x (LE) and 1.7x (GT) faster than the unbounded build
+// (110-113 registers, 2 blocks), 1.25x faster than 3 blocks, and 1.1-1.2x
+// faster than 5 or 6 (48 / 40 registers).
+#ifndef GRASS_MRW_MIN_BLOCKS
+#define GRASS_MRW_MIN_BLOCKS 4
+#endif
+
 template <int MODE>
-__global__ void __launch_bounds__(256) mrw_kernel(DevGraph g, uint32_t *__restrict__ roots,
+__global__ void __launch_bounds__(256, GRASS_MRW_MIN_BLOCKS) mrw_kernel(DevGraph g, uint32_t *__restrict__ roots,
                                                   uint64_t S, uint32_t R, uint32_t T, int select,
                                                   uint64_t seed, uint32_t *__restrict__ src,
                                                   uint32_t *__restrict__ dst,
