@@ -602,8 +602,12 @@ __global__ void __launch_bounds__(256) decode_range_kernel(DevGraph g, const uin
 // neighbor is in the record).
 constexpr uint32_t kFlatHub = kRange;  // degree from which a vertex is split into ranges
 
+// Resident 256-thread blocks per SM: 4 (64 registers, no spill; 4 x 33 KB of
+// shared memory).  Unbounded, the LE kernel took 80 registers (3 blocks) and
+// ran 1.08 ms against 0.94 ms at 4 (GT: 74 registers, 1.43 against 1.17 ms)
+// on R-MAT s22 ef32.
 #ifndef GRASS_DECODE_FLAT_MIN_BLOCKS
-#define GRASS_DECODE_FLAT_MIN_BLOCKS 1
+#define GRASS_DECODE_FLAT_MIN_BLOCKS 4
 #endif
 
 template <int MODE>
