@@ -206,7 +206,7 @@ int grass_decode_all(const grass_graph *g, uint64_t *d_rowptr, uint32_t *d_cols,
  * them.  Speed: once a grass_decode_all on the same graph has built its
  * decode plan (that call allocates, once), this call runs the same planned
  * sweep; before that it runs an unplanned sweep that needs no set-up, about
- * 3x slower (3.1 ms against 1.0 ms for 250 M neighbors on one B200). */
+ * 3x slower (3.1 ms against 0.94 ms for 250 M neighbors on one B200). */
 int grass_decode_all_noalloc(const grass_graph *g, uint64_t *d_rowptr, uint32_t *d_cols,
                              void *stream);
 
