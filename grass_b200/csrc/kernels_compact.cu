@@ -121,8 +121,16 @@ __global__ void __launch_bounds__(kThreads) compact_count_kernel(Plan pl, uint32
 // Each warp owns kWarpSlots consecutive slots of the tile: it ranks its valid
 // slots with one ballot per 32, learns the counts of the warps before it
 // through shared memory (the tile's only barrier), and writes in slot order.
+// Resident 256-thread blocks per SM for the fill kernel: 4 (64 registers,
+// with 40-148 bytes of spill).  On the k-hop (25, 10) frontiers of 65,536
+// seeds (R-MAT s22 ef32) the whole compaction took 0.103 ms, against 0.118-
+// 0.123 ms unbounded (96 / 76 registers, 2-3 blocks) and 0.111 ms at 3.
+#ifndef GRASS_COMPACT_MIN_BLOCKS
+#define GRASS_COMPACT_MIN_BLOCKS 4
+#endif
+
 template <int KIND>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, GRASS_COMPACT_MIN_BLOCKS)
     compact_fill_kernel(Plan pl, const uint64_t *offs, uint32_t *src, uint32_t *dst, uint64_t cap) {
   __shared__ uint32_t wsum[kWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
